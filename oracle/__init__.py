@@ -1,0 +1,286 @@
+"""TEST INFRASTRUCTURE -- the CPU checker for the CUDA path, never product code.
+
+ctypes bindings for
+
+* ``liboracle.so``: this project's plain-C restatement of the reference's MBFPA
+  forward projector, noise model and FBP (``vct_oracle.c``; each function cites
+  the reference lines it follows);
+* ``_ref/libvct_ref_mb.so`` / ``_ref/libvct_ref_fbp.so``: the reference's own
+  kernels, compiled from its sources by ``oracle/Makefile`` (present wherever
+  the reference sources were available at build time).
+
+Only ``tests/``, ``__graft_entry__.smoke()`` and ``bench.py`` (cpu_baseline leg
+and ``--impl reference``) import this package.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB = None
+_REF_MB = None
+_REF_FBP = None
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_fp = np.ctypeslib.ndpointer(dtype=np.float32, flags="C_CONTIGUOUS")
+_ip = np.ctypeslib.ndpointer(dtype=np.int32, flags="C_CONTIGUOUS")
+_u8p = np.ctypeslib.ndpointer(dtype=np.uint8, flags="C_CONTIGUOUS")
+
+
+class OrcGeom(C.Structure):
+    """Mirror of ``orc_geom`` (vct_oracle.h)."""
+
+    _fields_ = [
+        ("start_channel", C.c_int),
+        ("end_channel", C.c_int),
+        ("iso_channel", C.c_double),
+        ("max_alpha", C.c_double),
+        ("max_beta", C.c_double),
+        ("sid", C.c_double),
+        ("det_radius", C.c_double),
+        ("det_src_iso", C.c_double),
+        ("views", C.c_int),
+        ("width", C.c_int),
+        ("recon_size", C.c_int),
+        ("pixel_cm", C.c_double),
+        ("xfactor", C.c_int),
+    ]
+
+
+def geom(views=800, channels=609, recon_size=512, pixel_cm=0.1, xfactor=1, **kw) -> OrcGeom:
+    """Reference geometry (physParamsTOMO.h defaults) with the txt fields set.
+
+    ``channels`` sets End_Channel with the reference's own derived quantities:
+    isocenter = channels/2.0 (304.5 for 609); Max_alpha/Max_beta stay fixed.
+    """
+    g = OrcGeom()
+    lib().orc_geom_default(C.byref(g))
+    g.views = views
+    g.width = channels
+    g.end_channel = g.start_channel + channels
+    g.iso_channel = channels / 2.0
+    g.recon_size = recon_size
+    g.pixel_cm = pixel_cm
+    g.xfactor = xfactor
+    for k, v in kw.items():
+        setattr(g, k, v)
+    return g
+
+
+def lib():
+    global _LIB
+    if _LIB is None:
+        path = os.path.join(HERE, "liboracle.so")
+        if not os.path.exists(path):
+            raise RuntimeError(f"oracle not built: {path} (run `make -C oracle oracle`)")
+        L = C.CDLL(path)
+        L.orc_geom_default.argtypes = [C.POINTER(OrcGeom)]
+        L.orc_trig_tables.argtypes = [C.c_int, C.c_double, _dp, _dp]
+        L.orc_spectrum.argtypes = [C.c_char_p, C.c_int, _fp, _dp, C.c_int]
+        L.orc_spectrum.restype = C.c_int
+        L.orc_attenuation.argtypes = [_dp, C.c_int, _dp, _dp, C.c_int, _fp]
+        L.orc_walk.argtypes = [C.POINTER(OrcGeom), C.c_double, C.c_double, C.c_int, _dp, _ip, _dp, C.c_int]
+        L.orc_walk.restype = C.c_int
+        L.orc_forward_exact.argtypes = [C.POINTER(OrcGeom), _dp, _dp, _fp, C.c_int, _fp, _fp, C.c_int, _fp,
+                                        C.c_void_p, C.c_int]
+        L.orc_forward_fp64.argtypes = [C.POINTER(OrcGeom), _dp, _dp, _fp, C.c_int, _fp, _fp, C.c_int, _dp,
+                                       C.c_void_p, C.c_int]
+        L.orc_normalize_noise.argtypes = [_fp, C.c_int, C.c_double, C.c_uint, C.c_int]
+        L.orc_normalize_noise.restype = C.c_double
+        L.orc_fbp_constmap.argtypes = [C.POINTER(OrcGeom), C.c_int, _dp]
+        L.orc_fbp_filter.argtypes = [C.POINTER(OrcGeom), _fp, _dp, C.c_int, _fp]
+        L.orc_fbp_backproject.argtypes = [C.POINTER(OrcGeom), _fp, _dp, _dp, _fp]
+        L.orc_mask.argtypes = [C.c_int, _u8p]
+        _LIB = L
+    return _LIB
+
+
+# ---------------------------------------------------------------- restatement
+ELEMENTS_ZA = {
+    # (Z, A) as MB/prior_weight_production.cpp:250-255 (H, C, N, O, P, Ca); Mg and
+    # Si follow the same A ~ 2Z convention for the 8-element Gammex phantom.
+    "H": (1, 1), "C": (6, 12), "N": (7, 14), "O": (8, 16), "P": (15, 31), "Ca": (20, 40),
+    "Mg": (12, 24), "Si": (14, 28),
+}
+
+
+def trig_tables(views, start_deg=0.0):
+    c = np.zeros(views, np.float64)
+    s = np.zeros(views, np.float64)
+    lib().orc_trig_tables(views, start_deg, c, s)
+    return c, s
+
+
+def spectrum(path, nthin=1):
+    pdf = np.zeros(1024, np.float32)
+    e = np.zeros(1024, np.float64)
+    n = lib().orc_spectrum(str(path).encode(), nthin, pdf, e, 1024)
+    if n < 0:
+        raise FileNotFoundError(path)
+    return pdf[:n].copy(), e[:n].copy()
+
+
+def attenuation(energy_mev, elements=("H", "C", "N", "O", "P", "Ca")):
+    Z = np.array([ELEMENTS_ZA[e][0] for e in elements], np.float64)
+    A = np.array([ELEMENTS_ZA[e][1] for e in elements], np.float64)
+    e = np.ascontiguousarray(energy_mev, np.float64)
+    mu = np.zeros(len(elements) * len(e), np.float32)
+    lib().orc_attenuation(e, len(e), Z, A, len(elements), mu)
+    return mu.reshape(len(elements), len(e))
+
+
+def walk(g, cosb, sinb, jj):
+    cap = 4 * g.recon_size + 64
+    ln = np.zeros(cap, np.float64)
+    px = np.zeros(cap, np.int32)
+    r = np.zeros(cap, np.float64)
+    n = lib().orc_walk(C.byref(g), cosb, sinb, jj, ln, px, r, cap)
+    if n < 0:
+        raise RuntimeError("segment capacity exceeded")
+    return ln[:n].copy(), px[:n].copy(), r[:n].copy()
+
+
+def rho_from_maps(maps_i16):
+    """(float)short/1000 as MB/main.cpp:103."""
+    return (maps_i16.astype(np.float32) / np.float32(1000)).astype(np.float32)
+
+
+def forward_exact(g, cos_t, sin_t, rho, mu, pdf, nthreads=0, want_nseg=False):
+    M = rho.shape[0]
+    NE = len(pdf)
+    out = np.zeros((g.views, g.width), np.float32)
+    nseg = np.zeros((g.views, g.width), np.int32) if want_nseg else None
+    lib().orc_forward_exact(C.byref(g), cos_t, sin_t, np.ascontiguousarray(rho, np.float32), M,
+                            np.ascontiguousarray(mu, np.float32), np.ascontiguousarray(pdf, np.float32), NE,
+                            out, nseg.ctypes.data if want_nseg else None, nthreads)
+    return (out, nseg) if want_nseg else out
+
+
+def forward_fp64(g, cos_t, sin_t, rho, mu, pdf, nthreads=0, want_lint=False):
+    M = rho.shape[0]
+    NE = len(pdf)
+    out = np.zeros((g.views, g.width), np.float64)
+    lint = np.zeros((g.views, g.width, M), np.float64) if want_lint else None
+    lib().orc_forward_fp64(C.byref(g), cos_t, sin_t, np.ascontiguousarray(rho, np.float32), M,
+                           np.ascontiguousarray(mu, np.float32), np.ascontiguousarray(pdf, np.float32), NE,
+                           out, lint.ctypes.data if want_lint else None, nthreads)
+    return (out, lint) if want_lint else out
+
+
+def normalize_noise(sino, sigma, seed=1, order=0):
+    a = np.ascontiguousarray(sino, np.float32).copy()
+    pmin = lib().orc_normalize_noise(a.reshape(-1), a.size, sigma, seed, order)
+    return a, pmin
+
+
+def fbp_constmap(g, filt):
+    Cn = g.end_channel - g.start_channel
+    h = np.zeros(Cn * Cn, np.float64)
+    lib().orc_fbp_constmap(C.byref(g), filt, h)
+    return h.reshape(Cn, Cn)
+
+
+def fbp_filter(g, sino, h, in_mode=0):
+    Cn = g.end_channel - g.start_channel
+    out = np.zeros((g.views, Cn), np.float32)
+    lib().orc_fbp_filter(C.byref(g), np.ascontiguousarray(sino, np.float32), np.ascontiguousarray(h), in_mode,
+                         out)
+    return out
+
+
+def fbp_backproject(g, fltd, cos_t, sin_t):
+    img = np.zeros((g.recon_size, g.recon_size), np.float32)
+    lib().orc_fbp_backproject(C.byref(g), np.ascontiguousarray(fltd, np.float32), cos_t, sin_t, img)
+    return img
+
+
+def fbp(g, sino, filt, cos_t, sin_t, in_mode=0):
+    h = fbp_constmap(g, filt)
+    q = fbp_filter(g, sino, h, in_mode)
+    return fbp_backproject(g, q, cos_t, sin_t), q
+
+
+def mask(N):
+    m = np.zeros(N * N, np.uint8)
+    lib().orc_mask(N, m)
+    return m.reshape(N, N)
+
+
+# ------------------------------------------------------ the reference itself
+def ref_available() -> bool:
+    return all(os.path.exists(os.path.join(HERE, "_ref", f)) for f in ("libvct_ref_mb.so", "libvct_ref_fbp.so"))
+
+
+def ref_mb():
+    global _REF_MB
+    if _REF_MB is None:
+        L = C.CDLL(os.path.join(HERE, "_ref", "libvct_ref_mb.so"))
+        L.vctref_attenuation.argtypes = [C.c_char_p, C.c_int, _fp, _fp, C.POINTER(C.c_int)]
+        L.vctref_attenuation.restype = C.c_int
+        L.vctref_set_threads.argtypes = [C.c_int]
+        L.vctref_set_threads.restype = C.c_int
+        L.vctref_reprojection_bins.argtypes = [C.c_int, C.c_double, _fp, C.c_int, C.c_int, _dp, _dp, C.c_int,
+                                               _fp, _fp, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
+                                               C.c_void_p, C.POINTER(C.c_double)]
+        L.vctref_reprojection_bins.restype = C.c_int
+        _REF_MB = L
+    return _REF_MB
+
+
+def ref_fbp_lib():
+    global _REF_FBP
+    if _REF_FBP is None:
+        L = C.CDLL(os.path.join(HERE, "_ref", "libvct_ref_fbp.so"))
+        L.vctref_fbp.argtypes = [C.c_int, C.c_int, C.c_int, _fp, C.c_int, C.c_double, C.c_int, _dp, _dp, _fp,
+                                 C.c_void_p, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+        L.vctref_fbp.restype = C.c_int
+        _REF_FBP = L
+    return _REF_FBP
+
+
+def ref_attenuation(path, num_material=6):
+    att = np.zeros(1024 * num_material, np.float32)
+    pdf = np.zeros(1024, np.float32)
+    ne = C.c_int(0)
+    rc = ref_mb().vctref_attenuation(str(path).encode(), num_material, att, pdf, C.byref(ne))
+    if rc != 0:
+        raise RuntimeError("reference attenuation_coefficient failed")
+    n = ne.value
+    return pdf[:n].copy(), att[: num_material * n].reshape(num_material, n).copy()
+
+
+def ref_reprojection(N, pixel_cm, rho, views, width, cos_t, sin_t, xfactor, mu, pdf, ke0=0, ke1=None,
+                     threads=0, want_last=False):
+    """Runs the reference's reprojection_TOMO for bins [ke0, ke1) and sums them
+    in float (MB/main.cpp:492-506).  Returns (full, seconds[, last_bin])."""
+    NE = len(pdf)
+    ke1 = NE if ke1 is None else ke1
+    if threads:
+        ref_mb().vctref_set_threads(threads)
+    full = np.zeros((views, width), np.float32)
+    last = np.zeros((views, width), np.float32) if want_last else None
+    secs = C.c_double(0)
+    mu_flat = np.ascontiguousarray(mu, np.float32).reshape(-1)
+    rc = ref_mb().vctref_reprojection_bins(N, pixel_cm, np.ascontiguousarray(rho, np.float32), views, width,
+                                           cos_t, sin_t, xfactor, mu_flat, np.ascontiguousarray(pdf, np.float32),
+                                           NE, ke0, ke1, full.ctypes.data,
+                                           last.ctypes.data if want_last else None, None, C.byref(secs))
+    if rc != 0:
+        raise RuntimeError(f"reference reprojection failed ({rc})")
+    return (full, secs.value, last) if want_last else (full, secs.value)
+
+
+def ref_fbp(filt, sino, N, pixel_cm, xfactor, cos_t, sin_t):
+    """The reference's filterSinogram + reconstructImage. Returns (img, fltd, t_filter, t_bp)."""
+    V, W = sino.shape
+    img = np.zeros((N, N), np.float32)
+    fl = np.zeros((V, W), np.float32)
+    tf, tb = C.c_double(0), C.c_double(0)
+    rc = ref_fbp_lib().vctref_fbp(filt, V, W, np.ascontiguousarray(sino, np.float32), N, pixel_cm, xfactor, cos_t,
+                                  sin_t, img, fl.ctypes.data, C.byref(tf), C.byref(tb))
+    if rc != 0:
+        raise RuntimeError(f"reference fbp failed ({rc})")
+    return img, fl, tf.value, tb.value

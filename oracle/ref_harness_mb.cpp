@@ -1,0 +1,114 @@
+// Test-infrastructure harness: exposes the reference's own MBFPA kernels,
+// compiled from Release_MBFPA_CPU_human/*.cpp by oracle/Makefile, through a
+// plain C ABI so that tests and bench.py (reference arm, cpu_baseline leg) can
+// call them with ctypes.  This file contains no reference code: it only
+// allocates the buffers the reference functions expect and calls them.
+//
+//   attenuation_coefficient  Release_MBFPA_CPU_human/prior_weight_production.cpp:180
+//   reprojection_TOMO        Release_MBFPA_CPU_human/reprojection_TOMO.cpp:13
+//   energy loop + sum        Release_MBFPA_CPU_human/main.cpp:492-506
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <time.h>
+#include <unistd.h>
+#include <fcntl.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+#include "physParamsTOMO.h"
+#include "mallocMD.h"
+#include "reprojection_TOMO.h"
+#include "virtual_projection.h"
+
+static double now_s() {
+  struct timespec ts;
+  clock_gettime(CLOCK_MONOTONIC, &ts);
+  return ts.tv_sec + 1e-9 * ts.tv_nsec;
+}
+
+// attenuation_coefficient prints its whole table to stdout; keep the caller's
+// stdout clean by pointing fd 1 at /dev/null for the duration of the call.
+struct QuietStdout {
+  int saved = -1;
+  QuietStdout() {
+    fflush(stdout);
+    saved = dup(1);
+    int nul = open("/dev/null", O_WRONLY);
+    if (nul >= 0) { dup2(nul, 1); close(nul); }
+  }
+  ~QuietStdout() {
+    fflush(stdout);
+    if (saved >= 0) { dup2(saved, 1); close(saved); }
+  }
+};
+
+extern "C" {
+
+int vctref_mb_channels(void) { return End_Channel - Start_Channel; }
+
+// Fills att[num_material*NE] (bin index fastest) and pdf[NE]; both buffers must
+// hold 1024*num_material and 1024 floats as main.cpp:338-339 allocates them.
+int vctref_attenuation(const char* spectrum, int num_material, float* att, float* pdf, int* NE) {
+  QuietStdout q;
+  *NE = 0;
+  attenuation_coefficient((char*)spectrum, num_material, att, pdf, NE, 1);
+  return *NE > 0 ? 0 : -1;
+}
+
+int vctref_set_threads(int n) {
+#ifdef _OPENMP
+  if (n > 0) omp_set_num_threads(n);
+  return omp_get_max_threads();
+#else
+  (void)n;
+  return 1;
+#endif
+}
+
+// Runs reprojection_TOMO for energy bins [ke0, ke1) and accumulates each bin's
+// sinogram into full[] in float, in bin order, as main.cpp:492-506 does.
+// rho is the float density stack [6][N][N] (main.cpp:93-109); it is copied
+// because the reference clamps material 0 in place.  cos/sin hold V entries.
+// Returns the wall time of the reprojection_TOMO calls in *seconds.
+int vctref_reprojection_bins(int N, double pixel_cm, const float* rho, int V, int W,
+                             const double* cosT, const double* sinT, int xfactor,
+                             const float* att, const float* pdf, int NE, int ke0, int ke1,
+                             float* full, float* last_bin, int* nseg, double* seconds) {
+  if (W < End_Channel) return -1;
+  const int M = 6;
+  size_t n2 = (size_t)N * N;
+  float* work = (float*)malloc(sizeof(float) * M * n2);
+  float* proj = (float*)calloc((size_t)V * W, sizeof(float));
+  // Segment side tables written by the walk (never read on this path).  The
+  // reference sizes them W*V*N*2 (main.cpp:261-262); a ray has at most about
+  // 2N+4 segments, so the margin keeps small grids in bounds too.
+  size_t slots = (size_t)W * V * (size_t)(2 * N + 16);
+  float* sysmat = (float*)malloc(sizeof(float) * slots);
+  int* vnum = (int*)malloc(sizeof(int) * slots);
+  int* rsum = (int*)calloc((size_t)V * W, sizeof(int));
+  char* mask = (char*)calloc(n2, 1);
+  if (!work || !proj || !sysmat || !vnum || !rsum || !mask) {
+    free(work); free(proj); free(sysmat); free(vnum); free(rsum); free(mask);
+    return -2;
+  }
+  memcpy(work, rho, sizeof(float) * M * n2);
+  double xalpha[1] = {0.0};
+  double t0 = now_s();
+  for (int ke = ke0; ke < ke1; ke++) {
+    reprojection_TOMO(1, N, work, proj, pixel_cm, W, V, (double*)cosT, (double*)sinT, 0.0, 0.0,
+                      (double)xfactor, xalpha, mask, sysmat, vnum, rsum, 1, (float*)att, (float*)pdf,
+                      M, NE, ke);
+    if (full)
+      for (size_t i = 0; i < (size_t)V * W; i++) full[i] += proj[i];
+  }
+  double t1 = now_s();
+  if (seconds) *seconds = t1 - t0;
+  if (last_bin) memcpy(last_bin, proj, sizeof(float) * V * W);
+  if (nseg) memcpy(nseg, rsum, sizeof(int) * V * W);
+  free(work); free(proj); free(sysmat); free(vnum); free(rsum); free(mask);
+  return 0;
+}
+
+}  // extern "C"

@@ -1,0 +1,547 @@
+/*
+ * vct_oracle.c -- TEST INFRASTRUCTURE, NOT PRODUCT CODE.
+ *
+ * CPU restatement of the reference's MBFPA forward projector, noise model and
+ * fan-beam FBP (hagaakihiro/VirtualCT), used only to check the CUDA path.
+ * See vct_oracle.h for the contract.  Reference citations are
+ * "<dir>/<file>:<line>" with MB = Release_MBFPA_CPU_human and
+ * FBP = Release_FBP_CPU.
+ *
+ * Build: oracle/Makefile (gcc -O2 -ffp-contract=off -fopenmp).
+ */
+#include "vct_oracle.h"
+
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+/* PI as the reference spells it (MB/physParamsTOMO.h:1): rounds to M_PI. */
+#define ORC_PI 3.141592653589793238462643383279
+
+void orc_geom_default(orc_geom* g) {
+  g->start_channel = 0;
+  g->end_channel = 609;
+  g->iso_channel = 304.5;
+  g->max_alpha = 0.326086956;
+  g->max_beta = 0.326086956;
+  g->sid = 85.0;
+  g->det_radius = 142.6;
+  g->det_src_iso = 85.0;
+  g->views = 800;
+  g->width = 609;
+  g->recon_size = 512;
+  g->pixel_cm = 0.1;
+  g->xfactor = 1;
+}
+
+/* MB/projectionDataTOMO.cpp:362-368 and MB/misc_TOMO.cpp:93-97. */
+void orc_trig_tables(int views, double start_view_deg, double* cos_t, double* sin_t) {
+  for (int i = 0; i < views; i++) {
+    double angle = (double)(360.0 / views * i);
+    double rad = (start_view_deg + angle) * ORC_PI / 180.0;
+    cos_t[i] = cos(rad);
+    sin_t[i] = sin(rad);
+  }
+}
+
+/* MB/prior_weight_production.cpp:191-244.  energy_mev receives the bin
+ * centres as the reference stores them (a float, widened to double). */
+int orc_spectrum(const char* path, int nthin, float* pdf, double* energy_mev, int cap) {
+  FILE* fp = fopen(path, "r");
+  if (!fp) return -1;
+  char row[1024];
+  float d0 = 0, d1 = 0, d2 = 0;
+  double* pe = (double*)malloc(sizeof(double) * cap);
+  float* raw = (float*)malloc(sizeof(float) * cap);
+  int n = 0;
+  if (fgets(row, sizeof(row), fp) == NULL) { /* header line (:196) */ }
+  while (fgets(row, sizeof(row), fp) != NULL && n < cap) {
+    /* A line sscanf cannot parse keeps the previous values, as at :202. */
+    sscanf(row, "%f %f %f", &d0, &d1, &d2);
+    pe[n] = (d1 + d0) * 0.5;
+    raw[n] = d2;
+    n++;
+  }
+  fclose(fp);
+  /* Thinning (:210-235). */
+  double psum = 0.0, esum = 0.0, sum_thin = 0.0;
+  int nthin_out = 0;
+  for (int i = 0; i < n; i++) {
+    psum += raw[i];
+    esum += pe[i];
+    if (i - nthin + 1 == (i - nthin + 1) / nthin * nthin) {
+      int k = (i - nthin + 1) / nthin;
+      pdf[k] = (float)psum;
+      energy_mev[k] = (double)(float)(esum / nthin);
+      sum_thin += psum;
+      psum = 0.0;
+      esum = 0.0;
+      nthin_out = k + 1;
+    }
+  }
+  /* Normalisation in float (:229-244). */
+  float sum = (float)sum_thin;
+  for (int i = 0; i < nthin_out; i++) pdf[i] = pdf[i] / sum;
+  free(pe);
+  free(raw);
+  return nthin_out;
+}
+
+/* MB/prior_weight_production.cpp:249-295 (photoelectric Z^3/E^3 term,
+ * Klein-Nishina Compton term, pair term clamped at 0; Ek = 0). */
+void orc_attenuation(const double* energy_mev, int NE, const double* ZZ, const double* AA, int M,
+                     float* mu) {
+  const double Avogadro = 6.0221; /* MB/physParamsTOMO.h:89 */
+  double Ek = 0;
+  for (int iz = 0; iz < M; iz++) {
+    double Z = ZZ[iz], A = AA[iz];
+    double fact = Avogadro * Z / A * (2.81794 * 2.81794) * 0.001;
+    for (int i = 0; i < NE; i++) {
+      double E = energy_mev[i] / 0.511;
+      double photo = fact * 0.00000345 * (1.0 + 0.008 * Z) * (Z * Z * Z) / (E * E * E) *
+                     (1.0 - Ek / (4.0 * E) - Ek * Ek / (1.21 * E));
+      double compton = fact * 2 * ORC_PI *
+                       ((1.0 + E) / (E * E) * (2.0 * (1.0 + E) / (1.0 + 2 * E) - log(1.0 + 2 * E) / E) +
+                        log(1.0 + 2 * E) / (2 * E) - (1.0 + 3 * E) / ((1.0 + 2 * E) * (1.0 + 2 * E)));
+      double pair = fact * 0.2545 * (E - 2.332) * Z / 137;
+      if (pair < 0) pair = 0;
+      mu[NE * iz + i] = (float)(photo + compton + pair);
+    }
+  }
+}
+
+/* One ray: MB/reprojection_TOMO.cpp:53-283, segment emission order kept. */
+int orc_walk(const orc_geom* g, double cb, double sb, int jj, double* seg_len, int* seg_pix,
+             double* seg_r, int cap) {
+  const int N = g->recon_size;
+  const double s = g->pixel_cm;
+  const int nxm = (int)(N * 0.5); /* :25-26 */
+  const int nym = (int)(N * 0.5);
+  const int half = (g->end_channel - g->start_channel - 1) / 2; /* macro :57 */
+  double sx = g->sid * sb;                                      /* :53 */
+  double sy = g->sid * cb;                                      /* :54 */
+  double theta = (g->iso_channel - jj) * g->max_alpha / half;   /* :61 */
+  double ox0 = g->det_radius * sin(theta);                      /* :67 */
+  double oy0 = -g->det_radius * cos(theta);                     /* :68 */
+  double px0 = ox0;
+  double py0 = oy0 + g->det_src_iso;      /* :71 */
+  double px = +px0 * cb + py0 * sb;       /* :73 */
+  double py = -px0 * sb + py0 * cb;       /* :74 */
+  const double limx = (double)nxm * s, limy = (double)nym * s;
+  double xx[4] = {0, 0, 0, 0}, yy[4] = {0, 0, 0, 0};
+  int m = 0; /* grid-square intersections, :76-101 */
+  yy[m] = (double)nym * s;
+  if (fabs((yy[m] - sy) / (py - sy) * (px - sx) + sx) < limx) {
+    xx[m] = (yy[m] - sy) / (py - sy) * (px - sx) + sx;
+    m++;
+  }
+  yy[m] = -(double)nym * s;
+  if (fabs((yy[m] - sy) / (py - sy) * (px - sx) + sx) < limx) {
+    xx[m] = (yy[m] - sy) / (py - sy) * (px - sx) + sx;
+    m++;
+  }
+  xx[m] = (double)nxm * s;
+  if (fabs((xx[m] - sx) / (px - sx) * (py - sy) + sy) < limy) {
+    yy[m] = (xx[m] - sx) / (px - sx) * (py - sy) + sy;
+    m++;
+  }
+  xx[m] = -(double)nxm * s;
+  if (fabs((xx[m] - sx) / (px - sx) * (py - sy) + sy) < limy) {
+    yy[m] = (xx[m] - sx) / (px - sx) * (py - sy) + sy;
+    m++;
+  }
+  /* A ray that misses the square leaves xx/yy[1] unset in the reference; its
+   * walk loop is then never entered (no point of the line lies in the square),
+   * so transp stays 0.  Reported here as zero segments. */
+  if (m < 2) return 0;
+  double xi, yi, xf, yf; /* :102-108 */
+  if ((xx[0] - sx) * (xx[0] - sx) + (yy[0] - sy) * (yy[0] - sy) + 0.0 <
+      (xx[1] - sx) * (xx[1] - sx) + (yy[1] - sy) * (yy[1] - sy) + 0.0) {
+    xi = xx[0]; yi = yy[0]; xf = xx[1]; yf = yy[1];
+  } else {
+    xi = xx[1]; yi = yy[1]; xf = xx[0]; yf = yy[0];
+  }
+  double xb0 = xi, yb0 = yi, xb1, yb1, rr;
+  double xii, yii, xiii = 0, yiii = 0, yj, xj;
+  int n = 0;
+#define ORC_EMIT()                                                                      \
+  do {                                                                                  \
+    rr = sqrt((xb0 - xb1) * (xb0 - xb1) + (yb0 - yb1) * (yb0 - yb1));                   \
+    int xmc = (int)((xb0 + xb1) * 0.5 / s + nxm);                                      \
+    int ymc = (int)((-yb0 - yb1) * 0.5 / s + nym);                                     \
+    if (xmc >= 0 && ymc >= 0 && xmc <= N - 1 && ymc <= N - 1) {                         \
+      if (n >= cap) return -1;                                                          \
+      seg_len[n] = rr;                                                                  \
+      seg_pix[n] = xmc + ymc * N;                                                       \
+      seg_r[n] = sqrt((xb0 + xb1) * (xb0 + xb1) + (-yb0 - yb1) * (-yb0 - yb1)) * 0.5;    \
+      n++;                                                                              \
+    }                                                                                   \
+  } while (0)
+
+  if (fabs(xi - xf) > fabs(yi - yf)) { /* x-major walk, :113-200 */
+    double pha = (xf - xi) / fabs(xi - xf);
+    int xin, ik = 0, yma = 0, ymb;
+    if ((xi < 0 && (xf - xi) < 0) || (xi > 0 && (xf - xi) > 0))
+      xin = (int)((int)xi + (xf - xi) / fabs(xf - xi));
+    else
+      xin = (int)xi;
+    xii = xin;
+    yii = (xii - sx) / (px - sx) * (py - sy) + sy;
+    while (xii <= limx && xii >= -limx && yii <= limy && yii >= -limy) {
+      xii = xin + pha * ik * s;
+      ymb = yma;
+      yj = yii;
+      yii = (xii - sx) / (px - sx) * (py - sy) + sy;
+      yma = (int)(yii / s);
+      int icheck = 0;
+      double chy = 0;
+      if ((ik != 0 && yma != ymb) || (ik != 0 && (yii / fabs(yii) != yj / fabs(yj)))) {
+        if ((yii < 0 && (yf - yi) < 0) || (yii > 0 && (yf - yi) > 0))
+          yiii = (double)(yma * s);
+        else
+          yiii = (double)(yma * s) - (yf - yi) / fabs(yf - yi) * s;
+        xiii = (yiii - sy) / (py - sy) * (px - sx) + sx;
+        chy = (xii - xiii) * (xii - xiii) + (yii - yiii) * (yii - yiii);
+        icheck++;
+      }
+      if (icheck == 1 && chy != 0) {
+        xb1 = xiii;
+        yb1 = yiii;
+        ORC_EMIT();
+        xb0 = xb1;
+        yb0 = yb1;
+      }
+      xb1 = xii;
+      yb1 = yii;
+      ORC_EMIT();
+      xb0 = xb1;
+      yb0 = yb1;
+      ik++;
+    }
+  } else { /* y-major walk, :201-283 */
+    double pha = (yf - yi) / fabs(yi - yf);
+    int yin, ik = 0, xma = 0, xmb;
+    if ((yi < 0 && (yf - yi) < 0) || (yi > 0 && (yf - yi) > 0))
+      yin = (int)((int)yi + (yf - yi) / fabs(yf - yi));
+    else
+      yin = (int)yi;
+    yii = yin;
+    xii = (yii - sy) / (py - sy) * (px - sx) + sx;
+    while (xii <= limx && xii >= -limx && yii <= limy && yii >= -limy) {
+      yii = yin + pha * ik * s;
+      xmb = xma;
+      xj = xii;
+      xii = (yii - sy) / (py - sy) * (px - sx) + sx;
+      xma = (int)(xii / s);
+      int icheck = 0;
+      double chy = 0;
+      if ((ik != 0 && xma != xmb) || (ik != 0 && (xii / fabs(xii) != xj / fabs(xj)))) {
+        if ((xii < 0 && (xf - xi) < 0) || (xii > 0 && (xf - xi) > 0))
+          xiii = (double)(xma * s);
+        else
+          xiii = (double)(xma * s) - (xf - xi) / fabs(xf - xi) * s;
+        yiii = (xiii - sx) / (px - sx) * (py - sy) + sy;
+        chy = (xii - xiii) * (xii - xiii) + (yii - yiii) * (yii - yiii);
+        icheck++;
+      }
+      if (icheck == 1 && chy != 0) {
+        xb1 = xiii;
+        yb1 = yiii;
+        ORC_EMIT();
+        xb0 = xb1;
+        yb0 = yb1;
+      }
+      xb1 = xii;
+      yb1 = yii;
+      ORC_EMIT();
+      xb0 = xb1;
+      yb0 = yb1;
+      ik++;
+    }
+  }
+#undef ORC_EMIT
+  return n;
+}
+
+static int orc_seg_cap(const orc_geom* g) { return 4 * g->recon_size + 64; }
+
+/* Density seen by one segment for material mat: the reference zeroes
+ * material 0 in place and sets ph = 0 for other materials when the value is
+ * negative or the midpoint radius (cm) reaches rmax = N/2 (a pixel count),
+ * MB/reprojection_TOMO.cpp:150-156.  The in-place write only changes later
+ * rays when r >= rmax can occur (pixel >= 0.707 cm); it is not reproduced. */
+static inline float orc_rho_seen(const float* rho, size_t n2, int mat, int pix, double r,
+                                 double rmax, double* ph) {
+  float v = rho[(size_t)mat * n2 + pix];
+  *ph = 1.0;
+  if (mat == 0) {
+    if (v < 0 || r >= rmax) v = 0;
+  }
+  if (v < 0 || r >= rmax) *ph = 0.0;
+  return v;
+}
+
+void orc_forward_exact(const orc_geom* g, const double* cos_t, const double* sin_t, const float* rho,
+                       int M, const float* mu, const float* pdf, int NE, float* full_out,
+                       int* nseg_out, int nthreads) {
+  const int V = g->views, W = g->width, N = g->recon_size;
+  const int nviews = V / 2 * 2; /* end_angle_num, MB/reprojection_TOMO.cpp:35 */
+  const size_t n2 = (size_t)N * N;
+  const double rmax = N * 0.5 * 1.0; /* :37 */
+  const int cap = orc_seg_cap(g);
+  memset(full_out, 0, sizeof(float) * (size_t)V * W);
+  if (nseg_out) memset(nseg_out, 0, sizeof(int) * (size_t)V * W);
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel
+#endif
+  {
+    double* len = (double*)malloc(sizeof(double) * cap);
+    double* rad = (double*)malloc(sizeof(double) * cap);
+    int* pix = (int*)malloc(sizeof(int) * cap);
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 4)
+#endif
+    for (int j = 0; j < nviews; j++) {
+      for (int jj = g->start_channel; jj < g->end_channel; jj++) {
+        int ns = orc_walk(g, cos_t[j], sin_t[j], jj, len, pix, rad, cap);
+        if (ns < 0) ns = 0;
+        size_t o = (size_t)j * W + jj;
+        if (nseg_out) nseg_out[o] = ns;
+        float acc = 0.0f;
+        for (int ke = 0; ke < NE; ke++) {
+          double transp = 0.0;
+          for (int q = 0; q < ns; q++) {
+            for (int mat = 0; mat < M; mat++) {
+              double ph;
+              float v = orc_rho_seen(rho, n2, mat, pix[q], rad[q], rmax, &ph);
+              transp += (double)(v * mu[mat * NE + ke]) * len[q] * ph;
+            }
+          }
+          double intens = pdf[ke] * exp(-transp / (double)g->xfactor);
+          acc += (float)intens;
+        }
+        full_out[o] = acc;
+      }
+    }
+    free(len);
+    free(rad);
+    free(pix);
+  }
+}
+
+void orc_forward_fp64(const orc_geom* g, const double* cos_t, const double* sin_t, const float* rho,
+                      int M, const float* mu, const float* pdf, int NE, double* full_out,
+                      double* lint_out, int nthreads) {
+  const int V = g->views, W = g->width, N = g->recon_size;
+  const int nviews = V / 2 * 2;
+  const size_t n2 = (size_t)N * N;
+  const double rmax = N * 0.5 * 1.0;
+  const int cap = orc_seg_cap(g);
+  memset(full_out, 0, sizeof(double) * (size_t)V * W);
+  if (lint_out) memset(lint_out, 0, sizeof(double) * (size_t)V * W * M);
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel
+#endif
+  {
+    double* len = (double*)malloc(sizeof(double) * cap);
+    double* rad = (double*)malloc(sizeof(double) * cap);
+    int* pix = (int*)malloc(sizeof(int) * cap);
+    double L[16];
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 4)
+#endif
+    for (int j = 0; j < nviews; j++) {
+      for (int jj = g->start_channel; jj < g->end_channel; jj++) {
+        int ns = orc_walk(g, cos_t[j], sin_t[j], jj, len, pix, rad, cap);
+        if (ns < 0) ns = 0;
+        for (int mat = 0; mat < M; mat++) L[mat] = 0.0;
+        for (int q = 0; q < ns; q++) {
+          for (int mat = 0; mat < M; mat++) {
+            double ph;
+            float v = orc_rho_seen(rho, n2, mat, pix[q], rad[q], rmax, &ph);
+            L[mat] += (double)v * len[q] * ph;
+          }
+        }
+        size_t o = (size_t)j * W + jj;
+        if (lint_out)
+          for (int mat = 0; mat < M; mat++) lint_out[o * M + mat] = L[mat];
+        double acc = 0.0;
+        for (int ke = 0; ke < NE; ke++) {
+          double t = 0.0;
+          for (int mat = 0; mat < M; mat++) t += (double)mu[mat * NE + ke] * L[mat];
+          acc += (double)pdf[ke] * exp(-t / (double)g->xfactor);
+        }
+        full_out[o] = acc;
+      }
+    }
+    free(len);
+    free(rad);
+    free(pix);
+  }
+}
+
+/* MB/main.cpp:42-49 */
+static double orc_uniform0(void) { return ((double)rand() + 1.0) / ((double)RAND_MAX + 2.0); }
+
+double orc_normalize_noise(float* sino, int nn, double sigma, unsigned seed, int order) {
+  /* MB/main.cpp:511-522 */
+  float pmax = 0;
+  for (int i = 0; i < nn; i++)
+    if (pmax < sino[i]) pmax = sino[i];
+  for (int i = 0; i < nn; i++) sino[i] = sino[i] / pmax;
+  /* gaussiannoise0, MB/main.cpp:51-76 */
+  double pmin = 10000000;
+  for (int i = 0; i < nn; i++)
+    if (pmin > sino[i]) pmin = sino[i];
+  if (sigma <= 0) return pmin;
+  srand(seed);
+  for (int i = 0; i < nn; i++) {
+    double nstar = sino[i];
+    double u1, u2;
+    if (order == 0) {
+      u1 = orc_uniform0();
+      u2 = orc_uniform0();
+    } else {
+      u2 = orc_uniform0();
+      u1 = orc_uniform0();
+    }
+    double z = sqrt(-2.0 * log(u1)) * sin(2.0 * ORC_PI * u2);
+    double psn = 0 + sigma * z;
+    nstar = nstar + psn;
+    sino[i] = (float)nstar;
+    if (nstar < 0) sino[i] = (float)(pmin / 10);
+    if (nstar > 1.0) sino[i] = 1.0f;
+  }
+  return pmin;
+}
+
+/* FBP/filterSinogramTOMO.cpp:9-123.  h is [C][C], C = end-start. */
+void orc_fbp_constmap(const orc_geom* g, int filter, double* h) {
+  const int C = g->end_channel - g->start_channel;
+  const int half = (C - 1) / 2;
+  double arc = g->max_beta / half; /* :30, parenthesised macro */
+  double* sum = (double*)calloc(C, sizeof(double));
+  for (int m = 0; m < C; m++) {
+    sum[m] = 0.0;
+    for (int n = 0; n < C; n++) {
+      int MN = m - n;
+      double v = 0.0;
+      if (m == n) {
+        if (filter == 1) {
+          v = 0.125 / (arc * arc);
+        } else if (filter == 2) {
+          double oddterm = ORC_PI * ORC_PI * (arc);
+          v = 0.25 / oddterm * (1.0 / tan((0.5) * arc) - 1.0 / tan((-0.5) * arc));
+        }
+      } else if (MN % 2 != 0) {
+        if (filter == 1) {
+          double oddterm = ORC_PI * sin(MN * arc);
+          v = -0.5 / oddterm / oddterm;
+        } else if (filter == 2) {
+          double oddterm = ORC_PI * ORC_PI * arc;
+          v = 0.25 / oddterm * (1.0 / tan((MN + 0.5) * arc) - 1.0 / tan((MN - 0.5) * arc));
+        }
+      } else {
+        if (filter == 1) {
+          v = 0.0;
+        } else if (filter == 2) {
+          double oddterm = ORC_PI * ORC_PI * arc;
+          v = 0.25 / oddterm * (1.0 / tan((MN + 0.5) * arc) - 1.0 / tan((MN - 0.5) * arc));
+        }
+      }
+      h[(size_t)m * C + n] = v;
+      sum[m] += v;
+    }
+  }
+  /* Edge-row renormalisation (:114-123); rows 0..20 and C-20..C-1. */
+  for (int m = 0; m < C; m++)
+    for (int n = 0; n < C; n++)
+      if ((0 <= m && m <= 20) || (C - 20 <= m && m <= C))
+        h[(size_t)m * C + n] = h[(size_t)m * C + n] * sum[21] / sum[m];
+  free(sum);
+}
+
+/* FBP/filterSinogramTOMO.cpp:225-260.  sino is [V][width]; fltd is [V][C]. */
+void orc_fbp_filter(const orc_geom* g, const float* sino, const double* h, int in_mode,
+                    float* fltd) {
+  const int C = g->end_channel - g->start_channel;
+  const int half = (C - 1) / 2;
+  const int cw = C / 2; /* centWidth, :227 */
+  const int V = g->views, W = g->width;
+  double* coeff = (double*)malloc(sizeof(double) * C);
+  for (int k = 0; k < C; k++) coeff[k] = g->sid * cos((k - cw) * (g->max_beta / half));
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static)
+#endif
+  for (int n = 0; n < V; n++) {
+    for (int m = 0; m < C; m++) {
+      float acc = 0.0f;
+      for (int k = 0; k < C; k++) {
+        double projdat = sino[(size_t)n * W + k + g->start_channel];
+        acc += h[(size_t)m * C + k] * (-log(projdat) * coeff[k]) * g->max_beta / half;
+      }
+      if (in_mode && (acc < 1000.0 || acc > 300000.0)) acc = 0.0f;
+      fltd[(size_t)n * C + m] = acc;
+    }
+  }
+  free(coeff);
+}
+
+void orc_mask(int N, unsigned char* mask) {
+  double r = (double)(N - 1) / 2.0;
+  double r2 = r * r;
+  for (int j = 0; j < N; j++)
+    for (int i = 0; i < N; i++)
+      mask[j * N + i] = (((double)j - r) * ((double)j - r) + ((double)i - r) * ((double)i - r) <= r2);
+}
+
+/* FBP/reconstructImageTOMO.cpp:21-103 for one slice. */
+void orc_fbp_backproject(const orc_geom* g, const float* fltd, const double* cos_t,
+                         const double* sin_t, float* img) {
+  const int N = g->recon_size, V = g->views;
+  const int C = g->end_channel - g->start_channel;
+  const int half = (C - 1) / 2;
+  const int cw = C / 2;
+  const double scale = g->pixel_cm;
+  const double centerPos = (double)N / 2.0 - 0.5;
+  const int use = V / 2 * 2; /* usesinogram, :30 */
+  const double xfactor = (double)g->xfactor;
+  unsigned char* mask = (unsigned char*)malloc((size_t)N * N);
+  orc_mask(N, mask);
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static)
+#endif
+  for (int y = 0; y < N; y++) {
+    for (int x = 0; x < N; x++) {
+      float acc = 0.0f;
+      if (mask[y * N + x]) {
+        double xx = -(x - centerPos) * scale;
+        double yy = -(y - centerPos) * scale;
+        for (int th = 0; th < use; th++) {
+          double dbeta = 2.0 * ORC_PI / (V);
+          double c = cos_t[th], s = sin_t[th];
+          double X = xx * c + yy * s;
+          double Y = -xx * s + yy * c;
+          double L2 = (-Y + g->sid) * (-Y + g->sid) + X * X;
+          double fGAM = atan(X / (g->sid - Y)) / (g->max_beta / half) + cw;
+          int GAM = (int)(fGAM);
+          double w = fGAM - GAM;
+          if (GAM >= 0 && GAM < C - 1) {
+            double sum1 = (1 - w) * fltd[(size_t)th * C + GAM] + w * fltd[(size_t)th * C + GAM + 1];
+            double zw = 0.0, sum2 = 0;
+            double sum = (1.0 - zw) * sum1 + zw * sum2;
+            acc += (float)(1.0 / L2 * sum * dbeta * xfactor);
+          }
+        }
+      }
+      img[(size_t)y * N + x] = acc;
+    }
+  }
+  free(mask);
+}

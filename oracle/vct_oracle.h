@@ -1,0 +1,103 @@
+/*
+ * vct_oracle.h -- TEST INFRASTRUCTURE, NOT PRODUCT CODE.
+ *
+ * A plain-C restatement of the reference's MBFPA and FBP arithmetic
+ * (hagaakihiro/VirtualCT), used only as the checker by tests/,
+ * __graft_entry__.smoke() and the cpu_baseline leg of bench.py.  The product
+ * library (virtualct_b200/) never links, loads or calls it.
+ *
+ * Every function names the reference lines it restates.  Operation order and
+ * types follow the reference exactly (double geometry, float densities and mu,
+ * float accumulators where the reference has them), and the file is compiled
+ * with -ffp-contract=off so rounding matches the reference's x86-64 -O2 build.
+ *
+ * Parity pin: tests/test_oracle_pin.py compares these functions with the
+ * reference itself, compiled from its sources by oracle/Makefile into
+ * oracle/_ref/, and with the golden outputs the reference ships.
+ */
+#ifndef VCT_ORACLE_H
+#define VCT_ORACLE_H
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* Runtime copy of the physParamsTOMO.h geometry macros plus the txt fields
+ * the hot path reads.  orc_geom_default() gives the shipped values. */
+typedef struct orc_geom {
+  int start_channel;   /* Start_Channel 0          MB/physParamsTOMO.h:43 */
+  int end_channel;     /* End_Channel 609          :46 */
+  double iso_channel;  /* isocenter_channel 304.5  :47 */
+  double max_alpha;    /* Max_alpha 0.326086956    :56 */
+  double max_beta;     /* Max_beta  0.326086956    :60, FBP/physParamsTOMO.h:50 */
+  double sid;          /* DIST_BTWN_SRC_AND_ISOCENT_CM 85.0            :25 */
+  double det_radius;   /* DETECTOR_RADIUS_CURVATURE_CM 142.6           :27 */
+  double det_src_iso;  /* DIST_BTWN_DETERCTORSRC_AND_ISOCENT_CM 85.0   :28 */
+  int views;           /* projImgHeight (GantryRotationPeriod*DataSamplingRate) */
+  int width;           /* projImgWidth: sinogram row stride */
+  int recon_size;      /* N */
+  double pixel_cm;     /* reconPixSize */
+  int xfactor;         /* xfactor (txt field "Factor for output CT value") */
+} orc_geom;
+
+void orc_geom_default(orc_geom* g);
+
+/* View angles and trig tables: MB/projectionDataTOMO.cpp:362-368,
+ * MB/misc_TOMO.cpp:82-100 (FBP/projectionDataTOMO.cpp:201-208 is identical). */
+void orc_trig_tables(int views, double start_view_deg, double* cos_t, double* sin_t);
+
+/* Spectrum file + analytic mass attenuation: MB/prior_weight_production.cpp:180-297.
+ * Z/A give the element table (the reference hard-codes H,C,N,O,P,Ca at :250-255).
+ * mu is [M][NE] (bin fastest, stride NE).  Returns NE, or -1 on I/O error. */
+int orc_spectrum(const char* path, int nthin, float* pdf, double* energy_mev, int cap);
+void orc_attenuation(const double* energy_mev, int NE, const double* Z, const double* A, int M,
+                     float* mu);
+
+/* One ray walk (MB/reprojection_TOMO.cpp:53-283) for view cos/sin and channel
+ * jj.  Writes segment lengths (cm), pixel indices and midpoint radii (cm);
+ * returns the number of segments (0 when the ray misses the grid), or -1 when
+ * cap is too small. */
+int orc_walk(const orc_geom* g, double cosb, double sinb, int jj, double* seg_len, int* seg_pix,
+             double* seg_r, int cap);
+
+/* Forward projection, reference order: for every bin, transp is accumulated
+ * over segments and materials exactly as MB/reprojection_TOMO.cpp:152-157,
+ * the bin value is (float)(pdf*exp(-transp/xfactor)) (:196-197) and bins are
+ * summed in float in bin order (MB/main.cpp:492-506).
+ * rho: float densities [M][N][N] (int16/1000, MB/main.cpp:93-109).
+ * full_out: [views][width] (rows >= views/2*2 and channels outside
+ * [start,end) are left 0, as the reference leaves them).  nseg_out optional.
+ * nthreads <= 0 uses OpenMP's default. */
+void orc_forward_exact(const orc_geom* g, const double* cos_t, const double* sin_t, const float* rho,
+                       int M, const float* mu, const float* pdf, int NE, float* full_out,
+                       int* nseg_out, int nthreads);
+
+/* Same geometry, evaluated in FP64 throughout: L_m = sum rho_m*len,
+ * transp = sum_m mu_m*L_m, I = sum_E pdf*exp(-transp/xfactor), in double.
+ * Optionally returns the per-ray line integrals L [views][width][M] (g/cm^2). */
+void orc_forward_fp64(const orc_geom* g, const double* cos_t, const double* sin_t, const float* rho,
+                      int M, const float* mu, const float* pdf, int NE, double* full_out,
+                      double* lint_out, int nthreads);
+
+/* Max-normalisation (MB/main.cpp:511-522) followed by gaussiannoise0
+ * (MB/main.cpp:42-76) with glibc rand() after srand(seed) (the reference
+ * never seeds: seed 1).  order selects which Uniform0() call in rand_gauss0
+ * is evaluated first (the C++ expression leaves it unspecified); the shipped
+ * golden fixes it.  sigma <= 0 normalises only.  Returns the noise-free
+ * normalised minimum (projection_min). */
+double orc_normalize_noise(float* sino, int nn, double sigma, unsigned seed, int order);
+
+/* FBP: prepareConstMap (FBP/filterSinogramTOMO.cpp:9-138) -> h[C][C];
+ * filterSinogram (:205-275); reconstructImage (FBP/reconstructImageTOMO.cpp:11-105). */
+void orc_fbp_constmap(const orc_geom* g, int filter, double* h);
+void orc_fbp_filter(const orc_geom* g, const float* sino, const double* h, int in_mode,
+                    float* fltd);
+void orc_fbp_backproject(const orc_geom* g, const float* fltd, const double* cos_t,
+                         const double* sin_t, float* img);
+
+/* Inscribed-circle mask: MB/misc_TOMO.cpp:10-39, FBP/misc.cpp:9-37. */
+void orc_mask(int N, unsigned char* mask);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

@@ -1,0 +1,164 @@
+/*
+ * vct.h -- C ABI of the B200-native MBFPA + FBP library (libvct.so).
+ *
+ * Drop-in boundary for the two hot paths of hagaakihiro/VirtualCT:
+ *   MBFPA  Release_MBFPA_CPU_human/main.cpp:492-530  (energy loop over
+ *          reprojection_TOMO, spectral sum, max-normalisation, gaussiannoise0)
+ *   FBP    Release_FBP_CPU/main.cpp:137-167          (filterSinogram +
+ *          reconstructImage)
+ *
+ * Conventions
+ *   - Every function returns VCT_OK (0) or a negative VCT_E_* code; the text of
+ *     the last error on the calling thread is available from vct_last_error().
+ *   - Pointers without a _dev suffix are host pointers.  *_dev functions take
+ *     device pointers on the context's device and enqueue on the context's
+ *     stream (vct_set_stream); they return once the work is enqueued.
+ *   - The caller owns every buffer it passes; the context owns its device
+ *     scratch.  One host thread per context.
+ *   - Layouts are the reference's raw file layouts: sinograms float32
+ *     [views][width] (row = view), images float32 [N][N], element maps int16
+ *     [M][N][N] holding element partial density x 1000 (g/cm^3).
+ */
+#ifndef VCT_H
+#define VCT_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define VCT_OK 0
+#define VCT_E_ARG (-1)         /* invalid argument or size */
+#define VCT_E_CUDA (-2)        /* CUDA runtime error (message in vct_last_error) */
+#define VCT_E_TIMEOUT (-3)     /* a bounded device wait gave up */
+#define VCT_E_NOMEM (-4)       /* host or device allocation failed */
+#define VCT_E_IO (-5)          /* file missing, short or malformed */
+#define VCT_E_STATE (-6)       /* call order: e.g. forward before maps are set */
+#define VCT_E_UNSUPPORTED (-7) /* configuration outside this build's limits */
+
+#define VCT_MAX_MATERIALS 8
+#define VCT_MAX_BINS 1024 /* the reference's spectrum buffers hold 1024 bins (MB/main.cpp:338-339) */
+
+/* Fan-beam geometry.  The first block holds the compile-time macros of
+ * physParamsTOMO.h as runtime fields; the second block the input-txt fields
+ * the hot path reads.  vct_geometry_default() fills the shipped values. */
+typedef struct vct_geometry {
+  double sid_cm;         /* DIST_BTWN_SRC_AND_ISOCENT_CM 85.0           MB/physParamsTOMO.h:25 */
+  double det_radius_cm;  /* DETECTOR_RADIUS_CURVATURE_CM 142.6          MB/physParamsTOMO.h:27 */
+  double det_src_iso_cm; /* DIST_BTWN_DETERCTORSRC_AND_ISOCENT_CM 85.0  MB/physParamsTOMO.h:28 */
+  int start_channel;     /* Start_Channel 0                             MB/physParamsTOMO.h:43 */
+  int end_channel;       /* End_Channel 609                             MB/physParamsTOMO.h:46 */
+  double iso_channel;    /* isocenter_channel 304.5                     MB/physParamsTOMO.h:47 */
+  double max_alpha;      /* Max_alpha 0.326086956                       MB/physParamsTOMO.h:56 */
+  double max_beta;       /* Max_beta 0.326086956                        FBP/physParamsTOMO.h:50 */
+  int views;             /* projImgHeight = GantryRotationPeriod*DataSamplingRate */
+  int width;             /* projImgWidth: sinogram row stride (>= end_channel) */
+  double start_view_deg; /* StartViewAngle */
+  int recon_size;        /* reconSize N (square image) */
+  double pixel_cm;       /* reconPixSize */
+  int xfactor;           /* "Factor for output CT value" */
+} vct_geometry;
+
+/* Replaces the physParamsTOMO.h defaults + the shipped txt (800 views x 609
+ * channels, 512 x 512 at 0.1 cm, xfactor 1). */
+void vct_geometry_default(vct_geometry* g);
+
+const char* vct_strerror(int code);
+const char* vct_last_error(void);
+
+typedef struct vct_ctx vct_ctx;
+
+/* Creates a context on CUDA device `device` for geometry g.  Precomputes the
+ * view trig tables (MB/projectionDataTOMO.cpp:362-368, MB/misc_TOMO.cpp:82-100)
+ * and detector tables on the host and uploads them. */
+int vct_create(const vct_geometry* g, int device, vct_ctx** out);
+void vct_destroy(vct_ctx* ctx);
+/* cudaStream_t passed as an opaque pointer; NULL = the context's own stream. */
+int vct_set_stream(vct_ctx* ctx, void* stream);
+int vct_synchronize(vct_ctx* ctx);
+
+/* ---------------------------------------------------------------- spectrum
+ * Host-side restatement of attenuation_coefficient
+ * (MB/prior_weight_production.cpp:180-297): reads the spectrum txt
+ * (one header line, then "E_lo E_hi weight" in MeV), normalises the pdf in
+ * float and fills the analytic mass attenuation table mu[M][NE] (cm^2/g) for
+ * the elements given by atomic number Z (A = the reference's table for
+ * H,C,N,O,P,Ca and Mg=24, Si=28).  pdf must hold VCT_MAX_BINS floats and mu
+ * M*VCT_MAX_BINS floats.  Results are bit-identical to the reference. */
+int vct_attenuation_coefficient(const char* spectrum_path, int nthin, const int* Z, int M,
+                                float* mu, float* pdf, int* NE);
+
+/* ----------------------------------------------------------------- MBFPA
+ * Uploads the element maps int16 [M][N][N] (value = partial density x 1000;
+ * the reference reads them with fread as short, MB/main.cpp:421-429, and
+ * divides by 1000, :103).  Negative entries contribute nothing, as in
+ * MB/reprojection_TOMO.cpp:151-155. */
+int vct_set_maps(vct_ctx* ctx, const int16_t* maps, int M);
+int vct_set_maps_dev(vct_ctx* ctx, const int16_t* d_maps, int M);
+
+/* Uploads mu [M][NE] (bin fastest, the Attenuation layout of
+ * MB/reprojection_TOMO.cpp:156) and pdf [NE]. */
+int vct_set_spectrum(vct_ctx* ctx, const float* mu, const float* pdf, int M, int NE);
+
+/* Spectral summation mode of the forward epilogue. */
+#define VCT_SUM_COMPENSATED 0 /* bins summed in an FP64 accumulator (default) */
+#define VCT_SUM_REFERENCE 1   /* each bin rounded to float and summed in float in
+                                 bin order, as MB/main.cpp:504 */
+int vct_set_sum_mode(vct_ctx* ctx, int mode);
+
+/* Polyenergetic forward projection, un-normalised:
+ *   sino[v][c] = sum_E pdf[E] * exp(-sum_m mu_m(E) * L_m(v,c) / xfactor)
+ * with L_m the line integrals of the reference's ray walk
+ * (MB/reprojection_TOMO.cpp:13-289, one walk per ray for all bins).
+ * Rows v >= views/2*2 and channels outside [start_channel, end_channel) are 0,
+ * as the reference leaves them. */
+int vct_forward(vct_ctx* ctx, float* sino_out);
+int vct_forward_dev(vct_ctx* ctx, float* d_sino_out);
+
+/* Per-ray line integrals only: lint[v][c][m] in g/cm^2 (FP64). */
+int vct_line_integrals_dev(vct_ctx* ctx, double* d_lint_out);
+
+/* Full MBFPA as MB/main.cpp:492-530: forward, divide by the global maximum,
+ * then additive Gaussian noise of standard deviation sigma with the
+ * reference's clamps (p < 0 -> projection_min/10, p > 1 -> 1).  Noise is
+ * counter-based Philox4x32-10 keyed by (seed, view, channel); sigma <= 0
+ * skips it.  stats (optional, 3 floats) receives {max, min_normalised,
+ * sum-of-segments as float}. */
+int vct_mbfpa(vct_ctx* ctx, double sigma, uint64_t seed, float* sino_out, float* stats);
+int vct_mbfpa_dev(vct_ctx* ctx, double sigma, uint64_t seed, float* d_sino_out);
+
+/* Only the normalisation + noise step on a device sinogram (in place). */
+int vct_normalize_noise_dev(vct_ctx* ctx, float* d_sino, double sigma, uint64_t seed);
+
+/* ------------------------------------------------------------------- FBP
+ * filterSinogram + reconstructImage (Release_FBP_CPU/main.cpp:137-167) for
+ * one slice.  filter: 1 Ram-Lak, 2 Shepp-Logan (prepareConstMap,
+ * FBP/filterSinogramTOMO.cpp:9-138).  in_mode != 0 applies the "IN" class
+ * window (filtered values outside [1000, 3e5] -> 0, :250-255).
+ * sino: [views][width] transmission values p; img_out: [N][N]. */
+int vct_fbp(vct_ctx* ctx, const float* sino, int filter, int in_mode, float* img_out);
+int vct_fbp_dev(vct_ctx* ctx, const float* d_sino, int filter, int in_mode, float* d_img_out);
+/* The filtered sinogram of the last vct_fbp* call, [views][C]. */
+int vct_fbp_filtered_dev(vct_ctx* ctx, const float** d_fltd);
+
+/* ------------------------------------------------------------ inspection */
+/* Number of in-grid walk segments of the last forward (the algorithmic work
+ * unit of the forward kernel). */
+int vct_last_segment_count(vct_ctx* ctx, long long* segments);
+/* Number of kernels this context has launched since creation. */
+long long vct_kernel_launches(vct_ctx* ctx);
+int vct_version(void);
+/* Roofline denominators measured on `device`: L2 read bandwidth (GB/s,
+ * ld.global.cg over a 16 MB L2-resident buffer), FP64 and FP32 FMA
+ * throughput (TFLOP/s).  Any output pointer may be NULL. */
+int vct_probe_peaks(int device, double* l2_read_gbs, double* fp64_tflops, double* fp32_tflops);
+/* Philox4x32-10 (the noise generator of vct_mbfpa) evaluated on the host,
+ * for known-answer tests. */
+void vct_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VCT_H */

@@ -1,0 +1,102 @@
+/*
+ * vct_io.h -- the reference's input-txt and raw-file formats (host side of
+ * the drop-in executables vct_mbfpa and vct_fbp).
+ *
+ * The txt format is positional: 6 header lines, then for every field two
+ * skipped lines and one value line (MB/projectionDataTOMO.cpp:17-64).
+ */
+#ifndef VCT_IO_H
+#define VCT_IO_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#include "vct.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* The 31 fields of the MBFPA input txt, MB/projectionDataTOMO.h:2-68 and
+ * MB/projectionDataTOMO.cpp:83-121, plus the derived values of :126-134 and
+ * :332-333. */
+typedef struct vct_mb_config {
+  char in_pr_class[16];          /* "PR" or "IN" */
+  int prior_image_onoff;
+  int proj_width;                /* projImgWidth */
+  int proj_height;               /* projImgHeight after derivation */
+  char proj_data_type[16];
+  int proj_file_offset;
+  char proj_file[256];
+  char air_scan_file[256];
+  double gantry_rotation_period;
+  double data_sampling_rate;     /* after the >= 200 Hz thinning */
+  double data_sampling_rate_orig;
+  double start_view_angle;
+  double couch_speed;
+  double start_couch_position;
+  int recon_size;
+  double recon_pix_size;
+  char recon_tgt_class[16];
+  double recon_offset;
+  double recon_step;
+  int recon_slices;
+  int xfactor;
+  char recon_data_file[256];     /* prior image */
+  int fbp_slice;
+  double x_reg, y_reg, z_reg;    /* z_reg after the ScanListZvalue update (:109) */
+  double scan_list_z;
+  int osemset;
+  double total_variation, prior_const, markov_const;
+  double gradient_decent_const;
+  int num_ite;
+  int sino_fact;
+  char spectrum_file[256];
+  double photon_noise;
+  int total_proj_number;         /* (int)(txt height/(period*rate_orig)) */
+} vct_mb_config;
+
+/* The 21 fields of the FBP input txt, FBP/projectionDataTOMO.cpp:70-96. */
+typedef struct vct_fbp_config {
+  char in_pr_class[16];
+  int filter;                    /* 1 Ram-Lak, 2 Shepp-Logan */
+  int proj_width;
+  int proj_height;               /* (int)(period*rate) */
+  char proj_data_type[16];
+  int proj_file_offset;
+  char proj_file[256];
+  char air_scan_file[256];
+  double gantry_rotation_period;
+  double data_sampling_rate;
+  double start_view_angle;
+  double couch_speed;
+  double start_couch_position;
+  int recon_size;
+  double recon_pix_size;
+  char recon_tgt_class[16];
+  double recon_offset;
+  double recon_step;
+  int recon_slices;
+  int xfactor;
+  char output_file[256];         /* reconDataFilename: the output image */
+  int total_proj_number;
+} vct_fbp_config;
+
+/* Returns VCT_OK, or VCT_E_IO when the file cannot be opened (the reference
+ * prints "info file: ... not found" and exits). */
+int vct_load_mb_config(const char* path, vct_mb_config* cfg);
+int vct_load_fbp_config(const char* path, vct_fbp_config* cfg);
+
+/* Geometry for a parsed config: physParamsTOMO.h defaults + txt fields. */
+void vct_mb_geometry(const vct_mb_config* cfg, vct_geometry* g);
+void vct_fbp_geometry(const vct_fbp_config* cfg, vct_geometry* g);
+
+/* Reads exactly `bytes` bytes at `offset`; VCT_E_IO on a missing or short
+ * file.  *got (optional) receives the byte count actually read. */
+int vct_read_raw(const char* path, long offset, void* buf, size_t bytes, size_t* got);
+int vct_write_raw(const char* path, const void* buf, size_t bytes);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* VCT_IO_H */

@@ -83,14 +83,24 @@ int vctref_reprojection_bins(int N, double pixel_cm, const float* rho, int V, in
   float* proj = (float*)calloc((size_t)V * W, sizeof(float));
   // Segment side tables written by the walk (never read on this path).  The
   // reference sizes them W*V*N*2 (main.cpp:261-262); a ray has at most about
-  // 2N+4 segments, so the margin keeps small grids in bounds too.
+  // 2N+4 segments, so the margin keeps small grids in bounds too.  They are
+  // kept between calls, as the reference's main allocates them once, so only
+  // the first call pays for faulting their pages in.
+  static float* sysmat = nullptr;
+  static int* vnum = nullptr;
+  static size_t cap = 0;
   size_t slots = (size_t)W * V * (size_t)(2 * N + 16);
-  float* sysmat = (float*)malloc(sizeof(float) * slots);
-  int* vnum = (int*)malloc(sizeof(int) * slots);
+  if (slots > cap) {
+    free(sysmat);
+    free(vnum);
+    sysmat = (float*)malloc(sizeof(float) * slots);
+    vnum = (int*)malloc(sizeof(int) * slots);
+    cap = (sysmat && vnum) ? slots : 0;
+  }
   int* rsum = (int*)calloc((size_t)V * W, sizeof(int));
   char* mask = (char*)calloc(n2, 1);
   if (!work || !proj || !sysmat || !vnum || !rsum || !mask) {
-    free(work); free(proj); free(sysmat); free(vnum); free(rsum); free(mask);
+    free(work); free(proj); free(rsum); free(mask);
     return -2;
   }
   memcpy(work, rho, sizeof(float) * M * n2);
@@ -107,7 +117,7 @@ int vctref_reprojection_bins(int N, double pixel_cm, const float* rho, int V, in
   if (seconds) *seconds = t1 - t0;
   if (last_bin) memcpy(last_bin, proj, sizeof(float) * V * W);
   if (nseg) memcpy(nseg, rsum, sizeof(int) * V * W);
-  free(work); free(proj); free(sysmat); free(vnum); free(rsum); free(mask);
+  free(work); free(proj); free(rsum); free(mask);
   return 0;
 }
 

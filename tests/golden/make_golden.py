@@ -1,0 +1,128 @@
+"""Generates the golden fixtures in tests/golden/ from the reference itself.
+
+Run in a checkout that has the reference sources (REF, default
+/root/reference) and `make -C oracle` done:
+
+    python tests/golden/make_golden.py
+
+Every array below is produced by the reference's own code, compiled from its
+sources by oracle/Makefile (oracle/_ref/libvct_ref_*.so), except where noted
+as the pinned oracle (used only where the reference would need one run per
+energy bin for hours).  The GPU tests read these files; they never read REF.
+
+Fixtures
+  mu_tables.npz   attenuation_coefficient tables (pdf, mu) of the two shipped
+                  spectra and of the synthetic 120 kVp Kramers spectrum.
+  mb_small.npz    reprojection_TOMO summed over all bins (MB/main.cpp:492-506)
+                  for a seeded 64^2 ellipse phantom, 40 and 41 views.
+  fbp_small.npz   filterSinogram + reconstructImage of a 40-view sinogram onto
+                  64^2, Ram-Lak and Shepp-Logan.
+  c1_subset.npz   full-size C1 (512^2, 800 x 609, 6 elements, 110-bin Kramers
+                  spectrum, seeded ellipse phantom seed 0): every 20th view of
+                  the reference's un-normalised spectral sum, its global max
+                  and min, and the total segment count.
+"""
+from __future__ import annotations
+
+import os
+import sys
+import tempfile
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+sys.path.insert(0, ROOT)
+
+import oracle as O  # noqa: E402
+from virtualct_b200 import phantoms  # noqa: E402
+
+REF = os.environ.get("REF", "/root/reference")
+MB = os.path.join(REF, "Release_MBFPA_CPU_human")
+OUT = os.path.dirname(os.path.abspath(__file__))
+
+C1_SEED = 0
+C1_SUBSET_STEP = 20
+
+
+def kramers_file(tmp, kvp=120):
+    p = os.path.join(tmp, f"kramers_{kvp}.txt")
+    phantoms.write_spectrum_txt(p, phantoms.kramers_spectrum(kvp))
+    return p
+
+
+def mu_tables(tmp):
+    out = {}
+    for name, path in (("kv120", os.path.join(MB, "Spectrum/PhaseSpace_photon_120kV_0cm.txt")),
+                       ("mv6", os.path.join(MB, "Spectrum/PhaseSpace_photon_6MV_0cm.txt")),
+                       ("kramers120", kramers_file(tmp))):
+        pdf, mu = O.ref_attenuation(path)
+        out[f"{name}_pdf"] = pdf
+        out[f"{name}_mu"] = mu
+    np.savez_compressed(os.path.join(OUT, "mu_tables.npz"), **out)
+    # The Kramers text file itself, so the GPU box can parse the same bytes.
+    with open(kramers_file(tmp)) as f:
+        txt = f.read()
+    with open(os.path.join(OUT, "kramers_120kvp.txt"), "w") as f:
+        f.write(txt)
+    return out
+
+
+def mb_small(tabs):
+    N, pix = 64, 0.4
+    maps = phantoms.ellipse_phantom(7, N, border_px=2)
+    rho = O.rho_from_maps(maps)
+    pdf, mu = tabs["kv120_pdf"], tabs["kv120_mu"]
+    out = {"maps": maps, "N": N, "pixel_cm": pix}
+    for V in (40, 41):
+        c, s = O.trig_tables(V)
+        full, _ = O.ref_reprojection(N, pix, rho, V, 609, c, s, 1, mu, pdf)
+        out[f"full_v{V}"] = full
+    np.savez_compressed(os.path.join(OUT, "mb_small.npz"), **out)
+
+
+def fbp_small():
+    d = np.load(os.path.join(OUT, "mb_small.npz"))
+    full = d["full_v40"]
+    sino = (full / full.max()).astype(np.float32)
+    c, s = O.trig_tables(40)
+    out = {"sino": sino}
+    for filt in (1, 2):
+        img, fl, _, _ = O.ref_fbp(filt, sino, 64, 0.4, 1, c, s)
+        out[f"img_f{filt}"] = img
+        out[f"fltd_f{filt}"] = fl
+    np.savez_compressed(os.path.join(OUT, "fbp_small.npz"), **out)
+
+
+def c1_subset(tabs):
+    maps = phantoms.ellipse_phantom(C1_SEED, 512)
+    rho = O.rho_from_maps(maps)
+    pdf, mu = tabs["kramers120_pdf"], tabs["kramers120_mu"]
+    c, s = O.trig_tables(800)
+    g = O.geom()
+    # Pinned oracle in reference order (bit-identical to reprojection_TOMO on
+    # the shipped golden); cross-checked against the reference on two bins.
+    full, nseg = O.forward_exact(g, c, s, rho, mu, pdf, want_nseg=True)
+    ref2, _ = O.ref_reprojection(512, 0.1, rho, 800, 609, c, s, 1, mu, pdf, ke0=50, ke1=52)
+    ora2 = O.forward_exact(g, c, s, rho, np.ascontiguousarray(mu[:, 50:52]), pdf[50:52].copy())
+    assert np.array_equal(ora2, ref2), "oracle and reference disagree on bins 50-51"
+    rows = np.arange(0, 800, C1_SUBSET_STEP)
+    np.savez_compressed(os.path.join(OUT, "c1_subset.npz"), rows=rows, full_rows=full[rows],
+                        max=np.float32(full.max()), min=np.float32(full.min()),
+                        segments=np.int64(nseg.sum()), seed=C1_SEED,
+                        maps_sha=np.frombuffer(__import__("hashlib").sha256(maps.tobytes()).digest(), np.uint8))
+
+
+def main():
+    if not O.ref_available():
+        raise SystemExit("reference harness not built: make -C oracle ref")
+    with tempfile.TemporaryDirectory() as tmp:
+        tabs = mu_tables(tmp)
+    mb_small(tabs)
+    fbp_small()
+    c1_subset(tabs)
+    for f in sorted(os.listdir(OUT)):
+        print(f, os.path.getsize(os.path.join(OUT, f)))
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,62 @@
+"""Normalisation + Philox noise (gaussiannoise0, MB/main.cpp:51-76): checked by
+per-channel mean and variance, clamps and determinism, not sample by sample."""
+import numpy as np
+import pytest
+
+import virtualct_b200 as vct
+from conftest import golden
+
+pytestmark = pytest.mark.gpu
+
+
+def _run(sigma, seed, views=800):
+    t = golden("mu_tables.npz")
+    from virtualct_b200 import phantoms
+
+    maps = phantoms.ellipse_phantom(5, 128)
+    with vct.Context(vct.Geometry(views=views, recon_size=128, pixel_cm=0.4)) as ctx:
+        ctx.set_maps(maps)
+        ctx.set_spectrum(t["kramers120_mu"], t["kramers120_pdf"])
+        clean = ctx.mbfpa(0.0, seed)
+        noisy, st = ctx.mbfpa(sigma, seed, return_stats=True)
+    return clean, noisy, st
+
+
+def test_noise_statistics(cuda_device):
+    sigma = 2e-3
+    clean, noisy, st = _run(sigma, 1234)
+    assert clean.max() == 1.0
+    ok = (clean > 10 * sigma) & (clean < 1 - 10 * sigma)  # away from both clamps
+    d = noisy.astype(np.float64) - clean
+    cols = np.flatnonzero(ok.sum(0) >= 400)
+    assert len(cols) > 100
+    for c in cols:
+        x = d[ok[:, c], c]
+        n = len(x)
+        # per channel over views: mean ~ N(0, sigma^2/n), var ~ sigma^2 (1 +- sqrt(2/(n-1)))
+        assert abs(x.mean()) < 6 * sigma / np.sqrt(n)
+        assert abs(x.var(ddof=1) / sigma**2 - 1) < 6 * np.sqrt(2 / (n - 1))
+    x = d[ok]
+    assert abs(x.mean()) < 6 * sigma / np.sqrt(x.size)
+    assert abs(x.var() / sigma**2 - 1) < 6 * np.sqrt(2 / (x.size - 1))
+
+
+def test_noise_clamps_and_determinism(cuda_device):
+    sigma = 0.05
+    clean, noisy, st = _run(sigma, 7)
+    assert noisy.max() <= 1.0
+    pmin = float(st[1])
+    assert abs(pmin - clean.min()) <= 1e-7 * max(pmin, 1e-30)
+    assert noisy.min() >= 0.0
+    # p + noise < 0 -> projection_min/10: with sigma = 0.05 the darkest rays
+    # (p < 1e-3) go negative about half the time.
+    floor = np.float32(pmin / 10)
+    dark = clean < 1e-3
+    assert dark.sum() > 100
+    frac = float(np.mean(noisy[dark] == floor))
+    assert 0.3 < frac < 0.7
+    assert np.any(noisy == 1.0)
+    _, again, _ = _run(sigma, 7)
+    _, other, _ = _run(sigma, 8)
+    assert np.array_equal(noisy, again)
+    assert not np.array_equal(noisy, other)

@@ -1,0 +1,308 @@
+"""virtualct_b200 -- B200-native MBFPA forward projection and fan-beam FBP.
+
+Python view of the C ABI in ``include/vct.h`` (``lib/libvct.so``).  All compute
+runs in the CUDA kernels of ``csrc/``; there is no CPU fallback: if the library
+is missing, importing the bindings raises.
+
+    import virtualct_b200 as vct
+    g = vct.Geometry()                       # physParamsTOMO.h defaults, 800 x 609, 512^2
+    mu, pdf = vct.attenuation_coefficient("PhaseSpace_photon_120kV_0cm.txt")
+    with vct.Context(g) as ctx:
+        ctx.set_maps(maps_int16)             # [M][N][N], density x 1000
+        ctx.set_spectrum(mu, pdf)
+        sino = ctx.mbfpa(sigma=5.37e-5, seed=1)   # MB/main.cpp:492-530
+        img = ctx.fbp(sino, filter=2)        # FBP/main.cpp:137-167
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+from dataclasses import dataclass, fields
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "lib", "libvct.so")
+
+VCT_OK = 0
+VCT_E_ARG = -1
+VCT_E_CUDA = -2
+VCT_E_TIMEOUT = -3
+VCT_E_NOMEM = -4
+VCT_E_IO = -5
+VCT_E_STATE = -6
+VCT_E_UNSUPPORTED = -7
+SUM_COMPENSATED = 0
+SUM_REFERENCE = 1
+MAX_BINS = 1024
+
+ELEMENT_Z = {"H": 1, "C": 6, "N": 7, "O": 8, "P": 15, "Ca": 20, "Mg": 12, "Si": 14}
+HUMAN_ELEMENTS = ("H", "C", "N", "O", "P", "Ca")
+GAMMEX_ELEMENTS = ("H", "C", "N", "O", "P", "Ca", "Mg", "Si")
+
+# Every entry point include/vct.h and include/vct_io.h declare.
+EXPORTED_SYMBOLS = (
+    "vct_geometry_default", "vct_strerror", "vct_last_error", "vct_create", "vct_destroy", "vct_set_stream",
+    "vct_synchronize", "vct_attenuation_coefficient", "vct_set_maps", "vct_set_maps_dev", "vct_set_spectrum",
+    "vct_set_sum_mode", "vct_forward", "vct_forward_dev", "vct_line_integrals_dev", "vct_mbfpa", "vct_mbfpa_dev",
+    "vct_normalize_noise_dev", "vct_fbp", "vct_fbp_dev", "vct_fbp_filtered_dev", "vct_last_segment_count",
+    "vct_kernel_launches", "vct_version", "vct_philox4x32_10", "vct_probe_peaks",
+    "vct_load_mb_config", "vct_load_fbp_config", "vct_mb_geometry", "vct_fbp_geometry", "vct_read_raw",
+    "vct_write_raw",
+)
+
+
+class VctError(RuntimeError):
+    def __init__(self, code: int, where: str, msg: str):
+        super().__init__(f"{where}: {msg} (code {code})")
+        self.code = code
+
+
+class _CGeometry(C.Structure):
+    _fields_ = [
+        ("sid_cm", C.c_double), ("det_radius_cm", C.c_double), ("det_src_iso_cm", C.c_double),
+        ("start_channel", C.c_int), ("end_channel", C.c_int), ("iso_channel", C.c_double),
+        ("max_alpha", C.c_double), ("max_beta", C.c_double), ("views", C.c_int), ("width", C.c_int),
+        ("start_view_deg", C.c_double), ("recon_size", C.c_int), ("pixel_cm", C.c_double), ("xfactor", C.c_int),
+    ]
+
+
+@dataclass
+class Geometry:
+    """Runtime form of physParamsTOMO.h plus the txt fields of the hot path."""
+
+    sid_cm: float = 85.0
+    det_radius_cm: float = 142.6
+    det_src_iso_cm: float = 85.0
+    start_channel: int = 0
+    end_channel: int = 609
+    iso_channel: float = 304.5
+    max_alpha: float = 0.326086956
+    max_beta: float = 0.326086956
+    views: int = 800
+    width: int = 609
+    start_view_deg: float = 0.0
+    recon_size: int = 512
+    pixel_cm: float = 0.1
+    xfactor: int = 1
+
+    @classmethod
+    def with_channels(cls, channels: int, **kw) -> "Geometry":
+        """Geometry with ``channels`` detector channels; the iso-channel follows
+        the reference's convention (End_Channel/2.0, 304.5 for 609)."""
+        return cls(end_channel=channels, width=channels, iso_channel=channels / 2.0, **kw)
+
+    @property
+    def channels(self) -> int:
+        return self.end_channel - self.start_channel
+
+    def to_c(self) -> _CGeometry:
+        c = _CGeometry()
+        for f in fields(self):
+            setattr(c, f.name, getattr(self, f.name))
+        return c
+
+
+_lib = None
+
+
+def lib():
+    """The loaded libvct.so.  Raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(LIB_PATH):
+        raise RuntimeError(f"libvct.so not built ({LIB_PATH}); run `python -m virtualct_b200.build`")
+    L = C.CDLL(LIB_PATH)
+    vp = C.c_void_p
+    L.vct_strerror.restype = C.c_char_p
+    L.vct_strerror.argtypes = [C.c_int]
+    L.vct_last_error.restype = C.c_char_p
+    L.vct_geometry_default.argtypes = [C.POINTER(_CGeometry)]
+    L.vct_create.argtypes = [C.POINTER(_CGeometry), C.c_int, C.POINTER(vp)]
+    L.vct_destroy.argtypes = [vp]
+    L.vct_destroy.restype = None
+    L.vct_set_stream.argtypes = [vp, vp]
+    L.vct_synchronize.argtypes = [vp]
+    L.vct_attenuation_coefficient.argtypes = [C.c_char_p, C.c_int, vp, C.c_int, vp, vp, C.POINTER(C.c_int)]
+    L.vct_set_maps.argtypes = [vp, vp, C.c_int]
+    L.vct_set_maps_dev.argtypes = [vp, vp, C.c_int]
+    L.vct_set_spectrum.argtypes = [vp, vp, vp, C.c_int, C.c_int]
+    L.vct_set_sum_mode.argtypes = [vp, C.c_int]
+    L.vct_forward.argtypes = [vp, vp]
+    L.vct_forward_dev.argtypes = [vp, vp]
+    L.vct_line_integrals_dev.argtypes = [vp, vp]
+    L.vct_mbfpa.argtypes = [vp, C.c_double, C.c_uint64, vp, vp]
+    L.vct_mbfpa_dev.argtypes = [vp, C.c_double, C.c_uint64, vp]
+    L.vct_normalize_noise_dev.argtypes = [vp, vp, C.c_double, C.c_uint64]
+    L.vct_fbp.argtypes = [vp, vp, C.c_int, C.c_int, vp]
+    L.vct_fbp_dev.argtypes = [vp, vp, C.c_int, C.c_int, vp]
+    L.vct_fbp_filtered_dev.argtypes = [vp, C.POINTER(vp)]
+    L.vct_last_segment_count.argtypes = [vp, C.POINTER(C.c_longlong)]
+    L.vct_kernel_launches.argtypes = [vp]
+    L.vct_kernel_launches.restype = C.c_longlong
+    L.vct_philox4x32_10.argtypes = [vp, vp, vp]
+    L.vct_philox4x32_10.restype = None
+    L.vct_probe_peaks.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    _lib = L
+    return L
+
+
+def _check(rc: int, where: str) -> None:
+    if rc != VCT_OK:
+        msg = lib().vct_last_error().decode(errors="replace")
+        raise VctError(rc, where, msg)
+
+
+def _ptr(a: np.ndarray) -> int:
+    return a.ctypes.data
+
+
+def attenuation_coefficient(spectrum_path, elements=HUMAN_ELEMENTS, nthin: int = 1):
+    """Spectrum pdf [NE] and mass attenuation mu [M][NE] (cm^2/g), bit-identical
+    to MB/prior_weight_production.cpp:180-297 for the same elements."""
+    Z = np.array([ELEMENT_Z[e] for e in elements], np.int32)
+    mu = np.zeros(len(Z) * MAX_BINS, np.float32)
+    pdf = np.zeros(MAX_BINS, np.float32)
+    ne = C.c_int(0)
+    _check(lib().vct_attenuation_coefficient(str(spectrum_path).encode(), nthin, _ptr(Z), len(Z), _ptr(mu),
+                                             _ptr(pdf), C.byref(ne)), "vct_attenuation_coefficient")
+    n = ne.value
+    return mu[: len(Z) * n].reshape(len(Z), n).copy(), pdf[:n].copy()
+
+
+def philox4x32_10(ctr, key):
+    c = np.ascontiguousarray(ctr, np.uint32)
+    k = np.ascontiguousarray(key, np.uint32)
+    out = np.zeros(4, np.uint32)
+    lib().vct_philox4x32_10(_ptr(c), _ptr(k), _ptr(out))
+    return out
+
+
+def probe_peaks(device: int = 0) -> dict:
+    """Live roofline denominators on `device` (see vct_probe_peaks)."""
+    l2, f64, f32 = C.c_double(0), C.c_double(0), C.c_double(0)
+    _check(lib().vct_probe_peaks(device, C.byref(l2), C.byref(f64), C.byref(f32)), "vct_probe_peaks")
+    return {"l2_read_gbs": l2.value, "fp64_tflops": f64.value, "fp32_tflops": f32.value}
+
+
+class Context:
+    """One device context (vct_ctx): geometry tables, maps, spectrum and
+    scratch buffers live on the GPU between calls."""
+
+    def __init__(self, geometry: Geometry | None = None, device: int = 0):
+        self.geometry = geometry or Geometry()
+        self._g = self.geometry.to_c()
+        self._h = C.c_void_p()
+        _check(lib().vct_create(C.byref(self._g), device, C.byref(self._h)), "vct_create")
+        self.device = device
+
+    # lifetime ---------------------------------------------------------------
+    def close(self) -> None:
+        if self._h:
+            lib().vct_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def set_stream(self, stream_ptr: int | None) -> None:
+        _check(lib().vct_set_stream(self._h, stream_ptr or None), "vct_set_stream")
+
+    def synchronize(self) -> None:
+        _check(lib().vct_synchronize(self._h), "vct_synchronize")
+
+    @property
+    def kernel_launches(self) -> int:
+        return int(lib().vct_kernel_launches(self._h))
+
+    @property
+    def last_segment_count(self) -> int:
+        n = C.c_longlong(0)
+        _check(lib().vct_last_segment_count(self._h, C.byref(n)), "vct_last_segment_count")
+        return n.value
+
+    # MBFPA -------------------------------------------------------------------
+    def set_maps(self, maps) -> None:
+        """maps: int16 [M][N][N] (element density x 1000), host array or a CUDA
+        tensor (anything with ``data_ptr()`` is taken as a device pointer)."""
+        if hasattr(maps, "data_ptr"):
+            M = int(maps.shape[0])
+            _check(lib().vct_set_maps_dev(self._h, maps.data_ptr(), M), "vct_set_maps_dev")
+            return
+        a = np.ascontiguousarray(maps, np.int16)
+        N = self.geometry.recon_size
+        if a.ndim != 3 or a.shape[1:] != (N, N):
+            raise ValueError(f"maps must be [M][{N}][{N}] int16, got {a.shape}")
+        _check(lib().vct_set_maps(self._h, _ptr(a), a.shape[0]), "vct_set_maps")
+
+    def set_spectrum(self, mu, pdf) -> None:
+        mu = np.ascontiguousarray(mu, np.float32)
+        pdf = np.ascontiguousarray(pdf, np.float32)
+        M, NE = mu.shape
+        if pdf.shape != (NE,):
+            raise ValueError("pdf must have NE entries")
+        _check(lib().vct_set_spectrum(self._h, _ptr(mu), _ptr(pdf), M, NE), "vct_set_spectrum")
+
+    def set_sum_mode(self, mode: int) -> None:
+        _check(lib().vct_set_sum_mode(self._h, mode), "vct_set_sum_mode")
+
+    def _sino(self) -> np.ndarray:
+        return np.zeros((self.geometry.views, self.geometry.width), np.float32)
+
+    def forward(self) -> np.ndarray:
+        """Un-normalised polyenergetic sinogram [views][width]."""
+        out = self._sino()
+        _check(lib().vct_forward(self._h, _ptr(out)), "vct_forward")
+        return out
+
+    def forward_dev(self, out) -> None:
+        _check(lib().vct_forward_dev(self._h, out.data_ptr()), "vct_forward_dev")
+
+    def line_integrals_dev(self, out) -> None:
+        _check(lib().vct_line_integrals_dev(self._h, out.data_ptr()), "vct_line_integrals_dev")
+
+    def mbfpa(self, sigma: float = 0.0, seed: int = 1, return_stats: bool = False):
+        """MB/main.cpp:492-530: forward, max-normalise, Gaussian noise."""
+        out = self._sino()
+        st = np.zeros(3, np.float32)
+        _check(lib().vct_mbfpa(self._h, float(sigma), int(seed), _ptr(out), _ptr(st)), "vct_mbfpa")
+        return (out, st) if return_stats else out
+
+    def mbfpa_dev(self, sigma: float, seed: int, out) -> None:
+        _check(lib().vct_mbfpa_dev(self._h, float(sigma), int(seed), out.data_ptr()), "vct_mbfpa_dev")
+
+    def normalize_noise_dev(self, sino, sigma: float, seed: int) -> None:
+        _check(lib().vct_normalize_noise_dev(self._h, sino.data_ptr(), float(sigma), int(seed)),
+               "vct_normalize_noise_dev")
+
+    # FBP ---------------------------------------------------------------------
+    def fbp(self, sino, filter: int = 1, in_mode: bool = False) -> np.ndarray:
+        s = np.ascontiguousarray(sino, np.float32)
+        if s.shape != (self.geometry.views, self.geometry.width):
+            raise ValueError(f"sinogram must be [{self.geometry.views}][{self.geometry.width}]")
+        N = self.geometry.recon_size
+        img = np.zeros((N, N), np.float32)
+        _check(lib().vct_fbp(self._h, _ptr(s), filter, int(in_mode), _ptr(img)), "vct_fbp")
+        return img
+
+    def fbp_dev(self, sino, img, filter: int = 1, in_mode: bool = False) -> None:
+        _check(lib().vct_fbp_dev(self._h, sino.data_ptr(), filter, int(in_mode), img.data_ptr()), "vct_fbp_dev")
+
+    def fbp_filtered_ptr(self) -> int:
+        p = C.c_void_p()
+        _check(lib().vct_fbp_filtered_dev(self._h, C.byref(p)), "vct_fbp_filtered_dev")
+        return p.value

@@ -1,0 +1,98 @@
+"""Build libvct.so (and the drop-in executables) for sm_100a with nvcc.
+
+Usage: python -m virtualct_b200.build [--force]
+
+Outputs, all in-tree so they travel with the repository snapshot:
+  virtualct_b200/lib/libvct.so     C-ABI library (include/vct.h)
+  virtualct_b200/bin/vct_mbfpa     drop-in for Release_MBFPA_CPU_human/mvct.exe
+  virtualct_b200/bin/vct_fbp       drop-in for Release_FBP_CPU/mvct.exe
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(PKG)
+CSRC = os.path.join(PKG, "csrc")
+INC = os.path.join(ROOT, "include")
+BUILD = os.path.join(PKG, "_build")
+LIBDIR = os.path.join(PKG, "lib")
+BINDIR = os.path.join(PKG, "bin")
+LIB = os.path.join(LIBDIR, "libvct.so")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+NVCC_COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", INC, "-I", CSRC]
+
+# Per-translation-unit flags.  The forward walk must not fuse a*b+c: the
+# reference (x86-64, -O2, no FMA) rounds every product and sum separately,
+# and the walk's segment boundaries depend on those roundings.
+CU_SOURCES = {
+    "vct_forward.cu": ["--fmad=false"],
+    "vct_fbp.cu": [],
+    "vct_probe.cu": [],
+}
+CPP_SOURCES = ["vct_host.cpp", "vct_io.cpp"]
+APPS = {"vct_mbfpa": "vct_mbfpa_main.cpp", "vct_fbp": "vct_fbp_main.cpp"}
+HEADERS = ["vct_internal.h", "vct_philox.h"]
+
+
+def nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), shutil.which("nvcc"), "/usr/local/cuda/bin/nvcc"):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _newer(target: str, deps: list[str]) -> bool:
+    if not os.path.exists(target):
+        return False
+    t = os.path.getmtime(target)
+    return all(os.path.getmtime(d) <= t for d in deps if os.path.exists(d))
+
+
+def _run(cmd: list[str]) -> None:
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    if r.returncode != 0:
+        sys.stderr.write(" ".join(cmd) + "\n" + r.stdout + r.stderr)
+        raise RuntimeError(f"build step failed: {os.path.basename(cmd[-1])}")
+
+
+def build(force: bool = False, verbose: bool = False) -> str:
+    os.makedirs(BUILD, exist_ok=True)
+    os.makedirs(LIBDIR, exist_ok=True)
+    os.makedirs(BINDIR, exist_ok=True)
+    hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INC, h) for h in ("vct.h", "vct_io.h")]
+    objs = []
+    for src, extra in CU_SOURCES.items():
+        s = os.path.join(CSRC, src)
+        o = os.path.join(BUILD, src + ".o")
+        if force or not _newer(o, [s] + hdrs + [__file__]):
+            cmd = [nvcc(), *ARCH, *NVCC_COMMON, *extra, "-c", s, "-o", o]
+            if verbose:
+                print(" ".join(cmd))
+            _run(cmd)
+        objs.append(o)
+    for src in CPP_SOURCES:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(BUILD, src + ".o")
+        if force or not _newer(o, [s] + hdrs + [__file__]):
+            cmd = [nvcc(), *NVCC_COMMON, "-c", s, "-o", o]
+            if verbose:
+                print(" ".join(cmd))
+            _run(cmd)
+        objs.append(o)
+    if force or not _newer(LIB, objs):
+        _run([nvcc(), *ARCH, "-shared", "-Xcompiler", "-fPIC", *objs, "-o", LIB, "-cudart", "static"])
+    for app, src in APPS.items():
+        s = os.path.join(CSRC, src)
+        exe = os.path.join(BINDIR, app)
+        if force or not _newer(exe, [s, LIB] + hdrs):
+            _run([nvcc(), *NVCC_COMMON, s, "-o", exe, "-L", LIBDIR, "-lvct", "-Xlinker", "-rpath=$ORIGIN/../lib"])
+    return LIB
+
+
+if __name__ == "__main__":
+    print(build(force="--force" in sys.argv, verbose="-v" in sys.argv))

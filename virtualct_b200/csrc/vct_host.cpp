@@ -1,0 +1,592 @@
+// Host side of libvct: context, geometry tables, spectrum model and the C ABI
+// declared in include/vct.h.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <string>
+#include <vector>
+
+#include "vct_internal.h"
+#include "vct_philox.h"
+
+namespace vct {
+
+static thread_local std::string g_last_error;
+
+void set_error(const std::string& msg) { g_last_error = msg; }
+int fail(int code, const std::string& msg) {
+  set_error(msg);
+  return code;
+}
+int cuda_fail(cudaError_t e, const char* what) {
+  set_error(std::string(what) + ": " + cudaGetErrorString(e));
+  return e == cudaErrorMemoryAllocation ? VCT_E_NOMEM : VCT_E_CUDA;
+}
+
+// PI as the reference spells it (MB/physParamsTOMO.h:1); rounds to M_PI.
+static const double kPI = 3.141592653589793238462643383279;
+
+}  // namespace vct
+
+using namespace vct;
+
+// ---------------------------------------------------------------- device buffer
+namespace {
+template <typename T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  int ensure(size_t count) {
+    if (count <= n && p) return VCT_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    VCT_CUDA(cudaMalloc((void**)&p, count * sizeof(T)));
+    n = count;
+    return VCT_OK;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+}  // namespace
+
+struct vct_ctx {
+  int device = 0;
+  vct_geometry geo{};
+  DevGeom dg{};
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  long long launches = 0;
+  // geometry tables
+  DBuf<double> cos_t, sin_t, det_px0, det_py0;
+  DBuf<float> cs_f;  // (cos, sin) pairs in float for the backprojector
+  // MBFPA
+  int M = 0, NE = 0;
+  int maps_ready = 0, spectrum_ready = 0;
+  int sum_mode = VCT_SUM_COMPENSATED;
+  DBuf<int16_t> maps_raw;
+  DBuf<PixelRec> maps;
+  DBuf<double> mu_scaled;  // [NE][M], mu/xfactor
+  DBuf<float> pdf;
+  DBuf<float> full, out;   // [views][width]
+  DBuf<FwdStats> stats;       // [0] live, [1] the reset value
+  FwdStats* h_stats = nullptr;  // pinned
+  long long last_segments = 0;
+  // FBP
+  DBuf<double> fbp_coeff;  // SID*cos((k-cw)*dbeta)*dbeta
+  DBuf<float> fbp_h[3];    // constMap per filter (1 Ram-Lak, 2 Shepp-Logan), float [C][C]
+  DBuf<float> fbp_g, fbp_q, fbp_sino, fbp_img;
+};
+
+static int check_ctx(vct_ctx* c) {
+  if (!c) return fail(VCT_E_ARG, "null context");
+  cudaError_t e = cudaSetDevice(c->device);
+  if (e != cudaSuccess) return cuda_fail(e, "cudaSetDevice");
+  return VCT_OK;
+}
+
+extern "C" {
+
+int vct_version(void) { return 100; }
+
+void vct_geometry_default(vct_geometry* g) {
+  if (!g) return;
+  g->sid_cm = 85.0;
+  g->det_radius_cm = 142.6;
+  g->det_src_iso_cm = 85.0;
+  g->start_channel = 0;
+  g->end_channel = 609;
+  g->iso_channel = 304.5;
+  g->max_alpha = 0.326086956;
+  g->max_beta = 0.326086956;
+  g->views = 800;
+  g->width = 609;
+  g->start_view_deg = 0.0;
+  g->recon_size = 512;
+  g->pixel_cm = 0.1;
+  g->xfactor = 1;
+}
+
+const char* vct_strerror(int code) {
+  switch (code) {
+    case VCT_OK: return "ok";
+    case VCT_E_ARG: return "invalid argument";
+    case VCT_E_CUDA: return "CUDA error";
+    case VCT_E_TIMEOUT: return "device wait timed out";
+    case VCT_E_NOMEM: return "out of memory";
+    case VCT_E_IO: return "I/O error";
+    case VCT_E_STATE: return "invalid call order";
+    case VCT_E_UNSUPPORTED: return "unsupported configuration";
+    default: return "unknown error";
+  }
+}
+
+const char* vct_last_error(void) { return g_last_error.c_str(); }
+
+int vct_create(const vct_geometry* g, int device, vct_ctx** out) {
+  if (!g || !out) return fail(VCT_E_ARG, "vct_create: null argument");
+  *out = nullptr;
+  const int C = g->end_channel - g->start_channel;
+  if (g->views < 2 || g->views > 100000 || C < 3 || g->start_channel < 0 || g->width < g->end_channel ||
+      g->recon_size < 2 || g->recon_size > 8192 || !(g->pixel_cm > 0) || g->xfactor == 0)
+    return fail(VCT_E_ARG, "vct_create: geometry out of range");
+  if ((C - 1) / 2 == 0) return fail(VCT_E_ARG, "vct_create: too few channels");
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
+    return fail(VCT_E_CUDA, "vct_create: no CUDA device");
+  if (device < 0 || device >= ndev) return fail(VCT_E_ARG, "vct_create: bad device index");
+  VCT_CUDA(cudaSetDevice(device));
+  vct_ctx* c = new vct_ctx();
+  c->device = device;
+  c->geo = *g;
+  DevGeom& dg = c->dg;
+  dg.N = g->recon_size;
+  dg.nxm = (int)(g->recon_size * 0.5);
+  dg.s = g->pixel_cm;
+  dg.lim = (double)dg.nxm * g->pixel_cm;
+  dg.rmax = g->recon_size * 0.5 * 1.0;
+  // Largest midpoint radius a kept segment can have: half-diagonal of the
+  // square plus one (pixel-sized) poke-out step.
+  dg.rmax_active = (dg.lim * sqrt(2.0) + 2.0 * g->pixel_cm) >= dg.rmax ? 1 : 0;
+  dg.sid = g->sid_cm;
+  dg.views = g->views;
+  dg.views_used = g->views / 2 * 2;
+  dg.width = g->width;
+  dg.C = C;
+  dg.start = g->start_channel;
+
+  int rc = VCT_OK;
+  auto bail = [&](int code) {
+    vct_destroy(c);
+    return code;
+  };
+  if (cudaStreamCreateWithFlags(&c->own_stream, cudaStreamNonBlocking) != cudaSuccess)
+    return bail(fail(VCT_E_CUDA, "cudaStreamCreate"));
+  c->stream = c->own_stream;
+
+  // View angles and trig tables: MB/projectionDataTOMO.cpp:362-368,
+  // MB/misc_TOMO.cpp:93-97 (host libm, so the tables equal the reference's).
+  const int V = g->views;
+  std::vector<double> ct(V), st(V);
+  std::vector<float> csf(2 * V);
+  for (int i = 0; i < V; i++) {
+    double angle = (double)(360.0 / V * i);
+    double rad = (g->start_view_deg + angle) * kPI / 180.0;
+    ct[i] = cos(rad);
+    st[i] = sin(rad);
+    csf[2 * i] = (float)ct[i];
+    csf[2 * i + 1] = (float)st[i];
+  }
+  // Detector point of every channel before rotation (:61-71).
+  const int half = (C - 1) / 2;
+  std::vector<double> px0(C), py0(C);
+  for (int c0 = 0; c0 < C; c0++) {
+    int jj = g->start_channel + c0;
+    double theta = (g->iso_channel - jj) * g->max_alpha / half;
+    double ox0 = g->det_radius_cm * sin(theta);
+    double oy0 = -g->det_radius_cm * cos(theta);
+    px0[c0] = ox0;
+    py0[c0] = oy0 + g->det_src_iso_cm;
+  }
+  // FBP weight: SID*cos((k-centWidth)*dbeta) (FBP/filterSinogramTOMO.cpp:236),
+  // times dbeta, the constant factor of each filter term (:242).
+  const int cw = C / 2;
+  const double dbeta = g->max_beta / half;
+  std::vector<double> coeff(C);
+  for (int k = 0; k < C; k++) coeff[k] = g->sid_cm * cos((k - cw) * (g->max_beta / half)) * dbeta;
+
+  if ((rc = c->cos_t.ensure(V)) || (rc = c->sin_t.ensure(V)) || (rc = c->cs_f.ensure(2 * V)) ||
+      (rc = c->det_px0.ensure(C)) || (rc = c->det_py0.ensure(C)) || (rc = c->fbp_coeff.ensure(C)) ||
+      (rc = c->stats.ensure(2)))
+    return bail(rc);
+  if (cudaMallocHost((void**)&c->h_stats, sizeof(FwdStats)) != cudaSuccess)
+    return bail(fail(VCT_E_NOMEM, "cudaMallocHost"));
+  FwdStats init{};
+  init.max_bits = 0u;           // 0.0f
+  init.min_bits = 0x7f7fffffu;  // FLT_MAX
+  init.segments = 0ull;
+  cudaError_t e;
+  if ((e = cudaMemcpy(c->stats.p + 1, &init, sizeof(FwdStats), cudaMemcpyHostToDevice)))
+    return bail(cuda_fail(e, "vct_create: stats init"));
+  if ((e = cudaMemcpy(c->cos_t.p, ct.data(), V * sizeof(double), cudaMemcpyHostToDevice)) ||
+      (e = cudaMemcpy(c->sin_t.p, st.data(), V * sizeof(double), cudaMemcpyHostToDevice)) ||
+      (e = cudaMemcpy(c->cs_f.p, csf.data(), 2 * V * sizeof(float), cudaMemcpyHostToDevice)) ||
+      (e = cudaMemcpy(c->det_px0.p, px0.data(), C * sizeof(double), cudaMemcpyHostToDevice)) ||
+      (e = cudaMemcpy(c->det_py0.p, py0.data(), C * sizeof(double), cudaMemcpyHostToDevice)) ||
+      (e = cudaMemcpy(c->fbp_coeff.p, coeff.data(), C * sizeof(double), cudaMemcpyHostToDevice)))
+    return bail(cuda_fail(e, "vct_create: table upload"));
+  *out = c;
+  return VCT_OK;
+}
+
+void vct_destroy(vct_ctx* c) {
+  if (!c) return;
+  cudaSetDevice(c->device);
+  if (c->own_stream) cudaStreamSynchronize(c->own_stream);
+  c->cos_t.release(); c->sin_t.release(); c->cs_f.release(); c->det_px0.release(); c->det_py0.release();
+  c->maps_raw.release(); c->maps.release(); c->mu_scaled.release(); c->pdf.release();
+  c->full.release(); c->out.release(); c->stats.release();
+  c->fbp_coeff.release();
+  for (auto& h : c->fbp_h) h.release();
+  c->fbp_g.release(); c->fbp_q.release(); c->fbp_sino.release(); c->fbp_img.release();
+  if (c->h_stats) cudaFreeHost(c->h_stats);
+  if (c->own_stream) cudaStreamDestroy(c->own_stream);
+  delete c;
+}
+
+int vct_set_stream(vct_ctx* c, void* stream) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  c->stream = stream ? (cudaStream_t)stream : c->own_stream;
+  return VCT_OK;
+}
+
+int vct_synchronize(vct_ctx* c) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  VCT_CUDA(cudaStreamSynchronize(c->stream));
+  return VCT_OK;
+}
+
+long long vct_kernel_launches(vct_ctx* c) { return c ? c->launches : -1; }
+
+static int fetch_stats(vct_ctx* c);
+
+int vct_last_segment_count(vct_ctx* c, long long* segments) {
+  if (!c || !segments) return fail(VCT_E_ARG, "null argument");
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if ((rc = fetch_stats(c))) return rc;  // waits for the context's stream
+  *segments = c->last_segments;
+  return VCT_OK;
+}
+
+// ------------------------------------------------------------------ spectrum
+// Restates attenuation_coefficient, MB/prior_weight_production.cpp:180-297.
+int vct_attenuation_coefficient(const char* path, int nthin, const int* Zs, int M, float* mu, float* pdf,
+                                int* NE) {
+  if (!path || !Zs || !mu || !pdf || !NE || M < 1 || M > VCT_MAX_MATERIALS || nthin < 1)
+    return fail(VCT_E_ARG, "vct_attenuation_coefficient: bad argument");
+  *NE = 0;
+  FILE* fp = fopen(path, "r");
+  if (!fp) return fail(VCT_E_IO, std::string("ERROR: no photon energy file ") + path);
+  char row[1024];
+  float d0 = 0, d1 = 0, d2 = 0;
+  std::vector<double> pe;
+  std::vector<float> raw;
+  if (fgets(row, sizeof(row), fp) == NULL) { /* header line, :196 */ }
+  while (fgets(row, sizeof(row), fp) != NULL) {
+    if ((int)pe.size() >= VCT_MAX_BINS) {
+      fclose(fp);
+      return fail(VCT_E_UNSUPPORTED, "spectrum has more than 1024 bins");
+    }
+    sscanf(row, "%f %f %f", &d0, &d1, &d2);  // unparsable lines keep the last values (:202)
+    pe.push_back((d1 + d0) * 0.5);
+    raw.push_back(d2);
+  }
+  fclose(fp);
+  const int n = (int)pe.size();
+  if (n == 0) return fail(VCT_E_IO, "spectrum file has no bins");
+  // Thinning by nthin (:210-235).
+  std::vector<float> pdf_thin;
+  std::vector<double> e_thin;
+  double psum = 0.0, esum = 0.0, sum_thin = 0.0;
+  for (int i = 0; i < n; i++) {
+    psum += raw[i];
+    esum += pe[i];
+    if (i - nthin + 1 == (i - nthin + 1) / nthin * nthin) {
+      pdf_thin.push_back((float)psum);
+      e_thin.push_back((double)(float)(esum / nthin));
+      sum_thin += psum;
+      psum = 0.0;
+      esum = 0.0;
+    }
+  }
+  const int ne = (int)pdf_thin.size();
+  const float sum = (float)sum_thin;  // float normalisation (:236-244)
+  for (int i = 0; i < ne; i++) pdf[i] = pdf_thin[i] / sum;
+  // Element table: (Z, A) of :250-255 plus Mg and Si with A = 2Z.
+  const double Avogadro = 6.0221;  // MB/physParamsTOMO.h:89
+  for (int iz = 0; iz < M; iz++) {
+    double Z = Zs[iz], A;
+    switch (Zs[iz]) {
+      case 1: A = 1; break;
+      case 6: A = 12; break;
+      case 7: A = 14; break;
+      case 8: A = 16; break;
+      case 15: A = 31; break;
+      case 20: A = 40; break;
+      case 12: A = 24; break;
+      case 14: A = 28; break;
+      default: return fail(VCT_E_ARG, "element Z not in the reference's table");
+    }
+    double Ek = 0;
+    double fact = Avogadro * Z / A * (2.81794 * 2.81794) * 0.001;
+    for (int i = 0; i < ne; i++) {
+      double E = e_thin[i] / 0.511;
+      double photo = fact * 0.00000345 * (1.0 + 0.008 * Z) * (Z * Z * Z) / (E * E * E) *
+                     (1.0 - Ek / (4.0 * E) - Ek * Ek / (1.21 * E));
+      double compton = fact * 2 * kPI *
+                       ((1.0 + E) / (E * E) * (2.0 * (1.0 + E) / (1.0 + 2 * E) - log(1.0 + 2 * E) / E) +
+                        log(1.0 + 2 * E) / (2 * E) - (1.0 + 3 * E) / ((1.0 + 2 * E) * (1.0 + 2 * E)));
+      double pair = fact * 0.2545 * (E - 2.332) * Z / 137;
+      if (pair < 0) pair = 0;
+      mu[ne * iz + i] = (float)(photo + compton + pair);
+    }
+  }
+  *NE = ne;
+  return VCT_OK;
+}
+
+// ------------------------------------------------------------------- MBFPA
+int vct_set_maps_dev(vct_ctx* c, const int16_t* d_maps, int M) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!d_maps || M < 1 || M > VCT_MAX_MATERIALS) return fail(VCT_E_ARG, "vct_set_maps: bad argument");
+  if (c->spectrum_ready && M != c->M) return fail(VCT_E_ARG, "vct_set_maps: M differs from the spectrum's");
+  const size_t n2 = (size_t)c->dg.N * c->dg.N;
+  if ((rc = c->maps.ensure(n2))) return rc;
+  if ((rc = launch_pack_maps(d_maps, M, c->dg.N, c->maps.p, c->stream))) return rc;
+  c->launches++;
+  c->M = M;
+  c->maps_ready = 1;
+  return VCT_OK;
+}
+
+int vct_set_maps(vct_ctx* c, const int16_t* maps, int M) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!maps || M < 1 || M > VCT_MAX_MATERIALS) return fail(VCT_E_ARG, "vct_set_maps: bad argument");
+  const size_t n2 = (size_t)c->dg.N * c->dg.N;
+  if ((rc = c->maps_raw.ensure(n2 * M))) return rc;
+  VCT_CUDA(cudaMemcpyAsync(c->maps_raw.p, maps, n2 * M * sizeof(int16_t), cudaMemcpyHostToDevice, c->stream));
+  return vct_set_maps_dev(c, c->maps_raw.p, M);
+}
+
+int vct_set_spectrum(vct_ctx* c, const float* mu, const float* pdf, int M, int NE) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!mu || !pdf || M < 1 || M > VCT_MAX_MATERIALS || NE < 1 || NE > VCT_MAX_BINS)
+    return fail(VCT_E_ARG, "vct_set_spectrum: bad argument");
+  if (c->maps_ready && M != c->M) return fail(VCT_E_ARG, "vct_set_spectrum: M differs from the maps'");
+  // Transpose to [NE][M] and fold 1/xfactor (exp(-transp/xfactor), :196).
+  std::vector<double> t((size_t)NE * M);
+  for (int e = 0; e < NE; e++)
+    for (int m = 0; m < M; m++) t[(size_t)e * M + m] = (double)mu[(size_t)m * NE + e] / (double)c->geo.xfactor;
+  if ((rc = c->mu_scaled.ensure((size_t)NE * M)) || (rc = c->pdf.ensure(NE))) return rc;
+  VCT_CUDA(cudaMemcpyAsync(c->mu_scaled.p, t.data(), t.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  VCT_CUDA(cudaMemcpyAsync(c->pdf.p, pdf, NE * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  VCT_CUDA(cudaStreamSynchronize(c->stream));  // t is a host temporary
+  c->M = M;
+  c->NE = NE;
+  c->spectrum_ready = 1;
+  return VCT_OK;
+}
+
+int vct_set_sum_mode(vct_ctx* c, int mode) {
+  if (!c) return fail(VCT_E_ARG, "null context");
+  if (mode != VCT_SUM_COMPENSATED && mode != VCT_SUM_REFERENCE) return fail(VCT_E_ARG, "bad sum mode");
+  c->sum_mode = mode;
+  return VCT_OK;
+}
+
+static int forward_into(vct_ctx* c, float* d_out, double* d_lint) {
+  if (!c->maps_ready || !c->spectrum_ready) return fail(VCT_E_STATE, "forward: maps or spectrum not set");
+  const size_t nsino = (size_t)c->geo.views * c->geo.width;
+  VCT_CUDA(cudaMemcpyAsync(c->stats.p, c->stats.p + 1, sizeof(FwdStats), cudaMemcpyDeviceToDevice, c->stream));
+  if (d_out) VCT_CUDA(cudaMemsetAsync(d_out, 0, nsino * sizeof(float), c->stream));
+  int rc = launch_forward(c->dg, c->maps.p, c->M, c->mu_scaled.p, c->pdf.p, c->NE, c->cos_t.p, c->sin_t.p,
+                          c->det_px0.p, c->det_py0.p, c->sum_mode, d_out, d_lint, c->stats.p, c->stream);
+  if (rc) return rc;
+  c->launches++;
+  return VCT_OK;
+}
+
+static int fetch_stats(vct_ctx* c) {
+  VCT_CUDA(cudaMemcpyAsync(c->h_stats, c->stats.p, sizeof(FwdStats), cudaMemcpyDeviceToHost, c->stream));
+  VCT_CUDA(cudaStreamSynchronize(c->stream));
+  c->last_segments = (long long)c->h_stats->segments;
+  return VCT_OK;
+}
+
+int vct_forward_dev(vct_ctx* c, float* d_out) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!d_out) return fail(VCT_E_ARG, "null output");
+  return forward_into(c, d_out, nullptr);
+}
+
+int vct_forward(vct_ctx* c, float* out) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!out) return fail(VCT_E_ARG, "null output");
+  const size_t nsino = (size_t)c->geo.views * c->geo.width;
+  if ((rc = c->full.ensure(nsino))) return rc;
+  if ((rc = forward_into(c, c->full.p, nullptr))) return rc;
+  VCT_CUDA(cudaMemcpyAsync(out, c->full.p, nsino * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  return fetch_stats(c);
+}
+
+int vct_line_integrals_dev(vct_ctx* c, double* d_lint) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!d_lint) return fail(VCT_E_ARG, "null output");
+  return forward_into(c, nullptr, d_lint);
+}
+
+static int pad_zero_of(const vct_ctx* c) {
+  // The reference's min runs over the whole [views][width] array: rows past
+  // views/2*2 and channels outside [start,end) hold 0.
+  return (c->dg.views_used < c->dg.views || c->dg.C < c->dg.width) ? 1 : 0;
+}
+
+int vct_normalize_noise_dev(vct_ctx* c, float* d_sino, double sigma, uint64_t seed) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!d_sino) return fail(VCT_E_ARG, "null sinogram");
+  rc = launch_normalize_noise(c->dg, d_sino, d_sino, c->stats.p, pad_zero_of(c), sigma, seed, c->stream);
+  if (!rc) c->launches++;
+  return rc;
+}
+
+int vct_mbfpa_dev(vct_ctx* c, double sigma, uint64_t seed, float* d_out) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!d_out) return fail(VCT_E_ARG, "null output");
+  const size_t nsino = (size_t)c->geo.views * c->geo.width;
+  if ((rc = c->full.ensure(nsino))) return rc;
+  if ((rc = forward_into(c, c->full.p, nullptr))) return rc;
+  rc = launch_normalize_noise(c->dg, c->full.p, d_out, c->stats.p, pad_zero_of(c), sigma, seed, c->stream);
+  if (!rc) c->launches++;
+  return rc;
+}
+
+int vct_mbfpa(vct_ctx* c, double sigma, uint64_t seed, float* out, float* stats3) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!out) return fail(VCT_E_ARG, "null output");
+  const size_t nsino = (size_t)c->geo.views * c->geo.width;
+  if ((rc = c->out.ensure(nsino))) return rc;
+  if ((rc = vct_mbfpa_dev(c, sigma, seed, c->out.p))) return rc;
+  VCT_CUDA(cudaMemcpyAsync(out, c->out.p, nsino * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  if ((rc = fetch_stats(c))) return rc;
+  if (stats3) {
+    float mx = 0, mn = 0;
+    memcpy(&mx, &c->h_stats->max_bits, 4);
+    memcpy(&mn, &c->h_stats->min_bits, 4);
+    if (pad_zero_of(c)) mn = fminf(mn, 0.0f);
+    stats3[0] = mx;
+    stats3[1] = mn / mx;
+    stats3[2] = (float)c->h_stats->segments;
+  }
+  return VCT_OK;
+}
+
+// --------------------------------------------------------------------- FBP
+// prepareConstMap, FBP/filterSinogramTOMO.cpp:9-123, in double on the host,
+// stored as float for the device filter.
+static int build_filter(vct_ctx* c, int filter) {
+  if (c->fbp_h[filter].p) return VCT_OK;
+  const int C = c->dg.C;
+  const int half = (C - 1) / 2;
+  const double arc = c->geo.max_beta / half;
+  std::vector<double> h((size_t)C * C), sum(C, 0.0);
+  for (int m = 0; m < C; m++) {
+    for (int n = 0; n < C; n++) {
+      int MN = m - n;
+      double v = 0.0;
+      if (m == n) {
+        if (filter == 1) v = 0.125 / (arc * arc);
+        else {
+          double oddterm = kPI * kPI * (arc);
+          v = 0.25 / oddterm * (1.0 / tan((0.5) * arc) - 1.0 / tan((-0.5) * arc));
+        }
+      } else if (MN % 2 != 0) {
+        if (filter == 1) {
+          double oddterm = kPI * sin(MN * arc);
+          v = -0.5 / oddterm / oddterm;
+        } else {
+          double oddterm = kPI * kPI * arc;
+          v = 0.25 / oddterm * (1.0 / tan((MN + 0.5) * arc) - 1.0 / tan((MN - 0.5) * arc));
+        }
+      } else {
+        if (filter == 1) v = 0.0;
+        else {
+          double oddterm = kPI * kPI * arc;
+          v = 0.25 / oddterm * (1.0 / tan((MN + 0.5) * arc) - 1.0 / tan((MN - 0.5) * arc));
+        }
+      }
+      h[(size_t)m * C + n] = v;
+      sum[m] += v;
+    }
+  }
+  std::vector<float> hf((size_t)C * C);
+  const int r21 = C > 21 ? 21 : C - 1;
+  for (int m = 0; m < C; m++)
+    for (int n = 0; n < C; n++) {
+      double v = h[(size_t)m * C + n];
+      if ((0 <= m && m <= 20) || (C - 20 <= m && m <= C)) v = v * sum[r21] / sum[m];
+      hf[(size_t)m * C + n] = (float)v;
+    }
+  int rc = c->fbp_h[filter].ensure((size_t)C * C);
+  if (rc) return rc;
+  VCT_CUDA(cudaMemcpy(c->fbp_h[filter].p, hf.data(), hf.size() * sizeof(float), cudaMemcpyHostToDevice));
+  return VCT_OK;
+}
+
+int vct_fbp_dev(vct_ctx* c, const float* d_sino, int filter, int in_mode, float* d_img) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!d_sino || !d_img) return fail(VCT_E_ARG, "null buffer");
+  if (filter != 1 && filter != 2) return fail(VCT_E_ARG, "filter must be 1 (Ram-Lak) or 2 (Shepp-Logan)");
+  const int V = c->geo.views, C = c->dg.C;
+  if ((rc = build_filter(c, filter))) return rc;
+  if ((rc = c->fbp_g.ensure((size_t)V * C)) || (rc = c->fbp_q.ensure((size_t)V * C))) return rc;
+  if ((rc = launch_fbp_weight(d_sino, V, c->geo.width, c->geo.start_channel, C, c->fbp_coeff.p, c->fbp_g.p,
+                              c->stream)))
+    return rc;
+  if ((rc = launch_fbp_filter(c->fbp_g.p, c->fbp_h[filter].p, V, C, in_mode, c->fbp_q.p, c->stream)))
+    return rc;
+  if ((rc = launch_fbp_backproject(c->fbp_q.p, V, C, c->dg.N, c->geo.pixel_cm, c->geo.sid_cm, c->geo.max_beta,
+                                   c->geo.xfactor, c->cs_f.p, d_img, c->stream)))
+    return rc;
+  c->launches += 3;
+  return VCT_OK;
+}
+
+int vct_fbp(vct_ctx* c, const float* sino, int filter, int in_mode, float* img) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!sino || !img) return fail(VCT_E_ARG, "null buffer");
+  const size_t nsino = (size_t)c->geo.views * c->geo.width;
+  const size_t nimg = (size_t)c->dg.N * c->dg.N;
+  if ((rc = c->fbp_sino.ensure(nsino)) || (rc = c->fbp_img.ensure(nimg))) return rc;
+  VCT_CUDA(cudaMemcpyAsync(c->fbp_sino.p, sino, nsino * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  if ((rc = vct_fbp_dev(c, c->fbp_sino.p, filter, in_mode, c->fbp_img.p))) return rc;
+  VCT_CUDA(cudaMemcpyAsync(img, c->fbp_img.p, nimg * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  VCT_CUDA(cudaStreamSynchronize(c->stream));
+  return VCT_OK;
+}
+
+int vct_fbp_filtered_dev(vct_ctx* c, const float** d_fltd) {
+  if (!c || !d_fltd) return fail(VCT_E_ARG, "null argument");
+  if (!c->fbp_q.p) return fail(VCT_E_STATE, "no FBP has run on this context");
+  *d_fltd = c->fbp_q.p;
+  return VCT_OK;
+}
+
+// Philox4x32-10 on the host, for known-answer checks of the noise generator.
+void vct_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+  Philox4 c;
+  for (int i = 0; i < 4; i++) c.v[i] = ctr[i];
+  Philox4 r = philox4x32_10(c, key[0], key[1]);
+  for (int i = 0; i < 4; i++) out[i] = r.v[i];
+}
+
+}  // extern "C"

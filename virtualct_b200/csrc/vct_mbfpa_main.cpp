@@ -1,0 +1,133 @@
+// vct_mbfpa -- drop-in for Release_MBFPA_CPU_human/mvct.exe.
+//
+//   vct_mbfpa <input.txt> [--weights FILE] [--elements H,C,N,O,P,Ca[,Mg,Si]]
+//             [--seed N] [--device N] [--sum compensated|reference]
+//
+// Reads the reference's 31-field input txt, the int16 element maps (the
+// reference hard-codes Weight_input_ICRU110.raw and six elements,
+// MB/main.cpp:240,422) and the spectrum txt; writes reprojection_float.raw
+// (float32 [views][width]) and npf_float.raw (the reference's lengthproj_TOMO
+// output for its all-zero measured sinogram: zeros, MB/main.cpp:407-419).
+// The energy loop, spectral sum, normalisation and noise of
+// MB/main.cpp:492-530 are one call to vct_mbfpa() on the GPU.
+#include <stdio.h>
+#include <stdlib.h>
+#include <string.h>
+#include <sys/stat.h>
+#include <sys/types.h>
+
+#include <string>
+#include <vector>
+
+#include "vct.h"
+#include "vct_io.h"
+
+static int element_z(const std::string& s) {
+  if (s == "H") return 1;
+  if (s == "C") return 6;
+  if (s == "N") return 7;
+  if (s == "O") return 8;
+  if (s == "P") return 15;
+  if (s == "Ca") return 20;
+  if (s == "Mg") return 12;
+  if (s == "Si") return 14;
+  return -1;
+}
+
+int main(int argc, char* argv[]) {
+  if (argc < 2) {
+    fprintf(stderr, "\n[usage]$ mvct <info filename>\n\n");
+    return 0;
+  }
+  std::string weights = "Weight_input_ICRU110.raw";
+  std::vector<int> Z = {1, 6, 7, 8, 15, 20};
+  unsigned long long seed = 1;
+  int device = 0;
+  int sum_mode = VCT_SUM_COMPENSATED;
+  for (int i = 2; i < argc; i++) {
+    std::string a = argv[i];
+    if (a == "--weights" && i + 1 < argc) weights = argv[++i];
+    else if (a == "--seed" && i + 1 < argc) seed = strtoull(argv[++i], nullptr, 10);
+    else if (a == "--device" && i + 1 < argc) device = atoi(argv[++i]);
+    else if (a == "--sum" && i + 1 < argc) {
+      std::string m = argv[++i];
+      sum_mode = m == "reference" ? VCT_SUM_REFERENCE : VCT_SUM_COMPENSATED;
+    } else if (a == "--elements" && i + 1 < argc) {
+      Z.clear();
+      std::string list = argv[++i];
+      size_t p = 0;
+      while (p <= list.size()) {
+        size_t q = list.find(',', p);
+        if (q == std::string::npos) q = list.size();
+        int z = element_z(list.substr(p, q - p));
+        if (z < 0) {
+          fprintf(stderr, "unknown element %s\n", list.substr(p, q - p).c_str());
+          return 1;
+        }
+        Z.push_back(z);
+        p = q + 1;
+      }
+    } else {
+      fprintf(stderr, "unknown option %s\n", a.c_str());
+      return 1;
+    }
+  }
+  const int M = (int)Z.size();
+
+  vct_mb_config cfg;
+  if (vct_load_mb_config(argv[1], &cfg) != VCT_OK) {
+    fprintf(stderr, "%s\n", vct_last_error());
+    return 0;  // the reference exits 0 here (MB/main.cpp:225-228)
+  }
+  FILE* fp = fopen(cfg.recon_data_file, "rb");
+  if (!fp) fprintf(stderr, "No prior image \n");
+  else {
+    fprintf(stderr, "Prior image: %s \n", cfg.recon_data_file);
+    fclose(fp);
+  }
+  vct_geometry g;
+  vct_mb_geometry(&cfg, &g);
+  fprintf(stderr, "usedProj: %d SngrmH: %d SngrmW: %d\n", cfg.total_proj_number, g.views, g.width);
+  struct stat st;
+  if (stat("ReconImageRaw", &st) != 0) mkdir("ReconImageRaw", 0775);
+
+  std::vector<float> mu((size_t)M * VCT_MAX_BINS), pdf(VCT_MAX_BINS);
+  int NE = 0;
+  if (vct_attenuation_coefficient(cfg.spectrum_file, 1, Z.data(), M, mu.data(), pdf.data(), &NE) != VCT_OK) {
+    fprintf(stderr, "%s\n", vct_last_error());
+    return 1;
+  }
+  printf("%d energy bins, %d elements\n", NE, M);
+
+  const size_t n2 = (size_t)g.recon_size * g.recon_size;
+  std::vector<float> npf(n2, 0.0f);
+  vct_write_raw("npf_float.raw", npf.data(), n2 * sizeof(float));
+
+  std::vector<int16_t> maps((size_t)M * n2);
+  if (vct_read_raw(weights.c_str(), 0, maps.data(), maps.size() * sizeof(int16_t), nullptr) != VCT_OK) {
+    fprintf(stderr, "%s\n", vct_last_error());
+    return 1;
+  }
+  vct_ctx* ctx = nullptr;
+  int rc = vct_create(&g, device, &ctx);
+  if (rc == VCT_OK) rc = vct_set_sum_mode(ctx, sum_mode);
+  if (rc == VCT_OK) rc = vct_set_maps(ctx, maps.data(), M);
+  if (rc == VCT_OK) rc = vct_set_spectrum(ctx, mu.data(), pdf.data(), M, NE);
+  std::vector<float> sino((size_t)g.views * g.width);
+  float stats[3] = {0, 0, 0};
+  if (rc == VCT_OK) rc = vct_mbfpa(ctx, cfg.photon_noise, seed, sino.data(), stats);
+  if (rc != VCT_OK) {
+    fprintf(stderr, "vct_mbfpa failed: %s (%s)\n", vct_strerror(rc), vct_last_error());
+    vct_destroy(ctx);
+    return 1;
+  }
+  printf("projection_min = %lf, used noise = %lf\n", (double)stats[1], cfg.photon_noise);
+  rc = vct_write_raw("reprojection_float.raw", sino.data(), sino.size() * sizeof(float));
+  vct_destroy(ctx);
+  if (rc != VCT_OK) {
+    fprintf(stderr, "%s\n", vct_last_error());
+    return 1;
+  }
+  fprintf(stderr, "done.\n");
+  return 0;
+}

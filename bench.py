@@ -158,7 +158,7 @@ def run_ours(args, rank, world, dist):
     launches_mb = ctx.kernel_launches - launches0
     barrier()
     t_mb = max_over_ranks(t_mb)
-    segments = ctx.last_segment_count  # of the last step (same every step)
+    segments_visited = ctx.last_segment_count  # fast walk: includes zero-weight pieces
 
     barrier()
     t_fbp = max_over_ranks(timed(fbp_step, args.steps))
@@ -168,6 +168,12 @@ def run_ours(args, rank, world, dist):
     barrier()
     t_fwd = max_over_ranks(timed(lambda: ctx.forward_dev(d_sino), args.steps)) / args.steps
     clk.__exit__(None, None, None)
+    # Algorithmic work unit: the reference walk's in-grid segments, counted by
+    # one forward in exact-walk mode (outside every timed region).
+    ctx.set_walk_mode(vct.WALK_EXACT)
+    ctx.forward_dev(d_sino)
+    segments = ctx.last_segment_count
+    ctx.set_walk_mode(vct.WALK_FAST)
 
     # End to end through the public API with host buffers: per step the maps
     # go host->device from pinned memory and the noisy sinogram comes back.
@@ -241,6 +247,7 @@ def run_ours(args, rank, world, dist):
             "peak_source": "measured live: vct_probe_peaks L2 read (ld.global.cg, 16 MB resident)",
             "algorithmic_bytes_per_launch": int(alg_bytes),
             "segments_per_launch": int(segments),
+            "segments_visited_per_launch": int(segments_visited),
             "launch_ms": t_fwd * 1e3,
             "hbm_peak_gbs": measured.get("hbm_gbs"),
             "fp64": {"achieved_tflops": fp64_flops / t_fwd / 1e12, "peak_tflops": peaks["fp64_tflops"],

@@ -108,12 +108,28 @@ int vct_set_spectrum(vct_ctx* ctx, const float* mu, const float* pdf, int M, int
                                  bin order, as MB/main.cpp:504 */
 int vct_set_sum_mode(vct_ctx* ctx, int mode);
 
+/* Ray-walk mode.  Both walk the reference's segments (MB/reprojection_TOMO.cpp
+ * :113-283) with the same set-up, loop test and crossing rule.
+ * VCT_WALK_EXACT evaluates every segment with the reference's own double
+ * expressions (divisions and square roots included), so segment boundaries
+ * match it bit for bit.  VCT_WALK_FAST (default) advances the minor
+ * coordinate incrementally, tracks the next gridline, uses one precomputed
+ * step length and splits crossing steps in 30-bit fixed point; rays whose
+ * first major gridline is not a pixel boundary (pixel sizes that do not
+ * divide 1 cm) and geometries where the rmax test can fire take the exact
+ * walk.  Densities enter as s/1000 exactly in both modes. */
+#define VCT_WALK_FAST 0
+#define VCT_WALK_EXACT 1
+int vct_set_walk_mode(vct_ctx* ctx, int mode);
+
 /* Polyenergetic forward projection, un-normalised:
  *   sino[v][c] = sum_E pdf[E] * exp(-sum_m mu_m(E) * L_m(v,c) / xfactor)
  * with L_m the line integrals of the reference's ray walk
  * (MB/reprojection_TOMO.cpp:13-289, one walk per ray for all bins).
  * Rows v >= views/2*2 and channels outside [start_channel, end_channel) are 0,
- * as the reference leaves them. */
+ * as the reference leaves them.  With VCT_SUM_COMPENSATED each bin's
+ * exponential is 2^-y, y = transp*log2(e) in FP64 split into integer and
+ * fraction (the fraction through the SFU), and bins are summed in FP64. */
 int vct_forward(vct_ctx* ctx, float* sino_out);
 int vct_forward_dev(vct_ctx* ctx, float* d_sino_out);
 

@@ -88,6 +88,9 @@ def lib():
                                         C.c_void_p, C.c_int]
         L.orc_forward_fp64.argtypes = [C.POINTER(OrcGeom), _dp, _dp, _fp, C.c_int, _fp, _fp, C.c_int, _dp,
                                        C.c_void_p, C.c_int]
+        L.orc_forward_fp64_maps.argtypes = [C.POINTER(OrcGeom), _dp, _dp,
+                                            np.ctypeslib.ndpointer(dtype=np.int16, flags="C_CONTIGUOUS"), C.c_int,
+                                            _fp, _fp, C.c_int, _dp, C.c_void_p, C.c_int]
         L.orc_normalize_noise.argtypes = [_fp, C.c_int, C.c_double, C.c_uint, C.c_int]
         L.orc_normalize_noise.restype = C.c_double
         L.orc_fbp_constmap.argtypes = [C.POINTER(OrcGeom), C.c_int, _dp]
@@ -167,6 +170,19 @@ def forward_fp64(g, cos_t, sin_t, rho, mu, pdf, nthreads=0, want_lint=False):
     lib().orc_forward_fp64(C.byref(g), cos_t, sin_t, np.ascontiguousarray(rho, np.float32), M,
                            np.ascontiguousarray(mu, np.float32), np.ascontiguousarray(pdf, np.float32), NE,
                            out, lint.ctypes.data if want_lint else None, nthreads)
+    return (out, lint) if want_lint else out
+
+
+def forward_fp64_maps(g, cos_t, sin_t, maps, mu, pdf, nthreads=0, want_lint=False):
+    """FP64 forward with exact s/1000 densities (the device path's density semantics)."""
+    maps = np.ascontiguousarray(maps, np.int16)
+    M = maps.shape[0]
+    NE = len(pdf)
+    out = np.zeros((g.views, g.width), np.float64)
+    lint = np.zeros((g.views, g.width, M), np.float64) if want_lint else None
+    lib().orc_forward_fp64_maps(C.byref(g), cos_t, sin_t, maps, M, np.ascontiguousarray(mu, np.float32),
+                                np.ascontiguousarray(pdf, np.float32), NE, out,
+                                lint.ctypes.data if want_lint else None, nthreads)
     return (out, lint) if want_lint else out
 
 

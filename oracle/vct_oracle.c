@@ -386,6 +386,59 @@ void orc_forward_fp64(const orc_geom* g, const double* cos_t, const double* sin_
   }
 }
 
+void orc_forward_fp64_maps(const orc_geom* g, const double* cos_t, const double* sin_t,
+                           const short* maps, int M, const float* mu, const float* pdf, int NE,
+                           double* full_out, double* lint_out, int nthreads) {
+  const int V = g->views, W = g->width, N = g->recon_size;
+  const int nviews = V / 2 * 2;
+  const size_t n2 = (size_t)N * N;
+  const double rmax = N * 0.5 * 1.0;
+  const int cap = orc_seg_cap(g);
+  memset(full_out, 0, sizeof(double) * (size_t)V * W);
+  if (lint_out) memset(lint_out, 0, sizeof(double) * (size_t)V * W * M);
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel
+#endif
+  {
+    double* len = (double*)malloc(sizeof(double) * cap);
+    double* rad = (double*)malloc(sizeof(double) * cap);
+    int* pix = (int*)malloc(sizeof(int) * cap);
+    double L[16];
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 4)
+#endif
+    for (int j = 0; j < nviews; j++) {
+      for (int jj = g->start_channel; jj < g->end_channel; jj++) {
+        int ns = orc_walk(g, cos_t[j], sin_t[j], jj, len, pix, rad, cap);
+        if (ns < 0) ns = 0;
+        for (int mat = 0; mat < M; mat++) L[mat] = 0.0;
+        for (int q = 0; q < ns; q++) {
+          if (rad[q] >= rmax) continue;
+          for (int mat = 0; mat < M; mat++) {
+            short v = maps[(size_t)mat * n2 + pix[q]];
+            if (v > 0) L[mat] += (double)v * len[q];
+          }
+        }
+        for (int mat = 0; mat < M; mat++) L[mat] /= 1000.0;
+        size_t o = (size_t)j * W + jj;
+        if (lint_out)
+          for (int mat = 0; mat < M; mat++) lint_out[o * M + mat] = L[mat];
+        double acc = 0.0;
+        for (int ke = 0; ke < NE; ke++) {
+          double t = 0.0;
+          for (int mat = 0; mat < M; mat++) t += (double)mu[mat * NE + ke] * L[mat];
+          acc += (double)pdf[ke] * exp(-t / (double)g->xfactor);
+        }
+        full_out[o] = acc;
+      }
+    }
+    free(len);
+    free(rad);
+    free(pix);
+  }
+}
+
 /* MB/main.cpp:42-49 */
 static double orc_uniform0(void) { return ((double)rand() + 1.0) / ((double)RAND_MAX + 2.0); }
 

@@ -78,6 +78,14 @@ void orc_forward_fp64(const orc_geom* g, const double* cos_t, const double* sin_
                       int M, const float* mu, const float* pdf, int NE, double* full_out,
                       double* lint_out, int nthreads);
 
+/* As orc_forward_fp64, but densities are the stored integers divided by 1000
+ * exactly (s/1000 in double) instead of the reference's float rounding of
+ * (float)s/1000; the FP64 reference for a device path that carries s/1000
+ * exactly.  maps: int16 [M][N][N]; negative entries contribute nothing. */
+void orc_forward_fp64_maps(const orc_geom* g, const double* cos_t, const double* sin_t,
+                           const short* maps, int M, const float* mu, const float* pdf, int NE,
+                           double* full_out, double* lint_out, int nthreads);
+
 /* Max-normalisation (MB/main.cpp:511-522) followed by gaussiannoise0
  * (MB/main.cpp:42-76) with glibc rand() after srand(seed) (the reference
  * never seeds: seed 1).  order selects which Uniform0() call in rand_gauss0

@@ -34,6 +34,8 @@ VCT_E_STATE = -6
 VCT_E_UNSUPPORTED = -7
 SUM_COMPENSATED = 0
 SUM_REFERENCE = 1
+WALK_FAST = 0
+WALK_EXACT = 1
 MAX_BINS = 1024
 
 ELEMENT_Z = {"H": 1, "C": 6, "N": 7, "O": 8, "P": 15, "Ca": 20, "Mg": 12, "Si": 14}
@@ -44,7 +46,7 @@ GAMMEX_ELEMENTS = ("H", "C", "N", "O", "P", "Ca", "Mg", "Si")
 EXPORTED_SYMBOLS = (
     "vct_geometry_default", "vct_strerror", "vct_last_error", "vct_create", "vct_destroy", "vct_set_stream",
     "vct_synchronize", "vct_attenuation_coefficient", "vct_set_maps", "vct_set_maps_dev", "vct_set_spectrum",
-    "vct_set_sum_mode", "vct_forward", "vct_forward_dev", "vct_line_integrals_dev", "vct_mbfpa", "vct_mbfpa_dev",
+    "vct_set_sum_mode", "vct_set_walk_mode", "vct_forward", "vct_forward_dev", "vct_line_integrals_dev", "vct_mbfpa", "vct_mbfpa_dev",
     "vct_normalize_noise_dev", "vct_fbp", "vct_fbp_dev", "vct_fbp_filtered_dev", "vct_last_segment_count",
     "vct_kernel_launches", "vct_version", "vct_philox4x32_10", "vct_probe_peaks",
     "vct_load_mb_config", "vct_load_fbp_config", "vct_mb_geometry", "vct_fbp_geometry", "vct_read_raw",
@@ -129,6 +131,7 @@ def lib():
     L.vct_set_maps_dev.argtypes = [vp, vp, C.c_int]
     L.vct_set_spectrum.argtypes = [vp, vp, vp, C.c_int, C.c_int]
     L.vct_set_sum_mode.argtypes = [vp, C.c_int]
+    L.vct_set_walk_mode.argtypes = [vp, C.c_int]
     L.vct_forward.argtypes = [vp, vp]
     L.vct_forward_dev.argtypes = [vp, vp]
     L.vct_line_integrals_dev.argtypes = [vp, vp]
@@ -259,6 +262,9 @@ class Context:
 
     def set_sum_mode(self, mode: int) -> None:
         _check(lib().vct_set_sum_mode(self._h, mode), "vct_set_sum_mode")
+
+    def set_walk_mode(self, mode: int) -> None:
+        _check(lib().vct_set_walk_mode(self._h, mode), "vct_set_walk_mode")
 
     def _sino(self) -> np.ndarray:
         return np.zeros((self.geometry.views, self.geometry.width), np.float32)

@@ -1,77 +1,163 @@
 // MBFPA forward projection on sm_100a.
 //
-// One thread walks one ray (view v, channel c) through the N x N grid exactly
-// as MB/reprojection_TOMO.cpp:53-283 does -- same double-precision expressions
-// in the same order, compiled with --fmad=false so no product is fused -- and
-// accumulates the per-element line integrals L_m = sum_seg rho_m * len in FP64
-// registers.  The walk is done once per ray for all energy bins (the
-// reference repeats it for every bin, MB/main.cpp:492-506); the polyenergetic
-// epilogue then evaluates sum_E pdf(E) * exp(-sum_m mu_m(E) L_m) with the
-// mu table in shared memory.
+// One thread walks one ray (view v, channel c) through the N x N grid along
+// the reference's path (MB/reprojection_TOMO.cpp:53-283) and accumulates the
+// per-element line integrals L_m = sum_seg (s_m/1000) * len, s_m the stored
+// int16 density x 1000.  The walk is done once per ray for all energy bins
+// (the reference repeats it for every bin, MB/main.cpp:492-506); the
+// polyenergetic epilogue then evaluates sum_E pdf(E) exp(-sum_m mu_m(E) L_m)
+// with the mu table in shared memory.
 //
-// Maps are read as one 16-byte record (8 x int16) per pixel through the
-// read-only path; at 512^2 the record array is 4 MB and stays L2-resident.
+// Two walks:
+//   walk_exact  the reference's expressions, operation for operation
+//               (compiled with --fmad=false, IEEE division and square root),
+//               so segment boundaries match it bit for bit;
+//   walk_fast   the same segments found by a Siddon-style event loop (major
+//               gridline / minor gridline, whichever comes first), one
+//               segment per iteration, weights in 30-bit fixed point and
+//               integer multiply-add accumulation; no per-step division.
+//
+// Maps are one 16-byte record (8 x int16) per pixel in a padded
+// (N+4) x (N+4) layout whose border reproduces the reference's truncating
+// pixel index: row/column -1 repeats row/column 0 (a midpoint in (-1, 0)
+// truncates to 0), the other border cells are zero (rejected).  At 512^2 the
+// record array is 4.3 MB and stays L2-resident.
 #include <cuda_runtime.h>
+#include <string.h>
 
 #include "vct_internal.h"
 #include "vct_philox.h"
 
 namespace vct {
 
+// Padded map: kMapPad cells on every side of the N x N grid.  Row/column -1
+// repeats row/column 0 (the reference's (int) cast truncates a midpoint in
+// (-1, 0) to pixel 0); every other border cell is 0 (rejected).
+constexpr int kPad = kMapPad;
+VCT_HD int pad_index(int col, int row, int N) { return (col + kPad) + (row + kPad) * (N + 2 * kPad); }
+
 // ---------------------------------------------------------------- map packing
-__global__ void pack_maps_kernel(const int16_t* __restrict__ maps, int M, int n2,
+__global__ void pack_maps_kernel(const int16_t* __restrict__ maps, int M, int N,
                                  PixelRec* __restrict__ out) {
-  int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= n2) return;
-  PixelRec r;
+  const int P = N + 2 * kPad;
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P * P) return;
+  const int r = p / P - kPad, c = p % P - kPad;  // padded row/column in [-kPad, N+kPad)
+  PixelRec rec;
+  const bool inside = r >= -1 && c >= -1 && r < N && c < N;
+  const size_t src = (size_t)(r < 0 ? 0 : r) * N + (c < 0 ? 0 : c);
+  const size_t n2 = (size_t)N * N;
 #pragma unroll
   for (int m = 0; m < 8; m++) {
-    int16_t v = m < M ? maps[(size_t)m * n2 + p] : (int16_t)0;
-    r.m[m] = v < 0 ? (int16_t)0 : v;
+    int16_t v = (inside && m < M) ? maps[(size_t)m * n2 + src] : (int16_t)0;
+    rec.m[m] = v < 0 ? (int16_t)0 : v;  // negative densities weigh 0 (:151-155)
   }
-  out[p] = r;
+  out[p] = rec;
 }
 
 int launch_pack_maps(const int16_t* d_maps, int M, int N, PixelRec* d_packed, cudaStream_t st) {
-  int n2 = N * N;
-  pack_maps_kernel<<<(n2 + 255) / 256, 256, 0, st>>>(d_maps, M, n2, d_packed);
-  return cudaGetLastError() == cudaSuccess ? VCT_OK : cuda_fail(cudaGetLastError(), "pack_maps_kernel");
+  const int P = N + 2 * kPad;
+  pack_maps_kernel<<<(P * P + 255) / 256, 256, 0, st>>>(d_maps, M, N, d_packed);
+  VCT_CUDA(cudaGetLastError());
+  return VCT_OK;
 }
 
-// ------------------------------------------------------------------ the walk
+// ------------------------------------------------------------ host/device shims
+// The walks are __host__ __device__ so the same code can run on the CPU
+// (tests/host/walk_check.cu); these wrappers pick the device intrinsic or its
+// host equivalent.
+VCT_HD int4 ldg4(const int4* p) {
+#if defined(__CUDA_ARCH__)
+  return __ldg(p);
+#else
+  return *p;
+#endif
+}
+VCT_HD double fma_rn(double a, double b, double c) {
+#if defined(__CUDA_ARCH__)
+  return __fma_rn(a, b, c);
+#else
+  return fma(a, b, c);
+#endif
+}
+VCT_HD int d2i_rz(double d) {
+#if defined(__CUDA_ARCH__)
+  return __double2int_rz(d);
+#else
+  return (int)d;
+#endif
+}
+// Low 32 bits of a double's bit pattern.
+VCT_HD unsigned int lo32(double d) {
+#if defined(__CUDA_ARCH__)
+  return (unsigned int)__double2loint(d);
+#else
+  unsigned long long b;
+  memcpy(&b, &d, 8);
+  return (unsigned int)b;
+#endif
+}
+
 // (int)d as the reference's x86-64 build evaluates it (cvttsd2si): NaN and
 // out-of-range values give INT_MIN, whereas the PTX conversion saturates and
-// maps NaN to 0.  Only reachable on degenerate rays, but it keeps the
-// rejection of NaN segments identical.
-__device__ __forceinline__ int trunc_i32(double d) {
-  return (d >= -2147483648.0 && d < 2147483648.0) ? __double2int_rz(d) : (int)0x80000000;
+// maps NaN to 0.  Only degenerate rays reach it, but it keeps the rejection of
+// NaN segments identical.
+VCT_HD int trunc_i32(double d) {
+  return (d >= -2147483648.0 && d < 2147483648.0) ? d2i_rz(d) : (int)0x80000000;
 }
 
+VCT_HD unsigned int mat_of(const int4& w, int m) {
+  const unsigned int u = (m >> 1) == 0 ? (unsigned)w.x : (m >> 1) == 1 ? (unsigned)w.y
+                       : (m >> 1) == 2 ? (unsigned)w.z : (unsigned)w.w;
+  return (m & 1) ? (u >> 16) : (u & 0xffffu);
+}
+
+
+
+// ----------------------------------------------------------------- accumulators
+// Ld: sum s*len (cm) of segments emitted one by one (the exact walk, and the
+// fast walk's first segment).  Lq: sum s*w_q of the fast walk's segments, w_q
+// the segment's share of one major step in units of 2^-30; one major step is
+// `sec` cm long.
 struct RayAcc {
-  double L[8];
+  double Ld[8];
+  unsigned long long Lq[8];
+  double sec;
   int nseg;
 };
 
+VCT_HD void acc_init(RayAcc& a) {
+#pragma unroll
+  for (int m = 0; m < 8; m++) {
+    a.Ld[m] = 0.0;
+    a.Lq[m] = 0ull;
+  }
+  a.sec = 0.0;
+  a.nseg = 0;
+}
+
 template <int M>
-__device__ __forceinline__ void gather_add(const PixelRec* __restrict__ maps, int pix, double rr,
-                                           RayAcc& a) {
-  const int4 w = __ldg(reinterpret_cast<const int4*>(maps) + pix);
-  const unsigned int u[4] = {(unsigned)w.x, (unsigned)w.y, (unsigned)w.z, (unsigned)w.w};
+VCT_HD void finish_lines(const RayAcc& a, double L[8]) {
 #pragma unroll
   for (int m = 0; m < M; m++) {
-    unsigned int s = (m & 1) ? (u[m >> 1] >> 16) : (u[m >> 1] & 0xffffu);
-    // rho = (float)short/1000 as MB/main.cpp:103 (IEEE float division).
-    float rho = __fdiv_rn((float)s, 1000.0f);
-    a.L[m] = __fma_rn((double)rho, rr, a.L[m]);
+    const double steps = (double)a.Lq[m] * (1.0 / 1073741824.0);
+    L[m] = (a.Ld[m] + steps * a.sec) / 1000.0;
   }
+}
+
+template <int M>
+VCT_HD void gather_add_exact(const PixelRec* __restrict__ maps, int pix, double rr, RayAcc& a) {
+  const int4 w = ldg4(reinterpret_cast<const int4*>(maps) + pix);
+#pragma unroll
+  for (int m = 0; m < M; m++) a.Ld[m] = fma_rn((double)mat_of(w, m), rr, a.Ld[m]);
   a.nseg++;
 }
 
 // Segment emission of MB/reprojection_TOMO.cpp:145-163 / :171-189: length,
 // midpoint pixel (truncating casts), bounds test, then the gather.
 template <int M>
-__device__ __forceinline__ void emit(const DevGeom& g, const PixelRec* __restrict__ maps, double xb0,
-                                     double yb0, double xb1, double yb1, RayAcc& a) {
+VCT_HD void emit(const DevGeom& g, const PixelRec* __restrict__ maps, double xb0, double yb0,
+                 double xb1, double yb1, RayAcc& a) {
   double rr = sqrt((xb0 - xb1) * (xb0 - xb1) + (yb0 - yb1) * (yb0 - yb1));
   int xmc = trunc_i32((xb0 + xb1) * 0.5 / g.s + g.nxm);
   int ymc = trunc_i32((-yb0 - yb1) * 0.5 / g.s + g.nxm);
@@ -82,45 +168,56 @@ __device__ __forceinline__ void emit(const DevGeom& g, const PixelRec* __restric
       double r = sqrt((xb0 + xb1) * (xb0 + xb1) + (-yb0 - yb1) * (-yb0 - yb1)) * 0.5;
       if (r >= g.rmax) return;
     }
-    gather_add<M>(maps, xmc + ymc * g.N, rr, a);
+    gather_add_exact<M>(maps, pad_index(xmc, ymc, g.N), rr, a);
   }
 }
 
-template <int M>
-__device__ void walk_ray(const DevGeom& g, const PixelRec* __restrict__ maps, double cb, double sb,
-                         double px0, double py0, RayAcc& a) {
-  const double sx = g.sid * sb;  // :53
-  const double sy = g.sid * cb;  // :54
-  const double px = +px0 * cb + py0 * sb;  // :73
-  const double py = -px0 * sb + py0 * cb;  // :74
-  const double lim = g.lim;
-  // Grid-square intersections, :76-101.
+// -------------------------------------------------------------------- set-up
+// Shared by both walks, MB/reprojection_TOMO.cpp:53-108: source, rotated
+// detector point, intersections with the grid square, entry (xi,yi) and exit
+// (xf,yf).  Returns false when the ray misses the square (the reference's walk
+// loop is then never entered).
+struct Ray {
+  double sx, sy, px, py, xi, yi, xf, yf;
+};
+
+VCT_HD bool ray_setup(const DevGeom& g, double cb, double sb, double px0, double py0, Ray& r) {
+  r.sx = g.sid * sb;            // :53
+  r.sy = g.sid * cb;            // :54
+  r.px = +px0 * cb + py0 * sb;  // :73
+  r.py = -px0 * sb + py0 * cb;  // :74
+  const double sx = r.sx, sy = r.sy, px = r.px, py = r.py, lim = g.lim;
   double xx0 = 0, yy0 = 0, xx1 = 0, yy1 = 0;
   int m = 0;
-  {
-    double t;
-    double yv = lim;
-    t = (yv - sy) / (py - sy) * (px - sx) + sx;
-    if (fabs(t) < lim) { if (m == 0) { xx0 = t; yy0 = yv; } else { xx1 = t; yy1 = yv; } m++; }
-    yv = -lim;
-    t = (yv - sy) / (py - sy) * (px - sx) + sx;
-    if (fabs(t) < lim) { if (m == 0) { xx0 = t; yy0 = yv; } else if (m == 1) { xx1 = t; yy1 = yv; } m++; }
-    double xv = lim;
-    t = (xv - sx) / (px - sx) * (py - sy) + sy;
-    if (fabs(t) < lim) { if (m == 0) { xx0 = xv; yy0 = t; } else if (m == 1) { xx1 = xv; yy1 = t; } m++; }
-    xv = -lim;
-    t = (xv - sx) / (px - sx) * (py - sy) + sy;
-    if (fabs(t) < lim) { if (m == 0) { xx0 = xv; yy0 = t; } else if (m == 1) { xx1 = xv; yy1 = t; } m++; }
-  }
-  // A ray missing the square never enters the reference's walk loop.
-  if (m < 2) return;
-  double xi, yi, xf, yf;  // :103-108
+  double t;
+  double yv = lim;
+  t = (yv - sy) / (py - sy) * (px - sx) + sx;
+  if (fabs(t) < lim) { if (m == 0) { xx0 = t; yy0 = yv; } else { xx1 = t; yy1 = yv; } m++; }
+  yv = -lim;
+  t = (yv - sy) / (py - sy) * (px - sx) + sx;
+  if (fabs(t) < lim) { if (m == 0) { xx0 = t; yy0 = yv; } else if (m == 1) { xx1 = t; yy1 = yv; } m++; }
+  double xv = lim;
+  t = (xv - sx) / (px - sx) * (py - sy) + sy;
+  if (fabs(t) < lim) { if (m == 0) { xx0 = xv; yy0 = t; } else if (m == 1) { xx1 = xv; yy1 = t; } m++; }
+  xv = -lim;
+  t = (xv - sx) / (px - sx) * (py - sy) + sy;
+  if (fabs(t) < lim) { if (m == 0) { xx0 = xv; yy0 = t; } else if (m == 1) { xx1 = xv; yy1 = t; } m++; }
+  if (m < 2) return false;
   if ((xx0 - sx) * (xx0 - sx) + (yy0 - sy) * (yy0 - sy) + 0.0 <
       (xx1 - sx) * (xx1 - sx) + (yy1 - sy) * (yy1 - sy) + 0.0) {
-    xi = xx0; yi = yy0; xf = xx1; yf = yy1;
+    r.xi = xx0; r.yi = yy0; r.xf = xx1; r.yf = yy1;
   } else {
-    xi = xx1; yi = yy1; xf = xx0; yf = yy0;
+    r.xi = xx1; r.yi = yy1; r.xf = xx0; r.yf = yy0;
   }
+  return true;
+}
+
+// ---------------------------------------------------------------- exact walk
+// The reference walk, operation for operation (:113-283).
+template <int M>
+VCT_HD void walk_exact(const DevGeom& g, const PixelRec* __restrict__ maps, const Ray& r, RayAcc& a) {
+  const double sx = r.sx, sy = r.sy, px = r.px, py = r.py;
+  const double xi = r.xi, yi = r.yi, xf = r.xf, yf = r.yf, lim = g.lim;
   double xb0 = xi, yb0 = yi;
   const int max_steps = 4 * g.N + 64;  // a walk has at most ~N+2 steps
   if (fabs(xi - xf) > fabs(yi - yf)) {  // x-major, :113-200
@@ -198,7 +295,147 @@ __device__ void walk_ray(const DevGeom& g, const PixelRec* __restrict__ maps, do
   }
 }
 
-// ------------------------------------------------------------- the kernel
+// ------------------------------------------------------------------ fast walk
+// The same segments as walk_exact:
+//   - the first, lumped segment (entry point to the first major gridline,
+//     :118-121 / :206-209) is emitted exactly;
+//   - the reference then walks whole major steps u_k = uin + pha*k*s until a
+//     step ends outside the square (:125 / :212), splitting a step where the
+//     minor coordinate crosses a gridline (:134 / :221).  Here the number of
+//     steps K is found once, with the reference's own expressions, and the
+//     steps are walked as a Siddon event loop in units of major steps t:
+//     major events at integer t, minor events at t_min, t_min + dt, ...;
+//     every iteration closes one segment [t, min(next events)] and adds
+//     s * w_q, w_q = its length in 2^-30 steps.
+// When uin/s is an integer, every major step spans exactly one pixel column
+// and every piece between events lies inside one pixel, so the reference's
+// midpoint rule picks the same pixel as the event bookkeeping.  Rays it does
+// not cover return false and take walk_exact: uin/s not an integer (pixel
+// sizes that do not divide 1 cm), a minor direction with no slope, and rays
+// through the grid origin (the central channel of an even channel count):
+// there the minor coordinate can be exactly 0 at a major step, the
+// reference's sign test divides 0/0 and its crossing rule adds a backward
+// piece, which walk_exact reproduces.
+template <int M>
+VCT_HD bool walk_fast(const DevGeom& g, const PixelRec* __restrict__ maps, const Ray& r, RayAcc& a) {
+  const double orig = r.sx * r.py - r.sy * r.px;
+  if (fabs(orig) < 1e-9 * (fabs(r.px - r.sx) + fabs(r.py - r.sy))) return false;
+  const bool xmaj = fabs(r.xi - r.xf) > fabs(r.yi - r.yf);
+  const double ui = xmaj ? r.xi : r.yi, uf = xmaj ? r.xf : r.yf;
+  const double su = xmaj ? r.sx : r.sy, sw = xmaj ? r.sy : r.sx;
+  const double pu = xmaj ? r.px : r.py, pw = xmaj ? r.py : r.px;
+  const double pha = (uf - ui) / fabs(ui - uf);
+  int uin;
+  if ((ui < 0 && (uf - ui) < 0) || (ui > 0 && (uf - ui) > 0))
+    uin = trunc_i32((double)trunc_i32(ui) + (uf - ui) / fabs(uf - ui));
+  else
+    uin = trunc_i32(ui);
+  const double s = g.s, lim = g.lim;
+  const double Ua_d = (double)uin / s;
+  const double Ua_r = rint(Ua_d);
+  const double Wb = pha * ((pw - sw) / (pu - su));  // minor advance per step, pixels
+  if (fabs(Ua_d - Ua_r) > 1e-6 || !(Wb != 0.0)) return false;
+  const int N = g.N, n = g.nxm;
+  // First point (:120-121 / :208-209) and the loop's entry test (:125).
+  const double u0 = (double)uin;
+  const double w0 = (u0 - su) / (pu - su) * (pw - sw) + sw;
+  if (!(u0 <= lim && u0 >= -lim && w0 <= lim && w0 >= -lim)) return true;
+
+  // K: the first step whose end point is outside the square, evaluated with
+  // the reference's expressions near the estimated exit (the walk processes
+  // steps 1..K).
+  const double W0 = w0 / s;
+  int K = -1;
+  {
+    const double ku = (pha > 0 ? (lim - u0) : (u0 + lim)) / s;  // steps until |u| = lim
+    const double kw = (Wb > 0 ? ((double)n - W0) : (W0 + (double)n)) / fabs(Wb);
+    int k = (int)fmin(fmin(ku, kw), (double)(4 * N + 64)) - 1;
+    if (k < 1) k = 1;
+    for (int it = 0; it < 8; it++, k++) {
+      const double u = uin + pha * k * s;
+      const double w = (u - su) / (pu - su) * (pw - sw) + sw;
+      if (!(u <= lim && u >= -lim && w <= lim && w >= -lim)) {
+        K = k;
+        break;
+      }
+    }
+  }
+  if (K < 1) return false;
+
+  const int Ua = (int)Ua_r;
+  // Pixel of step 1: major floor index (midpoint at Ua + pha/2 pixels), minor
+  // cell (lo, lo+1) holding W0 in the direction of travel.
+  const int dirw = Wb > 0 ? 1 : -1;
+  const double gd = dirw > 0 ? floor(W0) + 1.0 : ceil(W0) - 1.0;  // first minor gridline ahead
+  const int lo = (int)(dirw > 0 ? gd - 1.0 : gd);
+  const double dt = 1.0 / fabs(Wb);  // steps between minor gridlines
+  const double tmin0 = (gd - W0) / Wb;
+  // Index range check: the major index moves K-1 times, the minor index once
+  // per minor event before K; both must end within one cell of the grid
+  // (the padded border), else the exact walk takes the ray.
+  const int nmin = tmin0 < (double)K ? (int)(((double)K - tmin0) / dt) + 1 : 0;
+  int maj0, majK, min0, minK;
+  if (xmaj) {
+    maj0 = Ua + n + (pha > 0 ? 0 : -1);  // column: floor(Ua + pha/2 + n)
+    majK = maj0 + (pha > 0 ? 1 : -1) * (K - 1);
+    min0 = n - lo - 1;                   // row: floor(n - Wmid)
+    minK = min0 - dirw * nmin;
+  } else {
+    maj0 = n - Ua + (pha > 0 ? -1 : 0);  // row: floor(n - (Ua + pha/2))
+    majK = maj0 + (pha > 0 ? -1 : 1) * (K - 1);
+    min0 = lo + n;                       // column: floor(Wmid + n)
+    minK = min0 + dirw * nmin;
+  }
+  if (maj0 < -1 || maj0 > N || majK < -1 || majK > N || min0 < -1 || min0 > N || minK < -1 || minK > N)
+    return false;
+
+  if (xmaj) emit<M>(g, maps, r.xi, r.yi, u0, w0, a);
+  else emit<M>(g, maps, r.xi, r.yi, w0, u0, a);
+  a.sec = s * sqrt(1.0 + Wb * Wb);
+  const int P = N + 2 * kPad;
+  int pix, dpix_maj, dpix_min;
+  if (xmaj) {
+    pix = pad_index(maj0, min0, N);
+    dpix_maj = pha > 0 ? 1 : -1;
+    dpix_min = -dirw * P;
+  } else {
+    pix = pad_index(min0, maj0, N);
+    dpix_maj = (pha > 0 ? -1 : 1) * P;
+    dpix_min = dirw;
+  }
+  double tmin = tmin0;  // next minor event, in steps
+  double tmaj = 1.0;
+  double t = 0.0;
+  const double tend = (double)K;
+  const int4* __restrict__ m4 = reinterpret_cast<const int4*>(maps);
+  unsigned long long acc[M];
+#pragma unroll
+  for (int m = 0; m < M; m++) acc[m] = 0ull;
+  int nseg = 0;
+  // Every iteration closes one segment; the indices stay inside the padded
+  // border because the walk ends within one step of the square.
+  for (int it = 0; it < 8 * N + 128 && t < tend; it++) {
+    const bool mj = tmaj <= tmin;
+    const double tn = mj ? tmaj : tmin;
+    // Segment weight in 2^-30 steps: adding 2^22 leaves round(w * 2^30) in
+    // the low mantissa bits (w < 2).
+    const unsigned int wq = lo32((tn - t) + 4194304.0);
+    const int4 wv = ldg4(m4 + pix);
+#pragma unroll
+    for (int m = 0; m < M; m++) acc[m] += (unsigned long long)mat_of(wv, m) * wq;
+    nseg++;
+    t = tn;
+    tmaj = mj ? tmaj + 1.0 : tmaj;
+    tmin = mj ? tmin : tmin + dt;
+    pix += mj ? dpix_maj : dpix_min;
+  }
+#pragma unroll
+  for (int m = 0; m < M; m++) a.Lq[m] += acc[m];
+  a.nseg += nseg;
+  return true;
+}
+
+// ------------------------------------------------------------- reductions
 __device__ __forceinline__ float warp_max(float v) {
 #pragma unroll
   for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_xor_sync(0xffffffffu, v, o));
@@ -215,19 +452,30 @@ __device__ __forceinline__ unsigned long long warp_sum_ull(unsigned long long v)
   return v;
 }
 
+__device__ __forceinline__ float ex2_approx(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
 constexpr int kFwdThreads = 128;
 
+// One thread per ray (view v, channel c), rays numbered view-major so a warp
+// holds 32 neighbouring channels of one view (similar paths and lengths).
+// mu: [NE][M] in shared memory -- mu/xfactor for the reference summation,
+// mu*log2(e)/xfactor for the compensated one.  Each warp publishes its
+// max/min/segment count with atomics, so no warp waits for the block.
 template <int M, int SUM_MODE>
 __global__ void __launch_bounds__(kFwdThreads)
-forward_kernel(DevGeom g, const PixelRec* __restrict__ maps, const double* __restrict__ mu_scaled,
+forward_kernel(DevGeom g, const PixelRec* __restrict__ maps, const double* __restrict__ mu_tab,
                const float* __restrict__ pdf, int NE, const double* __restrict__ cos_t,
                const double* __restrict__ sin_t, const double* __restrict__ det_px0,
-               const double* __restrict__ det_py0, float* __restrict__ out,
+               const double* __restrict__ det_py0, int fast, float* __restrict__ out,
                double* __restrict__ lint, FwdStats* __restrict__ stats) {
   extern __shared__ double smem[];
-  double* s_mu = smem;                              // [NE][M]
+  double* s_mu = smem;                                             // [NE][M]
   float* s_pdf = reinterpret_cast<float*>(smem + (size_t)NE * M);  // [NE]
-  for (int i = threadIdx.x; i < NE * M; i += blockDim.x) s_mu[i] = mu_scaled[i];
+  for (int i = threadIdx.x; i < NE * M; i += blockDim.x) s_mu[i] = mu_tab[i];
   for (int i = threadIdx.x; i < NE; i += blockDim.x) s_pdf[i] = pdf[i];
   __syncthreads();
 
@@ -235,67 +483,74 @@ forward_kernel(DevGeom g, const PixelRec* __restrict__ maps, const double* __res
   const long long ray = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   const bool active = ray < nrays;
   float val = 0.0f;
-  RayAcc a;
-#pragma unroll
-  for (int m = 0; m < 8; m++) a.L[m] = 0.0;
-  a.nseg = 0;
+  int nseg = 0;
   if (active) {
     const int v = (int)(ray / g.C);
     const int c = (int)(ray - (long long)v * g.C);
-    walk_ray<M>(g, maps, cos_t[v], sin_t[v], det_px0[c], det_py0[c], a);
+    RayAcc a;
+    acc_init(a);
+    Ray r;
+    if (ray_setup(g, cos_t[v], sin_t[v], det_px0[c], det_py0[c], r)) {
+      bool done = false;
+      if (fast) done = walk_fast<M>(g, maps, r, a);
+      if (!done) walk_exact<M>(g, maps, r, a);
+    }
+    nseg = a.nseg;
+    double L[8];
+    finish_lines<M>(a, L);
     if (lint) {
 #pragma unroll
-      for (int m = 0; m < M; m++) lint[ray * M + m] = a.L[m];
+      for (int m = 0; m < M; m++) lint[ray * M + m] = L[m];
     }
     if (out) {
-      float accf = 0.0f;
-      double accd = 0.0;
-      for (int e = 0; e < NE; e++) {
-        double t = 0.0;
+      if (SUM_MODE == VCT_SUM_REFERENCE) {
+        // (float)(pdf*exp(-transp/xfactor)) summed in float in bin order,
+        // MB/reprojection_TOMO.cpp:196-197 and MB/main.cpp:504.
+        float accf = 0.0f;
+        for (int e = 0; e < NE; e++) {
+          double t = 0.0;
 #pragma unroll
-        for (int m = 0; m < M; m++) t = __fma_rn(s_mu[e * M + m], a.L[m], t);
-        double intens = (double)s_pdf[e] * exp(-t);
-        if (SUM_MODE == VCT_SUM_REFERENCE)
-          accf = __fadd_rn(accf, (float)intens);
-        else
-          accd = __dadd_rn(accd, intens);
+          for (int m = 0; m < M; m++) t = __fma_rn(s_mu[e * M + m], L[m], t);
+          accf = __fadd_rn(accf, (float)((double)s_pdf[e] * exp(-t)));
+        }
+        val = accf;
+      } else {
+        // 2^-y with y = transp*log2(e) in FP64, split y = n + f: the
+        // fraction goes through the SFU exponential, the integer part into
+        // the float exponent; bins below 2^-126 contribute nothing.  FP64 sum.
+        double accd = 0.0;
+        for (int e = 0; e < NE; e++) {
+          double y = 0.0;
+#pragma unroll
+          for (int m = 0; m < M; m++) y = __fma_rn(s_mu[e * M + m], L[m], y);
+          const int nI = __double2int_rd(y);
+          if (nI <= 125) {
+            const float fr = (float)(y - (double)nI);
+            const float scale = __int_as_float((127 - nI) << 23);
+            accd += (double)(s_pdf[e] * ex2_approx(-fr) * scale);
+          }
+        }
+        val = (float)accd;
       }
-      val = SUM_MODE == VCT_SUM_REFERENCE ? accf : (float)accd;
       out[(size_t)v * g.width + g.start + c] = val;
     }
   }
-  // Block reductions: max/min of the output and the segment count.
-  __shared__ float s_max[kFwdThreads / 32], s_min[kFwdThreads / 32];
-  __shared__ unsigned long long s_seg[kFwdThreads / 32];
-  float vmax = active ? val : 0.0f;
-  float vmin = active ? val : 3.0e38f;
-  unsigned long long ns = (unsigned long long)a.nseg;
-  vmax = warp_max(vmax);
-  vmin = warp_min(vmin);
-  ns = warp_sum_ull(ns);
-  const int wid = threadIdx.x >> 5, lane = threadIdx.x & 31;
-  if (lane == 0) { s_max[wid] = vmax; s_min[wid] = vmin; s_seg[wid] = ns; }
-  __syncthreads();
-  if (threadIdx.x == 0) {
-    float bm = s_max[0], bn = s_min[0];
-    unsigned long long bs = s_seg[0];
-    for (int w = 1; w < kFwdThreads / 32; w++) {
-      bm = fmaxf(bm, s_max[w]);
-      bn = fminf(bn, s_min[w]);
-      bs += s_seg[w];
-    }
+  float vmax = warp_max(active ? val : 0.0f);
+  float vmin = warp_min(active ? val : 3.0e38f);
+  unsigned long long ns = warp_sum_ull((unsigned long long)nseg);
+  if ((threadIdx.x & 31) == 0) {
     // Non-negative floats order like their bit patterns.
-    atomicMax(&stats->max_bits, __float_as_uint(bm));
-    atomicMin(&stats->min_bits, __float_as_uint(bn));
-    atomicAdd(&stats->segments, bs);
+    atomicMax(&stats->max_bits, __float_as_uint(vmax));
+    atomicMin(&stats->min_bits, __float_as_uint(vmin));
+    atomicAdd(&stats->segments, ns);
   }
 }
 
 template <int M>
 static int launch_forward_m(const DevGeom& g, const PixelRec* d_maps, const double* d_mu,
                             const float* d_pdf, int NE, const double* d_cos, const double* d_sin,
-                            const double* d_px0, const double* d_py0, int sum_mode, float* d_out,
-                            double* d_lint, FwdStats* d_stats, cudaStream_t st) {
+                            const double* d_px0, const double* d_py0, int sum_mode, int fast,
+                            float* d_out, double* d_lint, FwdStats* d_stats, cudaStream_t st) {
   const long long nrays = (long long)g.views_used * g.C;
   const int blocks = (int)((nrays + kFwdThreads - 1) / kFwdThreads);
   const size_t smem = (size_t)NE * M * sizeof(double) + (size_t)NE * sizeof(float);
@@ -303,26 +558,27 @@ static int launch_forward_m(const DevGeom& g, const PixelRec* d_maps, const doub
   if (sum_mode == VCT_SUM_REFERENCE) {
     auto k = forward_kernel<M, VCT_SUM_REFERENCE>;
     VCT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k<<<blocks, kFwdThreads, smem, st>>>(g, d_maps, d_mu, d_pdf, NE, d_cos, d_sin, d_px0, d_py0,
+    k<<<blocks, kFwdThreads, smem, st>>>(g, d_maps, d_mu, d_pdf, NE, d_cos, d_sin, d_px0, d_py0, fast,
                                           d_out, d_lint, d_stats);
   } else {
     auto k = forward_kernel<M, VCT_SUM_COMPENSATED>;
     VCT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k<<<blocks, kFwdThreads, smem, st>>>(g, d_maps, d_mu, d_pdf, NE, d_cos, d_sin, d_px0, d_py0,
+    k<<<blocks, kFwdThreads, smem, st>>>(g, d_maps, d_mu, d_pdf, NE, d_cos, d_sin, d_px0, d_py0, fast,
                                           d_out, d_lint, d_stats);
   }
   VCT_CUDA(cudaGetLastError());
   return VCT_OK;
 }
 
-int launch_forward(const DevGeom& g, const PixelRec* d_maps, int M, const double* d_mu_scaled,
+int launch_forward(const DevGeom& g, const PixelRec* d_maps, int M, const double* d_mu_tab,
                    const float* d_pdf, int NE, const double* d_cos, const double* d_sin,
-                   const double* d_det_ox, const double* d_det_oy, int sum_mode, float* d_out,
+                   const double* d_det_ox, const double* d_det_oy, int sum_mode, int fast, float* d_out,
                    double* d_lint, FwdStats* d_stats, cudaStream_t st) {
+  fast = fast && !g.rmax_active;
   switch (M) {
 #define VCT_CASE(mm) \
   case mm:           \
-    return launch_forward_m<mm>(g, d_maps, d_mu_scaled, d_pdf, NE, d_cos, d_sin, d_det_ox, d_det_oy, sum_mode, d_out, d_lint, d_stats, st);
+    return launch_forward_m<mm>(g, d_maps, d_mu_tab, d_pdf, NE, d_cos, d_sin, d_det_ox, d_det_oy, sum_mode, fast, d_out, d_lint, d_stats, st);
     VCT_CASE(1) VCT_CASE(2) VCT_CASE(3) VCT_CASE(4) VCT_CASE(5) VCT_CASE(6) VCT_CASE(7) VCT_CASE(8)
 #undef VCT_CASE
     default:

@@ -70,9 +70,11 @@ struct vct_ctx {
   int M = 0, NE = 0;
   int maps_ready = 0, spectrum_ready = 0;
   int sum_mode = VCT_SUM_COMPENSATED;
+  int walk_mode = VCT_WALK_FAST;
   DBuf<int16_t> maps_raw;
   DBuf<PixelRec> maps;
-  DBuf<double> mu_scaled;  // [NE][M], mu/xfactor
+  DBuf<double> mu_scaled;  // [NE][M], mu/xfactor (reference summation)
+  DBuf<double> mu_log2;    // [NE][M], mu*log2(e)/xfactor (compensated summation)
   DBuf<float> pdf;
   DBuf<float> full, out;   // [views][width]
   DBuf<FwdStats> stats;       // [0] live, [1] the reset value
@@ -230,7 +232,7 @@ void vct_destroy(vct_ctx* c) {
   cudaSetDevice(c->device);
   if (c->own_stream) cudaStreamSynchronize(c->own_stream);
   c->cos_t.release(); c->sin_t.release(); c->cs_f.release(); c->det_px0.release(); c->det_py0.release();
-  c->maps_raw.release(); c->maps.release(); c->mu_scaled.release(); c->pdf.release();
+  c->maps_raw.release(); c->maps.release(); c->mu_scaled.release(); c->mu_log2.release(); c->pdf.release();
   c->full.release(); c->out.release(); c->stats.release();
   c->fbp_coeff.release();
   for (auto& h : c->fbp_h) h.release();
@@ -350,8 +352,7 @@ int vct_set_maps_dev(vct_ctx* c, const int16_t* d_maps, int M) {
   if (rc) return rc;
   if (!d_maps || M < 1 || M > VCT_MAX_MATERIALS) return fail(VCT_E_ARG, "vct_set_maps: bad argument");
   if (c->spectrum_ready && M != c->M) return fail(VCT_E_ARG, "vct_set_maps: M differs from the spectrum's");
-  const size_t n2 = (size_t)c->dg.N * c->dg.N;
-  if ((rc = c->maps.ensure(n2))) return rc;
+  if ((rc = c->maps.ensure(padded_pixels(c->dg.N)))) return rc;
   if ((rc = launch_pack_maps(d_maps, M, c->dg.N, c->maps.p, c->stream))) return rc;
   c->launches++;
   c->M = M;
@@ -376,11 +377,18 @@ int vct_set_spectrum(vct_ctx* c, const float* mu, const float* pdf, int M, int N
     return fail(VCT_E_ARG, "vct_set_spectrum: bad argument");
   if (c->maps_ready && M != c->M) return fail(VCT_E_ARG, "vct_set_spectrum: M differs from the maps'");
   // Transpose to [NE][M] and fold 1/xfactor (exp(-transp/xfactor), :196).
-  std::vector<double> t((size_t)NE * M);
+  std::vector<double> t((size_t)NE * M), t2((size_t)NE * M);
+  const double log2e = 1.4426950408889634073599246810019;
   for (int e = 0; e < NE; e++)
-    for (int m = 0; m < M; m++) t[(size_t)e * M + m] = (double)mu[(size_t)m * NE + e] / (double)c->geo.xfactor;
-  if ((rc = c->mu_scaled.ensure((size_t)NE * M)) || (rc = c->pdf.ensure(NE))) return rc;
+    for (int m = 0; m < M; m++) {
+      t[(size_t)e * M + m] = (double)mu[(size_t)m * NE + e] / (double)c->geo.xfactor;
+      t2[(size_t)e * M + m] = t[(size_t)e * M + m] * log2e;
+    }
+  if ((rc = c->mu_scaled.ensure((size_t)NE * M)) || (rc = c->mu_log2.ensure((size_t)NE * M)) ||
+      (rc = c->pdf.ensure(NE)))
+    return rc;
   VCT_CUDA(cudaMemcpyAsync(c->mu_scaled.p, t.data(), t.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+  VCT_CUDA(cudaMemcpyAsync(c->mu_log2.p, t2.data(), t2.size() * sizeof(double), cudaMemcpyHostToDevice, c->stream));
   VCT_CUDA(cudaMemcpyAsync(c->pdf.p, pdf, NE * sizeof(float), cudaMemcpyHostToDevice, c->stream));
   VCT_CUDA(cudaStreamSynchronize(c->stream));  // t is a host temporary
   c->M = M;
@@ -396,13 +404,22 @@ int vct_set_sum_mode(vct_ctx* c, int mode) {
   return VCT_OK;
 }
 
+int vct_set_walk_mode(vct_ctx* c, int mode) {
+  if (!c) return fail(VCT_E_ARG, "null context");
+  if (mode != VCT_WALK_FAST && mode != VCT_WALK_EXACT) return fail(VCT_E_ARG, "bad walk mode");
+  c->walk_mode = mode;
+  return VCT_OK;
+}
+
 static int forward_into(vct_ctx* c, float* d_out, double* d_lint) {
   if (!c->maps_ready || !c->spectrum_ready) return fail(VCT_E_STATE, "forward: maps or spectrum not set");
   const size_t nsino = (size_t)c->geo.views * c->geo.width;
   VCT_CUDA(cudaMemcpyAsync(c->stats.p, c->stats.p + 1, sizeof(FwdStats), cudaMemcpyDeviceToDevice, c->stream));
   if (d_out) VCT_CUDA(cudaMemsetAsync(d_out, 0, nsino * sizeof(float), c->stream));
-  int rc = launch_forward(c->dg, c->maps.p, c->M, c->mu_scaled.p, c->pdf.p, c->NE, c->cos_t.p, c->sin_t.p,
-                          c->det_px0.p, c->det_py0.p, c->sum_mode, d_out, d_lint, c->stats.p, c->stream);
+  const double* mu_tab = c->sum_mode == VCT_SUM_REFERENCE ? c->mu_scaled.p : c->mu_log2.p;
+  int rc = launch_forward(c->dg, c->maps.p, c->M, mu_tab, c->pdf.p, c->NE, c->cos_t.p, c->sin_t.p,
+                          c->det_px0.p, c->det_py0.p, c->sum_mode, c->walk_mode == VCT_WALK_FAST, d_out,
+                          d_lint, c->stats.p, c->stream);
   if (rc) return rc;
   c->launches++;
   return VCT_OK;

@@ -40,10 +40,13 @@ struct DevGeom {
 
 // Packed maps: one 16-byte record per pixel, 8 int16 materials (unused
 // materials 0).  Negative densities are stored as 0: the reference gives
-// them zero weight (MB/reprojection_TOMO.cpp:151-155).
+// them zero weight (MB/reprojection_TOMO.cpp:151-155).  The grid is padded
+// by kMapPad cells on every side (see vct_forward.cu).
 struct alignas(16) PixelRec {
   int16_t m[8];
 };
+constexpr int kMapPad = 2;
+inline size_t padded_pixels(int N) { return (size_t)(N + 2 * kMapPad) * (size_t)(N + 2 * kMapPad); }
 
 struct FwdStats {
   unsigned int max_bits;  // float bits of the maximum (values are >= 0)
@@ -56,9 +59,9 @@ struct Workspace;  // device buffers, defined in vct_host.cpp
 
 // Launchers (vct_forward.cu / vct_fbp.cu).  All enqueue on `st`.
 int launch_pack_maps(const int16_t* d_maps, int M, int N, PixelRec* d_packed, cudaStream_t st);
-int launch_forward(const DevGeom& g, const PixelRec* d_maps, int M, const double* d_mu_scaled,
+int launch_forward(const DevGeom& g, const PixelRec* d_maps, int M, const double* d_mu_tab,
                    const float* d_pdf, int NE, const double* d_cos, const double* d_sin,
-                   const double* d_det_ox, const double* d_det_oy, int sum_mode, float* d_out,
+                   const double* d_det_ox, const double* d_det_oy, int sum_mode, int fast, float* d_out,
                    double* d_lint, FwdStats* d_stats, cudaStream_t st);
 int launch_normalize_noise(const DevGeom& g, const float* d_in, float* d_out, const FwdStats* d_stats,
                            int pad_zero, double sigma, uint64_t seed, cudaStream_t st);

@@ -4,11 +4,13 @@
 //   1. weight:   g[v][k] = -ln p[v][k] * SID*cos((k-cw)*dbeta) * dbeta, once per
 //                sample (the reference re-evaluates the log inside its
 //                609-long inner loop, i.e. 609 times per sample).
-//   2. filter:   q[v][m] = sum_k h[m][k] g[v][k] -- a [V x C] x [C x C]^T
-//                product, tiled through shared memory, FP32 FMA.
+//   2. filter:   q[v][m] = sum_k h[m][k] g[v][k]; h is one kernel shifted
+//                per row (times an edge-row factor), so each view is a 1-D
+//                convolution, shared memory + register window, FP32 FMA.
 //   3. backproject: pixel-driven, equiangular fan weight 1/L^2, linear
-//                interpolation on the detector; views staged in shared memory
-//                in chunks; one thread per pixel.
+//                interpolation on the detector; 32 x 16 pixel tiles, views in
+//                chunks with each view's detector window for the tile staged
+//                in shared memory.
 #include <cuda_runtime.h>
 
 #include "vct_internal.h"
@@ -36,121 +38,280 @@ int launch_fbp_weight(const float* d_sino, int V, int W, int start, int C, const
 }
 
 // ------------------------------------------------------------------ filter
-// Q[V][C] = G[V][C] * H[C][C]^T.  Block tile 32 views x 64 channels, k step
-// 32; 128 threads, each owns a 4 x 4 register tile.
-constexpr int FB_M = 32, FB_N = 64, FB_K = 32, FB_T = 128;
+// q[v][m] = sum_k h[m][k] g[v][k] (FBP/filterSinogramTOMO.cpp:233-243 with the
+// constant factors folded into g).  prepareConstMap's rows are one kernel
+// shifted, h[m][k] = c_m h0(m-k), with c_m = 1 except the renormalised edge
+// rows (:114-123), so each view is a 1-D convolution: one block per view, g
+// and h0 in shared memory, each thread FC consecutive outputs with a sliding
+// register window over h0; k runs in ascending order as in the reference.
+constexpr int FC_T = 128, FC_R = 5;
 
-__global__ void __launch_bounds__(FB_T)
-fbp_filter_kernel(const float* __restrict__ G, const float* __restrict__ H, int V, int C,
-                  int in_mode, float* __restrict__ Q) {
-  __shared__ float sG[FB_K][FB_M + 4];
-  __shared__ float sH[FB_K][FB_N + 4];
-  const int v0 = blockIdx.y * FB_M, m0 = blockIdx.x * FB_N;
-  const int tx = threadIdx.x & 15;  // channel group (4 channels each)
-  const int ty = threadIdx.x >> 4;  // view group (4 views each)
-  float acc[4][4];
+__global__ void __launch_bounds__(FC_T)
+fbp_filter_kernel(const float* __restrict__ G, const float* __restrict__ h0, const float* __restrict__ cm,
+                  int V, int C, int in_mode, float* __restrict__ Q) {
+  extern __shared__ float sm[];
+  float* sg = sm;                 // [C + FC_R]  (zero tail)
+  float* sh = sm + C + FC_R;      // [2C + FC_R] h0(d) at index d + C, zero outside
+  const int v = blockIdx.x;
+  for (int k = threadIdx.x; k < C + FC_R; k += FC_T) sg[k] = k < C ? G[(size_t)v * C + k] : 0.0f;
+  for (int d = threadIdx.x; d < 2 * C + FC_R; d += FC_T) sh[d] = (d >= 1 && d < 2 * C) ? h0[d - 1] : 0.0f;
+  __syncthreads();
+  const int m0 = threadIdx.x * FC_R;
+  if (m0 >= C) return;
+  float acc[FC_R];
+  float win[FC_R];  // win[j] = h0(m0 + j - k)
 #pragma unroll
-  for (int i = 0; i < 4; i++)
+  for (int j = 0; j < FC_R; j++) {
+    acc[j] = 0.0f;
+    win[j] = sh[m0 + j + C];  // k = 0
+  }
+  for (int k = 0; k < C; k++) {
+    const float gk = sg[k];
 #pragma unroll
-    for (int j = 0; j < 4; j++) acc[i][j] = 0.0f;
-  for (int k0 = 0; k0 < C; k0 += FB_K) {
-    // G tile: 32 views x 32 k -> transposed into sG[k][v].
-    for (int e = threadIdx.x; e < FB_M * FB_K; e += FB_T) {
-      int vv = e / FB_K, kk = e % FB_K;
-      int v = v0 + vv, k = k0 + kk;
-      sG[kk][vv] = (v < V && k < C) ? G[(size_t)v * C + k] : 0.0f;
-    }
-    // H tile: 64 rows m x 32 k -> sH[k][m].
-    for (int e = threadIdx.x; e < FB_N * FB_K; e += FB_T) {
-      int mm = e / FB_K, kk = e % FB_K;
-      int m = m0 + mm, k = k0 + kk;
-      sH[kk][mm] = (m < C && k < C) ? H[(size_t)m * C + k] : 0.0f;
-    }
-    __syncthreads();
-#pragma unroll 8
-    for (int kk = 0; kk < FB_K; kk++) {
-      float a[4], b[4];
+    for (int j = 0; j < FC_R; j++) acc[j] = fmaf(win[j], gk, acc[j]);
+    // k -> k+1: h0(m0 + j - k - 1) = win[j-1]; win[0] needs a new value.
 #pragma unroll
-      for (int i = 0; i < 4; i++) a[i] = sG[kk][ty * 4 + i];
-#pragma unroll
-      for (int j = 0; j < 4; j++) b[j] = sH[kk][tx + 16 * j];
-#pragma unroll
-      for (int i = 0; i < 4; i++)
-#pragma unroll
-        for (int j = 0; j < 4; j++) acc[i][j] = fmaf(a[i], b[j], acc[i][j]);
-    }
-    __syncthreads();
+    for (int j = FC_R - 1; j > 0; j--) win[j] = win[j - 1];
+    win[0] = sh[m0 - k - 1 + C];
   }
 #pragma unroll
-  for (int i = 0; i < 4; i++) {
-    const int v = v0 + ty * 4 + i;
-    if (v >= V) continue;
-#pragma unroll
-    for (int j = 0; j < 4; j++) {
-      const int m = m0 + tx + 16 * j;
-      if (m >= C) continue;
-      float q = acc[i][j];
-      if (in_mode && (q < 1000.0f || q > 300000.0f)) q = 0.0f;  // :250-255
-      Q[(size_t)v * C + m] = q;
-    }
+  for (int j = 0; j < FC_R; j++) {
+    const int m = m0 + j;
+    if (m >= C) break;
+    float q = acc[j] * cm[m];
+    if (in_mode && (q < 1000.0f || q > 300000.0f)) q = 0.0f;  // :250-255
+    Q[(size_t)v * C + m] = q;
   }
 }
 
-int launch_fbp_filter(const float* d_g, const float* d_h, int V, int C, int in_mode, float* d_q,
-                      cudaStream_t st) {
-  dim3 grid((C + FB_N - 1) / FB_N, (V + FB_M - 1) / FB_M);
-  fbp_filter_kernel<<<grid, FB_T, 0, st>>>(d_g, d_h, V, C, in_mode, d_q);
+int launch_fbp_filter(const float* d_g, const float* d_h0, const float* d_cm, int V, int C, int in_mode,
+                      float* d_q, cudaStream_t st) {
+  if ((C + FC_R - 1) / FC_R > FC_T) return fail(VCT_E_UNSUPPORTED, "filter: more than 640 channels");
+  const size_t smem = (size_t)(3 * C + 2 * FC_R) * sizeof(float);
+  VCT_CUDA(cudaFuncSetAttribute(fbp_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  fbp_filter_kernel<<<V, FC_T, smem, st>>>(d_g, d_h0, d_cm, V, C, in_mode, d_q);
   VCT_CUDA(cudaGetLastError());
   return VCT_OK;
 }
 
 // ------------------------------------------------------------- backproject
-constexpr int BP_TX = 16, BP_TY = 16, BP_VCHUNK = 16;
+// atan(t) on |t| <= 0.5 as t*P(t^2), P of degree 5: a least-squares fit of
+// atan(t)/t on Chebyshev nodes in t^2 (made for this kernel); max error
+// 3.7e-8 rad in FP32.  Pixels inside the reconstruction circle see
+// |t| = |X/(SID-Y)| < 0.45 at the default geometry; larger |t| is outside
+// the fan and rejected by the channel test either way.
+__device__ __forceinline__ float atan_small(float t) {
+  const float u = t * t;
+  float p = -0.05077829957008362f;
+  p = fmaf(p, u, 0.10122803598642349f);
+  p = fmaf(p, u, -0.14165857434272766f);
+  p = fmaf(p, u, 0.19993248581886292f);
+  p = fmaf(p, u, -0.3333319127559662f);
+  p = fmaf(p, u, 1.0f);
+  return t * p;
+}
 
-__global__ void __launch_bounds__(BP_TX * BP_TY)
-fbp_bp_kernel(const float* __restrict__ Q, int V, int C, int N, float scale, float sid,
-              float inv_dbeta_det, float center_ch, float out_scale, const float2* __restrict__ cs,
+__device__ __forceinline__ float rcp_approx(float x) {
+  float y;
+  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
+
+// Fractional channel of pixel (xx, yy) cm in the view with (cos, sin):
+// FBP/reconstructImageTOMO.cpp:67-72.
+__device__ __forceinline__ float bp_channel(float xx, float yy, float c, float s, float sid,
+                                            float inv_dbeta, float center, float* L2) {
+  const float X = xx * c + yy * s;
+  const float Y = -xx * s + yy * c;
+  const float d = sid - Y;
+  *L2 = d * d + X * X;
+  return atan_small(__fdividef(X, d)) * inv_dbeta + center;
+}
+
+// 32 x 16 pixel tile per block, 256 threads, 2 pixels per thread (rows ty and
+// ty+8).  Views go in chunks of BP_VC; for each view only the detector window
+// the tile projects onto (from the tile's corner pixels, -2 channels) is
+// staged in shared memory as pairs (q[i], q[i+1]), `win` entries wide, so the
+// interpolation is one 8-byte load.
+constexpr int BP_TX = 32, BP_TY = 8, BP_PIX = 2, BP_VC = 32;
+
+__global__ void __launch_bounds__(BP_TX * BP_TY, 4)
+fbp_bp_kernel(const float* __restrict__ Q, int V, int C, int N, int win, float scale, float sid,
+              float inv_dbeta, float center, float out_scale, const float2* __restrict__ cs,
               float* __restrict__ img) {
-  extern __shared__ float sm[];
-  float* sQ = sm;                                           // [BP_VCHUNK][C]
-  float2* sCS = reinterpret_cast<float2*>(sm + BP_VCHUNK * C);  // [BP_VCHUNK]
-  const int x = blockIdx.x * BP_TX + threadIdx.x;
-  const int y = blockIdx.y * BP_TY + threadIdx.y;
+  extern __shared__ float2 sm2[];
+  float2* sQ = sm2;                                        // [BP_VC][win] pairs
+  float2* sCS = sQ + BP_VC * win;                          // [BP_VC]
+  int* sOff = reinterpret_cast<int*>(sCS + BP_VC);         // [BP_VC]
   const int tid = threadIdx.y * BP_TX + threadIdx.x;
+  const int x0 = blockIdx.x * BP_TX, y0 = blockIdx.y * (BP_TY * BP_PIX);
+  const int x = x0 + threadIdx.x;
+  const float cp = (float)N / 2.0f - 0.5f;
   // Inscribed-circle mask (FBP/misc.cpp:20-36): (y-r)^2 + (x-r)^2 <= r^2.
   const double r = (double)(N - 1) / 2.0;
-  const bool inside = x < N && y < N &&
-                      ((double)y - r) * ((double)y - r) + ((double)x - r) * ((double)x - r) <= r * r;
-  const float cp = (float)N / 2.0f - 0.5f;
   const float xx = -((float)x - cp) * scale;
-  const float yy = -((float)y - cp) * scale;
-  const int use = V / 2 * 2;  // usesinogram, :30
-  float acc = 0.0f;
-  for (int v0 = 0; v0 < use; v0 += BP_VCHUNK) {
-    const int nv = min(BP_VCHUNK, use - v0);
+  float yy[BP_PIX], acc[BP_PIX];
+  bool in[BP_PIX];
+#pragma unroll
+  for (int k = 0; k < BP_PIX; k++) {
+    const int y = y0 + threadIdx.y + BP_TY * k;
+    yy[k] = -((float)y - cp) * scale;
+    in[k] = x < N && y < N && ((double)y - r) * ((double)y - r) + ((double)x - r) * ((double)x - r) <= r * r;
+    acc[k] = 0.0f;
+  }
+  // A tile with no pixel inside the circle only writes zeros.
+  const bool any = __syncthreads_or(in[0] || in[1]);
+  const int use = any ? V / 2 * 2 : 0;  // usesinogram, :30
+  // Tile corners (pixel centres) for the per-view windows.
+  const int xe = min(x0 + BP_TX - 1, N - 1), ye = min(y0 + BP_TY * BP_PIX - 1, N - 1);
+  const float cx0 = -((float)x0 - cp) * scale, cx1 = -((float)xe - cp) * scale;
+  const float cy0 = -((float)y0 - cp) * scale, cy1 = -((float)ye - cp) * scale;
+  for (int v0 = 0; v0 < use; v0 += BP_VC) {
+    const int nv = min(BP_VC, use - v0);
     __syncthreads();
-    for (int e = tid; e < nv * C; e += BP_TX * BP_TY) sQ[e] = Q[(size_t)v0 * C + e];
-    if (tid < nv) sCS[tid] = cs[v0 + tid];
+    if (tid < nv) {
+      const float2 t = cs[v0 + tid];
+      float L2;
+      const float a = bp_channel(cx0, cy0, t.x, t.y, sid, inv_dbeta, center, &L2);
+      const float b = bp_channel(cx1, cy0, t.x, t.y, sid, inv_dbeta, center, &L2);
+      const float c2 = bp_channel(cx0, cy1, t.x, t.y, sid, inv_dbeta, center, &L2);
+      const float d = bp_channel(cx1, cy1, t.x, t.y, sid, inv_dbeta, center, &L2);
+      sOff[tid] = (int)floorf(fminf(fminf(a, b), fminf(c2, d))) - 2;
+      sCS[tid] = t;
+    }
     __syncthreads();
-    if (inside) {
-      for (int j = 0; j < nv; j++) {
-        const float2 t = sCS[j];  // (cos, sin)
-        const float X = xx * t.x + yy * t.y;
-        const float Y = -xx * t.y + yy * t.x;
-        const float d = sid - Y;
-        const float L2 = d * d + X * X;
-        const float fg = atanf(__fdividef(X, d)) * inv_dbeta_det + center_ch;
-        const int gi = (int)fg;  // truncation as (int)(fGAM), :73
-        if (gi >= 0 && gi < C - 1) {
-          const float w = fg - (float)gi;
-          const float* q = sQ + j * C + gi;
-          const float s1 = (1.0f - w) * q[0] + w * q[1];
-          acc += __fdividef(s1, L2);
+    for (int j = threadIdx.y; j < nv; j += BP_TY) {
+      const int off = sOff[j];
+      const float* qrow = Q + (size_t)(v0 + j) * C;
+      for (int k = threadIdx.x; k < win; k += BP_TX) {
+        const int ch = off + k;
+        const float q0 = (ch >= 0 && ch < C) ? qrow[ch] : 0.0f;
+        const float q1 = (ch + 1 >= 0 && ch + 1 < C) ? qrow[ch + 1] : 0.0f;
+        sQ[j * win + k] = make_float2(q0, q1);
+      }
+    }
+    __syncthreads();
+    for (int j = 0; j < nv; j++) {
+      const float2 t = sCS[j];
+      const int off = sOff[j];
+      const float2* q = sQ + j * win;
+      const float* qg = Q + (size_t)(v0 + j) * C;
+#pragma unroll
+      for (int k = 0; k < BP_PIX; k++) {
+        float L2;
+        const float fg = bp_channel(xx, yy[k], t.x, t.y, sid, inv_dbeta, center, &L2);
+        // (int)(fGAM) truncates toward zero (:73): adding 2^23 with round-to-
+        // zero leaves trunc(fg) in the low mantissa bits for 0 <= fg < 2^22;
+        // fg in (-1, 0) truncates to 0 and is kept (w < 0, as the reference).
+        const float big = __fadd_rz(fmaxf(fg, 0.0f), 8388608.0f);
+        const int gi = fg > -1.0f ? (__float_as_int(big) - 0x4B000000) : -1;
+        const float w = fg - (big - 8388608.0f);
+        if (in[k] && gi >= 0 && gi < C - 1) {
+          const int li = gi - off;
+          float2 qq;
+          if (li >= 0 && li < win) qq = q[li];
+          else qq = make_float2(qg[gi], qg[gi + 1]);  // outside the staged window
+          acc[k] += __fdividef(fmaf(w, qq.y - qq.x, qq.x), L2);
         }
       }
     }
   }
-  if (x < N && y < N) img[(size_t)y * N + x] = inside ? acc * out_scale : 0.0f;
+#pragma unroll
+  for (int k = 0; k < BP_PIX; k++) {
+    const int y = y0 + threadIdx.y + BP_TY * k;
+    if (x < N && y < N) img[(size_t)y * N + x] = in[k] ? acc[k] * out_scale : 0.0f;
+  }
+}
+
+// Backprojection with the square grid's quarter-turn symmetry, for V
+// divisible by 4 and even N.  Pixel (x, y) in view j and pixel
+// (N-1-y, x) in view j + V/4 have the same rotated coordinates (X, Y): with
+// beta' = beta + 90 deg, cos' = -sin, sin' = cos, and the pixel centre
+// (xx, yy) maps to (-yy, xx).  So the geometry (X, Y, L^2, fractional
+// channel) computed for p0 = (x, y) in view j also serves
+//   p1 = (N-1-y, x) in view j+V/4, p2 = (N-1-x, N-1-y) in view j+V/2,
+//   p3 = (y, N-1-x) in view j+3V/4   (views mod V);
+// running j over all V views gives each of the four pixels every view, with
+// a quarter of the geometry work.  Orbit representatives cover the top-left
+// quadrant.
+// The trig tables of the four views agree with the quarter-turn to double
+// rounding, below the FP32 resolution of the geometry.
+// 32 x 4 orbits per block; the base views are split over BS_VS groups of
+// warps (threadIdx.z), summed in shared memory at the end.  The four filtered
+// rows of each base view are read through the L1 cache (the 32 pixels of a
+// warp read neighbouring channels).
+constexpr int BS_TX = 32, BS_TY = 4, BS_VS = 4;
+
+__device__ __forceinline__ void bp_orbit_view(const float* __restrict__ Q, int V, int V4, int C, float xx, float yy,
+                                              float2 t, int j, float sid, float inv_dbeta, float center,
+                                              float acc[4]) {
+  // FBP/reconstructImageTOMO.cpp:67-73, shared by the orbit.
+  const float X = xx * t.x + yy * t.y;
+  const float Y = -xx * t.y + yy * t.x;
+  const float d = sid - Y;
+  const float rd = rcp_approx(d);
+  const float fg = atan_small(X * rd) * inv_dbeta + center;
+  const float iL2 = rcp_approx(fmaf(d, d, X * X));
+  // (int)(fGAM) truncates toward zero: trunc(fg) via 2^23 with round-to-zero;
+  // fg in (-1, 0) truncates to 0 and is kept (w < 0), as the reference.
+  const float big = __fadd_rz(fmaxf(fg, 0.0f), 8388608.0f);
+  const int gi = fg > -1.0f ? (__float_as_int(big) - 0x4B000000) : -1;
+  const float w = fg - (big - 8388608.0f);
+  if ((unsigned)gi < (unsigned)(C - 1)) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      int row = j + q * V4;
+      row = row >= V ? row - V : row;
+      const float* qr = Q + (size_t)row * C + gi;
+      const float q0 = __ldg(qr), q1 = __ldg(qr + 1);
+      acc[q] = fmaf(fmaf(w, q1 - q0, q0), iL2, acc[q]);
+    }
+  }
+}
+
+__global__ void __launch_bounds__(BS_TX * BS_TY * BS_VS)
+fbp_bp_sym_kernel(const float* __restrict__ Q, int V, int C, int N, float scale, float sid, float inv_dbeta,
+                  float center, float out_scale, const float2* __restrict__ cs, float* __restrict__ img) {
+  __shared__ float part[BS_VS - 1][4][BS_TX * BS_TY];
+  const int H = N / 2, V4 = V / 4;
+  const int x = blockIdx.x * BS_TX + threadIdx.x;
+  const int y = blockIdx.y * BS_TY + threadIdx.y;
+  const int lt = threadIdx.y * BS_TX + threadIdx.x;
+  const int z = threadIdx.z;
+  const double r = (double)(N - 1) / 2.0;
+  // The circle mask (FBP/misc.cpp:20-36) is invariant under the quarter turn.
+  const bool in = x < H && y < H &&
+                  ((double)y - r) * ((double)y - r) + ((double)x - r) * ((double)x - r) <= r * r;
+  float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+  if (in) {
+    const float cp = (float)N / 2.0f - 0.5f;
+    const float xx = -((float)x - cp) * scale;
+    const float yy = -((float)y - cp) * scale;
+    const int jb = (int)((long long)V * z / BS_VS), je = (int)((long long)V * (z + 1) / BS_VS);
+    int j = jb;
+    for (; j + 1 < je; j += 2) {
+      const float2 t0 = __ldg(cs + j), t1 = __ldg(cs + j + 1);
+      bp_orbit_view(Q, V, V4, C, xx, yy, t0, j, sid, inv_dbeta, center, acc);
+      bp_orbit_view(Q, V, V4, C, xx, yy, t1, j + 1, sid, inv_dbeta, center, acc);
+    }
+    if (j < je) bp_orbit_view(Q, V, V4, C, xx, yy, __ldg(cs + j), j, sid, inv_dbeta, center, acc);
+  }
+  if (z > 0) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) part[z - 1][q][lt] = acc[q];
+  }
+  __syncthreads();
+  if (z == 0 && x < H && y < H) {
+    const int px[4] = {x, N - 1 - y, N - 1 - x, y};
+    const int py[4] = {y, x, N - 1 - y, N - 1 - x};
+#pragma unroll
+    for (int q = 0; q < 4; q++) {
+      float a = acc[q];
+#pragma unroll
+      for (int k = 0; k < BS_VS - 1; k++) a += part[k][q][lt];
+      img[(size_t)py[q] * N + px[q]] = in ? a * out_scale : 0.0f;
+    }
+  }
 }
 
 int launch_fbp_backproject(const float* d_q, int V, int C, int N, double pixel_cm, double sid,
@@ -159,11 +320,29 @@ int launch_fbp_backproject(const float* d_q, int V, int C, int N, double pixel_c
   const int half = (C - 1) / 2;
   const double dbeta_det = max_beta / half;
   const double dbeta = 2.0 * 3.141592653589793 / V;
-  dim3 grid((N + BP_TX - 1) / BP_TX, (N + BP_TY - 1) / BP_TY);
+  // Window: the angle a tile's diagonal subtends from the source at the
+  // nearest approach of the reconstruction square, in channels, + margins.
+  const double tile_cm = (double)BP_TX * pixel_cm * 1.41421356237;
+  const double near_cm = sid - 0.5 * N * pixel_cm * 1.41421356237;
+  int win = C + 4;
+  if (near_cm > tile_cm) win = (int)(tile_cm / near_cm / dbeta_det) + 8;
+  win = ((win + 31) / 32) * 32;
+  if (win > C + 4) win = C + 4;
+  if (V % 4 == 0 && N % 2 == 0) {
+    const int H = N / 2;
+    dim3 grid((H + BS_TX - 1) / BS_TX, (H + BS_TY - 1) / BS_TY);
+    dim3 block(BS_TX, BS_TY, BS_VS);
+    fbp_bp_sym_kernel<<<grid, block, 0, st>>>(d_q, V, C, N, (float)pixel_cm, (float)sid, (float)(1.0 / dbeta_det),
+                                              (float)(C / 2), (float)(dbeta * xfactor),
+                                              reinterpret_cast<const float2*>(d_cs), d_img);
+    VCT_CUDA(cudaGetLastError());
+    return VCT_OK;
+  }
+  dim3 grid((N + BP_TX - 1) / BP_TX, (N + BP_TY * BP_PIX - 1) / (BP_TY * BP_PIX));
   dim3 block(BP_TX, BP_TY);
-  const size_t smem = (size_t)BP_VCHUNK * C * sizeof(float) + BP_VCHUNK * sizeof(float2);
+  const size_t smem = (size_t)BP_VC * win * sizeof(float2) + BP_VC * (sizeof(float2) + sizeof(int));
   VCT_CUDA(cudaFuncSetAttribute(fbp_bp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  fbp_bp_kernel<<<grid, block, smem, st>>>(d_q, V, C, N, (float)pixel_cm, (float)sid,
+  fbp_bp_kernel<<<grid, block, smem, st>>>(d_q, V, C, N, win, (float)pixel_cm, (float)sid,
                                            (float)(1.0 / dbeta_det), (float)(C / 2),
                                            (float)(dbeta * xfactor),
                                            reinterpret_cast<const float2*>(d_cs), d_img);

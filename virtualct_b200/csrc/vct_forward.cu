@@ -62,6 +62,15 @@ int launch_pack_maps(const int16_t* d_maps, int M, int N, PixelRec* d_packed, cu
   return VCT_OK;
 }
 
+// Resident blocks per SM the register allocation is held to, and the number
+// of walk segments whose gathers are issued together (chosen by measurement).
+#ifndef VCT_FWD_MINBLOCKS
+#define VCT_FWD_MINBLOCKS 0
+#endif
+#ifndef VCT_FWD_UNROLL
+#define VCT_FWD_UNROLL 4
+#endif
+
 // ------------------------------------------------------------ host/device shims
 // The walks are __host__ __device__ so the same code can run on the CPU
 // (tests/host/walk_check.cu); these wrappers pick the device intrinsic or its
@@ -389,8 +398,6 @@ VCT_HD bool walk_fast(const DevGeom& g, const PixelRec* __restrict__ maps, const
   if (maj0 < -1 || maj0 > N || majK < -1 || majK > N || min0 < -1 || min0 > N || minK < -1 || minK > N)
     return false;
 
-  if (xmaj) emit<M>(g, maps, r.xi, r.yi, u0, w0, a);
-  else emit<M>(g, maps, r.xi, r.yi, w0, u0, a);
   a.sec = s * sqrt(1.0 + Wb * Wb);
   const int P = N + 2 * kPad;
   int pix, dpix_maj, dpix_min;
@@ -403,6 +410,7 @@ VCT_HD bool walk_fast(const DevGeom& g, const PixelRec* __restrict__ maps, const
     dpix_maj = (pha > 0 ? -1 : 1) * P;
     dpix_min = dirw;
   }
+  const int pix_first = pix;
   double tmin = tmin0;  // next minor event, in steps
   double tmaj = 1.0;
   double t = 0.0;
@@ -412,26 +420,47 @@ VCT_HD bool walk_fast(const DevGeom& g, const PixelRec* __restrict__ maps, const
 #pragma unroll
   for (int m = 0; m < M; m++) acc[m] = 0ull;
   int nseg = 0;
-  // Every iteration closes one segment; the indices stay inside the padded
-  // border because the walk ends within one step of the square.
-  for (int it = 0; it < 8 * N + 128 && t < tend; it++) {
-    const bool mj = tmaj <= tmin;
-    const double tn = mj ? tmaj : tmin;
-    // Segment weight in 2^-30 steps: adding 2^22 leaves round(w * 2^30) in
-    // the low mantissa bits (w < 2).
-    const unsigned int wq = lo32((tn - t) + 4194304.0);
-    const int4 wv = ldg4(m4 + pix);
+  // Every iteration closes one segment.  The event logic does not depend on
+  // the map, so kUnroll segments are laid out first and their gathers issued
+  // together before any is consumed.  Past the end, slots repeat the first
+  // segment's pixel with weight 0; the indices stay inside the padded border
+  // because the walk ends within one step of the square.
+  constexpr int kUnroll = VCT_FWD_UNROLL;
+  for (int it = 0; it < (8 * N + 128) / kUnroll && t < tend; it++) {
+    int px[kUnroll];
+    unsigned int wq[kUnroll];
 #pragma unroll
-    for (int m = 0; m < M; m++) acc[m] += (unsigned long long)mat_of(wv, m) * wq;
-    nseg++;
-    t = tn;
-    tmaj = mj ? tmaj + 1.0 : tmaj;
-    tmin = mj ? tmin : tmin + dt;
-    pix += mj ? dpix_maj : dpix_min;
+    for (int u = 0; u < kUnroll; u++) {
+      const bool live = t < tend;
+      const bool mj = tmaj <= tmin;
+      const double tn = mj ? tmaj : tmin;
+      // Segment weight in 2^-30 steps: adding 2^22 leaves round(w * 2^30)
+      // in the low mantissa bits (0 <= w <= 1).
+      wq[u] = live ? lo32((tn - t) + 4194304.0) : 0u;
+      px[u] = live ? pix : pix_first;
+      nseg += live;
+      if (live) {
+        t = tn;
+        tmaj = mj ? tmaj + 1.0 : tmaj;
+        tmin = mj ? tmin : tmin + dt;
+        pix += mj ? dpix_maj : dpix_min;
+      }
+    }
+    int4 wv[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; u++) wv[u] = ldg4(m4 + px[u]);
+#pragma unroll
+    for (int u = 0; u < kUnroll; u++)
+#pragma unroll
+      for (int m = 0; m < M; m++) acc[m] += (unsigned long long)mat_of(wv[u], m) * wq[u];
   }
 #pragma unroll
   for (int m = 0; m < M; m++) a.Lq[m] += acc[m];
   a.nseg += nseg;
+  // The lumped first segment, after the loop so its FP64 sums are not live
+  // during it.
+  if (xmaj) emit<M>(g, maps, r.xi, r.yi, u0, w0, a);
+  else emit<M>(g, maps, r.xi, r.yi, w0, u0, a);
   return true;
 }
 
@@ -466,7 +495,7 @@ constexpr int kFwdThreads = 128;
 // mu*log2(e)/xfactor for the compensated one.  Each warp publishes its
 // max/min/segment count with atomics, so no warp waits for the block.
 template <int M, int SUM_MODE>
-__global__ void __launch_bounds__(kFwdThreads)
+__global__ void __launch_bounds__(kFwdThreads, VCT_FWD_MINBLOCKS)
 forward_kernel(DevGeom g, const PixelRec* __restrict__ maps, const double* __restrict__ mu_tab,
                const float* __restrict__ pdf, int NE, const double* __restrict__ cos_t,
                const double* __restrict__ sin_t, const double* __restrict__ det_px0,

@@ -82,7 +82,7 @@ struct vct_ctx {
   long long last_segments = 0;
   // FBP
   DBuf<double> fbp_coeff;  // SID*cos((k-cw)*dbeta)*dbeta
-  DBuf<float> fbp_h[3];    // constMap per filter (1 Ram-Lak, 2 Shepp-Logan), float [C][C]
+  DBuf<float> fbp_h[3];    // per filter (1 Ram-Lak, 2 Shepp-Logan): h0[2C-1] + row factors[C]
   DBuf<float> fbp_g, fbp_q, fbp_sino, fbp_img;
 };
 
@@ -506,54 +506,48 @@ int vct_mbfpa(vct_ctx* c, double sigma, uint64_t seed, float* out, float* stats3
 }
 
 // --------------------------------------------------------------------- FBP
-// prepareConstMap, FBP/filterSinogramTOMO.cpp:9-123, in double on the host,
-// stored as float for the device filter.
+// prepareConstMap, FBP/filterSinogramTOMO.cpp:9-123, in double on the host.
+// Every row is the kernel h0(m-k); rows m <= 20 and m >= C-20 are scaled by
+// sum[21]/sum[m] (:114-123).  Stored for the device as float
+// [h0(-(C-1)) .. h0(C-1)] followed by the C row factors.
 static int build_filter(vct_ctx* c, int filter) {
   if (c->fbp_h[filter].p) return VCT_OK;
   const int C = c->dg.C;
   const int half = (C - 1) / 2;
   const double arc = c->geo.max_beta / half;
-  std::vector<double> h((size_t)C * C), sum(C, 0.0);
-  for (int m = 0; m < C; m++) {
-    for (int n = 0; n < C; n++) {
-      int MN = m - n;
-      double v = 0.0;
-      if (m == n) {
-        if (filter == 1) v = 0.125 / (arc * arc);
-        else {
-          double oddterm = kPI * kPI * (arc);
-          v = 0.25 / oddterm * (1.0 / tan((0.5) * arc) - 1.0 / tan((-0.5) * arc));
-        }
-      } else if (MN % 2 != 0) {
-        if (filter == 1) {
-          double oddterm = kPI * sin(MN * arc);
-          v = -0.5 / oddterm / oddterm;
-        } else {
-          double oddterm = kPI * kPI * arc;
-          v = 0.25 / oddterm * (1.0 / tan((MN + 0.5) * arc) - 1.0 / tan((MN - 0.5) * arc));
-        }
-      } else {
-        if (filter == 1) v = 0.0;
-        else {
-          double oddterm = kPI * kPI * arc;
-          v = 0.25 / oddterm * (1.0 / tan((MN + 0.5) * arc) - 1.0 / tan((MN - 0.5) * arc));
-        }
+  auto kernel = [&](int MN) -> double {
+    if (MN == 0) {
+      if (filter == 1) return 0.125 / (arc * arc);
+      double oddterm = kPI * kPI * (arc);
+      return 0.25 / oddterm * (1.0 / tan((0.5) * arc) - 1.0 / tan((-0.5) * arc));
+    }
+    if (MN % 2 != 0) {
+      if (filter == 1) {
+        double oddterm = kPI * sin(MN * arc);
+        return -0.5 / oddterm / oddterm;
       }
-      h[(size_t)m * C + n] = v;
-      sum[m] += v;
+      double oddterm = kPI * kPI * arc;
+      return 0.25 / oddterm * (1.0 / tan((MN + 0.5) * arc) - 1.0 / tan((MN - 0.5) * arc));
     }
-  }
-  std::vector<float> hf((size_t)C * C);
-  const int r21 = C > 21 ? 21 : C - 1;
+    if (filter == 1) return 0.0;
+    double oddterm = kPI * kPI * arc;
+    return 0.25 / oddterm * (1.0 / tan((MN + 0.5) * arc) - 1.0 / tan((MN - 0.5) * arc));
+  };
+  std::vector<double> h0(2 * C - 1), sum(C, 0.0);
+  for (int d = -(C - 1); d <= C - 1; d++) h0[d + C - 1] = kernel(d);
   for (int m = 0; m < C; m++)
-    for (int n = 0; n < C; n++) {
-      double v = h[(size_t)m * C + n];
-      if ((0 <= m && m <= 20) || (C - 20 <= m && m <= C)) v = v * sum[r21] / sum[m];
-      hf[(size_t)m * C + n] = (float)v;
-    }
-  int rc = c->fbp_h[filter].ensure((size_t)C * C);
+    for (int n = 0; n < C; n++) sum[m] += h0[(m - n) + C - 1];  // row sums in n order, as :35-108
+  std::vector<float> buf(3 * C - 1);
+  for (int i = 0; i < 2 * C - 1; i++) buf[i] = (float)h0[i];
+  const int r21 = C > 21 ? 21 : C - 1;
+  for (int m = 0; m < C; m++) {
+    double f = 1.0;
+    if ((0 <= m && m <= 20) || (C - 20 <= m && m <= C)) f = sum[r21] / sum[m];
+    buf[2 * C - 1 + m] = (float)f;
+  }
+  int rc = c->fbp_h[filter].ensure(buf.size());
   if (rc) return rc;
-  VCT_CUDA(cudaMemcpy(c->fbp_h[filter].p, hf.data(), hf.size() * sizeof(float), cudaMemcpyHostToDevice));
+  VCT_CUDA(cudaMemcpy(c->fbp_h[filter].p, buf.data(), buf.size() * sizeof(float), cudaMemcpyHostToDevice));
   return VCT_OK;
 }
 
@@ -568,7 +562,8 @@ int vct_fbp_dev(vct_ctx* c, const float* d_sino, int filter, int in_mode, float*
   if ((rc = launch_fbp_weight(d_sino, V, c->geo.width, c->geo.start_channel, C, c->fbp_coeff.p, c->fbp_g.p,
                               c->stream)))
     return rc;
-  if ((rc = launch_fbp_filter(c->fbp_g.p, c->fbp_h[filter].p, V, C, in_mode, c->fbp_q.p, c->stream)))
+  if ((rc = launch_fbp_filter(c->fbp_g.p, c->fbp_h[filter].p, c->fbp_h[filter].p + 2 * C - 1, V, C, in_mode,
+                              c->fbp_q.p, c->stream)))
     return rc;
   if ((rc = launch_fbp_backproject(c->fbp_q.p, V, C, c->dg.N, c->geo.pixel_cm, c->geo.sid_cm, c->geo.max_beta,
                                    c->geo.xfactor, c->cs_f.p, d_img, c->stream)))

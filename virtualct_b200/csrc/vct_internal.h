@@ -67,8 +67,8 @@ int launch_normalize_noise(const DevGeom& g, const float* d_in, float* d_out, co
                            int pad_zero, double sigma, uint64_t seed, cudaStream_t st);
 int launch_fbp_weight(const float* d_sino, int V, int W, int start, int C, const double* d_coeff,
                       float* d_g, cudaStream_t st);
-int launch_fbp_filter(const float* d_g, const float* d_h, int V, int C, int in_mode, float* d_q,
-                      cudaStream_t st);
+int launch_fbp_filter(const float* d_g, const float* d_h0, const float* d_cm, int V, int C, int in_mode,
+                      float* d_q, cudaStream_t st);
 int launch_fbp_backproject(const float* d_q, int V, int C, int N, double pixel_cm, double sid,
                            double max_beta, int xfactor, const float* d_cs, float* d_img,
                            cudaStream_t st);

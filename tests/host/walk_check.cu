@@ -28,7 +28,8 @@ int main(int argc, char** argv) {
   fclose(f);
   // Padded layout of pack_maps_kernel: row/column -1 repeats 0, the rest of
   // the border is 0.
-  std::vector<PixelRec> packed(padded_pixels(N));
+  std::vector<PixelRec> packed(map_records(N));
+  const int P = N + 2 * kMapPad;
   for (int r = -kMapPad; r < N + kMapPad; r++)
     for (int c = -kMapPad; c < N + kMapPad; c++) {
       const bool inside = r >= -1 && c >= -1 && r < N && c < N;
@@ -38,6 +39,7 @@ int main(int argc, char** argv) {
         int16_t v = (inside && m < M) ? maps[m * (size_t)N * N + src] : 0;
         rec.m[m] = v < 0 ? 0 : v;
       }
+      packed[(size_t)P * P + (size_t)(c + kMapPad) * P + (r + kMapPad)] = rec;  // transposed copy
     }
   // Geometry exactly as vct_create derives it (defaults of physParamsTOMO.h).
   DevGeom dg;

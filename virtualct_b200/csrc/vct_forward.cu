@@ -36,9 +36,23 @@ namespace vct {
 constexpr int kPad = kMapPad;
 VCT_HD int pad_index(int col, int row, int N) { return (col + kPad) + (row + kPad) * (N + 2 * kPad); }
 
+// Resident blocks per SM the register allocation is held to, and the number
+// of walk segments whose gathers are issued together (chosen by measurement).
+#ifndef VCT_FWD_MINBLOCKS
+#define VCT_FWD_MINBLOCKS 0
+#endif
+#ifndef VCT_FWD_UNROLL
+#define VCT_FWD_UNROLL 4
+#endif
+// 1: a transposed copy of the padded map follows the row-major one; walks
+// with x as the major axis read it.
+#ifndef VCT_FWD_DUAL_LAYOUT
+#define VCT_FWD_DUAL_LAYOUT 1
+#endif
+
 // ---------------------------------------------------------------- map packing
 __global__ void pack_maps_kernel(const int16_t* __restrict__ maps, int M, int N,
-                                 PixelRec* __restrict__ out) {
+                                 PixelRec* __restrict__ out, PixelRec* __restrict__ out_t) {
   const int P = N + 2 * kPad;
   const int p = blockIdx.x * blockDim.x + threadIdx.x;
   if (p >= P * P) return;
@@ -53,23 +67,20 @@ __global__ void pack_maps_kernel(const int16_t* __restrict__ maps, int M, int N,
     rec.m[m] = v < 0 ? (int16_t)0 : v;  // negative densities weigh 0 (:151-155)
   }
   out[p] = rec;
+  // Transposed copy (column-major): walks whose major axis is x step along
+  // a column of it, so a warp's rays read neighbouring records.
+  if (out_t) out_t[(c + kPad) * P + (r + kPad)] = rec;
 }
 
 int launch_pack_maps(const int16_t* d_maps, int M, int N, PixelRec* d_packed, cudaStream_t st) {
   const int P = N + 2 * kPad;
-  pack_maps_kernel<<<(P * P + 255) / 256, 256, 0, st>>>(d_maps, M, N, d_packed);
+  PixelRec* d_t = VCT_FWD_DUAL_LAYOUT ? d_packed + padded_pixels(N) : nullptr;
+  pack_maps_kernel<<<(P * P + 255) / 256, 256, 0, st>>>(d_maps, M, N, d_packed, d_t);
   VCT_CUDA(cudaGetLastError());
   return VCT_OK;
 }
 
-// Resident blocks per SM the register allocation is held to, and the number
-// of walk segments whose gathers are issued together (chosen by measurement).
-#ifndef VCT_FWD_MINBLOCKS
-#define VCT_FWD_MINBLOCKS 0
-#endif
-#ifndef VCT_FWD_UNROLL
-#define VCT_FWD_UNROLL 4
-#endif
+
 
 // ------------------------------------------------------------ host/device shims
 // The walks are __host__ __device__ so the same code can run on the CPU
@@ -179,6 +190,17 @@ VCT_HD void emit(const DevGeom& g, const PixelRec* __restrict__ maps, double xb0
     }
     gather_add_exact<M>(maps, pad_index(xmc, ymc, g.N), rr, a);
   }
+}
+
+// The pixel (padded index, or -1 when rejected) and length of one segment
+// under the emit() rule, without the gather; for geometries where the rmax
+// test cannot fire.
+VCT_HD int segment_pixel(const DevGeom& g, double xb0, double yb0, double xb1, double yb1, double* rr) {
+  *rr = sqrt((xb0 - xb1) * (xb0 - xb1) + (yb0 - yb1) * (yb0 - yb1));
+  const int xmc = trunc_i32((xb0 + xb1) * 0.5 / g.s + g.nxm);
+  const int ymc = trunc_i32((-yb0 - yb1) * 0.5 / g.s + g.nxm);
+  if (xmc >= 0 && ymc >= 0 && xmc <= g.N - 1 && ymc <= g.N - 1) return pad_index(xmc, ymc, g.N);
+  return -1;
 }
 
 // -------------------------------------------------------------------- set-up
@@ -398,10 +420,22 @@ VCT_HD bool walk_fast(const DevGeom& g, const PixelRec* __restrict__ maps, const
   if (maj0 < -1 || maj0 > N || majK < -1 || majK > N || min0 < -1 || min0 > N || minK < -1 || minK > N)
     return false;
 
+  // The lumped first segment: resolved now, gathered after the loop, so the
+  // set-up values need not stay live through it.
+  double rr_first;
+  const int pix_lumped = xmaj ? segment_pixel(g, r.xi, r.yi, u0, w0, &rr_first)
+                              : segment_pixel(g, r.xi, r.yi, w0, u0, &rr_first);
   a.sec = s * sqrt(1.0 + Wb * Wb);
   const int P = N + 2 * kPad;
   int pix, dpix_maj, dpix_min;
-  if (xmaj) {
+  const PixelRec* __restrict__ mp = maps;
+  if (xmaj && VCT_FWD_DUAL_LAYOUT) {
+    // transposed copy: (col, row) at (col + kPad) * P + (row + kPad)
+    mp = maps + (size_t)P * P;
+    pix = (maj0 + kPad) * P + (min0 + kPad);
+    dpix_maj = (pha > 0 ? 1 : -1) * P;
+    dpix_min = -dirw;
+  } else if (xmaj) {
     pix = pad_index(maj0, min0, N);
     dpix_maj = pha > 0 ? 1 : -1;
     dpix_min = -dirw * P;
@@ -415,7 +449,7 @@ VCT_HD bool walk_fast(const DevGeom& g, const PixelRec* __restrict__ maps, const
   double tmaj = 1.0;
   double t = 0.0;
   const double tend = (double)K;
-  const int4* __restrict__ m4 = reinterpret_cast<const int4*>(maps);
+  const int4* __restrict__ m4 = reinterpret_cast<const int4*>(mp);
   unsigned long long acc[M];
 #pragma unroll
   for (int m = 0; m < M; m++) acc[m] = 0ull;
@@ -457,10 +491,7 @@ VCT_HD bool walk_fast(const DevGeom& g, const PixelRec* __restrict__ maps, const
 #pragma unroll
   for (int m = 0; m < M; m++) a.Lq[m] += acc[m];
   a.nseg += nseg;
-  // The lumped first segment, after the loop so its FP64 sums are not live
-  // during it.
-  if (xmaj) emit<M>(g, maps, r.xi, r.yi, u0, w0, a);
-  else emit<M>(g, maps, r.xi, r.yi, w0, u0, a);
+  if (pix_lumped >= 0) gather_add_exact<M>(maps, pix_lumped, rr_first, a);
   return true;
 }
 

@@ -352,7 +352,7 @@ int vct_set_maps_dev(vct_ctx* c, const int16_t* d_maps, int M) {
   if (rc) return rc;
   if (!d_maps || M < 1 || M > VCT_MAX_MATERIALS) return fail(VCT_E_ARG, "vct_set_maps: bad argument");
   if (c->spectrum_ready && M != c->M) return fail(VCT_E_ARG, "vct_set_maps: M differs from the spectrum's");
-  if ((rc = c->maps.ensure(padded_pixels(c->dg.N)))) return rc;
+  if ((rc = c->maps.ensure(map_records(c->dg.N)))) return rc;
   if ((rc = launch_pack_maps(d_maps, M, c->dg.N, c->maps.p, c->stream))) return rc;
   c->launches++;
   c->M = M;

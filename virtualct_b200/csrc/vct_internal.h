@@ -47,6 +47,9 @@ struct alignas(16) PixelRec {
 };
 constexpr int kMapPad = 2;
 inline size_t padded_pixels(int N) { return (size_t)(N + 2 * kMapPad) * (size_t)(N + 2 * kMapPad); }
+// The device map buffer holds the row-major padded grid followed by its
+// transposed copy.
+inline size_t map_records(int N) { return 2 * padded_pixels(N); }
 
 struct FwdStats {
   unsigned int max_bits;  // float bits of the maximum (values are >= 0)

@@ -156,6 +156,24 @@ int vct_normalize_noise_dev(vct_ctx* ctx, float* d_sino, double sigma, uint64_t 
  * sino: [views][width] transmission values p; img_out: [N][N]. */
 int vct_fbp(vct_ctx* ctx, const float* sino, int filter, int in_mode, float* img_out);
 int vct_fbp_dev(vct_ctx* ctx, const float* d_sino, int filter, int in_mode, float* d_img_out);
+/* FBP that allocates nothing (no counterpart in the reference).  For callers
+ * that cannot allocate device memory at the point where they reconstruct: a
+ * process whose device memory is owned by another allocator or a fixed
+ * budget, a real-time loop that must not wait on an allocation, library code
+ * that may not fail on one.  Same result as vct_fbp_dev, without a context:
+ * g gives the geometry, d_sino [views][width] and d_img [N][N] are the
+ * caller's device buffers on the current device, stream is a cudaStream_t
+ * (NULL: the legacy default stream); the call returns once the work is
+ * enqueued.  The intermediate buffers are static device arrays of libvct
+ * (about 8 MB, held on every GPU that loads the library until the process
+ * exits), limited to views <= 4096, channels <= 2048 (640 for the filter
+ * kernel, as vct_fbp) and views*channels <= 1048576; larger sizes return
+ * VCT_E_ARG.  The first call on a device looks up those arrays' device
+ * addresses for it; make it before any stream capture.  All calls share the
+ * arrays (each call rewrites every element it reads), so calls that overlap
+ * on the GPU -- on different streams, or from several threads -- race. */
+int vct_fbp_noalloc(const vct_geometry* g, const float* d_sino, int filter, int in_mode, float* d_img,
+                    void* stream);
 /* The filtered sinogram of the last vct_fbp* call, [views][C]. */
 int vct_fbp_filtered_dev(vct_ctx* ctx, const float** d_fltd);
 

@@ -47,7 +47,8 @@ EXPORTED_SYMBOLS = (
     "vct_geometry_default", "vct_strerror", "vct_last_error", "vct_create", "vct_destroy", "vct_set_stream",
     "vct_synchronize", "vct_attenuation_coefficient", "vct_set_maps", "vct_set_maps_dev", "vct_set_spectrum",
     "vct_set_sum_mode", "vct_set_walk_mode", "vct_forward", "vct_forward_dev", "vct_line_integrals_dev", "vct_mbfpa", "vct_mbfpa_dev",
-    "vct_normalize_noise_dev", "vct_fbp", "vct_fbp_dev", "vct_fbp_filtered_dev", "vct_last_segment_count",
+    "vct_normalize_noise_dev", "vct_fbp", "vct_fbp_dev", "vct_fbp_noalloc", "vct_fbp_filtered_dev",
+    "vct_last_segment_count",
     "vct_kernel_launches", "vct_version", "vct_philox4x32_10", "vct_probe_peaks",
     "vct_load_mb_config", "vct_load_fbp_config", "vct_mb_geometry", "vct_fbp_geometry", "vct_read_raw",
     "vct_write_raw",
@@ -141,6 +142,7 @@ def lib():
     L.vct_fbp.argtypes = [vp, vp, C.c_int, C.c_int, vp]
     L.vct_fbp_dev.argtypes = [vp, vp, C.c_int, C.c_int, vp]
     L.vct_fbp_filtered_dev.argtypes = [vp, C.POINTER(vp)]
+    L.vct_fbp_noalloc.argtypes = [C.POINTER(_CGeometry), vp, C.c_int, C.c_int, vp, vp]
     L.vct_last_segment_count.argtypes = [vp, C.POINTER(C.c_longlong)]
     L.vct_kernel_launches.argtypes = [vp]
     L.vct_kernel_launches.restype = C.c_longlong

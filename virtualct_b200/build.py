@@ -33,6 +33,7 @@ CU_SOURCES = {
     "vct_forward.cu": ["--fmad=false"],
     "vct_fbp.cu": [],
     "vct_probe.cu": [],
+    "vct_fbp_noalloc.cu": [],
 }
 CPP_SOURCES = ["vct_host.cpp", "vct_io.cpp"]
 APPS = {"vct_mbfpa": "vct_mbfpa_main.cpp", "vct_fbp": "vct_fbp_main.cpp"}

@@ -177,6 +177,37 @@ int vct_fbp_noalloc(const vct_geometry* g, const float* d_sino, int filter, int 
 /* The filtered sinogram of the last vct_fbp* call, [views][C]. */
 int vct_fbp_filtered_dev(vct_ctx* ctx, const float** d_fltd);
 
+/* ---------------------------------------------------------------- adjoint
+ * No counterpart in the reference (it has no gradient).  The model is the
+ * forward of vct_forward: line integrals L = A rho of the reference walk
+ * (A linear in the densities rho_m = maps_m / 1000, g/cm^3) and the
+ * polyenergetic intensity y = sum_E pdf exp(-sum_m mu_m(E) L_m / xfactor).
+ * The loss is the weighted log least squares of MB/main.cpp:125-126 with
+ * y / ynorm (ynorm = sum_E pdf, the un-attenuated intensity) as the
+ * normalised reprojection:
+ *     l = 1/2 sum_i w_i (ln(y_i / ynorm) - ln p_i)^2
+ * over rays (v < views/2*2, start_channel <= c < end_channel) with p_i > 0;
+ * w_i = p_i when weights is NULL.  grad receives dl/drho_m, [M][N][N]
+ * float, per g/cm^3 (divide by 1000 for per map unit).  A^T is the exact
+ * transpose of the walk (its lumped first segment and folded border cells
+ * included), computed pixel by pixel with no atomics; the result does not
+ * depend on scheduling.  Uses the maps and spectrum set on the context.
+ * Requires det_src_iso_cm == sid_cm (a fan centred on the source, as the
+ * reference's geometry) and returns VCT_E_UNSUPPORTED otherwise.  The first
+ * adjoint call of a context plans every ray once and waits for it.
+ * meas, weights: [views][width]; loss (optional): FP64. */
+int vct_forward_adjoint(vct_ctx* ctx, const float* meas, const float* weights, float* grad, double* loss);
+/* Device buffers; d_loss (optional) is a device double; nothing waits. */
+int vct_forward_adjoint_dev(vct_ctx* ctx, const float* d_meas, const float* d_weights, float* d_grad,
+                            double* d_loss);
+/* Vector-Jacobian product of the normalised forward: given d_dy = dl/d(y/ynorm)
+ * [views][width], d_grad = dl/drho_m [M][N][N]. */
+int vct_forward_vjp_dev(vct_ctx* ctx, const float* d_dy, float* d_grad);
+/* A^T alone: d_out[m][pix] = sum_rays d_g[ray][m] * len(ray, pix) for
+ * per-ray, per-element weights d_g [views/2*2][end-start][M] (float), M the
+ * maps' element count; the transpose of vct_line_integrals_dev. */
+int vct_adjoint_rays_dev(vct_ctx* ctx, const float* d_g, float* d_out);
+
 /* ------------------------------------------------------------ inspection */
 /* Number of in-grid walk segments of the last forward (the algorithmic work
  * unit of the forward kernel). */

@@ -91,6 +91,12 @@ def lib():
         L.orc_forward_fp64_maps.argtypes = [C.POINTER(OrcGeom), _dp, _dp,
                                             np.ctypeslib.ndpointer(dtype=np.int16, flags="C_CONTIGUOUS"), C.c_int,
                                             _fp, _fp, C.c_int, _dp, C.c_void_p, C.c_int]
+        L.orc_siddon.argtypes = [C.POINTER(OrcGeom), C.c_double, C.c_double, C.c_int, _dp, _ip, C.c_int]
+        L.orc_siddon.restype = C.c_int
+        L.orc_walk_project.argtypes = [C.POINTER(OrcGeom), _dp, _dp, _dp, C.c_int, _dp, C.c_int]
+        L.orc_walk_backproject.argtypes = [C.POINTER(OrcGeom), _dp, _dp, _dp, C.c_int, _dp, C.c_int]
+        L.orc_walk_project_rays.argtypes = [C.POINTER(OrcGeom), _dp, _dp, _dp, C.c_int, _ip, C.c_int, _dp, C.c_int]
+        L.orc_siddon_project.argtypes = [C.POINTER(OrcGeom), _dp, _dp, _dp, C.c_int, _dp, C.c_int]
         L.orc_normalize_noise.argtypes = [_fp, C.c_int, C.c_double, C.c_uint, C.c_int]
         L.orc_normalize_noise.restype = C.c_double
         L.orc_fbp_constmap.argtypes = [C.POINTER(OrcGeom), C.c_int, _dp]
@@ -184,6 +190,139 @@ def forward_fp64_maps(g, cos_t, sin_t, maps, mu, pdf, nthreads=0, want_lint=Fals
                                 np.ascontiguousarray(pdf, np.float32), NE, out,
                                 lint.ctypes.data if want_lint else None, nthreads)
     return (out, lint) if want_lint else out
+
+
+def siddon(g, cosb, sinb, jj):
+    cap = 4 * g.recon_size + 64
+    ln = np.zeros(cap, np.float64)
+    px = np.zeros(cap, np.int32)
+    n = lib().orc_siddon(C.byref(g), cosb, sinb, jj, ln, px, cap)
+    return ln[:n].copy(), px[:n].copy()
+
+
+def walk_project(g, cos_t, sin_t, rho):
+    """A rho: the reference walk's line integrals of FP64 densities rho
+    (double [M][N][N], g/cm^3) -> double [views][width][M] (cm * g/cm^3)."""
+    rho = np.ascontiguousarray(rho, np.float64)
+    M = rho.shape[0]
+    out = np.zeros((g.views, g.width, M), np.float64)
+    lib().orc_walk_project(C.byref(g), cos_t, sin_t, rho, M, out, 0)
+    return out
+
+
+def walk_backproject(g, cos_t, sin_t, w):
+    """A^T w for per-ray, per-element weights w (double [views][width][M])."""
+    w = np.ascontiguousarray(w, np.float64)
+    M = w.shape[2]
+    N = g.recon_size
+    out = np.zeros((M, N, N), np.float64)
+    lib().orc_walk_backproject(C.byref(g), cos_t, sin_t, w, M, out, 0)
+    return out
+
+
+def walk_project_rays(g, cos_t, sin_t, rho, rays):
+    """A rho on the rays listed (view * width + channel) -> [len(rays)][M]."""
+    rho = np.ascontiguousarray(rho, np.float64)
+    rays = np.ascontiguousarray(rays, np.int32)
+    M = rho.shape[0]
+    out = np.zeros((len(rays), M), np.float64)
+    lib().orc_walk_project_rays(C.byref(g), cos_t, sin_t, rho, M, rays, len(rays), out, 0)
+    return out
+
+
+def rays_near_pixel(g, cos_t, sin_t, col, row, margin_px=3.0):
+    """Every ray (view * width + channel) whose line passes within margin_px
+    pixels of the centre of pixel (col, row): a superset of the rays whose
+    walk can put a segment on that pixel (its lumped and folded border pieces
+    lie within one pixel of the ray)."""
+    N, s = g.recon_size, g.pixel_cm
+    n = int(N * 0.5)
+    cx, cy = (col - n + 0.5) * s, (n - row - 0.5) * s
+    half = (g.end_channel - g.start_channel - 1) // 2
+    jj = np.arange(g.start_channel, g.end_channel)
+    theta = (g.iso_channel - jj) * g.max_alpha / half
+    px0 = g.det_radius * np.sin(theta)
+    py0 = -g.det_radius * np.cos(theta) + g.det_src_iso
+    out = []
+    for v in range(g.views // 2 * 2):
+        cb, sb = cos_t[v], sin_t[v]
+        sx, sy = g.sid * sb, g.sid * cb
+        px, py = px0 * cb + py0 * sb, -px0 * sb + py0 * cb
+        dx, dy = px - sx, py - sy
+        d = np.abs(dx * (cy - sy) - dy * (cx - sx)) / np.hypot(dx, dy)
+        out.extend((v * g.width + jj[d <= margin_px * s]).tolist())
+    return np.asarray(out, np.int32)
+
+
+def loss_terms(L, mu, pdf, meas_r, wts_r, xfactor, ynorm):
+    """Per-ray loss 1/2 w (ln(y/ynorm) - ln p)^2 (0 where p <= 0)."""
+    y, _ = spectral(L, mu, pdf, xfactor)
+    p = np.asarray(meas_r, np.float64)
+    w = p if wts_r is None else np.asarray(wts_r, np.float64)
+    ok = p > 0
+    with np.errstate(divide="ignore", invalid="ignore"):
+        r = np.where(ok, np.log(y / ynorm) - np.log(np.where(ok, p, 1.0)), 0.0)
+    return np.where(ok, 0.5 * w * r * r, 0.0)
+
+
+def fd_pixel(g, cos_t, sin_t, rho, m, col, row, h, mu, pdf, meas, weights=None):
+    """Central difference (l(rho + h e) - l(rho - h e)) / 2h of the FP64 walk
+    loss for element m at pixel (col, row); rays that cannot touch the pixel
+    cancel exactly and are left out of both sums."""
+    rays = rays_near_pixel(g, cos_t, sin_t, col, row)
+    ynorm = float(np.asarray(pdf, np.float32).astype(np.float64).sum())
+    mr = np.asarray(meas, np.float32).reshape(-1)[rays]
+    wr = None if weights is None else np.asarray(weights, np.float32).reshape(-1)[rays]
+    tot = []
+    for sgn in (1.0, -1.0):
+        r2 = np.array(rho, np.float64, copy=True)
+        r2[m, row, col] += sgn * h
+        L = walk_project_rays(g, cos_t, sin_t, r2, rays)
+        tot.append(loss_terms(L, mu, pdf, mr, wr, g.xfactor, ynorm).sum())
+    return (tot[0] - tot[1]) / (2.0 * h)
+
+
+def spectral(L, mu, pdf, xfactor=1.0):
+    """Polyenergetic intensity y = sum_E pdf exp(-sum_m mu_mE L_m / xfactor) and
+    its derivative dy/dL_m = -D_m, both FP64; L: [..., M], mu: [M][NE]."""
+    mu = np.asarray(mu, np.float64) / float(xfactor)
+    pdf = np.asarray(pdf, np.float64)
+    e = pdf * np.exp(-(L @ mu))            # [..., NE]
+    y = e.sum(-1)
+    D = e @ mu.T                           # [..., M]
+    return y, D
+
+
+def loss_grad(g, cos_t, sin_t, rho, mu, pdf, meas, weights=None, want_grad=True):
+    """FP64 weighted log least squares of the walk model (the loss of
+    MB/main.cpp:125-126 with y/sum(pdf) in place of the max-normalised
+    reprojection): l = 1/2 sum_i w_i (ln(y_i/ynorm) - ln p_i)^2 over rays with
+    p_i > 0, w_i = p_i unless weights are given; returns (l, dl/drho)."""
+    L = walk_project(g, cos_t, sin_t, rho)
+    pdf = np.asarray(pdf, np.float64)
+    ynorm = float(np.asarray(pdf, np.float32).astype(np.float64).sum())
+    y, D = spectral(L, mu, pdf, g.xfactor)
+    p = np.asarray(meas, np.float64)
+    wt = p if weights is None else np.asarray(weights, np.float64)
+    valid = np.zeros(p.shape, bool)
+    nv = g.views // 2 * 2
+    valid[:nv, g.start_channel:g.end_channel] = True
+    valid &= p > 0
+    with np.errstate(divide="ignore", invalid="ignore"):
+        r = np.where(valid, np.log(y / ynorm) - np.log(np.where(valid, p, 1.0)), 0.0)
+    loss = 0.5 * float(np.sum(np.where(valid, wt * r * r, 0.0)))
+    if not want_grad:
+        return loss
+    w = np.where(valid[..., None], -(wt * r / y)[..., None] * D, 0.0)
+    return loss, walk_backproject(g, cos_t, sin_t, w)
+
+
+def siddon_project(g, cos_t, sin_t, x):
+    x = np.ascontiguousarray(x, np.float64)
+    M = x.shape[0]
+    out = np.zeros((g.views, g.width, M), np.float64)
+    lib().orc_siddon_project(C.byref(g), cos_t, sin_t, x, M, out, 0)
+    return out
 
 
 def normalize_noise(sino, sigma, seed=1, order=0):

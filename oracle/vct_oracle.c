@@ -598,3 +598,226 @@ void orc_fbp_backproject(const orc_geom* g, const float* fltd, const double* cos
   }
   free(mask);
 }
+
+
+/* ---------------------------------------------------------------- adjoint */
+static void orc_ray_points(const orc_geom* g, double cb, double sb, int jj, double* sx, double* sy,
+                           double* px, double* py) {
+  const int half = (g->end_channel - g->start_channel - 1) / 2;
+  double theta = (g->iso_channel - jj) * g->max_alpha / half;
+  double px0 = g->det_radius * sin(theta);
+  double py0 = -g->det_radius * cos(theta) + g->det_src_iso;
+  *sx = g->sid * sb;
+  *sy = g->sid * cb;
+  *px = +px0 * cb + py0 * sb;
+  *py = -px0 * sb + py0 * cb;
+}
+
+static int orc_cmp_double(const void* a, const void* b) {
+  double x = *(const double*)a, y = *(const double*)b;
+  return x < y ? -1 : x > y;
+}
+
+int orc_siddon(const orc_geom* g, double cb, double sb, int jj, double* seg_len, int* seg_pix, int cap) {
+  const int N = g->recon_size;
+  const double s = g->pixel_cm;
+  const double n = (double)(int)(N * 0.5);
+  double sx, sy, px, py;
+  orc_ray_points(g, cb, sb, jj, &sx, &sy, &px, &py);
+  const double dx = px - sx, dy = py - sy;
+  const double len = sqrt(dx * dx + dy * dy);
+  const double lo = -n * s, hi = (N - n) * s;
+  /* Clip the line (parameter t along S->P) to the grid square. */
+  double t0 = -1e300, t1 = 1e300;
+  if (dx != 0) {
+    double a = (lo - sx) / dx, b = (hi - sx) / dx;
+    if (a > b) { double t = a; a = b; b = t; }
+    if (a > t0) t0 = a;
+    if (b < t1) t1 = b;
+  } else if (sx < lo || sx > hi) return 0;
+  if (dy != 0) {
+    double a = (lo - sy) / dy, b = (hi - sy) / dy;
+    if (a > b) { double t = a; a = b; b = t; }
+    if (a > t0) t0 = a;
+    if (b < t1) t1 = b;
+  } else if (sy < lo || sy > hi) return 0;
+  if (!(t1 > t0)) return 0;
+  /* All gridline crossings inside (t0, t1), sorted. */
+  int cnt = 0;
+  double* ts = (double*)malloc(sizeof(double) * (2 * N + 8));
+  ts[cnt++] = t0;
+  for (int k = 0; k <= N; k++) {
+    double gx = lo + k * s;
+    if (dx != 0) {
+      double t = (gx - sx) / dx;
+      if (t > t0 && t < t1) ts[cnt++] = t;
+    }
+    if (dy != 0) {
+      double t = (gx - sy) / dy;
+      if (t > t0 && t < t1) ts[cnt++] = t;
+    }
+  }
+  ts[cnt++] = t1;
+  qsort(ts, cnt, sizeof(double), orc_cmp_double);
+  int ns = 0;
+  for (int q = 0; q + 1 < cnt; q++) {
+    double ta = ts[q], tb = ts[q + 1];
+    if (!(tb > ta)) continue;
+    double tm = 0.5 * (ta + tb);
+    double xm = sx + tm * dx, ym = sy + tm * dy;
+    int col = (int)floor(xm / s + n), row = (int)floor(n - ym / s);
+    if (col < 0 || col >= N || row < 0 || row >= N) continue;
+    if (ns >= cap) { free(ts); return -1; }
+    seg_len[ns] = (tb - ta) * len;
+    seg_pix[ns] = col + row * N;
+    ns++;
+  }
+  free(ts);
+  return ns;
+}
+
+void orc_siddon_project(const orc_geom* g, const double* cos_t, const double* sin_t, const double* x, int M,
+                        double* out, int nthreads) {
+  const int V = g->views, W = g->width, N = g->recon_size;
+  const int nviews = V / 2 * 2;
+  const size_t n2 = (size_t)N * N;
+  const int cap = 4 * N + 64;
+  memset(out, 0, sizeof(double) * (size_t)V * W * M);
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel
+#endif
+  {
+    double* len = (double*)malloc(sizeof(double) * cap);
+    int* pix = (int*)malloc(sizeof(int) * cap);
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 4)
+#endif
+    for (int j = 0; j < nviews; j++)
+      for (int jj = g->start_channel; jj < g->end_channel; jj++) {
+        int ns = orc_siddon(g, cos_t[j], sin_t[j], jj, len, pix, cap);
+        double* o = out + ((size_t)j * W + jj) * M;
+        for (int q = 0; q < ns; q++)
+          for (int m = 0; m < M; m++) o[m] += x[(size_t)m * n2 + pix[q]] * len[q];
+      }
+    free(len);
+    free(pix);
+  }
+}
+
+void orc_walk_project(const orc_geom* g, const double* cos_t, const double* sin_t, const double* rho, int M,
+                      double* out, int nthreads) {
+  const int V = g->views, W = g->width, N = g->recon_size;
+  const int nviews = V / 2 * 2;
+  const size_t n2 = (size_t)N * N;
+  const double rmax = N * 0.5 * 1.0;
+  const int cap = orc_seg_cap(g);
+  memset(out, 0, sizeof(double) * (size_t)V * W * M);
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel
+#endif
+  {
+    double* len = (double*)malloc(sizeof(double) * cap);
+    double* rad = (double*)malloc(sizeof(double) * cap);
+    int* pix = (int*)malloc(sizeof(int) * cap);
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 4)
+#endif
+    for (int j = 0; j < nviews; j++)
+      for (int jj = g->start_channel; jj < g->end_channel; jj++) {
+        int ns = orc_walk(g, cos_t[j], sin_t[j], jj, len, pix, rad, cap);
+        double* o = out + ((size_t)j * W + jj) * M;
+        for (int q = 0; q < ns; q++) {
+          if (rad[q] >= rmax) continue;
+          for (int m = 0; m < M; m++) o[m] += rho[(size_t)m * n2 + pix[q]] * len[q];
+        }
+      }
+    free(len);
+    free(rad);
+    free(pix);
+  }
+}
+
+/* Views are split statically over the threads; each thread scatters into its
+ * own image and the images are summed in thread order, so the result does not
+ * depend on scheduling. */
+void orc_walk_backproject(const orc_geom* g, const double* cos_t, const double* sin_t, const double* w, int M,
+                          double* out, int nthreads) {
+  const int V = g->views, W = g->width, N = g->recon_size;
+  const int nviews = V / 2 * 2;
+  const size_t n2 = (size_t)N * N;
+  const double rmax = N * 0.5 * 1.0;
+  const int cap = orc_seg_cap(g);
+  int nt = 1;
+#ifdef _OPENMP
+  nt = nthreads > 0 ? nthreads : omp_get_max_threads();
+#endif
+  double* part = (double*)calloc((size_t)nt * M * n2, sizeof(double));
+#ifdef _OPENMP
+#pragma omp parallel num_threads(nt)
+#endif
+  {
+    int tid = 0;
+#ifdef _OPENMP
+    tid = omp_get_thread_num();
+#endif
+    double* img = part + (size_t)tid * M * n2;
+    double* len = (double*)malloc(sizeof(double) * cap);
+    double* rad = (double*)malloc(sizeof(double) * cap);
+    int* pix = (int*)malloc(sizeof(int) * cap);
+    const int per = (nviews + nt - 1) / nt;
+    for (int j = tid * per; j < nviews && j < (tid + 1) * per; j++)
+      for (int jj = g->start_channel; jj < g->end_channel; jj++) {
+        const double* wr = w + ((size_t)j * W + jj) * M;
+        int any = 0;
+        for (int m = 0; m < M; m++) any |= wr[m] != 0.0;
+        if (!any) continue;
+        int ns = orc_walk(g, cos_t[j], sin_t[j], jj, len, pix, rad, cap);
+        for (int q = 0; q < ns; q++) {
+          if (rad[q] >= rmax) continue;
+          for (int m = 0; m < M; m++) img[(size_t)m * n2 + pix[q]] += wr[m] * len[q];
+        }
+      }
+    free(len);
+    free(rad);
+    free(pix);
+  }
+  memset(out, 0, sizeof(double) * M * n2);
+  for (int t = 0; t < nt; t++)
+    for (size_t i = 0; i < (size_t)M * n2; i++) out[i] += part[(size_t)t * M * n2 + i];
+  free(part);
+}
+
+void orc_walk_project_rays(const orc_geom* g, const double* cos_t, const double* sin_t, const double* rho, int M,
+                           const int* rays, int nrays, double* out, int nthreads) {
+  const int W = g->width, N = g->recon_size;
+  const size_t n2 = (size_t)N * N;
+  const double rmax = N * 0.5 * 1.0;
+  const int cap = orc_seg_cap(g);
+  memset(out, 0, sizeof(double) * (size_t)nrays * M);
+#ifdef _OPENMP
+  if (nthreads > 0) omp_set_num_threads(nthreads);
+#pragma omp parallel
+#endif
+  {
+    double* len = (double*)malloc(sizeof(double) * cap);
+    double* rad = (double*)malloc(sizeof(double) * cap);
+    int* pix = (int*)malloc(sizeof(int) * cap);
+#ifdef _OPENMP
+#pragma omp for schedule(dynamic, 64)
+#endif
+    for (int i = 0; i < nrays; i++) {
+      const int j = rays[i] / W, jj = rays[i] % W;
+      int ns = orc_walk(g, cos_t[j], sin_t[j], jj, len, pix, rad, cap);
+      double* o = out + (size_t)i * M;
+      for (int q = 0; q < ns; q++) {
+        if (rad[q] >= rmax) continue;
+        for (int m = 0; m < M; m++) o[m] += rho[(size_t)m * n2 + pix[q]] * len[q];
+      }
+    }
+    free(len);
+    free(rad);
+    free(pix);
+  }
+}

@@ -86,6 +86,32 @@ void orc_forward_fp64_maps(const orc_geom* g, const double* cos_t, const double*
                            const short* maps, int M, const float* mu, const float* pdf, int NE,
                            double* full_out, double* lint_out, int nthreads);
 
+/* ---- Adjoint support (no counterpart in the reference; FP64, test-only) ----
+ * Exact intersection of the reference's ray (view cos/sin, channel jj; source
+ * and detector as MB/reprojection_TOMO.cpp:53-74) with the N x N grid: every
+ * pixel the line crosses with its true chord length (cm), in walk order.
+ * Pixel index convention as the reference: col = floor(x/s + N/2),
+ * row = floor(N/2 - y/s).  Returns the count, -1 if cap is too small. */
+int orc_siddon(const orc_geom* g, double cosb, double sinb, int jj, double* seg_len, int* seg_pix, int cap);
+
+/* Exact-Siddon forward projection of per-material images x (double [M][N][N])
+ * to per-ray line integrals out (double [views][width][M]). */
+void orc_siddon_project(const orc_geom* g, const double* cos_t, const double* sin_t, const double* x, int M,
+                        double* out, int nthreads);
+
+/* The reference walk as a linear operator A on FP64 densities (no counterpart
+ * in the reference, which only walks int16 maps):
+ *   orc_walk_project:     out[j][jj][m] = sum_seg rho_m(pix) * len   (A rho)
+ *   orc_walk_backproject: out[m][pix]  = sum_rays w[j][jj][m] * len  (A^T w)
+ * Segments whose midpoint radius reaches rmax are dropped, as in the walk. */
+void orc_walk_project(const orc_geom* g, const double* cos_t, const double* sin_t, const double* rho, int M,
+                      double* out, int nthreads);
+/* A rho for a list of rays only (ray = view * width + channel); out [nrays][M]. */
+void orc_walk_project_rays(const orc_geom* g, const double* cos_t, const double* sin_t, const double* rho, int M,
+                           const int* rays, int nrays, double* out, int nthreads);
+void orc_walk_backproject(const orc_geom* g, const double* cos_t, const double* sin_t, const double* w, int M,
+                          double* out, int nthreads);
+
 /* Max-normalisation (MB/main.cpp:511-522) followed by gaussiannoise0
  * (MB/main.cpp:42-76) with glibc rand() after srand(seed) (the reference
  * never seeds: seed 1).  order selects which Uniform0() call in rand_gauss0

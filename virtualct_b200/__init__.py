@@ -48,6 +48,7 @@ EXPORTED_SYMBOLS = (
     "vct_synchronize", "vct_attenuation_coefficient", "vct_set_maps", "vct_set_maps_dev", "vct_set_spectrum",
     "vct_set_sum_mode", "vct_set_walk_mode", "vct_forward", "vct_forward_dev", "vct_line_integrals_dev", "vct_mbfpa", "vct_mbfpa_dev",
     "vct_normalize_noise_dev", "vct_fbp", "vct_fbp_dev", "vct_fbp_noalloc", "vct_fbp_filtered_dev",
+    "vct_forward_adjoint", "vct_forward_adjoint_dev", "vct_forward_vjp_dev", "vct_adjoint_rays_dev",
     "vct_last_segment_count",
     "vct_kernel_launches", "vct_version", "vct_philox4x32_10", "vct_probe_peaks",
     "vct_load_mb_config", "vct_load_fbp_config", "vct_mb_geometry", "vct_fbp_geometry", "vct_read_raw",
@@ -143,6 +144,10 @@ def lib():
     L.vct_fbp_dev.argtypes = [vp, vp, C.c_int, C.c_int, vp]
     L.vct_fbp_filtered_dev.argtypes = [vp, C.POINTER(vp)]
     L.vct_fbp_noalloc.argtypes = [C.POINTER(_CGeometry), vp, C.c_int, C.c_int, vp, vp]
+    L.vct_forward_adjoint.argtypes = [vp, vp, vp, vp, C.POINTER(C.c_double)]
+    L.vct_forward_adjoint_dev.argtypes = [vp, vp, vp, vp, vp]
+    L.vct_forward_vjp_dev.argtypes = [vp, vp, vp]
+    L.vct_adjoint_rays_dev.argtypes = [vp, vp, vp]
     L.vct_last_segment_count.argtypes = [vp, C.POINTER(C.c_longlong)]
     L.vct_kernel_launches.argtypes = [vp]
     L.vct_kernel_launches.restype = C.c_longlong
@@ -201,6 +206,7 @@ class Context:
         self._h = C.c_void_p()
         _check(lib().vct_create(C.byref(self._g), device, C.byref(self._h)), "vct_create")
         self.device = device
+        self._M = 0
 
     # lifetime ---------------------------------------------------------------
     def close(self) -> None:
@@ -247,12 +253,14 @@ class Context:
         if hasattr(maps, "data_ptr"):
             M = int(maps.shape[0])
             _check(lib().vct_set_maps_dev(self._h, maps.data_ptr(), M), "vct_set_maps_dev")
+            self._M = M
             return
         a = np.ascontiguousarray(maps, np.int16)
         N = self.geometry.recon_size
         if a.ndim != 3 or a.shape[1:] != (N, N):
             raise ValueError(f"maps must be [M][{N}][{N}] int16, got {a.shape}")
         _check(lib().vct_set_maps(self._h, _ptr(a), a.shape[0]), "vct_set_maps")
+        self._M = a.shape[0]
 
     def set_spectrum(self, mu, pdf) -> None:
         mu = np.ascontiguousarray(mu, np.float32)
@@ -296,6 +304,32 @@ class Context:
     def normalize_noise_dev(self, sino, sigma: float, seed: int) -> None:
         _check(lib().vct_normalize_noise_dev(self._h, sino.data_ptr(), float(sigma), int(seed)),
                "vct_normalize_noise_dev")
+
+    # Adjoint -----------------------------------------------------------------
+    def forward_adjoint(self, meas, weights=None):
+        """Loss 1/2 sum w (ln(y/ynorm) - ln p)^2 and its gradient w.r.t. the
+        element densities (g/cm^3), [M][N][N]; meas (and weights) [views][width]."""
+        g = self.geometry
+        m = np.ascontiguousarray(meas, np.float32)
+        if m.shape != (g.views, g.width):
+            raise ValueError(f"measured sinogram must be [{g.views}][{g.width}]")
+        w = None if weights is None else np.ascontiguousarray(weights, np.float32)
+        grad = np.zeros((self._M, g.recon_size, g.recon_size), np.float32)
+        loss = C.c_double()
+        _check(lib().vct_forward_adjoint(self._h, _ptr(m), None if w is None else _ptr(w), _ptr(grad),
+                                         C.byref(loss)), "vct_forward_adjoint")
+        return loss.value, grad
+
+    def forward_adjoint_dev(self, meas, grad, weights=None, loss=None) -> None:
+        _check(lib().vct_forward_adjoint_dev(self._h, meas.data_ptr(), None if weights is None else weights.data_ptr(),
+                                             grad.data_ptr(), None if loss is None else loss.data_ptr()),
+               "vct_forward_adjoint_dev")
+
+    def forward_vjp_dev(self, dy, grad) -> None:
+        _check(lib().vct_forward_vjp_dev(self._h, dy.data_ptr(), grad.data_ptr()), "vct_forward_vjp_dev")
+
+    def adjoint_rays_dev(self, g, out) -> None:
+        _check(lib().vct_adjoint_rays_dev(self._h, g.data_ptr(), out.data_ptr()), "vct_adjoint_rays_dev")
 
     # FBP ---------------------------------------------------------------------
     def fbp(self, sino, filter: int = 1, in_mode: bool = False) -> np.ndarray:

@@ -26,18 +26,20 @@ LIB = os.path.join(LIBDIR, "libvct.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", INC, "-I", CSRC]
 
-# Per-translation-unit flags.  The forward walk must not fuse a*b+c: the
-# reference (x86-64, -O2, no FMA) rounds every product and sum separately,
-# and the walk's segment boundaries depend on those roundings.
+# Per-translation-unit flags.  The walk (vct_walk.cuh, in the forward and the
+# adjoint) must not fuse a*b+c: the reference (x86-64, -O2, no FMA) rounds
+# every product and sum separately, and the walk's segment boundaries depend
+# on those roundings.
 CU_SOURCES = {
     "vct_forward.cu": ["--fmad=false"],
     "vct_fbp.cu": [],
     "vct_probe.cu": [],
     "vct_fbp_noalloc.cu": [],
+    "vct_adjoint.cu": ["--fmad=false"],
 }
 CPP_SOURCES = ["vct_host.cpp", "vct_io.cpp"]
 APPS = {"vct_mbfpa": "vct_mbfpa_main.cpp", "vct_fbp": "vct_fbp_main.cpp"}
-HEADERS = ["vct_internal.h", "vct_philox.h"]
+HEADERS = ["vct_internal.h", "vct_philox.h", "vct_walk.cuh", "vct_fastmath.cuh"]
 
 
 def nvcc() -> str:

@@ -14,6 +14,7 @@
 #include <cuda_runtime.h>
 
 #include "vct_internal.h"
+#include "vct_fastmath.cuh"
 
 namespace vct {
 
@@ -95,28 +96,6 @@ int launch_fbp_filter(const float* d_g, const float* d_h0, const float* d_cm, in
 }
 
 // ------------------------------------------------------------- backproject
-// atan(t) on |t| <= 0.5 as t*P(t^2), P of degree 5: a least-squares fit of
-// atan(t)/t on Chebyshev nodes in t^2 (made for this kernel); max error
-// 3.7e-8 rad in FP32.  Pixels inside the reconstruction circle see
-// |t| = |X/(SID-Y)| < 0.45 at the default geometry; larger |t| is outside
-// the fan and rejected by the channel test either way.
-__device__ __forceinline__ float atan_small(float t) {
-  const float u = t * t;
-  float p = -0.05077829957008362f;
-  p = fmaf(p, u, 0.10122803598642349f);
-  p = fmaf(p, u, -0.14165857434272766f);
-  p = fmaf(p, u, 0.19993248581886292f);
-  p = fmaf(p, u, -0.3333319127559662f);
-  p = fmaf(p, u, 1.0f);
-  return t * p;
-}
-
-__device__ __forceinline__ float rcp_approx(float x) {
-  float y;
-  asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
-  return y;
-}
-
 // Fractional channel of pixel (xx, yy) cm in the view with (cos, sin):
 // FBP/reconstructImageTOMO.cpp:67-72.
 __device__ __forceinline__ float bp_channel(float xx, float yy, float c, float s, float sid,

@@ -68,6 +68,7 @@ struct vct_ctx {
   DBuf<float> cs_f;  // (cos, sin) pairs in float for the backprojector
   // MBFPA
   int M = 0, NE = 0;
+  double ynorm = 0.0;  // sum of the pdf as uploaded (the un-attenuated intensity)
   int maps_ready = 0, spectrum_ready = 0;
   int sum_mode = VCT_SUM_COMPENSATED;
   int walk_mode = VCT_WALK_FAST;
@@ -84,6 +85,18 @@ struct vct_ctx {
   DBuf<double> fbp_coeff;  // SID*cos((k-cw)*dbeta)*dbeta
   DBuf<float> fbp_h[3];    // per filter (1 Ram-Lak, 2 Shepp-Logan): h0[2C-1] + row factors[C]
   DBuf<float> fbp_g, fbp_q, fbp_sino, fbp_img;
+  // Adjoint: per-ray walk plans (geometry only), ray factors, fixed-point
+  // accumulator of the exact-walk rays, loss partials.
+  int adj_ready = 0, adj_nspecial = 0, adj_tile = -1;
+  AdjGeom ag{};
+  DBuf<int4> adj_rec;
+  DBuf<int> adj_special, adj_ints;  // ints: [0] special count, [1] status
+  DBuf<double2> adj_dir;
+  DBuf<float> adj_g;
+  DBuf<double> adj_part, adj_loss;
+  DBuf<unsigned int> adj_gmax;
+  DBuf<unsigned long long> adj_sacc;
+  DBuf<float> adj_meas, adj_wts, adj_grad;
 };
 
 static int check_ctx(vct_ctx* c) {
@@ -237,6 +250,9 @@ void vct_destroy(vct_ctx* c) {
   c->fbp_coeff.release();
   for (auto& h : c->fbp_h) h.release();
   c->fbp_g.release(); c->fbp_q.release(); c->fbp_sino.release(); c->fbp_img.release();
+  c->adj_rec.release(); c->adj_special.release(); c->adj_ints.release(); c->adj_dir.release();
+  c->adj_g.release(); c->adj_part.release(); c->adj_loss.release(); c->adj_gmax.release();
+  c->adj_sacc.release(); c->adj_meas.release(); c->adj_wts.release(); c->adj_grad.release();
   if (c->h_stats) cudaFreeHost(c->h_stats);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
@@ -393,6 +409,8 @@ int vct_set_spectrum(vct_ctx* c, const float* mu, const float* pdf, int M, int N
   VCT_CUDA(cudaStreamSynchronize(c->stream));  // t is a host temporary
   c->M = M;
   c->NE = NE;
+  c->ynorm = 0.0;
+  for (int e = 0; e < NE; e++) c->ynorm += (double)pdf[e];
   c->spectrum_ready = 1;
   return VCT_OK;
 }
@@ -599,6 +617,163 @@ void vct_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t ou
   for (int i = 0; i < 4; i++) c.v[i] = ctr[i];
   Philox4 r = philox4x32_10(c, key[0], key[1]);
   for (int i = 0; i < 4; i++) out[i] = r.v[i];
+}
+
+}  // extern "C"
+
+// ----------------------------------------------------------------- adjoint
+// Plans every ray once per context (geometry only) and reads back how many
+// rays need the exact walk, which sizes the fixed-point scatter.
+static int adj_prepare(vct_ctx* c) {
+  if (c->adj_ready) return VCT_OK;
+  const vct_geometry& g = c->geo;
+  if (fabs(g.det_src_iso_cm - g.sid_cm) > 1e-9)
+    return fail(VCT_E_UNSUPPORTED, "adjoint: needs det_src_iso_cm == sid_cm (fan centred on the source)");
+  const DevGeom& dg = c->dg;
+  const int C = dg.C, half = (C - 1) / 2;
+  const long long nrays = (long long)dg.views_used * C;
+  AdjGeom& a = c->ag;
+  a.N = dg.N;
+  a.nxm = dg.nxm;
+  a.C = C;
+  a.start = dg.start;
+  a.views_used = dg.views_used;
+  a.s = dg.s;
+  a.sid = g.sid_cm;
+  a.iso = g.iso_channel;
+  a.inv_dalpha = half / g.max_alpha;
+  a.lmax = 2.0 * sqrt(2.0) * dg.lim + 4.0 * dg.s;
+  c->adj_tile = adj_pick_tile(a, dg.lim);
+  if (c->adj_tile < 0) return fail(VCT_E_UNSUPPORTED, "adjoint: pixel too large for the channel window");
+  // Unit direction of every channel's ray before rotation (detector point
+  // minus source, MB/reprojection_TOMO.cpp:61-71).
+  std::vector<double2> dir(C);
+  for (int c0 = 0; c0 < C; c0++) {
+    const int jj = g.start_channel + c0;
+    const double theta = (g.iso_channel - jj) * g.max_alpha / half;
+    const double ex = g.det_radius_cm * sin(theta);
+    const double ey = -g.det_radius_cm * cos(theta) + g.det_src_iso_cm - g.sid_cm;
+    const double nrm = sqrt(ex * ex + ey * ey);
+    dir[c0] = make_double2(ex / nrm, ey / nrm);
+  }
+  int rc;
+  if ((rc = c->adj_rec.ensure(nrays)) || (rc = c->adj_special.ensure(nrays)) || (rc = c->adj_ints.ensure(2)) ||
+      (rc = c->adj_dir.ensure(C)) || (rc = c->adj_part.ensure(adj_forward_blocks(dg))) ||
+      (rc = c->adj_loss.ensure(1)) || (rc = c->adj_gmax.ensure(1)))
+    return rc;
+  VCT_CUDA(cudaMemcpyAsync(c->adj_dir.p, dir.data(), C * sizeof(double2), cudaMemcpyHostToDevice, c->stream));
+  VCT_CUDA(cudaMemsetAsync(c->adj_ints.p, 0, 2 * sizeof(int), c->stream));
+  if ((rc = launch_adj_plan(dg, c->cos_t.p, c->sin_t.p, c->det_px0.p, c->det_py0.p, c->adj_rec.p,
+                            c->adj_special.p, c->adj_ints.p, c->stream)))
+    return rc;
+  c->launches++;
+  int ns = 0;
+  VCT_CUDA(cudaMemcpyAsync(&ns, c->adj_ints.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  VCT_CUDA(cudaStreamSynchronize(c->stream));
+  c->adj_nspecial = ns;
+  // Terms per pixel of the scatter: at most a few segments per ray and pixel.
+  a.log2_terms = (int)ceil(log2(4.0 * ns + 2.0));
+  c->adj_ready = 1;
+  return VCT_OK;
+}
+
+static int adj_run(vct_ctx* c, int mode, const float* d_meas, const float* d_wts, const float* d_g_in,
+                   float* d_grad, double* d_loss) {
+  int rc;
+  if ((rc = adj_prepare(c))) return rc;
+  const DevGeom& dg = c->dg;
+  const int M = c->M;
+  const long long nrays = (long long)dg.views_used * dg.C;
+  const size_t n2 = (size_t)dg.N * dg.N;
+  const float* d_g = d_g_in;
+  VCT_CUDA(cudaMemsetAsync(c->adj_gmax.p, 0, sizeof(unsigned int), c->stream));
+  if (!d_g) {
+    if (!c->maps_ready || !c->spectrum_ready) return fail(VCT_E_STATE, "adjoint: maps or spectrum not set");
+    if ((rc = c->adj_g.ensure((size_t)nrays * M))) return rc;
+    if ((rc = launch_adj_forward(dg, c->maps.p, M, c->mu_log2.p, c->pdf.p, c->NE, c->ynorm, c->cos_t.p, c->sin_t.p,
+                                 c->det_px0.p, c->det_py0.p, c->adj_rec.p, mode, d_meas, d_wts, c->adj_g.p,
+                                 c->adj_part.p, c->adj_gmax.p, c->stream)))
+      return rc;
+    c->launches++;
+    d_g = c->adj_g.p;
+    if (mode == 0) {
+      if ((rc = launch_adj_loss(c->adj_part.p, adj_forward_blocks(dg), d_loss ? d_loss : c->adj_loss.p,
+                                c->stream)))
+        return rc;
+      c->launches++;
+    }
+  } else if (c->adj_nspecial > 0) {
+    // Caller-given ray weights: their maximum over the exact-walk rays sets
+    // the fixed-point scale.
+    if ((rc = launch_adj_gmax(M, c->adj_special.p, c->adj_ints.p, c->adj_nspecial, d_g, c->adj_gmax.p, c->stream)))
+      return rc;
+    c->launches++;
+  }
+  const unsigned long long* sacc = nullptr;
+  if (c->adj_nspecial > 0) {
+    if ((rc = c->adj_sacc.ensure(n2 * M))) return rc;
+    VCT_CUDA(cudaMemsetAsync(c->adj_sacc.p, 0, n2 * M * sizeof(unsigned long long), c->stream));
+    if ((rc = launch_adj_special(dg, M, c->cos_t.p, c->sin_t.p, c->det_px0.p, c->det_py0.p, c->adj_special.p,
+                                 c->adj_ints.p, c->adj_nspecial, d_g, c->adj_gmax.p, c->ag.lmax, c->ag.log2_terms,
+                                 c->adj_sacc.p, c->stream)))
+      return rc;
+    c->launches++;
+    sacc = c->adj_sacc.p;
+  }
+  if ((rc = launch_adj_gather(c->ag, M, c->adj_tile, c->cos_t.p, c->sin_t.p, c->adj_dir.p, c->adj_rec.p, d_g, sacc,
+                              c->adj_gmax.p, d_grad, c->adj_ints.p + 1, c->stream)))
+    return rc;
+  c->launches++;
+  return VCT_OK;
+}
+
+extern "C" {
+
+int vct_forward_adjoint_dev(vct_ctx* c, const float* d_meas, const float* d_weights, float* d_grad, double* d_loss) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!d_meas || !d_grad) return fail(VCT_E_ARG, "vct_forward_adjoint_dev: null buffer");
+  return adj_run(c, 0, d_meas, d_weights, nullptr, d_grad, d_loss);
+}
+
+int vct_forward_vjp_dev(vct_ctx* c, const float* d_dy, float* d_grad) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!d_dy || !d_grad) return fail(VCT_E_ARG, "vct_forward_vjp_dev: null buffer");
+  return adj_run(c, 1, d_dy, nullptr, nullptr, d_grad, nullptr);
+}
+
+int vct_adjoint_rays_dev(vct_ctx* c, const float* d_g, float* d_out) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!d_g || !d_out) return fail(VCT_E_ARG, "vct_adjoint_rays_dev: null buffer");
+  if (!c->maps_ready) return fail(VCT_E_STATE, "vct_adjoint_rays_dev: maps not set (M unknown)");
+  return adj_run(c, 1, nullptr, nullptr, d_g, d_out, nullptr);
+}
+
+int vct_forward_adjoint(vct_ctx* c, const float* meas, const float* weights, float* grad, double* loss) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!meas || !grad) return fail(VCT_E_ARG, "vct_forward_adjoint: null buffer");
+  const size_t nsino = (size_t)c->geo.views * c->geo.width;
+  const size_t ng = (size_t)c->dg.N * c->dg.N * (c->M > 0 ? c->M : 1);
+  if ((rc = c->adj_meas.ensure(nsino)) || (rc = c->adj_grad.ensure(ng))) return rc;
+  VCT_CUDA(cudaMemcpyAsync(c->adj_meas.p, meas, nsino * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  if (weights) {
+    if ((rc = c->adj_wts.ensure(nsino))) return rc;
+    VCT_CUDA(cudaMemcpyAsync(c->adj_wts.p, weights, nsino * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  }
+  if ((rc = adj_run(c, 0, c->adj_meas.p, weights ? c->adj_wts.p : nullptr, nullptr, c->adj_grad.p, c->adj_loss.p)))
+    return rc;
+  VCT_CUDA(cudaMemcpyAsync(grad, c->adj_grad.p, ng * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  double l = 0.0;
+  int status = 0;
+  VCT_CUDA(cudaMemcpyAsync(&l, c->adj_loss.p, sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  VCT_CUDA(cudaMemcpyAsync(&status, c->adj_ints.p + 1, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  VCT_CUDA(cudaStreamSynchronize(c->stream));
+  if (status) return fail(VCT_E_UNSUPPORTED, "adjoint: a tile's channel window overflowed");
+  if (loss) *loss = l;
+  return VCT_OK;
 }
 
 }  // extern "C"

@@ -76,4 +76,35 @@ int launch_fbp_backproject(const float* d_q, int V, int C, int N, double pixel_c
                            double max_beta, int xfactor, const float* d_cs, float* d_img,
                            cudaStream_t st);
 
+// Adjoint (vct_adjoint.cu).  Ray kinds of the per-ray walk record.
+constexpr int kAdjRayNone = 0;   // no segment
+constexpr int kAdjRayFast = 1;   // fast walk: lumped segment + chords in a major-index range
+constexpr int kAdjRayExact = 2;  // exact walk (scattered in fixed point)
+
+struct AdjGeom {
+  int N, nxm, C, start, views_used;
+  int log2_terms;     // bound on log2(terms per pixel) of the exact-walk scatter
+  double s, sid, iso, inv_dalpha;
+  double lmax;        // longest possible segment (cm)
+};
+
+int launch_adj_plan(const DevGeom& g, const double* d_cos, const double* d_sin, const double* d_px0,
+                    const double* d_py0, int4* d_rec, int* d_special, int* d_nspecial, cudaStream_t st);
+int adj_forward_blocks(const DevGeom& g);
+int launch_adj_forward(const DevGeom& g, const PixelRec* d_maps, int M, const double* d_mu_l2, const float* d_pdf,
+                       int NE, double ynorm, const double* d_cos, const double* d_sin, const double* d_px0,
+                       const double* d_py0, const int4* d_rec, int mode, const float* d_meas, const float* d_wts,
+                       float* d_g, double* d_loss_part, unsigned int* d_gmax, cudaStream_t st);
+int launch_adj_loss(const double* d_part, int n, double* d_out, cudaStream_t st);
+int launch_adj_special(const DevGeom& g, int M, const double* d_cos, const double* d_sin, const double* d_px0,
+                       const double* d_py0, const int* d_special, const int* d_nspecial, int nspecial_host,
+                       const float* d_g, const unsigned int* d_gmax, double lmax, int log2_terms,
+                       unsigned long long* d_acc, cudaStream_t st);
+int launch_adj_gmax(int M, const int* d_special, const int* d_nspecial, int nspecial_host, const float* d_g,
+                    unsigned int* d_gmax, cudaStream_t st);
+int adj_pick_tile(const AdjGeom& a, double lim);
+int launch_adj_gather(const AdjGeom& a, int M, int tile, const double* d_cos, const double* d_sin,
+                      const double2* d_dir, const int4* d_rec, const float* d_g, const unsigned long long* d_sacc,
+                      const unsigned int* d_gmax, float* d_grad, int* d_status, cudaStream_t st);
+
 }  // namespace vct

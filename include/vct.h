@@ -166,14 +166,23 @@ int vct_fbp_dev(vct_ctx* ctx, const float* d_sino, int filter, int in_mode, floa
  * (NULL: the legacy default stream); the call returns once the work is
  * enqueued.  The intermediate buffers are static device arrays of libvct
  * (about 8 MB, held on every GPU that loads the library until the process
- * exits), limited to views <= 4096, channels <= 2048 (640 for the filter
- * kernel, as vct_fbp) and views*channels <= 1048576; larger sizes return
+ * exits), limited to views <= 4096, channels <= 2048 and
+ * views*channels <= 1048576; larger sizes return
  * VCT_E_ARG.  The first call on a device looks up those arrays' device
  * addresses for it; make it before any stream capture.  All calls share the
  * arrays (each call rewrites every element it reads), so calls that overlap
  * on the GPU -- on different streams, or from several threads -- race. */
 int vct_fbp_noalloc(const vct_geometry* g, const float* d_sino, int filter, int in_mode, float* d_img,
                     void* stream);
+/* Transpose of the FBP (no counterpart in the reference).  With in_mode 0
+ * the FBP image is linear in lam = -ln p: img = B F W lam (weight W,
+ * filter F, backprojection B).  vct_fbp_transpose returns
+ * lam_adj = W^T F^T B^T u for an image-space u [N][N], as [views][width]
+ * (0 outside [start_channel, end_channel) and in rows >= views/2*2); the
+ * gradient of a loss on the image w.r.t. p is then -lam_adj / p.  B^T is a
+ * gather (one thread per view and detector bin, no atomics). */
+int vct_fbp_transpose(vct_ctx* ctx, const float* u, int filter, float* lam_adj);
+int vct_fbp_transpose_dev(vct_ctx* ctx, const float* d_u, int filter, float* d_lam_adj);
 /* The filtered sinogram of the last vct_fbp* call, [views][C]. */
 int vct_fbp_filtered_dev(vct_ctx* ctx, const float** d_fltd);
 

@@ -102,6 +102,7 @@ def lib():
         L.orc_fbp_constmap.argtypes = [C.POINTER(OrcGeom), C.c_int, _dp]
         L.orc_fbp_filter.argtypes = [C.POINTER(OrcGeom), _fp, _dp, C.c_int, _fp]
         L.orc_fbp_backproject.argtypes = [C.POINTER(OrcGeom), _fp, _dp, _dp, _fp]
+        L.orc_fbp_transpose.argtypes = [C.POINTER(OrcGeom), _dp, _dp, _dp, _dp, _dp]
         L.orc_mask.argtypes = [C.c_int, _u8p]
         _LIB = L
     return _LIB
@@ -356,6 +357,15 @@ def fbp(g, sino, filt, cos_t, sin_t, in_mode=0):
     h = fbp_constmap(g, filt)
     q = fbp_filter(g, sino, h, in_mode)
     return fbp_backproject(g, q, cos_t, sin_t), q
+
+
+def fbp_transpose(g, u, filt, cos_t, sin_t):
+    """FP64 W^T F^T B^T u: the transpose of the FBP in lam = -ln p."""
+    h = fbp_constmap(g, filt)
+    u = np.ascontiguousarray(u, np.float64)
+    out = np.zeros((g.views, g.width), np.float64)
+    lib().orc_fbp_transpose(C.byref(g), h, cos_t, sin_t, u, out)
+    return out
 
 
 def mask(N):

@@ -599,6 +599,56 @@ void orc_fbp_backproject(const orc_geom* g, const float* fltd, const double* cos
   free(mask);
 }
 
+void orc_fbp_transpose(const orc_geom* g, const double* h, const double* cos_t, const double* sin_t,
+                       const double* u, double* out) {
+  const int N = g->recon_size, V = g->views, W = g->width;
+  const int C = g->end_channel - g->start_channel;
+  const int half = (C - 1) / 2;
+  const int cw = C / 2;
+  const double scale = g->pixel_cm;
+  const double centerPos = (double)N / 2.0 - 0.5;
+  const int use = V / 2 * 2;
+  const double xfactor = (double)g->xfactor;
+  const double dbeta = 2.0 * ORC_PI / (V);
+  unsigned char* mask = (unsigned char*)malloc((size_t)N * N);
+  orc_mask(N, mask);
+  double* qb = (double*)calloc((size_t)V * C, sizeof(double));
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static)
+#endif
+  for (int th = 0; th < use; th++) {
+    const double c = cos_t[th], s = sin_t[th];
+    double* q = qb + (size_t)th * C;
+    for (int y = 0; y < N; y++)
+      for (int x = 0; x < N; x++) {
+        if (!mask[y * N + x]) continue;
+        const double xx = -(x - centerPos) * scale, yy = -(y - centerPos) * scale;
+        const double X = xx * c + yy * s;
+        const double Y = -xx * s + yy * c;
+        const double L2 = (-Y + g->sid) * (-Y + g->sid) + X * X;
+        const double fGAM = atan(X / (g->sid - Y)) / (g->max_beta / half) + cw;
+        const int GAM = (int)(fGAM);
+        const double w = fGAM - GAM;
+        if (GAM >= 0 && GAM < C - 1) {
+          const double a = u[(size_t)y * N + x] / L2 * dbeta * xfactor;
+          q[GAM] += (1 - w) * a;
+          q[GAM + 1] += w * a;
+        }
+      }
+  }
+  memset(out, 0, sizeof(double) * (size_t)V * W);
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static)
+#endif
+  for (int n = 0; n < V; n++)
+    for (int k = 0; k < C; k++) {
+      double acc = 0.0;
+      for (int m = 0; m < C; m++) acc += h[(size_t)m * C + k] * qb[(size_t)n * C + m];
+      out[(size_t)n * W + g->start_channel + k] = acc * g->sid * cos((k - cw) * (g->max_beta / half)) * g->max_beta / half;
+    }
+  free(qb);
+  free(mask);
+}
 
 /* ---------------------------------------------------------------- adjoint */
 static void orc_ray_points(const orc_geom* g, double cb, double sb, int jj, double* sx, double* sy,

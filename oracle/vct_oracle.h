@@ -125,6 +125,13 @@ double orc_normalize_noise(float* sino, int nn, double sigma, unsigned seed, int
 void orc_fbp_constmap(const orc_geom* g, int filter, double* h);
 void orc_fbp_filter(const orc_geom* g, const float* sino, const double* h, int in_mode,
                     float* fltd);
+/* Transpose of the FBP's linear part (in_mode 0) as a map from lam = -ln p
+ * [views][width] to the image, in FP64 (no counterpart in the reference):
+ * out = W^T F^T B^T u for u [N][N]; h is prepareConstMap's [C][C] matrix.
+ * B^T follows orc_fbp_backproject's formula (FBP/reconstructImageTOMO.cpp:
+ * 57-93), F^T the filter of FBP/filterSinogramTOMO.cpp:233-243. */
+void orc_fbp_transpose(const orc_geom* g, const double* h, const double* cos_t, const double* sin_t,
+                       const double* u, double* out);
 void orc_fbp_backproject(const orc_geom* g, const float* fltd, const double* cos_t,
                          const double* sin_t, float* img);
 

@@ -60,3 +60,21 @@ def test_fp64_gradient_matches_central_differences(channels):
         # the full-loss difference gives the same number: rays that cannot
         # touch the pixel cancel exactly
         assert abs(fd - grad[m, row, col]) <= 1e-6 * abs(fd) + 1e-9 * scale, (m, row, col)
+
+
+@pytest.mark.parametrize("N,views,channels", [(64, 40, 609), (63, 36, 512)])
+@pytest.mark.parametrize("filt", [1, 2])
+def test_fbp_transpose_dot_product(N, views, channels, filt):
+    """<FBP(exp(-lam)), u> = <lam, FBP^T u>: the FP64 transpose against the
+    oracle FBP that is pinned to the reference."""
+    g = O.geom(views=views, channels=channels, recon_size=N, pixel_cm=0.1)
+    c, s = O.trig_tables(views)
+    rng = np.random.default_rng(N + filt)
+    p = np.exp(-rng.uniform(0.1, 3.0, (views, channels))).astype(np.float32)
+    lam = -np.log(p.astype(np.float64))
+    img, _ = O.fbp(g, p, filt, c, s)
+    u = rng.standard_normal((N, N))
+    lt = O.fbp_transpose(g, u, filt, c, s)
+    lhs = float((img.astype(np.float64) * u).sum())
+    rhs = float((lam * lt).sum())
+    assert abs(lhs - rhs) <= 1e-7 * float(np.abs(img * u).sum())

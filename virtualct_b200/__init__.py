@@ -48,6 +48,7 @@ EXPORTED_SYMBOLS = (
     "vct_synchronize", "vct_attenuation_coefficient", "vct_set_maps", "vct_set_maps_dev", "vct_set_spectrum",
     "vct_set_sum_mode", "vct_set_walk_mode", "vct_forward", "vct_forward_dev", "vct_line_integrals_dev", "vct_mbfpa", "vct_mbfpa_dev",
     "vct_normalize_noise_dev", "vct_fbp", "vct_fbp_dev", "vct_fbp_noalloc", "vct_fbp_filtered_dev",
+    "vct_fbp_transpose", "vct_fbp_transpose_dev",
     "vct_forward_adjoint", "vct_forward_adjoint_dev", "vct_forward_vjp_dev", "vct_adjoint_rays_dev",
     "vct_last_segment_count",
     "vct_kernel_launches", "vct_version", "vct_philox4x32_10", "vct_probe_peaks",
@@ -143,6 +144,8 @@ def lib():
     L.vct_fbp.argtypes = [vp, vp, C.c_int, C.c_int, vp]
     L.vct_fbp_dev.argtypes = [vp, vp, C.c_int, C.c_int, vp]
     L.vct_fbp_filtered_dev.argtypes = [vp, C.POINTER(vp)]
+    L.vct_fbp_transpose.argtypes = [vp, vp, C.c_int, vp]
+    L.vct_fbp_transpose_dev.argtypes = [vp, vp, C.c_int, vp]
     L.vct_fbp_noalloc.argtypes = [C.POINTER(_CGeometry), vp, C.c_int, C.c_int, vp, vp]
     L.vct_forward_adjoint.argtypes = [vp, vp, vp, vp, C.POINTER(C.c_double)]
     L.vct_forward_adjoint_dev.argtypes = [vp, vp, vp, vp, vp]
@@ -343,6 +346,20 @@ class Context:
 
     def fbp_dev(self, sino, img, filter: int = 1, in_mode: bool = False) -> None:
         _check(lib().vct_fbp_dev(self._h, sino.data_ptr(), filter, int(in_mode), img.data_ptr()), "vct_fbp_dev")
+
+    def fbp_transpose(self, u, filter: int = 1) -> np.ndarray:
+        """W^T F^T B^T u: the transpose of the FBP (in_mode 0) as a map from
+        lam = -ln p [views][width] to the image, applied to u [N][N]."""
+        N = self.geometry.recon_size
+        a = np.ascontiguousarray(u, np.float32)
+        if a.shape != (N, N):
+            raise ValueError(f"u must be [{N}][{N}]")
+        out = self._sino()
+        _check(lib().vct_fbp_transpose(self._h, _ptr(a), filter, _ptr(out)), "vct_fbp_transpose")
+        return out
+
+    def fbp_transpose_dev(self, u, out, filter: int = 1) -> None:
+        _check(lib().vct_fbp_transpose_dev(self._h, u.data_ptr(), filter, out.data_ptr()), "vct_fbp_transpose_dev")
 
     def fbp_filtered_ptr(self) -> int:
         p = C.c_void_p()

@@ -45,8 +45,12 @@ int launch_fbp_weight(const float* d_sino, int V, int W, int start, int C, const
 // rows (:114-123), so each view is a 1-D convolution: one block per view, g
 // and h0 in shared memory, each thread FC consecutive outputs with a sliding
 // register window over h0; k runs in ascending order as in the reference.
+// TRANSPOSE: the transposed filter, g[v][k] = sum_m h0(m-k) c_m q[v][m]; h0
+// is even (both kernels depend on |m-k| only), so it is the same convolution
+// with the row factor applied to the input instead of the output.
 constexpr int FC_T = 128, FC_R = 5;
 
+template <bool TRANSPOSE>
 __global__ void __launch_bounds__(FC_T)
 fbp_filter_kernel(const float* __restrict__ G, const float* __restrict__ h0, const float* __restrict__ cm,
                   int V, int C, int in_mode, float* __restrict__ Q) {
@@ -54,43 +58,79 @@ fbp_filter_kernel(const float* __restrict__ G, const float* __restrict__ h0, con
   float* sg = sm;                 // [C + FC_R]  (zero tail)
   float* sh = sm + C + FC_R;      // [2C + FC_R] h0(d) at index d + C, zero outside
   const int v = blockIdx.x;
-  for (int k = threadIdx.x; k < C + FC_R; k += FC_T) sg[k] = k < C ? G[(size_t)v * C + k] : 0.0f;
+  for (int k = threadIdx.x; k < C + FC_R; k += FC_T)
+    sg[k] = k < C ? (TRANSPOSE ? G[(size_t)v * C + k] * cm[k] : G[(size_t)v * C + k]) : 0.0f;
   for (int d = threadIdx.x; d < 2 * C + FC_R; d += FC_T) sh[d] = (d >= 1 && d < 2 * C) ? h0[d - 1] : 0.0f;
   __syncthreads();
-  const int m0 = threadIdx.x * FC_R;
-  if (m0 >= C) return;
-  float acc[FC_R];
-  float win[FC_R];  // win[j] = h0(m0 + j - k)
+  // Each pass covers FC_T * FC_R outputs (one pass up to 640 channels).
+  for (int m0 = threadIdx.x * FC_R; m0 < C; m0 += FC_T * FC_R) {
+    float acc[FC_R];
+    float win[FC_R];  // win[j] = h0(m0 + j - k)
 #pragma unroll
-  for (int j = 0; j < FC_R; j++) {
-    acc[j] = 0.0f;
-    win[j] = sh[m0 + j + C];  // k = 0
-  }
-  for (int k = 0; k < C; k++) {
-    const float gk = sg[k];
+    for (int j = 0; j < FC_R; j++) {
+      acc[j] = 0.0f;
+      win[j] = sh[m0 + j + C];  // k = 0
+    }
+    for (int k = 0; k < C; k++) {
+      const float gk = sg[k];
 #pragma unroll
-    for (int j = 0; j < FC_R; j++) acc[j] = fmaf(win[j], gk, acc[j]);
-    // k -> k+1: h0(m0 + j - k - 1) = win[j-1]; win[0] needs a new value.
+      for (int j = 0; j < FC_R; j++) acc[j] = fmaf(win[j], gk, acc[j]);
+      // k -> k+1: h0(m0 + j - k - 1) = win[j-1]; win[0] needs a new value.
 #pragma unroll
-    for (int j = FC_R - 1; j > 0; j--) win[j] = win[j - 1];
-    win[0] = sh[m0 - k - 1 + C];
-  }
+      for (int j = FC_R - 1; j > 0; j--) win[j] = win[j - 1];
+      win[0] = sh[m0 - k - 1 + C];
+    }
 #pragma unroll
-  for (int j = 0; j < FC_R; j++) {
-    const int m = m0 + j;
-    if (m >= C) break;
-    float q = acc[j] * cm[m];
-    if (in_mode && (q < 1000.0f || q > 300000.0f)) q = 0.0f;  // :250-255
-    Q[(size_t)v * C + m] = q;
+    for (int j = 0; j < FC_R; j++) {
+      const int m = m0 + j;
+      if (m >= C) break;
+      if (TRANSPOSE) {
+        Q[(size_t)v * C + m] = acc[j];
+      } else {
+        float q = acc[j] * cm[m];
+        if (in_mode && (q < 1000.0f || q > 300000.0f)) q = 0.0f;  // :250-255
+        Q[(size_t)v * C + m] = q;
+      }
+    }
   }
 }
 
 int launch_fbp_filter(const float* d_g, const float* d_h0, const float* d_cm, int V, int C, int in_mode,
                       float* d_q, cudaStream_t st) {
-  if ((C + FC_R - 1) / FC_R > FC_T) return fail(VCT_E_UNSUPPORTED, "filter: more than 640 channels");
   const size_t smem = (size_t)(3 * C + 2 * FC_R) * sizeof(float);
-  VCT_CUDA(cudaFuncSetAttribute(fbp_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  fbp_filter_kernel<<<V, FC_T, smem, st>>>(d_g, d_h0, d_cm, V, C, in_mode, d_q);
+  if (smem > 220 * 1024) return fail(VCT_E_UNSUPPORTED, "filter: channel count above the shared-memory limit");
+  VCT_CUDA(cudaFuncSetAttribute(fbp_filter_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  fbp_filter_kernel<false><<<V, FC_T, smem, st>>>(d_g, d_h0, d_cm, V, C, in_mode, d_q);
+  VCT_CUDA(cudaGetLastError());
+  return VCT_OK;
+}
+
+int launch_fbp_filter_t(const float* d_q, const float* d_h0, const float* d_cm, int V, int C, float* d_g,
+                        cudaStream_t st) {
+  const size_t smem = (size_t)(3 * C + 2 * FC_R) * sizeof(float);
+  if (smem > 220 * 1024) return fail(VCT_E_UNSUPPORTED, "filter: channel count above the shared-memory limit");
+  VCT_CUDA(cudaFuncSetAttribute(fbp_filter_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  fbp_filter_kernel<true><<<V, FC_T, smem, st>>>(d_q, d_h0, d_cm, V, C, 0, d_g);
+  VCT_CUDA(cudaGetLastError());
+  return VCT_OK;
+}
+
+// Transposed weight: lam[v][start + k] = coeff[k] * g[v][k] (the linear part
+// of the weight step, g = -ln p * coeff); other channels stay 0.
+__global__ void fbp_weight_t_kernel(const float* __restrict__ g, int V, int W, int start, int C,
+                                    const double* __restrict__ coeff, float* __restrict__ lam) {
+  const long long n = (long long)V * W;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int v = (int)(i / W);
+  const int k = (int)(i - (long long)v * W) - start;
+  lam[i] = (k >= 0 && k < C) ? (float)((double)g[(size_t)v * C + k] * coeff[k]) : 0.0f;
+}
+
+int launch_fbp_weight_t(const float* d_g, int V, int W, int start, int C, const double* d_coeff, float* d_lam,
+                        cudaStream_t st) {
+  const long long n = (long long)V * W;
+  fbp_weight_t_kernel<<<(int)((n + 255) / 256), 256, 0, st>>>(d_g, V, W, start, C, d_coeff, d_lam);
   VCT_CUDA(cudaGetLastError());
   return VCT_OK;
 }
@@ -291,6 +331,126 @@ fbp_bp_sym_kernel(const float* __restrict__ Q, int V, int C, int N, float scale,
       img[(size_t)py[q] * N + px[q]] = in ? a * out_scale : 0.0f;
     }
   }
+}
+
+// ------------------------------------------------- backprojection transpose
+// qb[v][m] = out_scale * sum over mask pixels p of wt(p, v, m) u[p] / L2(p, v),
+// wt = 1 - w where trunc(fg) = m and w where trunc(fg) = m - 1: the transpose
+// of the interpolating backprojection above.  One thread per (view, bin)
+// gathers, so no two threads write one output.  The pixels whose fractional
+// channel fg lies in the bin's interval (m-1, m+1) -- from -1 for m <= 1,
+// since (int) truncates (-1, 0) to 0 -- are the pixels between two rays from
+// the source; each image row (or column, whichever the rays cross more
+// steeply) meets that wedge in a short run found in closed form, and every
+// pixel of the run is evaluated with the forward's own formula.
+// SYM: the quarter-turn orbit of fbp_bp_sym_kernel -- the geometry of pixel p
+// in view j is that of its rotations in views j + V/4, j + V/2, j + 3V/4, so
+// one evaluation serves four outputs (V % 4 == 0, N even).
+template <bool SYM>
+__global__ void __launch_bounds__(128)
+fbp_bp_t_kernel(const float* __restrict__ U, int V, int C, int N, float scale, float sid, float inv_dbeta,
+                float dbeta_det, float center, float out_scale, const float2* __restrict__ cs,
+                float* __restrict__ QB) {
+  const int m = blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = blockIdx.y;
+  if (m >= C) return;
+  const float2 t = cs[j];
+  const float c = t.x, s = t.y;
+  const float cp = (float)N / 2.0f - 0.5f;
+  // The wedge: fan angles of fg = lo and fg = m + 1 (a margin is added below).
+  const float lo = m <= 1 ? -1.0f : (float)(m - 1);
+  const float T1 = tanf((lo - center) * dbeta_det), T2 = tanf(((float)(m + 1) - center) * dbeta_det);
+  const float Tm = 0.5f * (T1 + T2);
+  const bool rows = fabsf(c - Tm * s) >= fabsf(s + Tm * c);
+  const int V4 = V / 4;
+  const int n1 = N - 1;
+  float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
+  for (int line = 0; line < N; line++) {
+    // Fixed coordinate of the line and the run of the other one.
+    float a0, a1;
+    if (rows) {
+      const float yy = -((float)line - cp) * scale;
+      const float x1 = (T1 * (sid - yy * c) - yy * s) / (c - T1 * s);
+      const float x2 = (T2 * (sid - yy * c) - yy * s) / (c - T2 * s);
+      a0 = cp - x1 / scale;
+      a1 = cp - x2 / scale;
+    } else {
+      const float xx = -((float)line - cp) * scale;
+      const float y1 = (T1 * (sid + xx * s) - xx * c) / (s + T1 * c);
+      const float y2 = (T2 * (sid + xx * s) - xx * c) / (s + T2 * c);
+      a0 = cp - y1 / scale;
+      a1 = cp - y2 / scale;
+    }
+    const int k0 = max((int)floorf(fminf(a0, a1)) - 1, 0);
+    const int k1 = min((int)ceilf(fmaxf(a0, a1)) + 1, n1);
+    for (int k = k0; k <= k1; k++) {
+      const int x = rows ? k : line, y = rows ? line : k;
+      // Inscribed-circle mask, exactly: (2y-N+1)^2 + (2x-N+1)^2 <= (N-1)^2.
+      const int dy2 = 2 * y - n1, dx2 = 2 * x - n1;
+      if (dy2 * dy2 + dx2 * dx2 > n1 * n1) continue;
+      const float xx = -((float)x - cp) * scale, yy = -((float)y - cp) * scale;
+      float fg, iL2;
+      if (SYM) {
+        const float X = xx * c + yy * s;
+        const float Y = -xx * s + yy * c;
+        const float d = sid - Y;
+        const float rd = rcp_approx(d);
+        fg = atan_small(X * rd) * inv_dbeta + center;
+        iL2 = rcp_approx(fmaf(d, d, X * X));
+      } else {
+        float L2;
+        fg = bp_channel(xx, yy, c, s, sid, inv_dbeta, center, &L2);
+        iL2 = __fdividef(1.0f, L2);
+      }
+      const float big = __fadd_rz(fmaxf(fg, 0.0f), 8388608.0f);
+      const int gi = fg > -1.0f ? (__float_as_int(big) - 0x4B000000) : -1;
+      const float w = fg - (big - 8388608.0f);
+      if ((unsigned)gi >= (unsigned)(C - 1)) continue;
+      float wt;
+      if (gi == m) wt = 1.0f - w;
+      else if (gi == m - 1) wt = w;
+      else continue;
+      wt *= iL2;
+      if (SYM) {
+        acc[0] = fmaf(wt, U[(size_t)y * N + x], acc[0]);
+        acc[1] = fmaf(wt, U[(size_t)x * N + (n1 - y)], acc[1]);
+        acc[2] = fmaf(wt, U[(size_t)(n1 - y) * N + (n1 - x)], acc[2]);
+        acc[3] = fmaf(wt, U[(size_t)(n1 - x) * N + y], acc[3]);
+      } else {
+        acc[0] = fmaf(wt, U[(size_t)y * N + x], acc[0]);
+      }
+    }
+  }
+  if (SYM) {
+#pragma unroll
+    for (int q = 0; q < 4; q++) QB[(size_t)(j + q * V4) * C + m] = acc[q] * out_scale;
+  } else {
+    QB[(size_t)j * C + m] = acc[0] * out_scale;
+  }
+}
+
+// Transpose of launch_fbp_backproject (same kernel choice, same geometry).
+// Rows v >= V/2*2 of qb are 0, as the backprojection never reads them.
+int launch_fbp_backproject_t(const float* d_u, int V, int C, int N, double pixel_cm, double sid, double max_beta,
+                             int xfactor, const float* d_cs, float* d_qb, cudaStream_t st) {
+  const int half = (C - 1) / 2;
+  const double dbeta_det = max_beta / half;
+  const double dbeta = 2.0 * 3.141592653589793 / V;
+  const int Vu = V / 2 * 2;
+  const bool sym = V % 4 == 0 && N % 2 == 0;
+  if (Vu < V) VCT_CUDA(cudaMemsetAsync(d_qb + (size_t)Vu * C, 0, (size_t)(V - Vu) * C * sizeof(float), st));
+  dim3 grid((C + 127) / 128, sym ? V / 4 : Vu);
+  if (grid.y == 0) return VCT_OK;
+  if (sym)
+    fbp_bp_t_kernel<true><<<grid, 128, 0, st>>>(d_u, V, C, N, (float)pixel_cm, (float)sid, (float)(1.0 / dbeta_det),
+                                                (float)dbeta_det, (float)(C / 2), (float)(dbeta * xfactor),
+                                                reinterpret_cast<const float2*>(d_cs), d_qb);
+  else
+    fbp_bp_t_kernel<false><<<grid, 128, 0, st>>>(d_u, V, C, N, (float)pixel_cm, (float)sid,
+                                                 (float)(1.0 / dbeta_det), (float)dbeta_det, (float)(C / 2),
+                                                 (float)(dbeta * xfactor), reinterpret_cast<const float2*>(d_cs), d_qb);
+  VCT_CUDA(cudaGetLastError());
+  return VCT_OK;
 }
 
 int launch_fbp_backproject(const float* d_q, int V, int C, int N, double pixel_cm, double sid,

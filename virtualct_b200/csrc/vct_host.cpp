@@ -604,6 +604,43 @@ int vct_fbp(vct_ctx* c, const float* sino, int filter, int in_mode, float* img) 
   return VCT_OK;
 }
 
+// Transpose of the FBP's linear part (no counterpart in the reference):
+// backprojection, filter and weight transposed, in reverse order.
+int vct_fbp_transpose_dev(vct_ctx* c, const float* d_u, int filter, float* d_lam) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!d_u || !d_lam) return fail(VCT_E_ARG, "null buffer");
+  if (filter != 1 && filter != 2) return fail(VCT_E_ARG, "filter must be 1 (Ram-Lak) or 2 (Shepp-Logan)");
+  const int V = c->geo.views, C = c->dg.C;
+  if ((rc = build_filter(c, filter))) return rc;
+  if ((rc = c->fbp_g.ensure((size_t)V * C)) || (rc = c->fbp_q.ensure((size_t)V * C))) return rc;
+  if ((rc = launch_fbp_backproject_t(d_u, V, C, c->dg.N, c->geo.pixel_cm, c->geo.sid_cm, c->geo.max_beta,
+                                     c->geo.xfactor, c->cs_f.p, c->fbp_q.p, c->stream)))
+    return rc;
+  if ((rc = launch_fbp_filter_t(c->fbp_q.p, c->fbp_h[filter].p, c->fbp_h[filter].p + 2 * C - 1, V, C, c->fbp_g.p,
+                                c->stream)))
+    return rc;
+  if ((rc = launch_fbp_weight_t(c->fbp_g.p, V, c->geo.width, c->geo.start_channel, C, c->fbp_coeff.p, d_lam,
+                                c->stream)))
+    return rc;
+  c->launches += 3;
+  return VCT_OK;
+}
+
+int vct_fbp_transpose(vct_ctx* c, const float* u, int filter, float* lam) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!u || !lam) return fail(VCT_E_ARG, "null buffer");
+  const size_t nsino = (size_t)c->geo.views * c->geo.width;
+  const size_t nimg = (size_t)c->dg.N * c->dg.N;
+  if ((rc = c->fbp_sino.ensure(nsino)) || (rc = c->fbp_img.ensure(nimg))) return rc;
+  VCT_CUDA(cudaMemcpyAsync(c->fbp_img.p, u, nimg * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  if ((rc = vct_fbp_transpose_dev(c, c->fbp_img.p, filter, c->fbp_sino.p))) return rc;
+  VCT_CUDA(cudaMemcpyAsync(lam, c->fbp_sino.p, nsino * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  VCT_CUDA(cudaStreamSynchronize(c->stream));
+  return VCT_OK;
+}
+
 int vct_fbp_filtered_dev(vct_ctx* c, const float** d_fltd) {
   if (!c || !d_fltd) return fail(VCT_E_ARG, "null argument");
   if (!c->fbp_q.p) return fail(VCT_E_STATE, "no FBP has run on this context");

@@ -75,6 +75,13 @@ int launch_fbp_filter(const float* d_g, const float* d_h0, const float* d_cm, in
 int launch_fbp_backproject(const float* d_q, int V, int C, int N, double pixel_cm, double sid,
                            double max_beta, int xfactor, const float* d_cs, float* d_img,
                            cudaStream_t st);
+// Transposes of the three FBP steps (vct_fbp.cu).
+int launch_fbp_backproject_t(const float* d_u, int V, int C, int N, double pixel_cm, double sid, double max_beta,
+                             int xfactor, const float* d_cs, float* d_qb, cudaStream_t st);
+int launch_fbp_filter_t(const float* d_q, const float* d_h0, const float* d_cm, int V, int C, float* d_g,
+                        cudaStream_t st);
+int launch_fbp_weight_t(const float* d_g, int V, int W, int start, int C, const double* d_coeff, float* d_lam,
+                        cudaStream_t st);
 
 // Adjoint (vct_adjoint.cu).  Ray kinds of the per-ray walk record.
 constexpr int kAdjRayNone = 0;   // no segment

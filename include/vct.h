@@ -217,6 +217,51 @@ int vct_forward_vjp_dev(vct_ctx* ctx, const float* d_dy, float* d_grad);
  * maps' element count; the transpose of vct_line_integrals_dev. */
 int vct_adjoint_rays_dev(vct_ctx* ctx, const float* d_g, float* d_out);
 
+/* ------------------------------------------------------------------ batch
+ * Many slices of uneven size (geometry, grid, spectrum) in one captured CUDA
+ * graph; no counterpart in the reference, which runs one slice per process.
+ * A job either runs vct_mbfpa (+ vct_fbp) -- d_sino set, d_grad NULL -- or
+ * the adjoint -- d_grad set.  All jobs of a batch have M elements and run
+ * the same kind of work.  One run of an MBFPA batch packs every job's maps,
+ * walks the rays of all jobs in ONE persistent launch (tiles of rays taken
+ * from a global counter, so uneven jobs share the GPU without a tail per
+ * job), then normalises, adds noise and reconstructs each job on parallel
+ * streams.  An adjoint batch runs each job's vct_forward_adjoint_dev on the
+ * parallel streams.  Device buffers are the caller's and are read or
+ * written at every run; the maps may change between runs, the geometry and
+ * spectrum may not.  With tune != 0, creation times candidate ray-tile sizes
+ * of the persistent launch and view splits of the backprojector on the batch
+ * itself and keeps the fastest. */
+typedef struct vct_job {
+  vct_geometry geo;
+  const int16_t* d_maps;  /* device [M][N][N], density x 1000 */
+  const float* mu;        /* host [M][NE], copied at creation */
+  const float* pdf;       /* host [NE] */
+  int NE;
+  /* MBFPA jobs */
+  double sigma;           /* noise standard deviation; <= 0: none */
+  uint64_t seed;
+  float* d_sino;          /* device [views][width]: the vct_mbfpa result */
+  float* d_img;           /* device [N][N]: FBP of d_sino, or NULL */
+  int filter;             /* 1 Ram-Lak, 2 Shepp-Logan (with d_img) */
+  /* adjoint jobs (vct_forward_adjoint_dev) */
+  const float* d_meas;    /* device [views][width] */
+  const float* d_weights; /* device [views][width] or NULL */
+  float* d_grad;          /* device [M][N][N] */
+  double* d_loss;         /* device double, or NULL */
+} vct_job;
+typedef struct vct_batch vct_batch;
+int vct_batch_create(const vct_job* jobs, int n, int M, int device, int tune, vct_batch** out);
+/* Enqueue one run on stream (NULL: the batch's own stream). */
+int vct_batch_run(vct_batch* b, void* stream);
+/* Wait for runs on the batch's own stream. */
+int vct_batch_synchronize(vct_batch* b);
+/* The chosen launch parameters and the number of kernel nodes per run. */
+int vct_batch_config(const vct_batch* b, int* tile_rays, int* blocks_per_sm, int* view_groups, int* kernels);
+void vct_batch_destroy(vct_batch* b);
+/* create (untuned) + run + wait + destroy. */
+int vct_forward_batched(const vct_job* jobs, int n, int M, int device);
+
 /* ------------------------------------------------------------ inspection */
 /* Number of in-grid walk segments of the last forward (the algorithmic work
  * unit of the forward kernel). */

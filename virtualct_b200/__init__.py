@@ -50,6 +50,8 @@ EXPORTED_SYMBOLS = (
     "vct_normalize_noise_dev", "vct_fbp", "vct_fbp_dev", "vct_fbp_noalloc", "vct_fbp_filtered_dev",
     "vct_fbp_transpose", "vct_fbp_transpose_dev",
     "vct_forward_adjoint", "vct_forward_adjoint_dev", "vct_forward_vjp_dev", "vct_adjoint_rays_dev",
+    "vct_batch_create", "vct_batch_run", "vct_batch_synchronize", "vct_batch_config", "vct_batch_destroy",
+    "vct_forward_batched",
     "vct_last_segment_count",
     "vct_kernel_launches", "vct_version", "vct_philox4x32_10", "vct_probe_peaks",
     "vct_load_mb_config", "vct_load_fbp_config", "vct_mb_geometry", "vct_fbp_geometry", "vct_read_raw",
@@ -69,6 +71,15 @@ class _CGeometry(C.Structure):
         ("start_channel", C.c_int), ("end_channel", C.c_int), ("iso_channel", C.c_double),
         ("max_alpha", C.c_double), ("max_beta", C.c_double), ("views", C.c_int), ("width", C.c_int),
         ("start_view_deg", C.c_double), ("recon_size", C.c_int), ("pixel_cm", C.c_double), ("xfactor", C.c_int),
+    ]
+
+
+class _CJob(C.Structure):
+    _fields_ = [
+        ("geo", _CGeometry), ("d_maps", C.c_void_p), ("mu", C.c_void_p), ("pdf", C.c_void_p), ("NE", C.c_int),
+        ("sigma", C.c_double), ("seed", C.c_uint64), ("d_sino", C.c_void_p), ("d_img", C.c_void_p),
+        ("filter", C.c_int), ("d_meas", C.c_void_p), ("d_weights", C.c_void_p), ("d_grad", C.c_void_p),
+        ("d_loss", C.c_void_p),
     ]
 
 
@@ -151,6 +162,14 @@ def lib():
     L.vct_forward_adjoint_dev.argtypes = [vp, vp, vp, vp, vp]
     L.vct_forward_vjp_dev.argtypes = [vp, vp, vp]
     L.vct_adjoint_rays_dev.argtypes = [vp, vp, vp]
+    L.vct_batch_create.argtypes = [C.POINTER(_CJob), C.c_int, C.c_int, C.c_int, C.c_int, C.POINTER(vp)]
+    L.vct_batch_run.argtypes = [vp, vp]
+    L.vct_batch_synchronize.argtypes = [vp]
+    L.vct_batch_config.argtypes = [vp, C.POINTER(C.c_int), C.POINTER(C.c_int), C.POINTER(C.c_int),
+                                   C.POINTER(C.c_int)]
+    L.vct_batch_destroy.argtypes = [vp]
+    L.vct_batch_destroy.restype = None
+    L.vct_forward_batched.argtypes = [C.POINTER(_CJob), C.c_int, C.c_int, C.c_int]
     L.vct_last_segment_count.argtypes = [vp, C.POINTER(C.c_longlong)]
     L.vct_kernel_launches.argtypes = [vp]
     L.vct_kernel_launches.restype = C.c_longlong
@@ -365,3 +384,73 @@ class Context:
         p = C.c_void_p()
         _check(lib().vct_fbp_filtered_dev(self._h, C.byref(p)), "vct_fbp_filtered_dev")
         return p.value
+
+
+def _dp(t):
+    return None if t is None else t.data_ptr()
+
+
+class Job:
+    """One slice of a Batch.  Device buffers are CUDA tensors (anything with
+    ``data_ptr()``); mu [M][NE] and pdf [NE] are host arrays."""
+
+    def __init__(self, geometry: Geometry, maps, mu, pdf, *, sino=None, img=None, filter: int = 1,
+                 sigma: float = 0.0, seed: int = 1, meas=None, weights=None, grad=None, loss=None):
+        self.geometry = geometry
+        self.maps, self.sino, self.img, self.meas, self.weights, self.grad, self.loss = (
+            maps, sino, img, meas, weights, grad, loss)
+        self.mu = np.ascontiguousarray(mu, np.float32)
+        self.pdf = np.ascontiguousarray(pdf, np.float32)
+        self.filter, self.sigma, self.seed = filter, sigma, seed
+
+    def to_c(self) -> _CJob:
+        j = _CJob()
+        j.geo = self.geometry.to_c()
+        j.d_maps = self.maps.data_ptr()
+        j.mu = self.mu.ctypes.data
+        j.pdf = self.pdf.ctypes.data
+        j.NE = int(self.pdf.shape[0])
+        j.sigma = float(self.sigma)
+        j.seed = int(self.seed)
+        j.d_sino, j.d_img, j.filter = _dp(self.sino), _dp(self.img), int(self.filter)
+        j.d_meas, j.d_weights, j.d_grad, j.d_loss = _dp(self.meas), _dp(self.weights), _dp(self.grad), _dp(self.loss)
+        return j
+
+
+class Batch:
+    """vct_batch: many slices in one captured CUDA graph (see include/vct.h)."""
+
+    def __init__(self, jobs, M: int = 6, device: int = 0, tune: bool = True):
+        self.jobs = list(jobs)  # keeps the buffers alive
+        arr = (_CJob * len(self.jobs))(*[j.to_c() for j in self.jobs])
+        self._h = C.c_void_p()
+        _check(lib().vct_batch_create(arr, len(self.jobs), M, device, int(tune), C.byref(self._h)),
+               "vct_batch_create")
+
+    def run(self, stream_ptr: int | None = None) -> None:
+        _check(lib().vct_batch_run(self._h, stream_ptr), "vct_batch_run")
+
+    def synchronize(self) -> None:
+        _check(lib().vct_batch_synchronize(self._h), "vct_batch_synchronize")
+
+    def config(self) -> dict:
+        t, b, v, k = C.c_int(), C.c_int(), C.c_int(), C.c_int()
+        _check(lib().vct_batch_config(self._h, C.byref(t), C.byref(b), C.byref(v), C.byref(k)), "vct_batch_config")
+        return {"tile_rays": t.value, "blocks_per_sm": b.value, "view_groups": v.value, "kernels_per_run": k.value}
+
+    def close(self) -> None:
+        if self._h:
+            lib().vct_batch_destroy(self._h)
+            self._h = C.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

@@ -37,9 +37,9 @@ CU_SOURCES = {
     "vct_fbp_noalloc.cu": [],
     "vct_adjoint.cu": ["--fmad=false"],
 }
-CPP_SOURCES = ["vct_host.cpp", "vct_io.cpp"]
+CPP_SOURCES = ["vct_host.cpp", "vct_io.cpp", "vct_batch.cpp"]
 APPS = {"vct_mbfpa": "vct_mbfpa_main.cpp", "vct_fbp": "vct_fbp_main.cpp"}
-HEADERS = ["vct_internal.h", "vct_philox.h", "vct_walk.cuh", "vct_fastmath.cuh"]
+HEADERS = ["vct_internal.h", "vct_philox.h", "vct_walk.cuh", "vct_fastmath.cuh", "vct_ctx.h"]
 
 
 def nvcc() -> str:

@@ -1,0 +1,358 @@
+// Batch engine: many slices of uneven size in one captured CUDA graph (no
+// counterpart in the reference, which runs one slice per process).
+//
+// Per run, the graph holds
+//   - the packing of every job's maps into its padded layout;
+//   - ONE persistent forward launch over the ray tiles of all jobs
+//     (forward_batch_kernel), which writes every job's un-normalised sinogram
+//     and statistics;
+//   - then, on `branches` parallel streams, per job: the max-normalisation and
+//     noise of vct_mbfpa, and the FBP when the job asks for an image;
+//   or, for jobs that ask for a gradient, the adjoint (loss and dl/drho) of
+//   each job on the parallel streams.
+// The ray-tile size of the persistent launch and the view split of the
+// backprojector are chosen by timing candidates on (a sample of) the batch
+// itself when it is created.
+#include <cuda_runtime.h>
+#include <math.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "vct_ctx.h"
+
+using namespace vct;
+
+struct vct_batch {
+  int device = 0;
+  int n = 0, M = 0, ne_max = 0;
+  int adjoint = 0;  // 1: jobs compute loss and gradient instead of MBFPA (+FBP)
+  std::vector<vct_job> jobs;
+  std::vector<vct_ctx*> ctx;
+  cudaStream_t stream = nullptr;
+  std::vector<cudaStream_t> branch;
+  std::vector<cudaEvent_t> ev;  // [0] fork, [1..] joins
+  // persistent forward
+  DBuf<FwdJob> d_jobs;
+  DBuf<unsigned int> d_counter;
+  unsigned int ntiles = 0;
+  int tile_rays = 256, blocks_per_sm = 0, grid = 0, view_groups = 4;
+  double tuned_ms = 0.0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+};
+
+namespace {
+
+constexpr int kBranches = 8;
+
+int sm_count(int device) {
+  int n = 0;
+  cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, device);
+  return n > 0 ? n : 1;
+}
+
+// The job table for a tile size: tile0 of every job, total tiles.
+int upload_jobs(vct_batch* b, int tile_rays) {
+  std::vector<FwdJob> h(b->n);
+  unsigned long long tiles = 0;
+  for (int i = 0; i < b->n; i++) {
+    const vct_ctx* c = b->ctx[i];
+    FwdJob& J = h[i];
+    J.g = c->dg;
+    J.maps = c->maps.p;
+    J.mu = c->mu_log2.p;
+    J.pdf = c->pdf.p;
+    J.cos_t = c->cos_t.p;
+    J.sin_t = c->sin_t.p;
+    J.px0 = c->det_px0.p;
+    J.py0 = c->det_py0.p;
+    J.out = b->jobs[i].d_sino;
+    J.stats = c->stats.p;
+    J.NE = c->NE;
+    J.fast = !c->dg.rmax_active;
+    J.tile0 = (unsigned int)tiles;
+    const long long nrays = (long long)c->dg.views_used * c->dg.C;
+    tiles += (unsigned long long)((nrays + tile_rays - 1) / tile_rays);
+  }
+  if (tiles >= 0xffffffffull) return fail(VCT_E_ARG, "batch: too many ray tiles");
+  b->ntiles = (unsigned int)tiles;
+  VCT_CUDA(cudaMemcpy(b->d_jobs.p, h.data(), h.size() * sizeof(FwdJob), cudaMemcpyHostToDevice));
+  return VCT_OK;
+}
+
+int enqueue_forward(vct_batch* b, cudaStream_t st) {
+  return launch_forward_batch(b->d_jobs.p, b->n, b->M, b->tile_rays, b->ntiles, b->ne_max, b->grid,
+                              b->d_counter.p, st);
+}
+
+// Everything after the forward, per job, spread over the branch streams.
+int enqueue_jobs(vct_batch* b) {
+  VCT_CUDA(cudaEventRecord(b->ev[0], b->stream));
+  const int K = (int)b->branch.size();
+  for (int k = 0; k < K; k++) VCT_CUDA(cudaStreamWaitEvent(b->branch[k], b->ev[0], 0));
+  int rc = VCT_OK;
+  for (int i = 0; i < b->n && !rc; i++) {
+    vct_ctx* c = b->ctx[i];
+    const vct_job& j = b->jobs[i];
+    cudaStream_t st = b->branch[i % K];
+    cudaStream_t saved = c->stream;
+    c->stream = st;
+    if (b->adjoint) {
+      rc = ctx_adj_run(c, 0, j.d_meas, j.d_weights, nullptr, j.d_grad, j.d_loss);
+    } else {
+      rc = launch_normalize_noise(c->dg, j.d_sino, j.d_sino, c->stats.p, ctx_pad_zero(c), j.sigma, j.seed, st);
+      if (!rc && j.d_img) rc = ctx_fbp(c, j.d_sino, j.filter, j.d_img, b->view_groups);
+    }
+    c->stream = saved;
+  }
+  if (rc) return rc;
+  for (int k = 0; k < K; k++) {
+    VCT_CUDA(cudaEventRecord(b->ev[1 + k], b->branch[k]));
+    VCT_CUDA(cudaStreamWaitEvent(b->stream, b->ev[1 + k], 0));
+  }
+  return VCT_OK;
+}
+
+int enqueue_all(vct_batch* b) {
+  int rc;
+  for (int i = 0; i < b->n; i++) {
+    vct_ctx* c = b->ctx[i];
+    if ((rc = launch_pack_maps(b->jobs[i].d_maps, b->M, c->dg.N, c->maps.p, b->stream))) return rc;
+  }
+  if (!b->adjoint && (rc = enqueue_forward(b, b->stream))) return rc;
+  return enqueue_jobs(b);
+}
+
+// Milliseconds of fn() on the batch stream: best of `reps` after one warm-up.
+template <class F>
+int time_ms(vct_batch* b, int reps, F fn, double* best) {
+  cudaEvent_t e0, e1;
+  VCT_CUDA(cudaEventCreate(&e0));
+  VCT_CUDA(cudaEventCreate(&e1));
+  int rc = fn();
+  *best = 1e30;
+  for (int r = 0; r < reps && !rc; r++) {
+    cudaEventRecord(e0, b->stream);
+    rc = fn();
+    cudaEventRecord(e1, b->stream);
+    if (!rc && cudaEventSynchronize(e1) == cudaSuccess) {
+      float ms = 0;
+      cudaEventElapsedTime(&ms, e0, e1);
+      *best = std::min(*best, (double)ms);
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  if (!rc) VCT_CUDA(cudaStreamSynchronize(b->stream));
+  return rc;
+}
+
+// The tuner: ray-tile size of the persistent forward, then the view split of
+// the quarter-turn backprojector on the batch's largest image.
+int autotune(vct_batch* b) {
+  int rc;
+  double best_total = 0.0;
+  if (!b->adjoint) {
+    const int cand[] = {128, 256, 512, 1024};
+    double best = 1e30;
+    int best_t = b->tile_rays;
+    for (int t : cand) {
+      if ((rc = upload_jobs(b, t))) return rc;
+      b->tile_rays = t;
+      double ms;
+      if ((rc = time_ms(b, 2, [&] { return enqueue_forward(b, b->stream); }, &ms))) return rc;
+      if (ms < best) {
+        best = ms;
+        best_t = t;
+      }
+    }
+    b->tile_rays = best_t;
+    if ((rc = upload_jobs(b, best_t))) return rc;
+    best_total += best;
+  }
+  // backprojector view split on the largest FBP job
+  int big = -1;
+  long long big_px = -1;
+  for (int i = 0; i < b->n; i++)
+    if (!b->adjoint && b->jobs[i].d_img && (long long)b->ctx[i]->dg.N * b->ctx[i]->dg.N > big_px) {
+      big = i;
+      big_px = (long long)b->ctx[i]->dg.N * b->ctx[i]->dg.N;
+    }
+  if (big >= 0) {
+    vct_ctx* c = b->ctx[big];
+    const vct_job& j = b->jobs[big];
+    double best = 1e30;
+    int best_vs = 4;
+    cudaStream_t saved = c->stream;
+    c->stream = b->stream;
+    for (int vs : {2, 4, 8}) {
+      double ms;
+      rc = time_ms(b, 3, [&] { return ctx_fbp(c, j.d_sino, j.filter, j.d_img, vs); }, &ms);
+      if (rc) break;
+      if (ms < best) {
+        best = ms;
+        best_vs = vs;
+      }
+    }
+    c->stream = saved;
+    if (rc) return rc;
+    b->view_groups = best_vs;
+  }
+  b->tuned_ms = best_total;
+  return VCT_OK;
+}
+
+void release(vct_batch* b) {
+  if (b->exec) cudaGraphExecDestroy(b->exec);
+  if (b->graph) cudaGraphDestroy(b->graph);
+  for (auto e : b->ev) cudaEventDestroy(e);
+  for (auto s : b->branch) cudaStreamDestroy(s);
+  if (b->stream) cudaStreamDestroy(b->stream);
+  for (auto c : b->ctx) vct_destroy(c);
+  b->d_jobs.release();
+  b->d_counter.release();
+}
+
+}  // namespace
+
+extern "C" {
+
+int vct_batch_create(const vct_job* jobs, int n, int M, int device, int tune, vct_batch** out) {
+  if (!jobs || n < 1 || !out || M < 1 || M > VCT_MAX_MATERIALS) return fail(VCT_E_ARG, "vct_batch_create: bad argument");
+  *out = nullptr;
+  int adj = jobs[0].d_grad != nullptr;
+  for (int i = 0; i < n; i++) {
+    const vct_job& j = jobs[i];
+    if ((j.d_grad != nullptr) != adj) return fail(VCT_E_ARG, "vct_batch_create: mixed gradient and MBFPA jobs");
+    if (!j.d_maps || !j.mu || !j.pdf || j.NE < 1) return fail(VCT_E_ARG, "vct_batch_create: job without maps or spectrum");
+    if (adj ? !j.d_meas : !j.d_sino) return fail(VCT_E_ARG, "vct_batch_create: job without its output/input sinogram");
+    if (!adj && j.d_img && j.filter != 1 && j.filter != 2) return fail(VCT_E_ARG, "vct_batch_create: bad filter");
+  }
+  VCT_CUDA(cudaSetDevice(device));
+  vct_batch* b = new vct_batch();
+  b->device = device;
+  b->n = n;
+  b->M = M;
+  b->adjoint = adj;
+  b->jobs.assign(jobs, jobs + n);
+  int rc = VCT_OK;
+  auto bail = [&](int code) {
+    release(b);
+    delete b;
+    return code;
+  };
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
+    return bail(fail(VCT_E_CUDA, "vct_batch_create: stream"));
+  for (int k = 0; k < kBranches; k++) {
+    cudaStream_t s;
+    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess)
+      return bail(fail(VCT_E_CUDA, "vct_batch_create: stream"));
+    b->branch.push_back(s);
+  }
+  for (int k = 0; k <= kBranches; k++) {
+    cudaEvent_t e;
+    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
+      return bail(fail(VCT_E_CUDA, "vct_batch_create: event"));
+    b->ev.push_back(e);
+  }
+  // One context per job: geometry tables, packed maps, spectrum, scratch.
+  for (int i = 0; i < n; i++) {
+    const vct_job& j = jobs[i];
+    vct_ctx* c = nullptr;
+    if ((rc = vct_create(&j.geo, device, &c))) return bail(rc);
+    b->ctx.push_back(c);
+    if ((rc = vct_set_spectrum(c, j.mu, j.pdf, M, j.NE)) || (rc = vct_set_maps_dev(c, j.d_maps, M))) return bail(rc);
+    b->ne_max = std::max(b->ne_max, j.NE);
+    if (adj) {
+      if ((rc = ctx_adj_prepare(c))) return bail(rc);
+      // allocates the adjoint's scratch (and checks the call) before capture
+      if ((rc = ctx_adj_run(c, 0, j.d_meas, j.d_weights, nullptr, j.d_grad, j.d_loss))) return bail(rc);
+    } else if (j.d_img) {
+      if ((rc = ctx_build_filter(c, j.filter))) return bail(rc);
+      const size_t vc = (size_t)j.geo.views * (j.geo.end_channel - j.geo.start_channel);
+      if ((rc = c->fbp_g.ensure(vc)) || (rc = c->fbp_q.ensure(vc))) return bail(rc);
+    }
+    if (cudaStreamSynchronize(c->stream) != cudaSuccess) return bail(fail(VCT_E_CUDA, "vct_batch_create: job set-up"));
+  }
+  if ((rc = b->d_jobs.ensure(n)) || (rc = b->d_counter.ensure(1))) return bail(rc);
+  if (!adj) {
+    int occ = 0;
+    if ((rc = forward_batch_occupancy(M, b->ne_max, &occ))) return bail(rc);
+    b->blocks_per_sm = std::max(occ, 1);
+    b->grid = b->blocks_per_sm * sm_count(device);
+    if ((rc = upload_jobs(b, b->tile_rays))) return bail(rc);
+  }
+  if (tune && (rc = autotune(b))) return bail(rc);
+  // Capture one run.
+  cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
+  if (e != cudaSuccess) return bail(cuda_fail(e, "vct_batch_create: begin capture"));
+  rc = enqueue_all(b);
+  cudaGraph_t g = nullptr;
+  e = cudaStreamEndCapture(b->stream, &g);
+  if (rc) {
+    if (g) cudaGraphDestroy(g);
+    return bail(rc);
+  }
+  if (e != cudaSuccess) return bail(cuda_fail(e, "vct_batch_create: end capture"));
+  b->graph = g;
+  if ((e = cudaGraphInstantiate(&b->exec, g, 0)) != cudaSuccess) return bail(cuda_fail(e, "vct_batch_create: instantiate"));
+  *out = b;
+  return VCT_OK;
+}
+
+int vct_batch_run(vct_batch* b, void* stream) {
+  if (!b) return fail(VCT_E_ARG, "vct_batch_run: null batch");
+  VCT_CUDA(cudaSetDevice(b->device));
+  VCT_CUDA(cudaGraphLaunch(b->exec, stream ? (cudaStream_t)stream : b->stream));
+  return VCT_OK;
+}
+
+int vct_batch_synchronize(vct_batch* b) {
+  if (!b) return fail(VCT_E_ARG, "vct_batch_synchronize: null batch");
+  VCT_CUDA(cudaSetDevice(b->device));
+  VCT_CUDA(cudaStreamSynchronize(b->stream));
+  return VCT_OK;
+}
+
+int vct_batch_config(const vct_batch* b, int* tile_rays, int* blocks_per_sm, int* view_groups, int* kernels) {
+  if (!b) return fail(VCT_E_ARG, "vct_batch_config: null batch");
+  if (tile_rays) *tile_rays = b->adjoint ? 0 : b->tile_rays;
+  if (blocks_per_sm) *blocks_per_sm = b->blocks_per_sm;
+  if (view_groups) *view_groups = b->view_groups;
+  if (kernels) {
+    size_t nodes = 0;
+    int k = 0;
+    if (b->graph && cudaGraphGetNodes(b->graph, nullptr, &nodes) == cudaSuccess) {
+      std::vector<cudaGraphNode_t> v(nodes);
+      cudaGraphGetNodes(b->graph, v.data(), &nodes);
+      for (auto nd : v) {
+        cudaGraphNodeType t;
+        if (cudaGraphNodeGetType(nd, &t) == cudaSuccess && t == cudaGraphNodeTypeKernel) k++;
+      }
+    }
+    *kernels = k;
+  }
+  return VCT_OK;
+}
+
+void vct_batch_destroy(vct_batch* b) {
+  if (!b) return;
+  cudaSetDevice(b->device);
+  if (b->stream) cudaStreamSynchronize(b->stream);
+  release(b);
+  delete b;
+}
+
+int vct_forward_batched(const vct_job* jobs, int n, int M, int device) {
+  vct_batch* b = nullptr;
+  int rc = vct_batch_create(jobs, n, M, device, 0, &b);
+  if (rc) return rc;
+  rc = vct_batch_run(b, nullptr);
+  if (!rc) rc = vct_batch_synchronize(b);
+  vct_batch_destroy(b);
+  return rc;
+}
+
+}  // extern "C"

@@ -1,0 +1,84 @@
+// The context behind vct_ctx* (include/vct.h), shared by the host code
+// (vct_host.cpp) and the batch engine (vct_batch.cpp).
+#pragma once
+#include <cuda_runtime.h>
+
+#include "vct_internal.h"
+
+namespace vct {
+// Device buffer that grows on demand.
+template <typename T>
+struct DBuf {
+  T* p = nullptr;
+  size_t n = 0;
+  int ensure(size_t count) {
+    if (count <= n && p) return VCT_OK;
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+    VCT_CUDA(cudaMalloc((void**)&p, count * sizeof(T)));
+    n = count;
+    return VCT_OK;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    n = 0;
+  }
+};
+}  // namespace vct
+
+struct vct_ctx {
+  int device = 0;
+  vct_geometry geo{};
+  vct::DevGeom dg{};
+  cudaStream_t own_stream = nullptr;
+  cudaStream_t stream = nullptr;
+  long long launches = 0;
+  // geometry tables
+  vct::DBuf<double> cos_t, sin_t, det_px0, det_py0;
+  vct::DBuf<float> cs_f;  // (cos, sin) pairs in float for the backprojector
+  // MBFPA
+  int M = 0, NE = 0;
+  double ynorm = 0.0;  // sum of the pdf as uploaded (the un-attenuated intensity)
+  int maps_ready = 0, spectrum_ready = 0;
+  int sum_mode = VCT_SUM_COMPENSATED;
+  int walk_mode = VCT_WALK_FAST;
+  vct::DBuf<int16_t> maps_raw;
+  vct::DBuf<vct::PixelRec> maps;
+  vct::DBuf<double> mu_scaled;  // [NE][M], mu/xfactor (reference summation)
+  vct::DBuf<double> mu_log2;    // [NE][M], mu*log2(e)/xfactor (compensated summation)
+  vct::DBuf<float> pdf;
+  vct::DBuf<float> full, out;   // [views][width]
+  vct::DBuf<vct::FwdStats> stats;       // [0] live, [1] the reset value
+  vct::FwdStats* h_stats = nullptr;  // pinned
+  long long last_segments = 0;
+  // FBP
+  vct::DBuf<double> fbp_coeff;  // SID*cos((k-cw)*dbeta)*dbeta
+  vct::DBuf<float> fbp_h[3];    // per filter (1 Ram-Lak, 2 Shepp-Logan): h0[2C-1] + row factors[C]
+  vct::DBuf<float> fbp_g, fbp_q, fbp_sino, fbp_img;
+  // Adjoint: per-ray walk plans (geometry only), ray factors, fixed-point
+  // accumulator of the exact-walk rays, loss partials.
+  int adj_ready = 0, adj_nspecial = 0, adj_tile = -1;
+  vct::AdjGeom ag{};
+  vct::DBuf<int4> adj_rec;
+  vct::DBuf<int> adj_special, adj_ints;  // ints: [0] special count, [1] status
+  vct::DBuf<double2> adj_dir;
+  vct::DBuf<float> adj_g;
+  vct::DBuf<double> adj_part, adj_loss;
+  vct::DBuf<unsigned int> adj_gmax;
+  vct::DBuf<unsigned long long> adj_sacc;
+  vct::DBuf<float> adj_meas, adj_wts, adj_grad;
+};
+
+
+namespace vct {
+// Internal helpers of vct_host.cpp.
+int ctx_check(vct_ctx* c);
+int ctx_build_filter(vct_ctx* c, int filter);
+int ctx_pad_zero(const vct_ctx* c);
+int ctx_fbp(vct_ctx* c, const float* d_sino, int filter, float* d_img, int view_groups);
+int ctx_adj_prepare(vct_ctx* c);
+int ctx_adj_run(vct_ctx* c, int mode, const float* d_meas, const float* d_wts, const float* d_g, float* d_grad,
+                double* d_loss);
+}  // namespace vct

@@ -255,11 +255,12 @@ fbp_bp_kernel(const float* __restrict__ Q, int V, int C, int N, int win, float s
 // quadrant.
 // The trig tables of the four views agree with the quarter-turn to double
 // rounding, below the FP32 resolution of the geometry.
-// 32 x 4 orbits per block; the base views are split over BS_VS groups of
-// warps (threadIdx.z), summed in shared memory at the end.  The four filtered
+// 32 x 4 orbits per block; the base views are split over VS groups of warps
+// (threadIdx.z; VS = 4 unless a batch's tuner picks another), summed in
+// shared memory at the end.  The four filtered
 // rows of each base view are read through the L1 cache (the 32 pixels of a
 // warp read neighbouring channels).
-constexpr int BS_TX = 32, BS_TY = 4, BS_VS = 4;
+constexpr int BS_TX = 32, BS_TY = 4, BS_VS = 4;  // BS_VS: the default view split
 
 __device__ __forceinline__ void bp_orbit_view(const float* __restrict__ Q, int V, int V4, int C, float xx, float yy,
                                               float2 t, int j, float sid, float inv_dbeta, float center,
@@ -288,10 +289,11 @@ __device__ __forceinline__ void bp_orbit_view(const float* __restrict__ Q, int V
   }
 }
 
-__global__ void __launch_bounds__(BS_TX * BS_TY * BS_VS)
+template <int VS>
+__global__ void __launch_bounds__(BS_TX * BS_TY * VS)
 fbp_bp_sym_kernel(const float* __restrict__ Q, int V, int C, int N, float scale, float sid, float inv_dbeta,
                   float center, float out_scale, const float2* __restrict__ cs, float* __restrict__ img) {
-  __shared__ float part[BS_VS - 1][4][BS_TX * BS_TY];
+  __shared__ float part[VS - 1][4][BS_TX * BS_TY];
   const int H = N / 2, V4 = V / 4;
   const int x = blockIdx.x * BS_TX + threadIdx.x;
   const int y = blockIdx.y * BS_TY + threadIdx.y;
@@ -306,7 +308,7 @@ fbp_bp_sym_kernel(const float* __restrict__ Q, int V, int C, int N, float scale,
     const float cp = (float)N / 2.0f - 0.5f;
     const float xx = -((float)x - cp) * scale;
     const float yy = -((float)y - cp) * scale;
-    const int jb = (int)((long long)V * z / BS_VS), je = (int)((long long)V * (z + 1) / BS_VS);
+    const int jb = (int)((long long)V * z / VS), je = (int)((long long)V * (z + 1) / VS);
     int j = jb;
     for (; j + 1 < je; j += 2) {
       const float2 t0 = __ldg(cs + j), t1 = __ldg(cs + j + 1);
@@ -327,7 +329,7 @@ fbp_bp_sym_kernel(const float* __restrict__ Q, int V, int C, int N, float scale,
     for (int q = 0; q < 4; q++) {
       float a = acc[q];
 #pragma unroll
-      for (int k = 0; k < BS_VS - 1; k++) a += part[k][q][lt];
+      for (int k = 0; k < VS - 1; k++) a += part[k][q][lt];
       img[(size_t)py[q] * N + px[q]] = in ? a * out_scale : 0.0f;
     }
   }
@@ -455,7 +457,7 @@ int launch_fbp_backproject_t(const float* d_u, int V, int C, int N, double pixel
 
 int launch_fbp_backproject(const float* d_q, int V, int C, int N, double pixel_cm, double sid,
                            double max_beta, int xfactor, const float* d_cs, float* d_img,
-                           cudaStream_t st) {
+                           cudaStream_t st, int view_groups) {
   const int half = (C - 1) / 2;
   const double dbeta_det = max_beta / half;
   const double dbeta = 2.0 * 3.141592653589793 / V;
@@ -470,10 +472,14 @@ int launch_fbp_backproject(const float* d_q, int V, int C, int N, double pixel_c
   if (V % 4 == 0 && N % 2 == 0) {
     const int H = N / 2;
     dim3 grid((H + BS_TX - 1) / BS_TX, (H + BS_TY - 1) / BS_TY);
-    dim3 block(BS_TX, BS_TY, BS_VS);
-    fbp_bp_sym_kernel<<<grid, block, 0, st>>>(d_q, V, C, N, (float)pixel_cm, (float)sid, (float)(1.0 / dbeta_det),
-                                              (float)(C / 2), (float)(dbeta * xfactor),
-                                              reinterpret_cast<const float2*>(d_cs), d_img);
+    const float a_sc = (float)pixel_cm, a_sid = (float)sid, a_ib = (float)(1.0 / dbeta_det), a_c = (float)(C / 2),
+                a_os = (float)(dbeta * xfactor);
+    const float2* cs2 = reinterpret_cast<const float2*>(d_cs);
+    switch (view_groups) {
+      case 2: fbp_bp_sym_kernel<2><<<grid, dim3(BS_TX, BS_TY, 2), 0, st>>>(d_q, V, C, N, a_sc, a_sid, a_ib, a_c, a_os, cs2, d_img); break;
+      case 8: fbp_bp_sym_kernel<8><<<grid, dim3(BS_TX, BS_TY, 8), 0, st>>>(d_q, V, C, N, a_sc, a_sid, a_ib, a_c, a_os, cs2, d_img); break;
+      default: fbp_bp_sym_kernel<BS_VS><<<grid, dim3(BS_TX, BS_TY, BS_VS), 0, st>>>(d_q, V, C, N, a_sc, a_sid, a_ib, a_c, a_os, cs2, d_img); break;
+    }
     VCT_CUDA(cudaGetLastError());
     return VCT_OK;
   }

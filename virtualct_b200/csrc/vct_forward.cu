@@ -88,6 +88,27 @@ __device__ __forceinline__ float ex2_approx(float x) {
 
 constexpr int kFwdThreads = 128;
 
+// 2^-y with y = transp*log2(e) in FP64, split y = n + f: the fraction goes
+// through the SFU exponential, the integer part into the float exponent; bins
+// below 2^-126 contribute nothing.  FP64 sum.  mu: [NE][M] mu*log2(e)/xfactor.
+template <int M>
+__device__ __forceinline__ float spectral_compensated(const double L[8], const double* __restrict__ s_mu,
+                                                      const float* __restrict__ s_pdf, int NE) {
+  double accd = 0.0;
+  for (int e = 0; e < NE; e++) {
+    double y = 0.0;
+#pragma unroll
+    for (int m = 0; m < M; m++) y = __fma_rn(s_mu[e * M + m], L[m], y);
+    const int nI = __double2int_rd(y);
+    if (nI <= 125) {
+      const float fr = (float)(y - (double)nI);
+      const float scale = __int_as_float((127 - nI) << 23);
+      accd += (double)(s_pdf[e] * ex2_approx(-fr) * scale);
+    }
+  }
+  return (float)accd;
+}
+
 // One thread per ray (view v, channel c), rays numbered view-major so a warp
 // holds 32 neighbouring channels of one view (similar paths and lengths).
 // mu: [NE][M] in shared memory -- mu/xfactor for the reference summation,
@@ -143,22 +164,7 @@ forward_kernel(DevGeom g, const PixelRec* __restrict__ maps, const double* __res
         }
         val = accf;
       } else {
-        // 2^-y with y = transp*log2(e) in FP64, split y = n + f: the
-        // fraction goes through the SFU exponential, the integer part into
-        // the float exponent; bins below 2^-126 contribute nothing.  FP64 sum.
-        double accd = 0.0;
-        for (int e = 0; e < NE; e++) {
-          double y = 0.0;
-#pragma unroll
-          for (int m = 0; m < M; m++) y = __fma_rn(s_mu[e * M + m], L[m], y);
-          const int nI = __double2int_rd(y);
-          if (nI <= 125) {
-            const float fr = (float)(y - (double)nI);
-            const float scale = __int_as_float((127 - nI) << 23);
-            accd += (double)(s_pdf[e] * ex2_approx(-fr) * scale);
-          }
-        }
-        val = (float)accd;
+        val = spectral_compensated<M>(L, s_mu, s_pdf, NE);
       }
       out[(size_t)v * g.width + g.start + c] = val;
     }
@@ -212,6 +218,145 @@ int launch_forward(const DevGeom& g, const PixelRec* d_maps, int M, const double
     default:
       return fail(VCT_E_ARG, "number of materials must be 1..8");
   }
+}
+
+// --------------------------------------------------------- batched forward
+// Many slices (jobs) with one element count in one persistent launch.  The
+// rays of every job are cut into tiles of `tile_rays` rays (view-major, as
+// the plain kernel numbers them); resident blocks take tiles from a global
+// counter in job order, so jobs of uneven size share the GPU without a tail
+// per job.  At a job change a block copies the job's descriptor and mu/pdf
+// tables into shared memory.  Per ray the work and the outputs are the plain
+// kernel's (compensated summation; statistics per job).
+template <int M>
+__global__ void __launch_bounds__(kFwdThreads)
+forward_batch_kernel(const FwdJob* __restrict__ jobs, int njobs, int tile_rays, unsigned int ntiles, int ne_max,
+                     unsigned int* __restrict__ counter) {
+  extern __shared__ double smem[];
+  double* s_mu = smem;                                                 // [ne_max][M]
+  float* s_pdf = reinterpret_cast<float*>(smem + (size_t)ne_max * M);  // [ne_max]
+  __shared__ FwdJob s_job;
+  __shared__ unsigned int s_tile;
+  __shared__ int s_j;
+  int cur = -1;
+  for (;;) {
+    if (threadIdx.x == 0) {
+      const unsigned int t = atomicAdd(counter, 1u);
+      int j = 0;
+      if (t < ntiles) {
+        int lo = 0, hi = njobs - 1;  // last job whose first tile is <= t
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (jobs[mid].tile0 <= t) lo = mid;
+          else hi = mid - 1;
+        }
+        j = lo;
+      }
+      s_tile = t;
+      s_j = j;
+    }
+    __syncthreads();
+    const unsigned int t = s_tile;
+    const int j = s_j;
+    if (t >= ntiles) break;
+    if (j != cur) {
+      if (threadIdx.x == 0) s_job = jobs[j];
+      const FwdJob& J = jobs[j];
+      for (int i = threadIdx.x; i < J.NE * M; i += blockDim.x) s_mu[i] = J.mu[i];
+      for (int i = threadIdx.x; i < J.NE; i += blockDim.x) s_pdf[i] = J.pdf[i];
+      __syncthreads();
+      cur = j;
+    }
+    const DevGeom& g = s_job.g;
+    const long long nrays = (long long)g.views_used * g.C;
+    const long long base = (long long)(t - s_job.tile0) * tile_rays;
+    for (int r = threadIdx.x; r < tile_rays; r += blockDim.x) {
+      const long long ray = base + r;
+      const bool active = ray < nrays;
+      float val = 0.0f;
+      int nseg = 0;
+      if (active) {
+        const int v = (int)(ray / g.C);
+        const int c = (int)(ray - (long long)v * g.C);
+        RayAcc a;
+        acc_init(a);
+        Ray rr;
+        if (ray_setup(g, s_job.cos_t[v], s_job.sin_t[v], s_job.px0[c], s_job.py0[c], rr)) {
+          bool done = false;
+          if (s_job.fast) done = walk_fast<M>(g, s_job.maps, rr, a);
+          if (!done) walk_exact<M>(g, s_job.maps, rr, a);
+        }
+        nseg = a.nseg;
+        double L[8];
+        finish_lines<M>(a, L);
+        val = spectral_compensated<M>(L, s_mu, s_pdf, s_job.NE);
+        s_job.out[(size_t)v * g.width + g.start + c] = val;
+      }
+      float vmax = warp_max(active ? val : 0.0f);
+      float vmin = warp_min(active ? val : 3.0e38f);
+      unsigned long long ns = warp_sum_ull((unsigned long long)nseg);
+      if ((threadIdx.x & 31) == 0) {
+        atomicMax(&s_job.stats->max_bits, __float_as_uint(vmax));
+        atomicMin(&s_job.stats->min_bits, __float_as_uint(vmin));
+        atomicAdd(&s_job.stats->segments, ns);
+      }
+    }
+    __syncthreads();  // the tile and job slots are rewritten next
+  }
+}
+
+// Statistics of every job back to their initial values.
+__global__ void reset_stats_kernel(const FwdJob* __restrict__ jobs, int njobs) {
+  const int j = blockIdx.x * blockDim.x + threadIdx.x;
+  if (j >= njobs) return;
+  FwdStats* st = jobs[j].stats;
+  st->max_bits = 0u;           // 0.0f
+  st->min_bits = 0x7f7fffffu;  // FLT_MAX
+  st->segments = 0ull;
+}
+
+template <int M>
+static int launch_forward_batch_m(const FwdJob* d_jobs, int njobs, int tile_rays, unsigned int ntiles, int ne_max,
+                                  int grid, unsigned int* d_counter, cudaStream_t st) {
+  const size_t smem = (size_t)ne_max * M * sizeof(double) + (size_t)ne_max * sizeof(float);
+  auto k = forward_batch_kernel<M>;
+  VCT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  k<<<grid, kFwdThreads, smem, st>>>(d_jobs, njobs, tile_rays, ntiles, ne_max, d_counter);
+  VCT_CUDA(cudaGetLastError());
+  return VCT_OK;
+}
+
+int launch_forward_batch(const FwdJob* d_jobs, int njobs, int M, int tile_rays, unsigned int ntiles, int ne_max,
+                         int grid, unsigned int* d_counter, cudaStream_t st) {
+  if (tile_rays % kFwdThreads) return fail(VCT_E_ARG, "batch: tile size must be a multiple of 128 rays");
+  reset_stats_kernel<<<(njobs + 127) / 128, 128, 0, st>>>(d_jobs, njobs);
+  VCT_CUDA(cudaGetLastError());
+  VCT_CUDA(cudaMemsetAsync(d_counter, 0, sizeof(unsigned int), st));
+  switch (M) {
+#define VCT_CASE(mm) \
+  case mm: return launch_forward_batch_m<mm>(d_jobs, njobs, tile_rays, ntiles, ne_max, grid, d_counter, st);
+    VCT_CASE(1) VCT_CASE(2) VCT_CASE(3) VCT_CASE(4) VCT_CASE(5) VCT_CASE(6) VCT_CASE(7) VCT_CASE(8)
+#undef VCT_CASE
+    default: return fail(VCT_E_ARG, "number of materials must be 1..8");
+  }
+}
+
+int forward_batch_occupancy(int M, int ne_max, int* blocks_per_sm) {
+  const size_t smem = (size_t)ne_max * M * sizeof(double) + (size_t)ne_max * sizeof(float);
+  cudaError_t e = cudaSuccess;
+  switch (M) {
+#define VCT_CASE(mm)                                                                                      \
+  case mm:                                                                                                \
+    e = cudaFuncSetAttribute(forward_batch_kernel<mm>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem); \
+    if (e == cudaSuccess)                                                                                 \
+      e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(blocks_per_sm, forward_batch_kernel<mm>, kFwdThreads, smem); \
+    break;
+    VCT_CASE(1) VCT_CASE(2) VCT_CASE(3) VCT_CASE(4) VCT_CASE(5) VCT_CASE(6) VCT_CASE(7) VCT_CASE(8)
+#undef VCT_CASE
+    default: return fail(VCT_E_ARG, "number of materials must be 1..8");
+  }
+  if (e != cudaSuccess) return cuda_fail(e, "forward_batch_occupancy");
+  return VCT_OK;
 }
 
 // -------------------------------------------------- normalisation and noise

@@ -33,71 +33,7 @@ static const double kPI = 3.141592653589793238462643383279;
 
 using namespace vct;
 
-// ---------------------------------------------------------------- device buffer
-namespace {
-template <typename T>
-struct DBuf {
-  T* p = nullptr;
-  size_t n = 0;
-  int ensure(size_t count) {
-    if (count <= n && p) return VCT_OK;
-    if (p) cudaFree(p);
-    p = nullptr;
-    n = 0;
-    VCT_CUDA(cudaMalloc((void**)&p, count * sizeof(T)));
-    n = count;
-    return VCT_OK;
-  }
-  void release() {
-    if (p) cudaFree(p);
-    p = nullptr;
-    n = 0;
-  }
-};
-}  // namespace
-
-struct vct_ctx {
-  int device = 0;
-  vct_geometry geo{};
-  DevGeom dg{};
-  cudaStream_t own_stream = nullptr;
-  cudaStream_t stream = nullptr;
-  long long launches = 0;
-  // geometry tables
-  DBuf<double> cos_t, sin_t, det_px0, det_py0;
-  DBuf<float> cs_f;  // (cos, sin) pairs in float for the backprojector
-  // MBFPA
-  int M = 0, NE = 0;
-  double ynorm = 0.0;  // sum of the pdf as uploaded (the un-attenuated intensity)
-  int maps_ready = 0, spectrum_ready = 0;
-  int sum_mode = VCT_SUM_COMPENSATED;
-  int walk_mode = VCT_WALK_FAST;
-  DBuf<int16_t> maps_raw;
-  DBuf<PixelRec> maps;
-  DBuf<double> mu_scaled;  // [NE][M], mu/xfactor (reference summation)
-  DBuf<double> mu_log2;    // [NE][M], mu*log2(e)/xfactor (compensated summation)
-  DBuf<float> pdf;
-  DBuf<float> full, out;   // [views][width]
-  DBuf<FwdStats> stats;       // [0] live, [1] the reset value
-  FwdStats* h_stats = nullptr;  // pinned
-  long long last_segments = 0;
-  // FBP
-  DBuf<double> fbp_coeff;  // SID*cos((k-cw)*dbeta)*dbeta
-  DBuf<float> fbp_h[3];    // per filter (1 Ram-Lak, 2 Shepp-Logan): h0[2C-1] + row factors[C]
-  DBuf<float> fbp_g, fbp_q, fbp_sino, fbp_img;
-  // Adjoint: per-ray walk plans (geometry only), ray factors, fixed-point
-  // accumulator of the exact-walk rays, loss partials.
-  int adj_ready = 0, adj_nspecial = 0, adj_tile = -1;
-  AdjGeom ag{};
-  DBuf<int4> adj_rec;
-  DBuf<int> adj_special, adj_ints;  // ints: [0] special count, [1] status
-  DBuf<double2> adj_dir;
-  DBuf<float> adj_g;
-  DBuf<double> adj_part, adj_loss;
-  DBuf<unsigned int> adj_gmax;
-  DBuf<unsigned long long> adj_sacc;
-  DBuf<float> adj_meas, adj_wts, adj_grad;
-};
+#include "vct_ctx.h"
 
 static int check_ctx(vct_ctx* c) {
   if (!c) return fail(VCT_E_ARG, "null context");
@@ -569,7 +505,7 @@ static int build_filter(vct_ctx* c, int filter) {
   return VCT_OK;
 }
 
-int vct_fbp_dev(vct_ctx* c, const float* d_sino, int filter, int in_mode, float* d_img) {
+static int fbp_into(vct_ctx* c, const float* d_sino, int filter, int in_mode, float* d_img, int view_groups) {
   int rc = check_ctx(c);
   if (rc) return rc;
   if (!d_sino || !d_img) return fail(VCT_E_ARG, "null buffer");
@@ -584,10 +520,14 @@ int vct_fbp_dev(vct_ctx* c, const float* d_sino, int filter, int in_mode, float*
                               c->fbp_q.p, c->stream)))
     return rc;
   if ((rc = launch_fbp_backproject(c->fbp_q.p, V, C, c->dg.N, c->geo.pixel_cm, c->geo.sid_cm, c->geo.max_beta,
-                                   c->geo.xfactor, c->cs_f.p, d_img, c->stream)))
+                                   c->geo.xfactor, c->cs_f.p, d_img, c->stream, view_groups)))
     return rc;
   c->launches += 3;
   return VCT_OK;
+}
+
+int vct_fbp_dev(vct_ctx* c, const float* d_sino, int filter, int in_mode, float* d_img) {
+  return fbp_into(c, d_sino, filter, in_mode, d_img, 4);
 }
 
 int vct_fbp(vct_ctx* c, const float* sino, int filter, int in_mode, float* img) {
@@ -814,3 +754,18 @@ int vct_forward_adjoint(vct_ctx* c, const float* meas, const float* weights, flo
 }
 
 }  // extern "C"
+
+// Internal entry points for the batch engine (vct_batch.cpp).
+namespace vct {
+int ctx_check(vct_ctx* c) { return check_ctx(c); }
+int ctx_build_filter(vct_ctx* c, int filter) { return build_filter(c, filter); }
+int ctx_pad_zero(const vct_ctx* c) { return pad_zero_of(c); }
+int ctx_fbp(vct_ctx* c, const float* d_sino, int filter, float* d_img, int view_groups) {
+  return fbp_into(c, d_sino, filter, 0, d_img, view_groups);
+}
+int ctx_adj_prepare(vct_ctx* c) { return adj_prepare(c); }
+int ctx_adj_run(vct_ctx* c, int mode, const float* d_meas, const float* d_wts, const float* d_g, float* d_grad,
+                double* d_loss) {
+  return adj_run(c, mode, d_meas, d_wts, d_g, d_grad, d_loss);
+}
+}  // namespace vct

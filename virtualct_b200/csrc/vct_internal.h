@@ -66,15 +66,36 @@ int launch_forward(const DevGeom& g, const PixelRec* d_maps, int M, const double
                    const float* d_pdf, int NE, const double* d_cos, const double* d_sin,
                    const double* d_det_ox, const double* d_det_oy, int sum_mode, int fast, float* d_out,
                    double* d_lint, FwdStats* d_stats, cudaStream_t st);
+// One slice of a batched forward (vct_batch.cpp): its geometry, device
+// tables and outputs.  tile0 is the index of its first ray tile.
+struct FwdJob {
+  DevGeom g;
+  const PixelRec* maps;
+  const double* mu;  // [NE][M] mu*log2(e)/xfactor
+  const float* pdf;
+  const double* cos_t;
+  const double* sin_t;
+  const double* px0;
+  const double* py0;
+  float* out;        // [views][width]
+  FwdStats* stats;
+  unsigned int tile0;
+  int NE, fast;
+};
+int launch_forward_batch(const FwdJob* d_jobs, int njobs, int M, int tile_rays, unsigned int ntiles, int ne_max,
+                         int grid, unsigned int* d_counter, cudaStream_t st);
+int forward_batch_occupancy(int M, int ne_max, int* blocks_per_sm);
 int launch_normalize_noise(const DevGeom& g, const float* d_in, float* d_out, const FwdStats* d_stats,
                            int pad_zero, double sigma, uint64_t seed, cudaStream_t st);
 int launch_fbp_weight(const float* d_sino, int V, int W, int start, int C, const double* d_coeff,
                       float* d_g, cudaStream_t st);
 int launch_fbp_filter(const float* d_g, const float* d_h0, const float* d_cm, int V, int C, int in_mode,
                       float* d_q, cudaStream_t st);
+// view_groups: how many warp groups split the views of the quarter-turn
+// backprojector (2, 4 or 8; other values mean 4).
 int launch_fbp_backproject(const float* d_q, int V, int C, int N, double pixel_cm, double sid,
                            double max_beta, int xfactor, const float* d_cs, float* d_img,
-                           cudaStream_t st);
+                           cudaStream_t st, int view_groups = 4);
 // Transposes of the three FBP steps (vct_fbp.cu).
 int launch_fbp_backproject_t(const float* d_u, int V, int C, int N, double pixel_cm, double sid, double max_beta,
                              int xfactor, const float* d_cs, float* d_qb, cudaStream_t st);

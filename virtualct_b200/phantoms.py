@@ -236,3 +236,39 @@ def write_fbp_txt(path, *, sino: str, out: str, filter: int = 1, width: int = 60
     _write_txt(path, _FBP_FIELDS, dict(cls=cls, filter=filter, width=width, height=views, sino=sino,
                                        period=f"{period:g}", rate=f"{rate:g}", start_angle=f"{start_angle:g}", N=N,
                                        pixel=f"{pixel_cm:g}", xfactor=xfactor, out=out))
+
+
+# ------------------------------------------------------- batched workloads
+def kramers_tables(kvp: float, elements=ELEMENTS8[:6], e_min_kev: float = 10.0, bin_kev: float = 1.0):
+    """mu [M][NE] and pdf [NE] of a Kramers spectrum through the reference's
+    attenuation model (the spectrum goes through its txt format)."""
+    import os
+    import tempfile
+
+    from . import attenuation_coefficient
+
+    fd, path = tempfile.mkstemp(suffix=".txt", prefix=f"kramers{int(kvp)}_")
+    os.close(fd)
+    try:
+        write_spectrum_txt(path, kramers_spectrum(kvp, e_min_kev, bin_kev))
+        return attenuation_coefficient(path, elements)
+    finally:
+        os.unlink(path)
+
+
+def batch_specs(n: int, seed: int = 0, grids=(256, 384, 512), kvps=(80, 100, 120, 140), rate=(36, 90),
+                channels=(512, 800)):
+    """The uneven batch: per slice a seeded ellipse phantom, grid N from
+    `grids` (0.1 cm pixels), kVp from `kvps`, views = 10 * DataSamplingRate
+    with the rate uniform in `rate`, channels uniform in `channels`."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for i in range(n):
+        out.append({
+            "seed": seed * 100003 + i,
+            "N": int(rng.choice(grids)),
+            "kvp": int(rng.choice(kvps)),
+            "views": 10 * int(rng.integers(rate[0], rate[1] + 1)),
+            "channels": int(rng.integers(channels[0], channels[1] + 1)),
+        })
+    return out

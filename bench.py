@@ -167,6 +167,14 @@ def run_ours(args, rank, world, dist):
     # device time for the roofline, same flush discipline.
     barrier()
     t_fwd = max_over_ranks(timed(lambda: ctx.forward_dev(d_sino), args.steps)) / args.steps
+    extras = {}
+    want = set() if args.no_extras or world > 1 else set(args.extras.split(","))
+    if "adjoint" in want:
+        extras["adjoint"] = bench_adjoint(ctx, d_maps, mu, pdf, stream, timed, args.steps, args.warmup)
+    if "batched" in want:
+        extras["batched"] = bench_batched(stream, args.warmup)
+    if "batched_adjoint" in want:
+        extras["batched_adjoint"] = bench_batched_adjoint(stream, args.warmup)
     clk.__exit__(None, None, None)
     # Algorithmic work unit: the reference walk's in-grid segments, counted by
     # one forward in exact-walk mode (outside every timed region).
@@ -256,9 +264,172 @@ def run_ours(args, rank, world, dist):
         },
         "clocks": clk.summary(),
     }
+    line.update(extras)
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(maps, mu, pdf)
     return line
+
+
+# ------------------------------------------------ adjoint and batched lines
+def _event_ms(stream, fn, reps):
+    """Best of `reps` CUDA-event timings of fn() on `stream` (after one run)."""
+    import torch
+
+    fn()
+    best = float("inf")
+    for _ in range(reps):
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        best = min(best, e0.elapsed_time(e1))
+    return best
+
+
+def bench_adjoint(ctx, d_maps, mu, pdf, stream, timed, steps, warmup):
+    """Loss + gradient at 512^2, 6 elements, 120 kVp, 800 x 609 (the adjoint
+    configuration): measured sinogram = the noisy MBFPA of the phantom, the
+    gradient taken at densities x 0.97.  One step = vct_forward_adjoint_dev
+    (walk + ray factors, exact-walk scatter when needed, pixel-driven A^T
+    gather, fixed-order loss sum); A^T alone is timed with fixed ray factors."""
+    import torch
+
+    meas = torch.empty((V, C), dtype=torch.float32, device="cuda")
+    ctx.mbfpa_dev(SIGMA, 7, meas)
+    at = (d_maps.double() * 0.97).round().to(torch.int16)
+    ctx.set_maps(at)
+    grad = torch.empty((6, N, N), dtype=torch.float32, device="cuda")
+    loss = torch.zeros(1, dtype=torch.float64, device="cuda")
+    fn = lambda: ctx.forward_adjoint_dev(meas, grad, loss=loss)  # noqa: E731
+    for _ in range(warmup):
+        fn()
+    n0 = ctx.kernel_launches
+    t = timed(fn, steps) / steps
+    launches = (ctx.kernel_launches - n0) // steps
+    gr = torch.randn((V, C, 6), dtype=torch.float32, device="cuda", generator=torch.Generator("cuda").manual_seed(3))
+    g_fn = lambda: ctx.adjoint_rays_dev(gr, grad)  # noqa: E731
+    for _ in range(warmup):
+        g_fn()
+    t_g = timed(g_fn, steps) / steps
+    ctx.set_maps(d_maps)
+    NE = len(pdf)
+    return {"workload": "loss + dl/drho: 512^2, 6 elements, 120 kVp 110 bins, 800 views x 609 channels",
+            "ms_per_gradient": t * 1e3, "rays_bins_per_s": V * C * NE / t,
+            "gather_ms": t_g * 1e3, "gather_pixel_views_per_s": N * N * V / t_g,
+            "kernels_per_gradient": int(launches), "loss": float(loss.item()),
+            "notes": "deterministic: pixel-driven A^T, no float atomics"}
+
+
+def _batch_inputs(n, seed, kvps_tabs):
+    import torch
+
+    import virtualct_b200 as vct
+    from virtualct_b200 import phantoms
+
+    specs = phantoms.batch_specs(n, seed=seed)
+    out = []
+    for i, sp in enumerate(specs):
+        g = vct.Geometry.with_channels(sp["channels"], views=sp["views"], recon_size=sp["N"], pixel_cm=PIX)
+        m = torch.from_numpy(phantoms.ellipse_phantom(sp["seed"], sp["N"])).cuda()
+        out.append((sp, g, m, kvps_tabs[sp["kvp"]]))
+    return out
+
+
+def bench_batched(stream, warmup, n=256):
+    """The batched configuration: 256 seeded ellipse phantoms of uneven grids
+    (256^2/384^2/512^2), kVp 80-140 (1 keV bins), 360-900 views, 512-800
+    channels; MBFPA (noise) + Ram-Lak FBP of every slice.  Plain = one slice
+    per call on one stream (vct_set_maps_dev + vct_mbfpa_dev + vct_fbp_dev);
+    batched = one replay of the captured graph.  The batch's inputs and
+    outputs (about 1 GB) exceed L2."""
+    import torch
+
+    import virtualct_b200 as vct
+    from virtualct_b200 import phantoms
+
+    tabs = {k: phantoms.kramers_tables(k) for k in (80, 100, 120, 140)}
+    inp = _batch_inputs(n, 0, tabs)
+    units = sum(sp["views"] // 2 * 2 * sp["channels"] * len(tab[1]) for sp, _, _, tab in inp)
+    jobs, ctxs = [], []
+    for i, (sp, g, m, tab) in enumerate(inp):
+        jobs.append(vct.Job(g, m, *tab, sino=torch.empty((g.views, g.width), dtype=torch.float32, device="cuda"),
+                            img=torch.empty((g.recon_size, g.recon_size), dtype=torch.float32, device="cuda"),
+                            filter=1, sigma=SIGMA, seed=i))
+        c = vct.Context(g)
+        c.set_stream(stream.cuda_stream)
+        c.set_spectrum(*tab)
+        c.set_maps(m)
+        ctxs.append(c)
+    torch.cuda.synchronize()
+
+    def plain():
+        for c, j in zip(ctxs, jobs):
+            c.set_maps(j.maps)
+            c.mbfpa_dev(j.sigma, j.seed, j.sino)
+            c.fbp_dev(j.sino, j.img, 1)
+
+    t_plain = _event_ms(stream, plain, max(warmup, 3))
+    t0 = time.perf_counter()
+    b = vct.Batch(jobs, tune=True)
+    t_create = time.perf_counter() - t0
+    t_batch = _event_ms(stream, lambda: b.run(stream.cuda_stream), max(warmup, 3))
+    cfg = b.config()
+    b.close()
+    for c in ctxs:
+        c.close()
+    return {"workload": f"{n} uneven slices: grids 256/384/512, kVp 80-140, 360-900 views, 512-800 channels, "
+                        "MBFPA + noise + Ram-Lak FBP",
+            "value": units / t_batch * 1e3, "unit": "rays*bins/s", "slices_per_s": n / t_batch * 1e3,
+            "ms_per_batch": t_batch, "plain_value": units / t_plain * 1e3, "plain_ms_per_batch": t_plain,
+            "speedup_vs_plain": t_plain / t_batch, "rays_bins_per_batch": units, "create_and_tune_s": t_create,
+            "tuned": cfg, "l2": "inputs and outputs of one batch exceed L2"}
+
+
+def bench_batched_adjoint(stream, warmup, n=64):
+    """Forward + adjoint of 64 uneven slices (the batched generator, seed 1):
+    plain = vct_forward_adjoint_dev slice by slice on one stream; batched =
+    one replay of an adjoint batch."""
+    import torch
+
+    import virtualct_b200 as vct
+    from virtualct_b200 import phantoms
+
+    tabs = {k: phantoms.kramers_tables(k) for k in (80, 100, 120, 140)}
+    inp = _batch_inputs(n, 1, tabs)
+    units = sum(sp["views"] // 2 * 2 * sp["channels"] * len(tab[1]) for sp, _, _, tab in inp)
+    jobs, ctxs = [], []
+    for i, (sp, g, m, tab) in enumerate(inp):
+        c = vct.Context(g)
+        c.set_stream(stream.cuda_stream)
+        c.set_spectrum(*tab)
+        c.set_maps(m)
+        meas = torch.empty((g.views, g.width), dtype=torch.float32, device="cuda")
+        c.mbfpa_dev(SIGMA, 100 + i, meas)
+        at = (m.double() * 0.95).round().to(torch.int16)
+        c.set_maps(at)
+        grad = torch.empty((6, g.recon_size, g.recon_size), dtype=torch.float32, device="cuda")
+        loss = torch.zeros(1, dtype=torch.float64, device="cuda")
+        jobs.append(vct.Job(g, at, *tab, meas=meas, grad=grad, loss=loss))
+        ctxs.append(c)
+    torch.cuda.synchronize()
+
+    def plain():
+        for c, j in zip(ctxs, jobs):
+            c.set_maps(j.maps)
+            c.forward_adjoint_dev(j.meas, j.grad, loss=j.loss)
+
+    t_plain = _event_ms(stream, plain, max(warmup, 3))
+    b = vct.Batch(jobs, tune=True)
+    t_batch = _event_ms(stream, lambda: b.run(stream.cuda_stream), max(warmup, 3))
+    cfg = b.config()
+    b.close()
+    for c in ctxs:
+        c.close()
+    return {"workload": f"{n} uneven slices (batched generator, seed 1): loss + dl/drho per slice",
+            "value": units / t_batch * 1e3, "unit": "rays*bins/s (forward + adjoint)",
+            "slices_per_s": n / t_batch * 1e3, "ms_per_batch": t_batch, "plain_value": units / t_plain * 1e3,
+            "plain_ms_per_batch": t_plain, "speedup_vs_plain": t_plain / t_batch, "tuned": cfg}
 
 
 def cpu_baseline(maps, mu, pdf):
@@ -348,6 +519,9 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-extras", action="store_true", help="skip the adjoint and batched lines")
+    ap.add_argument("--extras", default="adjoint,batched,batched_adjoint",
+                    help="comma list of extra lines (1 GPU): adjoint, batched, batched_adjoint")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world = int(os.environ.get("WORLD_SIZE", "1"))

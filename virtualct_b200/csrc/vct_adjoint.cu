@@ -344,45 +344,50 @@ constexpr int kAdjCap = kAdjVB * kAdjWMax;
 // unrotated direction.  Only v < 0 occurs (the grid lies below the source).
 // It only picks candidate channels, whose ranges carry a margin.
 __device__ __forceinline__ float fan_angle(float u, float v) {
-  const float t = u / -v;
+  const float t = u * rcp_approx(-v);
   return fabsf(t) <= 0.5f ? atan_small(t) : atanf(t);
 }
 
+// The gather runs over the (N+1) x (N+1) cells with indices -1..N-1: cells
+// at index -1 lie outside the grid, but the walk's truncating cast puts their
+// pieces on index 0 (adj_fold_kernel adds them there).  One thread per cell.
+// Staged per ray (shared memory, vector loads):
+//   A = (dx, dy, offset of the ray from the tile centre, h*(|dx|+|dy|))
+//   B = (2h/max(|dx|,|dy|), 1/(|dx||dy|), lumped length, lumped pixel bits)
+//   K = (xmaj, (maj_lo+1) | (maj_hi+1) << 16), G = the ray's M factors.
+// A ray that the fast walk does not take gets h*(|dx|+|dy|) = -inf (no
+// chord) and no lumped pixel.  The chord of a line at offset b from the
+// centre of a square of half-size h, direction with components a >= c:
+// 2h/a while |b| <= h(a-c), then (h(a+c) - |b|)/(a c) down to 0.
 template <int M, int TX, int TY>
 __global__ void __launch_bounds__(TX * TY)
 adj_gather_kernel(AdjGeom a, const double* __restrict__ cos_t, const double* __restrict__ sin_t,
                   const double2* __restrict__ dir, const int4* __restrict__ rec, const float* __restrict__ gr,
-                  const unsigned long long* __restrict__ sacc, const unsigned int* __restrict__ gmax,
-                  float* __restrict__ grad, int* __restrict__ status) {
-  __shared__ float s_dx[kAdjCap], s_dy[kAdjCap], s_bt[kAdjCap], s_hac[kAdjCap], s_cmax[kAdjCap], s_iac[kAdjCap];
-  __shared__ int s_kind[kAdjCap], s_rng[kAdjCap], s_lp[kAdjCap];
-  __shared__ float s_ll[kAdjCap];
-  __shared__ float s_g[kAdjCap * M];
+                  float* __restrict__ ext, int* __restrict__ status) {
+  constexpr int MG = (M + 3) / 4 * 4;
+  __shared__ float4 s_A[kAdjCap];
+  __shared__ float4 s_B[kAdjCap];
+  __shared__ int2 s_K[kAdjCap];
+  __shared__ __align__(16) float s_g[kAdjCap * MG];
   __shared__ int s_jlo[kAdjVB], s_jn[kAdjVB], s_base[kAdjVB + 1];
-  __shared__ float s_cb[kAdjVB], s_sb[kAdjVB];
+  __shared__ float s_cb[kAdjVB], s_sb[kAdjVB], s_dtx[kAdjVB], s_dty[kAdjVB];
 
-  const int N = a.N;
+  const int N = a.N, NE1 = N + 1;
   const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
-  const int col0 = blockIdx.x * TX, row0 = blockIdx.y * TY;
-  const int col = col0 + tx, row = row0 + ty;
+  const int e0 = blockIdx.x * TX, f0 = blockIdx.y * TY;  // first extended column / row
+  const int col = e0 + tx - 1, row = f0 + ty - 1;         // cell indices, -1..N-1
   const bool live = col < N && row < N;
   const double s = a.s;
   const float h = (float)(0.5 * s);
   // Tile centre (world cm; x right, y up; row r spans y in ((n-r-1)s, (n-r)s]).
-  const double Tx = (col0 + 0.5 * TX - a.nxm) * s;
-  const double Ty = (a.nxm - row0 - 0.5 * TY) * s;
-  // Cells of this thread: its pixel, plus the cells at index -1 that fold
-  // onto it (column 0 and row 0).
-  const int ncell = live ? 1 + (col == 0) + (row == 0) + (col == 0 && row == 0) : 0;
-  int ccol[4], crow[4];
-  ccol[0] = col; crow[0] = row;
-  {
-    int k = 1;
-    if (col == 0) { ccol[k] = -1; crow[k] = row; k++; }
-    if (row == 0) { ccol[k] = col; crow[k] = -1; k++; }
-    if (col == 0 && row == 0) { ccol[k] = -1; crow[k] = -1; }
-  }
-  const int pix = row * N + col;
+  const double Tx = (e0 - 1 + 0.5 * TX - a.nxm) * s;
+  const double Ty = (a.nxm - (f0 - 1) - 0.5 * TY) * s;
+  const float lx = (float)((tx + 0.5 - 0.5 * TX) * s);
+  const float ly = (float)((0.5 * TY - ty - 0.5) * s);
+  const int pix = (col >= 0 && row >= 0) ? row * N + col : -2;  // -2: never a lumped pixel
+  const int colx = col + 1, rowx = row + 1;
+  const float iso = (float)a.iso, ida = (float)a.inv_dalpha;
+  const float kdj = h * ida * 1.05f;
 
   double dacc[M];
 #pragma unroll
@@ -391,14 +396,14 @@ adj_gather_kernel(AdjGeom a, const double* __restrict__ cos_t, const double* __r
   const int V = a.views_used;
   for (int v0 = 0; v0 < V; v0 += kAdjVB) {
     const int nvb = min(kAdjVB, V - v0);
-    // Channel window of the tile for each view: the angles of the corners of
-    // the tile grown by one cell (the folded cells), plus two channels.
+    // Channel window of the tile for each view: the angles of the tile's
+    // corners grown by one cell, plus two channels.
     if (threadIdx.x < nvb) {
       const int v = v0 + threadIdx.x;
       const double cb = cos_t[v], sb = sin_t[v];
       const double Sx = a.sid * sb, Sy = a.sid * cb;
-      const double x0 = (col0 - 1 - a.nxm) * s, x1 = (col0 + TX + 1 - a.nxm) * s;
-      const double y0 = (a.nxm - row0 - TY - 1) * s, y1 = (a.nxm - row0 + 1) * s;
+      const double x0 = (e0 - 2 - a.nxm) * s, x1 = (e0 + TX - a.nxm) * s;
+      const double y0 = (a.nxm - f0 - TY) * s, y1 = (a.nxm - f0 + 2) * s;
       float tmin = 1e30f, tmax = -1e30f;
 #pragma unroll
       for (int k = 0; k < 4; k++) {
@@ -408,8 +413,8 @@ adj_gather_kernel(AdjGeom a, const double* __restrict__ cos_t, const double* __r
         tmin = fminf(tmin, t);
         tmax = fmaxf(tmax, t);
       }
-      int jlo = (int)floorf((float)a.iso - tmax * (float)a.inv_dalpha) - 2 - a.start;
-      int jhi = (int)ceilf((float)a.iso - tmin * (float)a.inv_dalpha) + 2 - a.start;
+      int jlo = (int)floorf(iso - tmax * ida) - 2 - a.start;
+      int jhi = (int)ceilf(iso - tmin * ida) + 2 - a.start;
       jlo = max(jlo, 0);
       jhi = min(jhi, a.C - 1);
       int jn = jhi - jlo + 1;
@@ -422,6 +427,8 @@ adj_gather_kernel(AdjGeom a, const double* __restrict__ cos_t, const double* __r
       s_jn[threadIdx.x] = jn;
       s_cb[threadIdx.x] = (float)cb;
       s_sb[threadIdx.x] = (float)sb;
+      s_dtx[threadIdx.x] = (float)(Tx - Sx);
+      s_dty[threadIdx.x] = (float)(Ty - Sy);
     }
     __syncthreads();
     if (threadIdx.x == 0) {
@@ -433,9 +440,8 @@ adj_gather_kernel(AdjGeom a, const double* __restrict__ cos_t, const double* __r
       s_base[nvb] = b;
     }
     __syncthreads();
-    // Stage the window's rays: direction, offset from the tile centre (FP64,
-    // then float: it is small for every ray that can hit the tile), chord
-    // constants, walk record and ray factors.
+    // Stage the window's rays: direction and offset from the tile centre in
+    // FP64, then float (small for every ray that can reach the tile).
     const int total = s_base[nvb];
     for (int k = threadIdx.x; k < total; k += TX * TY) {
       int vb = 0;
@@ -449,19 +455,14 @@ adj_gather_kernel(AdjGeom a, const double* __restrict__ cos_t, const double* __r
       const double Sx = a.sid * sb, Sy = a.sid * cb;
       const double bt = dx * (Ty - Sy) - dy * (Tx - Sx);
       const float ax = fabsf((float)dx), ay = fabsf((float)dy);
-      s_dx[k] = (float)dx;
-      s_dy[k] = (float)dy;
-      s_bt[k] = (float)bt;
-      s_hac[k] = h * (ax + ay);
-      s_cmax[k] = 2.0f * h / fmaxf(ax, ay);
-      s_iac[k] = 1.0f / (ax * ay);
       const int4 r = rec[ray];
-      s_kind[k] = r.x;
-      s_rng[k] = r.y;
-      s_lp[k] = r.z;
-      s_ll[k] = __int_as_float(r.w);
+      const bool fast = (r.x & 3) == kAdjRayFast;
+      s_A[k] = make_float4((float)dx, (float)dy, (float)bt, fast ? h * (ax + ay) : -INFINITY);
+      s_B[k] = make_float4(2.0f * h / fmaxf(ax, ay), 1.0f / (ax * ay), fast ? __int_as_float(r.w) : 0.0f,
+                           __int_as_float(fast ? r.z : -1));
+      s_K[k] = make_int2(r.x >> 2, r.y);
 #pragma unroll
-      for (int m = 0; m < M; m++) s_g[k * M + m] = gr[ray * M + m];
+      for (int m = 0; m < MG; m++) s_g[k * MG + m] = m < M ? gr[ray * M + m] : 0.0f;
     }
     __syncthreads();
 
@@ -470,39 +471,30 @@ adj_gather_kernel(AdjGeom a, const double* __restrict__ cos_t, const double* __r
     for (int m = 0; m < M; m++) acc[m] = 0.0f;
     for (int vb = 0; vb < nvb; vb++) {
       const float cb = s_cb[vb], sb = s_sb[vb];
-      const float Sx = (float)a.sid * sb, Sy = (float)a.sid * cb;
       const int jlo = s_jlo[vb], jn = s_jn[vb], base = s_base[vb];
-      for (int ci = 0; ci < ncell; ci++) {
-        const int cc = ccol[ci], cr = crow[ci];
-        // Cell centre relative to the tile centre, and relative to the source.
-        const float lx = (float)((cc - col0 + 0.5 - 0.5 * TX) * s);
-        const float ly = (float)((row0 - cr - 0.5 + 0.5 * TY) * s);
-        const float qx = (float)(Tx + lx) - Sx, qy = (float)(Ty + ly) - Sy;
-        const float u = qx * cb - qy * sb, w = qx * sb + qy * cb;
-        const float jc = (float)a.iso - fan_angle(u, w) * (float)a.inv_dalpha;
-        // Angular half-width of the cell seen from the source, in channels,
-        // with a margin.
-        const float q2 = qx * qx + qy * qy;
-        const float hw = h * (fabsf(qx) + fabsf(qy)) * rsqrtf(q2);
-        const float dj = hw * rsqrtf(q2) * (float)a.inv_dalpha * 1.05f + 0.05f;
-        const int j0 = max((int)ceilf(jc - dj) - a.start - jlo, 0);
-        const int j1 = min((int)floorf(jc + dj) - a.start - jlo, jn - 1);
-        for (int j = j0; j <= j1; j++) {
-          const int k = base + j;
-          const int kind = s_kind[k];
-          if ((kind & 3) != kAdjRayFast) continue;
-          const float b = fmaf(s_dx[k], ly, fmaf(-s_dy[k], lx, s_bt[k]));
-          const float num = s_hac[k] - fabsf(b);
-          float len = num > 0.0f ? fminf(s_cmax[k], num * s_iac[k]) : 0.0f;
-          const int rng = s_rng[k];
-          const int mi = ((kind >> 2) ? cc : cr) + 1;
-          if (mi < (rng & 0xffff) || mi > (rng >> 16)) len = 0.0f;
-          if (ci == 0 && s_lp[k] == pix) len += s_ll[k];
-          if (len != 0.0f) {
+      // Cell centre relative to the source, its fan angle and angular
+      // half-width in channels (with a margin).
+      const float qx = s_dtx[vb] + lx, qy = s_dty[vb] + ly;
+      const float u = qx * cb - qy * sb, w = qx * sb + qy * cb;
+      const float jc = iso - fan_angle(u, w) * ida;
+      const float iq = rsqrtf(fmaf(qx, qx, qy * qy));
+      const float dj = fmaf((fabsf(qx) + fabsf(qy)) * iq * iq, kdj, 0.05f);
+      const int j0 = max((int)ceilf(jc - dj) - a.start - jlo, 0);
+      const int j1 = min((int)floorf(jc + dj) - a.start - jlo, jn - 1);
+      for (int j = j0; j <= j1; j++) {
+        const int k = base + j;
+        const float4 A = s_A[k];
+        const float4 B = s_B[k];
+        const int2 K = s_K[k];
+        const float b = fmaf(A.x, ly, fmaf(-A.y, lx, A.z));
+        const float num = A.w - fabsf(b);
+        float len = num > 0.0f ? fminf(B.x, num * B.y) : 0.0f;
+        const int mi = K.x ? colx : rowx;
+        if (mi < (K.y & 0xffff) || mi > (K.y >> 16)) len = 0.0f;
+        if (__float_as_int(B.w) == pix) len += B.z;
+        const float* g = s_g + k * MG;
 #pragma unroll
-            for (int m = 0; m < M; m++) acc[m] = fmaf(len, s_g[k * M + m], acc[m]);
-          }
-        }
+        for (int m = 0; m < M; m++) acc[m] = fmaf(len, g[m], acc[m]);
       }
     }
 #pragma unroll
@@ -510,14 +502,32 @@ adj_gather_kernel(AdjGeom a, const double* __restrict__ cos_t, const double* __r
     __syncthreads();
   }
   if (!live) return;
-  const size_t n2 = (size_t)N * N;
-  if (sacc) {
-    const double inv = 1.0 / special_scale(*gmax, a.lmax, a.log2_terms);
+  const size_t n2 = (size_t)NE1 * NE1;
+  const size_t o = (size_t)(row + 1) * NE1 + (col + 1);
 #pragma unroll
-    for (int m = 0; m < M; m++) dacc[m] += (double)(long long)sacc[m * n2 + pix] * inv;
-  }
-#pragma unroll
-  for (int m = 0; m < M; m++) grad[m * n2 + pix] = (float)dacc[m];
+  for (int m = 0; m < M; m++) ext[m * n2 + o] = (float)dacc[m];
+}
+
+// grad[m][r][c] = ext at (r, c), plus the folded cells at index -1 (row -1
+// onto row 0, column -1 onto column 0), plus the exact-walk rays'
+// fixed-point sums; fixed order, so the result is deterministic.
+__global__ void adj_fold_kernel(int M, int N, const float* __restrict__ ext, const unsigned long long* __restrict__ sacc,
+                                const unsigned int* __restrict__ gmax, double lmax, int log2_terms,
+                                float* __restrict__ grad) {
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const size_t n2 = (size_t)N * N, e2 = (size_t)(N + 1) * (N + 1);
+  if (i >= (long long)M * n2) return;
+  const int m = (int)(i / n2);
+  const int p = (int)(i - (long long)m * n2);
+  const int r = p / N, c = p - (p / N) * N;
+  const float* e = ext + m * e2;
+  const int N1 = N + 1;
+  double v = e[(r + 1) * N1 + (c + 1)];
+  if (c == 0) v += e[(r + 1) * N1];
+  if (r == 0) v += e[c + 1];
+  if (r == 0 && c == 0) v += e[0];
+  if (sacc) v += (double)(long long)sacc[i] / special_scale(*gmax, lmax, log2_terms);
+  grad[i] = (float)v;
 }
 
 // Tile shapes, largest first; the channel window of a tile grows with its
@@ -541,16 +551,15 @@ int adj_pick_tile(const AdjGeom& a, double lim) {
 
 template <int M>
 static int launch_adj_gather_m(const AdjGeom& a, int tile, const double* d_cos, const double* d_sin,
-                               const double2* d_dir, const int4* d_rec, const float* d_g,
-                               const unsigned long long* d_sacc, const unsigned int* d_gmax, float* d_grad,
-                               int* d_status, cudaStream_t st) {
+                               const double2* d_dir, const int4* d_rec, const float* d_g, float* d_ext, int* d_status,
+                               cudaStream_t st) {
   const int TX = kTiles[tile][0], TY = kTiles[tile][1];
-  dim3 grid((a.N + TX - 1) / TX, (a.N + TY - 1) / TY);
+  dim3 grid((a.N + 1 + TX - 1) / TX, (a.N + 1 + TY - 1) / TY);
   switch (tile) {
-    case 0: adj_gather_kernel<M, 32, 8><<<grid, 256, 0, st>>>(a, d_cos, d_sin, d_dir, d_rec, d_g, d_sacc, d_gmax, d_grad, d_status); break;
-    case 1: adj_gather_kernel<M, 16, 8><<<grid, 128, 0, st>>>(a, d_cos, d_sin, d_dir, d_rec, d_g, d_sacc, d_gmax, d_grad, d_status); break;
-    case 2: adj_gather_kernel<M, 8, 8><<<grid, 64, 0, st>>>(a, d_cos, d_sin, d_dir, d_rec, d_g, d_sacc, d_gmax, d_grad, d_status); break;
-    default: adj_gather_kernel<M, 8, 4><<<grid, 32, 0, st>>>(a, d_cos, d_sin, d_dir, d_rec, d_g, d_sacc, d_gmax, d_grad, d_status); break;
+    case 0: adj_gather_kernel<M, 32, 8><<<grid, 256, 0, st>>>(a, d_cos, d_sin, d_dir, d_rec, d_g, d_ext, d_status); break;
+    case 1: adj_gather_kernel<M, 16, 8><<<grid, 128, 0, st>>>(a, d_cos, d_sin, d_dir, d_rec, d_g, d_ext, d_status); break;
+    case 2: adj_gather_kernel<M, 8, 8><<<grid, 64, 0, st>>>(a, d_cos, d_sin, d_dir, d_rec, d_g, d_ext, d_status); break;
+    default: adj_gather_kernel<M, 8, 4><<<grid, 32, 0, st>>>(a, d_cos, d_sin, d_dir, d_rec, d_g, d_ext, d_status); break;
   }
   VCT_CUDA(cudaGetLastError());
   return VCT_OK;
@@ -558,15 +567,22 @@ static int launch_adj_gather_m(const AdjGeom& a, int tile, const double* d_cos, 
 
 int launch_adj_gather(const AdjGeom& a, int M, int tile, const double* d_cos, const double* d_sin,
                       const double2* d_dir, const int4* d_rec, const float* d_g, const unsigned long long* d_sacc,
-                      const unsigned int* d_gmax, float* d_grad, int* d_status, cudaStream_t st) {
+                      const unsigned int* d_gmax, float* d_ext, float* d_grad, int* d_status, cudaStream_t st) {
   if (tile < 0 || tile > 3) return fail(VCT_E_UNSUPPORTED, "adjoint: no tile fits the channel window");
+  int rc;
   switch (M) {
 #define VCT_CASE(mm) \
-  case mm: return launch_adj_gather_m<mm>(a, tile, d_cos, d_sin, d_dir, d_rec, d_g, d_sacc, d_gmax, d_grad, d_status, st);
+  case mm: rc = launch_adj_gather_m<mm>(a, tile, d_cos, d_sin, d_dir, d_rec, d_g, d_ext, d_status, st); break;
     VCT_CASE(1) VCT_CASE(2) VCT_CASE(3) VCT_CASE(4) VCT_CASE(5) VCT_CASE(6) VCT_CASE(7) VCT_CASE(8)
 #undef VCT_CASE
     default: return fail(VCT_E_ARG, "adjoint: 1..8 materials");
   }
+  if (rc) return rc;
+  const long long n = (long long)M * a.N * a.N;
+  adj_fold_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(M, a.N, d_ext, d_sacc, d_gmax, a.lmax, a.log2_terms,
+                                                                d_grad);
+  VCT_CUDA(cudaGetLastError());
+  return VCT_OK;
 }
 
 }  // namespace vct

@@ -189,6 +189,7 @@ void vct_destroy(vct_ctx* c) {
   c->adj_rec.release(); c->adj_special.release(); c->adj_ints.release(); c->adj_dir.release();
   c->adj_g.release(); c->adj_part.release(); c->adj_loss.release(); c->adj_gmax.release();
   c->adj_sacc.release(); c->adj_meas.release(); c->adj_wts.release(); c->adj_grad.release();
+  c->adj_ext.release();
   if (c->h_stats) cudaFreeHost(c->h_stats);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
@@ -697,10 +698,11 @@ static int adj_run(vct_ctx* c, int mode, const float* d_meas, const float* d_wts
     c->launches++;
     sacc = c->adj_sacc.p;
   }
+  if ((rc = c->adj_ext.ensure((size_t)M * (dg.N + 1) * (dg.N + 1)))) return rc;
   if ((rc = launch_adj_gather(c->ag, M, c->adj_tile, c->cos_t.p, c->sin_t.p, c->adj_dir.p, c->adj_rec.p, d_g, sacc,
-                              c->adj_gmax.p, d_grad, c->adj_ints.p + 1, c->stream)))
+                              c->adj_gmax.p, c->adj_ext.p, d_grad, c->adj_ints.p + 1, c->stream)))
     return rc;
-  c->launches++;
+  c->launches += 2;
   return VCT_OK;
 }
 

@@ -131,8 +131,11 @@ int launch_adj_special(const DevGeom& g, int M, const double* d_cos, const doubl
 int launch_adj_gmax(int M, const int* d_special, const int* d_nspecial, int nspecial_host, const float* d_g,
                     unsigned int* d_gmax, cudaStream_t st);
 int adj_pick_tile(const AdjGeom& a, double lim);
+// Gather into d_ext [M][N+1][N+1] (cells -1..N-1), then fold into d_grad
+// [M][N][N] together with the exact-walk rays' fixed-point sums (d_sacc may
+// be NULL).  Two launches.
 int launch_adj_gather(const AdjGeom& a, int M, int tile, const double* d_cos, const double* d_sin,
                       const double2* d_dir, const int4* d_rec, const float* d_g, const unsigned long long* d_sacc,
-                      const unsigned int* d_gmax, float* d_grad, int* d_status, cudaStream_t st);
+                      const unsigned int* d_gmax, float* d_ext, float* d_grad, int* d_status, cudaStream_t st);
 
 }  // namespace vct

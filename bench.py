@@ -171,10 +171,12 @@ def run_ours(args, rank, world, dist):
     want = set() if args.no_extras or world > 1 else set(args.extras.split(","))
     if "adjoint" in want:
         extras["adjoint"] = bench_adjoint(ctx, d_maps, mu, pdf, stream, timed, args.steps, args.warmup)
+    if "fbp_transpose" in want:
+        extras["fbp_transpose"] = bench_fbp_transpose(ctx, stream, timed, args.steps, args.warmup)
     if "batched" in want:
-        extras["batched"] = bench_batched(stream, args.warmup)
+        extras["batched"] = bench_batched(stream, args.warmup, n=args.batch_slices)
     if "batched_adjoint" in want:
-        extras["batched_adjoint"] = bench_batched_adjoint(stream, args.warmup)
+        extras["batched_adjoint"] = bench_batched_adjoint(stream, args.warmup, n=max(args.batch_slices // 4, 1))
     clk.__exit__(None, None, None)
     # Algorithmic work unit: the reference walk's in-grid segments, counted by
     # one forward in exact-walk mode (outside every timed region).
@@ -319,6 +321,21 @@ def bench_adjoint(ctx, d_maps, mu, pdf, stream, timed, steps, warmup):
             "gather_ms": t_g * 1e3, "gather_pixel_views_per_s": N * N * V / t_g,
             "kernels_per_gradient": int(launches), "loss": float(loss.item()),
             "notes": "deterministic: pixel-driven A^T, no float atomics"}
+
+
+def bench_fbp_transpose(ctx, stream, timed, steps, warmup):
+    """The FBP transpose (backprojection gather, transposed filter and
+    weight) of an image-space gradient at 512^2 -> 800 x 609."""
+    import torch
+
+    u = torch.randn((N, N), dtype=torch.float32, device="cuda", generator=torch.Generator("cuda").manual_seed(5))
+    out = torch.empty((V, C), dtype=torch.float32, device="cuda")
+    fn = lambda: ctx.fbp_transpose_dev(u, out, 1)  # noqa: E731
+    for _ in range(warmup):
+        fn()
+    t = timed(fn, steps) / steps
+    return {"workload": "W^T F^T B^T u: 512^2 image-space gradient -> 800 x 609 (Ram-Lak)",
+            "ms_per_slice": t * 1e3, "slices_per_s": 1.0 / t}
 
 
 def _batch_inputs(n, seed, kvps_tabs):
@@ -520,8 +537,10 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-extras", action="store_true", help="skip the adjoint and batched lines")
-    ap.add_argument("--extras", default="adjoint,batched,batched_adjoint",
-                    help="comma list of extra lines (1 GPU): adjoint, batched, batched_adjoint")
+    ap.add_argument("--batch-slices", type=int, default=256,
+                    help="slices of the batched line (the batched adjoint line takes a quarter)")
+    ap.add_argument("--extras", default="adjoint,fbp_transpose,batched,batched_adjoint",
+                    help="comma list of extra lines (1 GPU): adjoint, fbp_transpose, batched, batched_adjoint")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world = int(os.environ.get("WORLD_SIZE", "1"))

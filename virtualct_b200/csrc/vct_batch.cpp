@@ -37,7 +37,7 @@ struct vct_batch {
   DBuf<FwdJob> d_jobs;
   DBuf<unsigned int> d_counter;
   unsigned int ntiles = 0;
-  int tile_rays = 256, blocks_per_sm = 0, grid = 0, view_groups = 4;
+  int tile_rays = 64, blocks_per_sm = 0, grid = 0, view_groups = 4;
   double tuned_ms = 0.0;
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
@@ -155,7 +155,7 @@ int autotune(vct_batch* b) {
   int rc;
   double best_total = 0.0;
   if (!b->adjoint) {
-    const int cand[] = {128, 256, 512, 1024};
+    const int cand[] = {32, 64, 128, 256};
     double best = 1e30;
     int best_t = b->tile_rays;
     for (int t : cand) {

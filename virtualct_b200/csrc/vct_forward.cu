@@ -223,26 +223,37 @@ int launch_forward(const DevGeom& g, const PixelRec* d_maps, int M, const double
 // --------------------------------------------------------- batched forward
 // Many slices (jobs) with one element count in one persistent launch.  The
 // rays of every job are cut into tiles of `tile_rays` rays (view-major, as
-// the plain kernel numbers them); resident blocks take tiles from a global
-// counter in job order, so jobs of uneven size share the GPU without a tail
-// per job.  At a job change a block copies the job's descriptor and mu/pdf
-// tables into shared memory.  Per ray the work and the outputs are the plain
-// kernel's (compensated summation; statistics per job).
+// the plain kernel numbers them); every resident WARP takes tiles from a
+// global counter in job order, so jobs of uneven size share the GPU without a
+// tail per job and no warp waits for another's rays.  At a job change a warp
+// copies the job's descriptor and mu/pdf tables into its own shared-memory
+// slot.  Per ray the work and the outputs are the plain kernel's (compensated
+// summation; statistics per job).
+constexpr int kBatchWarps = kFwdThreads / 32;
+#ifndef VCT_BATCH_MINBLOCKS
+#define VCT_BATCH_MINBLOCKS 5
+#endif
+
+__host__ __device__ inline size_t batch_slot_doubles(int ne_max, int M) {
+  return (size_t)ne_max * M + (size_t)(ne_max + 1) / 2;  // mu [ne_max][M] + pdf [ne_max] floats
+}
+
 template <int M>
-__global__ void __launch_bounds__(kFwdThreads)
+__global__ void __launch_bounds__(kFwdThreads, VCT_BATCH_MINBLOCKS)
 forward_batch_kernel(const FwdJob* __restrict__ jobs, int njobs, int tile_rays, unsigned int ntiles, int ne_max,
                      unsigned int* __restrict__ counter) {
   extern __shared__ double smem[];
-  double* s_mu = smem;                                                 // [ne_max][M]
-  float* s_pdf = reinterpret_cast<float*>(smem + (size_t)ne_max * M);  // [ne_max]
-  __shared__ FwdJob s_job;
-  __shared__ unsigned int s_tile;
-  __shared__ int s_j;
+  __shared__ FwdJob s_job[kBatchWarps];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  double* s_mu = smem + (size_t)warp * batch_slot_doubles(ne_max, M);  // [ne_max][M]
+  float* s_pdf = reinterpret_cast<float*>(s_mu + (size_t)ne_max * M);  // [ne_max]
+  FwdJob& J = s_job[warp];
   int cur = -1;
   for (;;) {
-    if (threadIdx.x == 0) {
-      const unsigned int t = atomicAdd(counter, 1u);
-      int j = 0;
+    unsigned int t = 0;
+    int j = 0;
+    if (lane == 0) {
+      t = atomicAdd(counter, 1u);
       if (t < ntiles) {
         int lo = 0, hi = njobs - 1;  // last job whose first tile is <= t
         while (lo < hi) {
@@ -252,25 +263,23 @@ forward_batch_kernel(const FwdJob* __restrict__ jobs, int njobs, int tile_rays, 
         }
         j = lo;
       }
-      s_tile = t;
-      s_j = j;
     }
-    __syncthreads();
-    const unsigned int t = s_tile;
-    const int j = s_j;
+    t = __shfl_sync(0xffffffffu, t, 0);
+    j = __shfl_sync(0xffffffffu, j, 0);
     if (t >= ntiles) break;
     if (j != cur) {
-      if (threadIdx.x == 0) s_job = jobs[j];
-      const FwdJob& J = jobs[j];
-      for (int i = threadIdx.x; i < J.NE * M; i += blockDim.x) s_mu[i] = J.mu[i];
-      for (int i = threadIdx.x; i < J.NE; i += blockDim.x) s_pdf[i] = J.pdf[i];
-      __syncthreads();
+      __syncwarp();  // every lane is done with the previous job's slot
+      if (lane == 0) J = jobs[j];
+      const FwdJob& G = jobs[j];
+      for (int i = lane; i < G.NE * M; i += 32) s_mu[i] = G.mu[i];
+      for (int i = lane; i < G.NE; i += 32) s_pdf[i] = G.pdf[i];
+      __syncwarp();
       cur = j;
     }
-    const DevGeom& g = s_job.g;
+    const DevGeom& g = J.g;
     const long long nrays = (long long)g.views_used * g.C;
-    const long long base = (long long)(t - s_job.tile0) * tile_rays;
-    for (int r = threadIdx.x; r < tile_rays; r += blockDim.x) {
+    const long long base = (long long)(t - J.tile0) * tile_rays;
+    for (int r = lane; r < tile_rays; r += 32) {
       const long long ray = base + r;
       const bool active = ray < nrays;
       float val = 0.0f;
@@ -281,27 +290,26 @@ forward_batch_kernel(const FwdJob* __restrict__ jobs, int njobs, int tile_rays, 
         RayAcc a;
         acc_init(a);
         Ray rr;
-        if (ray_setup(g, s_job.cos_t[v], s_job.sin_t[v], s_job.px0[c], s_job.py0[c], rr)) {
+        if (ray_setup(g, J.cos_t[v], J.sin_t[v], J.px0[c], J.py0[c], rr)) {
           bool done = false;
-          if (s_job.fast) done = walk_fast<M>(g, s_job.maps, rr, a);
-          if (!done) walk_exact<M>(g, s_job.maps, rr, a);
+          if (J.fast) done = walk_fast<M>(g, J.maps, rr, a);
+          if (!done) walk_exact<M>(g, J.maps, rr, a);
         }
         nseg = a.nseg;
         double L[8];
         finish_lines<M>(a, L);
-        val = spectral_compensated<M>(L, s_mu, s_pdf, s_job.NE);
-        s_job.out[(size_t)v * g.width + g.start + c] = val;
+        val = spectral_compensated<M>(L, s_mu, s_pdf, J.NE);
+        J.out[(size_t)v * g.width + g.start + c] = val;
       }
       float vmax = warp_max(active ? val : 0.0f);
       float vmin = warp_min(active ? val : 3.0e38f);
       unsigned long long ns = warp_sum_ull((unsigned long long)nseg);
-      if ((threadIdx.x & 31) == 0) {
-        atomicMax(&s_job.stats->max_bits, __float_as_uint(vmax));
-        atomicMin(&s_job.stats->min_bits, __float_as_uint(vmin));
-        atomicAdd(&s_job.stats->segments, ns);
+      if (lane == 0) {
+        atomicMax(&J.stats->max_bits, __float_as_uint(vmax));
+        atomicMin(&J.stats->min_bits, __float_as_uint(vmin));
+        atomicAdd(&J.stats->segments, ns);
       }
     }
-    __syncthreads();  // the tile and job slots are rewritten next
   }
 }
 
@@ -318,7 +326,7 @@ __global__ void reset_stats_kernel(const FwdJob* __restrict__ jobs, int njobs) {
 template <int M>
 static int launch_forward_batch_m(const FwdJob* d_jobs, int njobs, int tile_rays, unsigned int ntiles, int ne_max,
                                   int grid, unsigned int* d_counter, cudaStream_t st) {
-  const size_t smem = (size_t)ne_max * M * sizeof(double) + (size_t)ne_max * sizeof(float);
+  const size_t smem = kBatchWarps * batch_slot_doubles(ne_max, M) * sizeof(double);
   auto k = forward_batch_kernel<M>;
   VCT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k<<<grid, kFwdThreads, smem, st>>>(d_jobs, njobs, tile_rays, ntiles, ne_max, d_counter);
@@ -328,7 +336,7 @@ static int launch_forward_batch_m(const FwdJob* d_jobs, int njobs, int tile_rays
 
 int launch_forward_batch(const FwdJob* d_jobs, int njobs, int M, int tile_rays, unsigned int ntiles, int ne_max,
                          int grid, unsigned int* d_counter, cudaStream_t st) {
-  if (tile_rays % kFwdThreads) return fail(VCT_E_ARG, "batch: tile size must be a multiple of 128 rays");
+  if (tile_rays < 32 || tile_rays % 32) return fail(VCT_E_ARG, "batch: tile size must be a multiple of 32 rays");
   reset_stats_kernel<<<(njobs + 127) / 128, 128, 0, st>>>(d_jobs, njobs);
   VCT_CUDA(cudaGetLastError());
   VCT_CUDA(cudaMemsetAsync(d_counter, 0, sizeof(unsigned int), st));
@@ -342,7 +350,7 @@ int launch_forward_batch(const FwdJob* d_jobs, int njobs, int M, int tile_rays, 
 }
 
 int forward_batch_occupancy(int M, int ne_max, int* blocks_per_sm) {
-  const size_t smem = (size_t)ne_max * M * sizeof(double) + (size_t)ne_max * sizeof(float);
+  const size_t smem = kBatchWarps * batch_slot_doubles(ne_max, M) * sizeof(double);
   cudaError_t e = cudaSuccess;
   switch (M) {
 #define VCT_CASE(mm)                                                                                      \

@@ -37,6 +37,9 @@ V, C, N, PIX = 800, 609, 512, 0.1
 SIGMA = 0.0000537  # txt field "Photon noise in detector" of the shipped 120 kV input
 SPECTRUM = os.path.join(ROOT, "tests", "golden", "kramers_120kvp.txt")
 METRIC = "MBFPA rays*bins/s (FBP slices/s alongside)"
+# DRAM bytes (read + write) of one forward_kernel launch on this workload,
+# from one ncu capture: the two map copies once; the gathers hit L1/L2.
+FWD_DRAM_BYTES = 8579584
 CONFIG_NAME = "plain MBFPA+FBP single slice: 512^2, 6 elements, 800 views x 609 channels, 120 kVp Kramers 110 bins"
 
 
@@ -253,7 +256,9 @@ def run_ours(args, rank, world, dist):
             "peak": peaks["l2_read_gbs"],
             "unit": "GB/s",
             "frac": achieved / peaks["l2_read_gbs"],
-            "traffic": None,
+            "traffic": FWD_DRAM_BYTES,
+            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one forward_kernel launch "
+                              "(profiles/forward_kernel_c1_512_800x609.md)",
             "peak_source": "measured live: vct_probe_peaks L2 read (ld.global.cg, 16 MB resident)",
             "algorithmic_bytes_per_launch": int(alg_bytes),
             "segments_per_launch": int(segments),

@@ -96,6 +96,11 @@ int vct_attenuation_coefficient(const char* spectrum_path, int nthin, const int*
  * divides by 1000, :103).  Negative entries contribute nothing, as in
  * MB/reprojection_TOMO.cpp:151-155. */
 int vct_set_maps(vct_ctx* ctx, const int16_t* maps, int M);
+/* Stored map units per g/cm^3 (default 1000, the reference's "density x
+ * 1000").  A finer scale (e.g. 16384: densities up to 2 g/cm^3 in steps of
+ * 6e-5) lets iterative callers take small steps; no counterpart in the
+ * reference.  Applies to the maps of every later call. */
+int vct_set_density_scale(vct_ctx* ctx, double units_per_gcc);
 int vct_set_maps_dev(vct_ctx* ctx, const int16_t* d_maps, int M);
 
 /* Uploads mu [M][NE] (bin fastest, the Attenuation layout of
@@ -217,6 +222,15 @@ int vct_forward_vjp_dev(vct_ctx* ctx, const float* d_dy, float* d_grad);
  * maps' element count; the transpose of vct_line_integrals_dev. */
 int vct_adjoint_rays_dev(vct_ctx* ctx, const float* d_g, float* d_out);
 
+/* One projected gradient-descent step on device densities (no counterpart in
+ * the reference): rho[i] = max(0, rho[i] - step * (grad_a[i] + grad_b[i]))
+ * for i < count (grad_b may be NULL: one gradient), then maps[i] =
+ * rho[i] * units rounded to nearest and clamped to [0, 32767], ready for
+ * vct_set_maps_dev.  Enqueued on stream (a cudaStream_t, NULL: legacy
+ * default stream); allocates nothing. */
+int vct_descent_step_dev(float* d_rho, const float* d_grad_a, const float* d_grad_b, double step, double units,
+                         int16_t* d_maps, long long count, void* stream);
+
 /* ------------------------------------------------------------------ batch
  * Many slices of uneven size (geometry, grid, spectrum) in one captured CUDA
  * graph; no counterpart in the reference, which runs one slice per process.
@@ -249,6 +263,7 @@ typedef struct vct_job {
   const float* d_weights; /* device [views][width] or NULL */
   float* d_grad;          /* device [M][N][N] */
   double* d_loss;         /* device double, or NULL */
+  double density_units;   /* map units per g/cm^3; 0 means 1000 (vct_set_density_scale) */
 } vct_job;
 typedef struct vct_batch vct_batch;
 int vct_batch_create(const vct_job* jobs, int n, int M, int device, int tune, vct_batch** out);

@@ -49,6 +49,7 @@ EXPORTED_SYMBOLS = (
     "vct_set_sum_mode", "vct_set_walk_mode", "vct_forward", "vct_forward_dev", "vct_line_integrals_dev", "vct_mbfpa", "vct_mbfpa_dev",
     "vct_normalize_noise_dev", "vct_fbp", "vct_fbp_dev", "vct_fbp_noalloc", "vct_fbp_filtered_dev",
     "vct_fbp_transpose", "vct_fbp_transpose_dev",
+    "vct_set_density_scale", "vct_descent_step_dev",
     "vct_forward_adjoint", "vct_forward_adjoint_dev", "vct_forward_vjp_dev", "vct_adjoint_rays_dev",
     "vct_batch_create", "vct_batch_run", "vct_batch_synchronize", "vct_batch_config", "vct_batch_destroy",
     "vct_forward_batched",
@@ -79,7 +80,7 @@ class _CJob(C.Structure):
         ("geo", _CGeometry), ("d_maps", C.c_void_p), ("mu", C.c_void_p), ("pdf", C.c_void_p), ("NE", C.c_int),
         ("sigma", C.c_double), ("seed", C.c_uint64), ("d_sino", C.c_void_p), ("d_img", C.c_void_p),
         ("filter", C.c_int), ("d_meas", C.c_void_p), ("d_weights", C.c_void_p), ("d_grad", C.c_void_p),
-        ("d_loss", C.c_void_p),
+        ("d_loss", C.c_void_p), ("density_units", C.c_double),
     ]
 
 
@@ -158,6 +159,8 @@ def lib():
     L.vct_fbp_transpose.argtypes = [vp, vp, C.c_int, vp]
     L.vct_fbp_transpose_dev.argtypes = [vp, vp, C.c_int, vp]
     L.vct_fbp_noalloc.argtypes = [C.POINTER(_CGeometry), vp, C.c_int, C.c_int, vp, vp]
+    L.vct_set_density_scale.argtypes = [vp, C.c_double]
+    L.vct_descent_step_dev.argtypes = [vp, vp, vp, C.c_double, C.c_double, vp, C.c_longlong, vp]
     L.vct_forward_adjoint.argtypes = [vp, vp, vp, vp, C.POINTER(C.c_double)]
     L.vct_forward_adjoint_dev.argtypes = [vp, vp, vp, vp, vp]
     L.vct_forward_vjp_dev.argtypes = [vp, vp, vp]
@@ -284,6 +287,10 @@ class Context:
         _check(lib().vct_set_maps(self._h, _ptr(a), a.shape[0]), "vct_set_maps")
         self._M = a.shape[0]
 
+    def set_density_scale(self, units_per_gcc: float) -> None:
+        """Map units per g/cm^3 (default 1000)."""
+        _check(lib().vct_set_density_scale(self._h, float(units_per_gcc)), "vct_set_density_scale")
+
     def set_spectrum(self, mu, pdf) -> None:
         mu = np.ascontiguousarray(mu, np.float32)
         pdf = np.ascontiguousarray(pdf, np.float32)
@@ -395,13 +402,15 @@ class Job:
     ``data_ptr()``); mu [M][NE] and pdf [NE] are host arrays."""
 
     def __init__(self, geometry: Geometry, maps, mu, pdf, *, sino=None, img=None, filter: int = 1,
-                 sigma: float = 0.0, seed: int = 1, meas=None, weights=None, grad=None, loss=None):
+                 sigma: float = 0.0, seed: int = 1, meas=None, weights=None, grad=None, loss=None,
+                 density_units: float = 0.0):
         self.geometry = geometry
         self.maps, self.sino, self.img, self.meas, self.weights, self.grad, self.loss = (
             maps, sino, img, meas, weights, grad, loss)
         self.mu = np.ascontiguousarray(mu, np.float32)
         self.pdf = np.ascontiguousarray(pdf, np.float32)
         self.filter, self.sigma, self.seed = filter, sigma, seed
+        self.density_units = density_units
 
     def to_c(self) -> _CJob:
         j = _CJob()
@@ -414,6 +423,7 @@ class Job:
         j.seed = int(self.seed)
         j.d_sino, j.d_img, j.filter = _dp(self.sino), _dp(self.img), int(self.filter)
         j.d_meas, j.d_weights, j.d_grad, j.d_loss = _dp(self.meas), _dp(self.weights), _dp(self.grad), _dp(self.loss)
+        j.density_units = float(self.density_units)
         return j
 
 
@@ -454,3 +464,10 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def descent_step_dev(rho, grad_a, grad_b, step: float, units: float, maps, stream_ptr: int | None = None) -> None:
+    """rho -= step * (grad_a + grad_b), clamped at 0; maps = round(rho * units)
+    (device tensors of the same element count; grad_b may be None)."""
+    _check(lib().vct_descent_step_dev(rho.data_ptr(), grad_a.data_ptr(), _dp(grad_b), float(step), float(units),
+                                      maps.data_ptr(), rho.numel(), stream_ptr), "vct_descent_step_dev")

@@ -143,7 +143,7 @@ adj_forward_kernel(DevGeom g, const PixelRec* __restrict__ maps, const double* _
         walk_exact<M>(g, maps, r, a);
     }
     double L[8];
-    finish_lines<M>(a, L);
+    finish_lines<M>(a, L, g.dens_div);
     double y = 0.0, D[M];
 #pragma unroll
     for (int m = 0; m < M; m++) D[m] = 0.0;

@@ -263,6 +263,7 @@ int vct_batch_create(const vct_job* jobs, int n, int M, int device, int tune, vc
     vct_ctx* c = nullptr;
     if ((rc = vct_create(&j.geo, device, &c))) return bail(rc);
     b->ctx.push_back(c);
+    if (j.density_units > 0 && (rc = vct_set_density_scale(c, j.density_units))) return bail(rc);
     if ((rc = vct_set_spectrum(c, j.mu, j.pdf, M, j.NE)) || (rc = vct_set_maps_dev(c, j.d_maps, M))) return bail(rc);
     b->ne_max = std::max(b->ne_max, j.NE);
     if (adj) {

@@ -146,7 +146,7 @@ forward_kernel(DevGeom g, const PixelRec* __restrict__ maps, const double* __res
     }
     nseg = a.nseg;
     double L[8];
-    finish_lines<M>(a, L);
+    finish_lines<M>(a, L, g.dens_div);
     if (lint) {
 #pragma unroll
       for (int m = 0; m < M; m++) lint[ray * M + m] = L[m];
@@ -297,7 +297,7 @@ forward_batch_kernel(const FwdJob* __restrict__ jobs, int njobs, int tile_rays, 
         }
         nseg = a.nseg;
         double L[8];
-        finish_lines<M>(a, L);
+        finish_lines<M>(a, L, g.dens_div);
         val = spectral_compensated<M>(L, s_mu, s_pdf, J.NE);
         J.out[(size_t)v * g.width + g.start + c] = val;
       }

@@ -106,6 +106,7 @@ int vct_create(const vct_geometry* g, int device, vct_ctx** out) {
   // square plus one (pixel-sized) poke-out step.
   dg.rmax_active = (dg.lim * sqrt(2.0) + 2.0 * g->pixel_cm) >= dg.rmax ? 1 : 0;
   dg.sid = g->sid_cm;
+  dg.dens_div = 1000.0;
   dg.views = g->views;
   dg.views_used = g->views / 2 * 2;
   dg.width = g->width;
@@ -349,6 +350,14 @@ int vct_set_spectrum(vct_ctx* c, const float* mu, const float* pdf, int M, int N
   c->ynorm = 0.0;
   for (int e = 0; e < NE; e++) c->ynorm += (double)pdf[e];
   c->spectrum_ready = 1;
+  return VCT_OK;
+}
+
+int vct_set_density_scale(vct_ctx* c, double units_per_gcc) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!(units_per_gcc > 0) || !(units_per_gcc < 1e9)) return fail(VCT_E_ARG, "vct_set_density_scale: bad scale");
+  c->dg.dens_div = units_per_gcc;
   return VCT_OK;
 }
 

@@ -36,6 +36,7 @@ struct DevGeom {
   int width;       // projImgWidth
   int C;           // end_channel - start_channel
   int start;       // start_channel
+  double dens_div; // stored density units per g/cm^3 (1000: the reference's maps)
 };
 
 // Packed maps: one 16-byte record per pixel, 8 int16 materials (unused

@@ -106,13 +106,19 @@ VCT_HD void acc_init(RayAcc& a) {
   a.nseg = 0;
 }
 
+// L_m in g/cm^2: densities are the stored values divided by `div` (1000, the
+// reference's density x 1000, unless the context sets another scale).
 template <int M>
-VCT_HD void finish_lines(const RayAcc& a, double L[8]) {
+VCT_HD void finish_lines(const RayAcc& a, double L[8], double div) {
 #pragma unroll
   for (int m = 0; m < M; m++) {
     const double steps = (double)a.Lq[m] * (1.0 / 1073741824.0);
-    L[m] = (a.Ld[m] + steps * a.sec) / 1000.0;
+    L[m] = (a.Ld[m] + steps * a.sec) / div;
   }
+}
+template <int M>
+VCT_HD void finish_lines(const RayAcc& a, double L[8]) {
+  finish_lines<M>(a, L, 1000.0);
 }
 
 template <int M>

@@ -1,0 +1,121 @@
+"""Material decomposition by projected gradient descent on the element
+density maps, driven by the adjoint of the forward projector (no counterpart
+in the reference, whose iterative step is a multiplicative ratio update).
+
+Each slice has one measured sinogram per spectrum (dual energy: two).  One
+iteration takes, per slice, a trial step from the last accepted point along
+the sum of its spectra's gradients (vct_descent_step_dev),
+
+    rho <- max(0, rho - step_s * sum_E dl_E/drho),   maps <- round(rho * units)
+
+then evaluates the loss and gradient of every (slice, spectrum) pair at the
+trial points -- all pairs in ONE adjoint batch replay, the path lengths
+recomputed by the walk, never stored.  A slice whose loss fell keeps the
+trial point and grows its step by 1.25; otherwise it returns to its previous
+point and halves its step, so every slice's loss falls monotonically.  The
+device holds rho (float) and the maps (int16 at `units` per g/cm^3, 16384 by
+default: steps of 6e-5 g/cm^3); the host reads S x E losses per iteration.
+"""
+from __future__ import annotations
+
+import numpy as np
+
+from . import Batch, Geometry, Job, descent_step_dev
+
+
+class Decomposition:
+    def __init__(self, geometry: Geometry, spectra, measured, rho0, *, units: float = 16384.0,
+                 step: float | None = None, max_change: float = 0.003, tune: bool = True, device: int = 0):
+        """geometry: one Geometry for every slice; spectra: [(mu [M][NE], pdf
+        [NE]), ...] one per energy; measured: [slice][energy] CUDA tensors
+        [views][width] (max-normalised transmissions); rho0: CUDA float tensor
+        [S][M][N][N] (g/cm^3), updated in place.  step: fixed step (g/cm^3 per
+        gradient unit); None picks max_change / max|gradient| of the first
+        evaluation."""
+        import torch
+
+        self.geometry, self.units = geometry, float(units)
+        S, M = int(rho0.shape[0]), int(rho0.shape[1])
+        E = len(spectra)
+        if len(measured) != S or any(len(m) != E for m in measured):
+            raise ValueError("measured must be [slices][energies]")
+        self.S, self.M, self.E = S, M, E
+        self.rho = rho0
+        self.maps = torch.round(rho0 * self.units).clamp(0, 32767).to(torch.int16).contiguous()
+        N = geometry.recon_size
+        self.grads = torch.zeros((S, E, M, N, N), dtype=torch.float32, device=rho0.device)
+        self.loss = torch.zeros((S, E), dtype=torch.float64, device=rho0.device)
+        jobs = []
+        for s in range(S):
+            for e, (mu, pdf) in enumerate(spectra):
+                jobs.append(Job(geometry, self.maps[s], mu, pdf, meas=measured[s][e], grad=self.grads[s, e],
+                                loss=self.loss[s, e:e + 1], density_units=self.units))
+        self.batch = Batch(jobs, M=M, device=device, tune=tune)
+        self.rho_prev = torch.empty_like(rho0)
+        self.g = torch.zeros((S, M, N, N), dtype=torch.float32, device=rho0.device)  # at the accepted point
+        self.step_size = np.full(S, np.nan if step is None else float(step))
+        self.max_change = max_change
+        self.cur_loss = None
+        self.history: list[float] = []
+        self.accepted = 0
+        self.rejected = 0
+
+    def gradients(self, stream_ptr: int | None = None) -> None:
+        """Loss and gradient of every (slice, energy) pair at the current maps."""
+        self.batch.run(stream_ptr)
+
+    def _requantize(self, s: int, stream_ptr) -> None:
+        descent_step_dev(self.rho[s], self.g[s], None, 0.0, self.units, self.maps[s], stream_ptr)
+
+    def iterate(self, n: int = 1, stream_ptr: int | None = None) -> None:
+        """n iterations (n loss + gradient evaluations of the whole batch)."""
+        import torch
+
+        if self.cur_loss is None:
+            self._requantize_all(stream_ptr)
+            self.gradients(stream_ptr)
+            torch.cuda.synchronize()
+            self.cur_loss = self.loss.sum(1).cpu().numpy()
+            torch.sum(self.grads, 1, out=self.g)
+            gmax = self.g.abs().amax(dim=(1, 2, 3)).cpu().numpy()
+            fresh = np.isnan(self.step_size)
+            self.step_size[fresh] = np.where(gmax[fresh] > 0, self.max_change / np.maximum(gmax[fresh], 1e-30), 0.0)
+            self.history.append(float(self.cur_loss.sum()))
+            n -= 1
+        for _ in range(max(n, 0)):
+            self.rho_prev.copy_(self.rho)
+            for s in range(self.S):
+                descent_step_dev(self.rho[s], self.g[s], None, float(self.step_size[s]), self.units, self.maps[s],
+                                 stream_ptr)
+            self.gradients(stream_ptr)
+            torch.cuda.synchronize()
+            new = self.loss.sum(1).cpu().numpy()
+            for s in range(self.S):
+                if new[s] < self.cur_loss[s]:
+                    self.cur_loss[s] = new[s]
+                    torch.sum(self.grads[s], 0, out=self.g[s])
+                    self.step_size[s] *= 1.25
+                    self.accepted += 1
+                else:
+                    self.rho[s].copy_(self.rho_prev[s])
+                    self._requantize(s, stream_ptr)
+                    self.step_size[s] *= 0.5
+                    self.rejected += 1
+            self.history.append(float(self.cur_loss.sum()))
+
+    def _requantize_all(self, stream_ptr) -> None:
+        for s in range(self.S):
+            self._requantize(s, stream_ptr)
+
+    def total_loss(self) -> float:
+        """Total loss at the accepted points."""
+        return float(self.cur_loss.sum()) if self.cur_loss is not None else float("nan")
+
+    def close(self) -> None:
+        self.batch.close()
+
+
+def rays_bins_per_iteration(geometry: Geometry, spectra, slices: int) -> int:
+    """Rays x energy bins of one iteration (every slice, every spectrum)."""
+    rays = geometry.views // 2 * 2 * geometry.channels
+    return int(slices * rays * sum(len(np.asarray(p)) for _, p in spectra))

@@ -178,6 +178,8 @@ def run_ours(args, rank, world, dist):
         extras["fbp_transpose"] = bench_fbp_transpose(ctx, stream, timed, args.steps, args.warmup)
     if "batched" in want:
         extras["batched"] = bench_batched(stream, args.warmup, n=args.batch_slices)
+    if "scale" in want:
+        extras["scale"] = bench_scale(stream, args.scale_slices, args.scale_iters)
     if "batched_adjoint" in want:
         extras["batched_adjoint"] = bench_batched_adjoint(stream, args.warmup, n=max(args.batch_slices // 4, 1))
     clk.__exit__(None, None, None)
@@ -454,6 +456,62 @@ def bench_batched_adjoint(stream, warmup, n=64):
             "plain_ms_per_batch": t_plain, "speedup_vs_plain": t_plain / t_batch, "tuned": cfg}
 
 
+def bench_scale(stream, slices=64, iters=2):
+    """The scale configuration: 1024^2 at 0.05 cm, 8 elements (H C N O P Ca
+    Mg Si), 1440 views x 1600 channels, dual energy 80/140 kVp, `slices`
+    seeded slices; projected gradient-descent material decomposition, each
+    iteration the loss + gradient of every (slice, spectrum) pair in one
+    adjoint batch (path lengths recomputed by the walk) and a descent step per
+    slice.  Measured sinograms: the noisy MBFPA of each phantom; start: 0.9 x
+    the phantom.  One untimed first evaluation, then `iters` timed
+    iterations (CUDA events; the per-iteration host read of the losses is
+    inside)."""
+    import torch
+
+    import virtualct_b200 as vct
+    from virtualct_b200 import phantoms
+    from virtualct_b200.decomposition import Decomposition, rays_bins_per_iteration
+
+    el = phantoms.ELEMENTS8
+    tabs = [phantoms.kramers_tables(k, el) for k in (80, 140)]
+    geo = vct.Geometry.with_channels(1600, views=1440, recon_size=1024, pixel_cm=0.05)
+    t0 = time.perf_counter()
+    meas, rho0 = [], []
+    with vct.Context(geo) as ctx:
+        for s in range(slices):
+            m = phantoms.ellipse_phantom(1000 + s, 1024, elements=el)
+            ctx.set_maps(m)
+            per = []
+            for e, tab in enumerate(tabs):
+                ctx.set_spectrum(*tab)
+                out = torch.empty((geo.views, geo.width), dtype=torch.float32, device="cuda")
+                ctx.mbfpa_dev(SIGMA, 2 * s + e, out)
+                per.append(out)
+            meas.append(per)
+            rho0.append(torch.from_numpy(m.astype(np.float32) / 1000.0 * 0.9))
+        ctx.synchronize()
+    rho = torch.stack(rho0).cuda()
+    dec = Decomposition(geo, tabs, meas, rho)
+    dec.iterate(1)
+    setup_s = time.perf_counter() - t0
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    dec.iterate(iters)
+    e1.record()
+    torch.cuda.synchronize()
+    t = e0.elapsed_time(e1) / iters
+    units = rays_bins_per_iteration(geo, tabs, slices)
+    line = {"workload": f"{slices} slices, 1024^2 at 0.05 cm, 8 elements, 1440 views x 1600 channels, 80/140 kVp; "
+                        "projected gradient descent, loss + gradient of every slice and spectrum per iteration",
+            "ms_per_iteration": t, "value": units / t * 1e3, "unit": "rays*bins/s (forward + adjoint)",
+            "iterations_timed": iters, "projected_50_iterations_s": 50 * t / 1e3,
+            "loss_first": dec.history[0], "loss_last": dec.history[-1], "accepted": dec.accepted,
+            "rejected": dec.rejected, "setup_s": setup_s}
+    dec.close()
+    return line
+
+
 def cpu_baseline(maps, mu, pdf):
     """The reference's reprojection_TOMO (oracle/_ref, built from its sources)
     on all host cores for a bounded sample: 2 of the 110 energy bins over the
@@ -544,8 +602,11 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the adjoint and batched lines")
     ap.add_argument("--batch-slices", type=int, default=256,
                     help="slices of the batched line (the batched adjoint line takes a quarter)")
-    ap.add_argument("--extras", default="adjoint,fbp_transpose,batched,batched_adjoint",
-                    help="comma list of extra lines (1 GPU): adjoint, fbp_transpose, batched, batched_adjoint")
+    ap.add_argument("--extras", default="adjoint,fbp_transpose,batched,batched_adjoint,scale",
+                    help="comma list of extra lines (1 GPU): adjoint, fbp_transpose, batched, batched_adjoint, scale")
+    ap.add_argument("--scale-slices", type=int, default=64, help="slices of the scale line")
+    ap.add_argument("--scale-iters", type=int, default=2,
+                    help="timed descent iterations of the scale line (the configuration runs 50)")
     args = ap.parse_args()
     args.warmup = max(args.warmup, 3) if args.impl == "ours" else args.warmup
     world = int(os.environ.get("WORLD_SIZE", "1"))

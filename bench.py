@@ -174,6 +174,8 @@ def run_ours(args, rank, world, dist):
     want = set() if args.no_extras or world > 1 else set(args.extras.split(","))
     if "adjoint" in want:
         extras["adjoint"] = bench_adjoint(ctx, d_maps, mu, pdf, stream, timed, args.steps, args.warmup)
+    if "lengthproj" in want:
+        extras["lengthproj"] = bench_lengthproj(ctx, stream, timed, args.steps, args.warmup)
     if "fbp_transpose" in want:
         extras["fbp_transpose"] = bench_fbp_transpose(ctx, stream, timed, args.steps, args.warmup)
     if "batched" in want:
@@ -328,6 +330,22 @@ def bench_adjoint(ctx, d_maps, mu, pdf, stream, timed, steps, warmup):
             "gather_ms": t_g * 1e3, "gather_pixel_views_per_s": N * N * V / t_g,
             "kernels_per_gradient": int(launches), "loss": float(loss.item()),
             "notes": "deterministic: pixel-driven A^T, no float atomics"}
+
+
+def bench_lengthproj(ctx, stream, timed, steps, warmup):
+    """lengthproj_TOMO of a 800 x 609 sinogram onto the 512^2 mask (helical
+    couch 0.8 cm/rotation at z = 3 cm), FP64 geometry per pixel and view."""
+    import torch
+
+    proj = torch.rand((V, C), dtype=torch.float32, device="cuda", generator=torch.Generator("cuda").manual_seed(7))
+    npf = torch.empty((N, N), dtype=torch.float32, device="cuda")
+    fn = lambda: ctx.lengthproj_dev(proj, npf, 3.0, 0.8)  # noqa: E731
+    for _ in range(warmup):
+        fn()
+    t = timed(fn, steps) / steps
+    mask_px = 205012
+    return {"workload": "lengthproj_TOMO: 512^2 mask (205,012 pixels) x 800 views, 609 channels",
+            "ms_per_slice": t * 1e3, "pixel_views_per_s": mask_px * V / t}
 
 
 def bench_fbp_transpose(ctx, stream, timed, steps, warmup):
@@ -602,8 +620,9 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the adjoint and batched lines")
     ap.add_argument("--batch-slices", type=int, default=256,
                     help="slices of the batched line (the batched adjoint line takes a quarter)")
-    ap.add_argument("--extras", default="adjoint,fbp_transpose,batched,batched_adjoint,scale",
-                    help="comma list of extra lines (1 GPU): adjoint, fbp_transpose, batched, batched_adjoint, scale")
+    ap.add_argument("--extras", default="adjoint,lengthproj,fbp_transpose,batched,batched_adjoint,scale",
+                    help="comma list of extra lines (1 GPU): adjoint, lengthproj, fbp_transpose, batched, "
+                         "batched_adjoint, scale")
     ap.add_argument("--scale-slices", type=int, default=64, help="slices of the scale line")
     ap.add_argument("--scale-iters", type=int, default=2,
                     help="timed descent iterations of the scale line (the configuration runs 50)")

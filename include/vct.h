@@ -150,6 +150,21 @@ int vct_line_integrals_dev(vct_ctx* ctx, double* d_lint_out);
 int vct_mbfpa(vct_ctx* ctx, double sigma, uint64_t seed, float* sino_out, float* stats);
 int vct_mbfpa_dev(vct_ctx* ctx, double sigma, uint64_t seed, float* d_sino_out);
 
+/* lengthproj_TOMO (MB/lengthproj_TOMO.cpp:14-185; the reference's main calls
+ * it at MB/main.cpp:407 and writes npf_float.raw): for every pixel of the
+ * reconstruction circle, npf = sum over the views/2*2 views used of
+ * (float)(lerp(proj, dj) * rr) -- rr the pixel-width chord of the line from
+ * the source to the pixel centre, dj the channel where that line meets the
+ * curved detector, edge channels clamped -- in float, in view order.
+ * proj: [views/2*2][width], row k = the k-th view used (as main.cpp:354-370
+ * builds it); z and couch_speed are the txt's reconstruction z and couch
+ * speed.  The first view is the reference's (int)(z/pitch - views/2 + 1e-8)
+ * (pitch = couch_speed/views), wrapped into the rotation; with couch_speed 0
+ * (where the reference divides 0/0) the views start at 0.  npf: [N][N], 0
+ * outside the circle.  The reference's [N][N][V] side tables are not kept. */
+int vct_lengthproj(vct_ctx* ctx, const float* proj, double z, double couch_speed, float* npf);
+int vct_lengthproj_dev(vct_ctx* ctx, const float* d_proj, double z, double couch_speed, float* d_npf);
+
 /* Only the normalisation + noise step on a device sinogram (in place). */
 int vct_normalize_noise_dev(vct_ctx* ctx, float* d_sino, double sigma, uint64_t seed);
 

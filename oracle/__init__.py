@@ -95,6 +95,7 @@ def lib():
         L.orc_siddon.restype = C.c_int
         L.orc_walk_project.argtypes = [C.POINTER(OrcGeom), _dp, _dp, _dp, C.c_int, _dp, C.c_int]
         L.orc_walk_backproject.argtypes = [C.POINTER(OrcGeom), _dp, _dp, _dp, C.c_int, _dp, C.c_int]
+        L.orc_lengthproj.argtypes = [C.POINTER(OrcGeom), _dp, _dp, _fp, C.c_double, C.c_double, _fp]
         L.orc_walk_project_rays.argtypes = [C.POINTER(OrcGeom), _dp, _dp, _dp, C.c_int, _ip, C.c_int, _dp, C.c_int]
         L.orc_siddon_project.argtypes = [C.POINTER(OrcGeom), _dp, _dp, _dp, C.c_int, _dp, C.c_int]
         L.orc_normalize_noise.argtypes = [_fp, C.c_int, C.c_double, C.c_uint, C.c_int]
@@ -368,6 +369,26 @@ def fbp_transpose(g, u, filt, cos_t, sin_t):
     return out
 
 
+def ref_lengthproj(N, pixel_cm, proj, V, cos_t, sin_t, z, couch_speed):
+    """The reference's own lengthproj_TOMO (oracle/_ref); 609 channels."""
+    proj = np.ascontiguousarray(proj, np.float32)
+    out = np.zeros((N, N), np.float32)
+    secs = C.c_double()
+    rc = ref_mb().vctref_lengthproj(N, pixel_cm, proj, proj.shape[1], V, np.ascontiguousarray(cos_t),
+                                    np.ascontiguousarray(sin_t), float(z), float(couch_speed), out, C.byref(secs))
+    if rc:
+        raise RuntimeError(f"vctref_lengthproj failed ({rc})")
+    return out, secs.value
+
+
+def lengthproj(g, cos_t, sin_t, proj, z=0.0, couch_speed=0.0):
+    """lengthproj_TOMO restated: npf [N][N] from proj [views used][width]."""
+    proj = np.ascontiguousarray(proj, np.float32)
+    out = np.zeros((g.recon_size, g.recon_size), np.float32)
+    lib().orc_lengthproj(C.byref(g), cos_t, sin_t, proj, float(z), float(couch_speed), out)
+    return out
+
+
 def mask(N):
     m = np.zeros(N * N, np.uint8)
     lib().orc_mask(N, m)
@@ -387,6 +408,9 @@ def ref_mb():
         L.vctref_attenuation.restype = C.c_int
         L.vctref_set_threads.argtypes = [C.c_int]
         L.vctref_set_threads.restype = C.c_int
+        L.vctref_lengthproj.argtypes = [C.c_int, C.c_double, _fp, C.c_int, C.c_int, _dp, _dp, C.c_double, C.c_double,
+                                        _fp, C.POINTER(C.c_double)]
+        L.vctref_lengthproj.restype = C.c_int
         L.vctref_reprojection_bins.argtypes = [C.c_int, C.c_double, _fp, C.c_int, C.c_int, _dp, _dp, C.c_int,
                                                _fp, _fp, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
                                                C.c_void_p, C.POINTER(C.c_double)]

@@ -7,6 +7,8 @@
 //   attenuation_coefficient  Release_MBFPA_CPU_human/prior_weight_production.cpp:180
 //   reprojection_TOMO        Release_MBFPA_CPU_human/reprojection_TOMO.cpp:13
 //   energy loop + sum        Release_MBFPA_CPU_human/main.cpp:492-506
+//   lengthproj_TOMO          Release_MBFPA_CPU_human/lengthproj_TOMO.cpp:14
+//   prepareMaskData          Release_MBFPA_CPU_human/misc_TOMO.cpp:10
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -20,6 +22,8 @@
 #include "physParamsTOMO.h"
 #include "mallocMD.h"
 #include "reprojection_TOMO.h"
+#include "lengthproj_TOMO.h"
+#include "misc_TOMO.h"
 #include "virtual_projection.h"
 
 static double now_s() {
@@ -118,6 +122,32 @@ int vctref_reprojection_bins(int N, double pixel_cm, const float* rho, int V, in
   if (last_bin) memcpy(last_bin, proj, sizeof(float) * V * W);
   if (nseg) memcpy(nseg, rsum, sizeof(int) * V * W);
   free(work); free(proj); free(rsum); free(mask);
+  return 0;
+}
+
+// Runs lengthproj_TOMO on one slice: proj is the sinogram the reference's
+// main passes (rows j_one = 0.. of the views used, W floats each), cos/sin
+// the V-entry trig tables, z and couch_speed the txt's values.  The system
+// matrix and detector-position side tables it writes ([N][N][V] floats each)
+// are allocated here and dropped.
+int vctref_lengthproj(int N, double pixel_cm, const float* proj, int W, int V, const double* cosT,
+                      const double* sinT, double z, double couch_speed, float* npf, double* seconds) {
+  if (W < End_Channel) return -1;
+  size_t n2 = (size_t)N * N;
+  float* sysmat = (float*)malloc(sizeof(float) * n2 * V);
+  float* tracedet = (float*)malloc(sizeof(float) * n2 * V);
+  char* mask = prepareMaskData(N);
+  if (!sysmat || !tracedet || !mask) {
+    free(sysmat); free(tracedet);
+    return -2;
+  }
+  memset(npf, 0, sizeof(float) * n2);
+  double t0 = now_s();
+  lengthproj_TOMO(0, N, npf, (float*)proj, pixel_cm, W, V, (double*)cosT, (double*)sinT, z, couch_speed, mask,
+                  sysmat, tracedet, 1);
+  if (seconds) *seconds = now_s() - t0;
+  free(sysmat); free(tracedet);
+  delete1DArray(mask);
   return 0;
 }
 

@@ -871,3 +871,105 @@ void orc_walk_project_rays(const orc_geom* g, const double* cos_t, const double*
     free(pix);
   }
 }
+
+/* ------------------------------------------------------------ lengthproj */
+/* First view of the slice and view count, MB/lengthproj_TOMO.cpp:36-47. */
+static void orc_lp_views(const orc_geom* g, double z, double couch_speed, int* start, int* count, int* nrot) {
+  const int V = g->views;
+  const int used = V / 2 * 2; /* sngrmHeight/UsedReconAngle*2 with UsedReconAngle 2 */
+  int s0 = 0;
+  if (couch_speed != 0.0) {
+    const double pitch = (double)(couch_speed / V);
+    s0 = (int)(z / pitch - V / 2 + 0.00000001);
+  }
+  *start = s0;
+  *count = used;
+  *nrot = s0 / V;
+}
+
+void orc_lengthproj(const orc_geom* g, const double* cos_t, const double* sin_t, const float* proj, double z,
+                    double couch_speed, float* npf) {
+  const int N = g->recon_size, V = g->views, W = g->width;
+  const double s = g->pixel_cm;
+  const int C = g->end_channel - g->start_channel;
+  const int half = (C - 1) / 2;
+  const double dalpha = g->max_alpha / half;
+  const double R = g->det_radius;            /* DETECTOR_RADIUS_CURVATURE_CM */
+  const double dsrc = g->det_src_iso;        /* DIST_BTWN_DETERCTORSRC_AND_ISOCENT_CM */
+  const double diso = g->det_radius - g->sid; /* DIST_BTWN_ISO_AND_DETECTOR_CM (142.6 - 85) */
+  int start, count, nrot;
+  orc_lp_views(g, z, couch_speed, &start, &count, &nrot);
+  unsigned char* mask = (unsigned char*)malloc((size_t)N * N);
+  orc_mask(N, mask);
+  memset(npf, 0, sizeof(float) * (size_t)N * N);
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static)
+#endif
+  for (int jy = 0; jy < N; jy++) {
+    const double ry = N * s * 0.5 - (jy + 0.5) * s;
+    for (int jx = 0; jx < N; jx++) {
+      if (!mask[jy * N + jx]) continue;
+      const double rx = -N * s * 0.5 + (jx + 0.5) * s;
+      float acc = 0.0f;
+      for (int k = 0; k < count; k++) {
+        int v = start + k - nrot * V;
+        if (v >= V) v -= V;
+        if (v < 0) v += V; /* the reference reads its tables out of range here */
+        const double cb = cos_t[v], sb = sin_t[v];
+        const double sx = g->sid * sb, sy = g->sid * cb;
+        double len;
+        if (fabs(rx - sx) > fabs(ry - sy)) {
+          /* chord across the pixel column, x-major */
+          const double x0 = rx - 0.5 * s, x1 = rx + 0.5 * s;
+          const double y0 = (x0 - sx) / (rx - sx) * (ry - sy) + sy;
+          const double y1 = (x1 - sx) / (rx - sx) * (ry - sy) + sy;
+          len = sqrt((x0 - x1) * (x0 - x1) + (y0 - y1) * (y0 - y1));
+        } else {
+          /* y-major: the reference evaluates both ends at y0, so only the
+           * y extent remains (:95-101) */
+          const double y0 = ry - 0.5 * s, y1 = ry + 0.5 * s;
+          len = sqrt((y0 - y1) * (y0 - y1));
+        }
+        /* the source-pixel line meets the detector circle (centre dsrc on
+         * the source side, radius R); the hit nearer the origin (:110-134) */
+        const double dx = dsrc * sb, dy = dsrc * cb;
+        const double a = (sy - ry) / (sx - rx);
+        const double b = -sx * (sy - ry) / (sx - rx) + sy;
+        const double qa = 1.0 + a * a;
+        const double qb = 2.0 * a * b - 2.0 * a * dy - 2.0 * dx;
+        const double qc = dx * dx + b * b + dy * dy - 2.0 * b * dy - R * R;
+        const double disc = sqrt(qb * qb - 4.0 * qa * qc);
+        const double x1 = (-qb + disc) / (2.0 * qa), y1 = a * x1 + b;
+        const double x2 = (-qb - disc) / (2.0 * qa), y2 = a * x2 + b;
+        double px, py;
+        if (x1 * x1 + y1 * y1 > x2 * x2 + y2 * y2) {
+          px = x2;
+          py = y2;
+        } else {
+          px = x1;
+          py = y1;
+        }
+        /* detector angle from the detector's centre point (:136-150) */
+        const double ox = -diso * sb, oy = -diso * cb;
+        const double d2 = (px - ox) * (px - ox) + (py - oy) * (py - oy);
+        const double ang = acos(1.0 - d2 / (2.0 * R * R));
+        const double rpx = px * cb - py * sb;
+        const double dj = rpx > 0.0 ? g->iso_channel - ang / dalpha : g->iso_channel + ang / dalpha;
+        const int ij = dj == dj ? (int)dj : 0;
+        const double f = dj - (double)ij;
+        const float* row = proj + (size_t)k * W;
+        /* three explicit tests, as :158-172: a NaN channel (a source on the
+         * pixel's vertical, 0/0 in the line slope) matches none and adds
+         * nothing */
+        if (g->start_channel <= dj && dj < g->end_channel - 1)
+          acc += (float)(((1.0 - f) * row[ij] + f * row[ij + 1]) * len);
+        else if (g->start_channel > dj)
+          acc += (float)(row[g->start_channel] * len);
+        else if (dj >= g->end_channel - 1)
+          acc += (float)(row[g->end_channel - 1] * len);
+      }
+      npf[jy * N + jx] = acc;
+    }
+  }
+  free(mask);
+}

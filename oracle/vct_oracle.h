@@ -112,6 +112,17 @@ void orc_walk_project_rays(const orc_geom* g, const double* cos_t, const double*
 void orc_walk_backproject(const orc_geom* g, const double* cos_t, const double* sin_t, const double* w, int M,
                           double* out, int nthreads);
 
+/* lengthproj_TOMO (MB/lengthproj_TOMO.cpp:14-185) for one slice: for every
+ * mask pixel, npf = sum over the views used of (float)(lerp(proj, dj) * rr),
+ * rr the pixel-width chord of the source-to-pixel-centre line, dj its hit on
+ * the curved detector in channels, accumulated in float in view order.
+ * proj: [views used][width] (row = view index from the first view used).
+ * The first view follows the reference's z / pitch formula; with
+ * couch_speed == 0 (pitch 0, where the reference divides 0/0 and reads its
+ * trig tables out of range) the views start at 0. */
+void orc_lengthproj(const orc_geom* g, const double* cos_t, const double* sin_t, const float* proj, double z,
+                    double couch_speed, float* npf);
+
 /* Max-normalisation (MB/main.cpp:511-522) followed by gaussiannoise0
  * (MB/main.cpp:42-76) with glibc rand() after srand(seed) (the reference
  * never seeds: seed 1).  order selects which Uniform0() call in rand_gauss0

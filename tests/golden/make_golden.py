@@ -21,6 +21,12 @@ Fixtures
                   spectrum, seeded ellipse phantom seed 0): every 20th view of
                   the reference's un-normalised spectral sum, its global max
                   and min, and the total segment count.
+  lengthproj.npz  lengthproj_TOMO on seeded sinograms (uniform(0.1, 1) from
+                  numpy's default_rng(seed), regenerated by the tests): small
+                  helical cases in full, and the 512^2 x 800-view case as
+                  every 16th row of npf.
+
+    python tests/golden/make_golden.py [fixture ...]   (default: all)
 """
 from __future__ import annotations
 
@@ -112,14 +118,39 @@ def c1_subset(tabs):
                         maps_sha=np.frombuffer(__import__("hashlib").sha256(maps.tobytes()).digest(), np.uint8))
 
 
+sys.path.insert(0, os.path.join(ROOT, "tests"))
+from golden_cases import LP_C1, LP_C1_STEP, LP_CASES, lp_proj  # noqa: E402
+
+
+def lengthproj():
+    out = {}
+    for k, (N, V, pix, z, cs, seed) in enumerate(LP_CASES + [LP_C1]):
+        c, s = O.trig_tables(V)
+        npf, _ = O.ref_lengthproj(N, pix, lp_proj(V, seed), V, c, s, z, cs)
+        if (N, V, pix, z, cs, seed) == LP_C1:
+            out["c1_rows"] = np.arange(0, N, LP_C1_STEP)
+            out["c1_npf_rows"] = npf[::LP_C1_STEP]
+        else:
+            out[f"npf_{k}"] = npf
+    np.savez_compressed(os.path.join(OUT, "lengthproj.npz"), **out)
+
+
 def main():
     if not O.ref_available():
         raise SystemExit("reference harness not built: make -C oracle ref")
-    with tempfile.TemporaryDirectory() as tmp:
-        tabs = mu_tables(tmp)
-    mb_small(tabs)
-    fbp_small()
-    c1_subset(tabs)
+    want = set(sys.argv[1:]) or {"mu_tables", "mb_small", "fbp_small", "c1_subset", "lengthproj"}
+    tabs = None
+    if want & {"mu_tables", "mb_small", "c1_subset"}:
+        with tempfile.TemporaryDirectory() as tmp:
+            tabs = mu_tables(tmp)
+    if "mb_small" in want:
+        mb_small(tabs)
+    if "fbp_small" in want:
+        fbp_small()
+    if "c1_subset" in want:
+        c1_subset(tabs)
+    if "lengthproj" in want:
+        lengthproj()
     for f in sorted(os.listdir(OUT)):
         print(f, os.path.getsize(os.path.join(OUT, f)))
 

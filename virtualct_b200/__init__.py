@@ -49,7 +49,7 @@ EXPORTED_SYMBOLS = (
     "vct_set_sum_mode", "vct_set_walk_mode", "vct_forward", "vct_forward_dev", "vct_line_integrals_dev", "vct_mbfpa", "vct_mbfpa_dev",
     "vct_normalize_noise_dev", "vct_fbp", "vct_fbp_dev", "vct_fbp_noalloc", "vct_fbp_filtered_dev",
     "vct_fbp_transpose", "vct_fbp_transpose_dev",
-    "vct_set_density_scale", "vct_descent_step_dev",
+    "vct_set_density_scale", "vct_descent_step_dev", "vct_lengthproj", "vct_lengthproj_dev",
     "vct_forward_adjoint", "vct_forward_adjoint_dev", "vct_forward_vjp_dev", "vct_adjoint_rays_dev",
     "vct_batch_create", "vct_batch_run", "vct_batch_synchronize", "vct_batch_config", "vct_batch_destroy",
     "vct_forward_batched",
@@ -160,6 +160,8 @@ def lib():
     L.vct_fbp_transpose_dev.argtypes = [vp, vp, C.c_int, vp]
     L.vct_fbp_noalloc.argtypes = [C.POINTER(_CGeometry), vp, C.c_int, C.c_int, vp, vp]
     L.vct_set_density_scale.argtypes = [vp, C.c_double]
+    L.vct_lengthproj.argtypes = [vp, vp, C.c_double, C.c_double, vp]
+    L.vct_lengthproj_dev.argtypes = [vp, vp, C.c_double, C.c_double, vp]
     L.vct_descent_step_dev.argtypes = [vp, vp, vp, C.c_double, C.c_double, vp, C.c_longlong, vp]
     L.vct_forward_adjoint.argtypes = [vp, vp, vp, vp, C.POINTER(C.c_double)]
     L.vct_forward_adjoint_dev.argtypes = [vp, vp, vp, vp, vp]
@@ -333,6 +335,20 @@ class Context:
     def normalize_noise_dev(self, sino, sigma: float, seed: int) -> None:
         _check(lib().vct_normalize_noise_dev(self._h, sino.data_ptr(), float(sigma), int(seed)),
                "vct_normalize_noise_dev")
+
+    def lengthproj(self, proj, z: float = 0.0, couch_speed: float = 0.0) -> np.ndarray:
+        """lengthproj_TOMO: npf [N][N] from proj [views/2*2][width]."""
+        g = self.geometry
+        p = np.ascontiguousarray(proj, np.float32)
+        if p.shape != (g.views // 2 * 2, g.width):
+            raise ValueError(f"proj must be [{g.views // 2 * 2}][{g.width}]")
+        out = np.zeros((g.recon_size, g.recon_size), np.float32)
+        _check(lib().vct_lengthproj(self._h, _ptr(p), float(z), float(couch_speed), _ptr(out)), "vct_lengthproj")
+        return out
+
+    def lengthproj_dev(self, proj, npf, z: float = 0.0, couch_speed: float = 0.0) -> None:
+        _check(lib().vct_lengthproj_dev(self._h, proj.data_ptr(), float(z), float(couch_speed), npf.data_ptr()),
+               "vct_lengthproj_dev")
 
     # Adjoint -----------------------------------------------------------------
     def forward_adjoint(self, meas, weights=None):

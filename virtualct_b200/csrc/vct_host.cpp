@@ -554,6 +554,57 @@ int vct_fbp(vct_ctx* c, const float* sino, int filter, int in_mode, float* img) 
   return VCT_OK;
 }
 
+// lengthproj_TOMO, MB/lengthproj_TOMO.cpp:14-185.  The first view follows the
+// reference's formula (:36-47: z over the couch advance per view, minus half
+// a rotation); with no couch motion the reference divides 0/0 there and reads
+// its trig tables out of range, and this build starts at view 0, as the
+// reference's main does for the sinogram it passes in (MB/main.cpp:350).
+int vct_lengthproj_dev(vct_ctx* c, const float* d_proj, double z, double couch_speed, float* d_npf) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!d_proj || !d_npf) return fail(VCT_E_ARG, "vct_lengthproj_dev: null buffer");
+  const vct_geometry& g = c->geo;
+  LpGeom q{};
+  q.N = c->dg.N;
+  q.V = g.views;
+  q.W = g.width;
+  q.start_ch = g.start_channel;
+  q.end_ch = g.end_channel;
+  q.count = g.views / 2 * 2;  // sngrmHeight/UsedReconAngle*2
+  q.start = 0;
+  if (couch_speed != 0.0) {
+    const double pitch = (double)(couch_speed / g.views);
+    const double sv = z / pitch - g.views / 2 + 0.00000001;
+    if (!(sv > -2147483648.0 && sv < 2147483647.0)) return fail(VCT_E_ARG, "vct_lengthproj_dev: view index overflow");
+    q.start = (int)sv;
+  }
+  q.nrot = q.start / g.views;
+  q.s = g.pixel_cm;
+  q.sid = g.sid_cm;
+  q.dsrc = g.det_src_iso_cm;
+  q.R = g.det_radius_cm;
+  q.diso = g.det_radius_cm - g.sid_cm;  // DIST_BTWN_ISO_AND_DETECTOR_CM (57.6 = 142.6 - 85)
+  q.iso = g.iso_channel;
+  q.dalpha = g.max_alpha / ((g.end_channel - g.start_channel - 1) / 2);
+  if ((rc = launch_lengthproj(q, c->cos_t.p, c->sin_t.p, d_proj, d_npf, c->stream))) return rc;
+  c->launches++;
+  return VCT_OK;
+}
+
+int vct_lengthproj(vct_ctx* c, const float* proj, double z, double couch_speed, float* npf) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!proj || !npf) return fail(VCT_E_ARG, "vct_lengthproj: null buffer");
+  const size_t nproj = (size_t)(c->geo.views / 2 * 2) * c->geo.width;
+  const size_t nimg = (size_t)c->dg.N * c->dg.N;
+  if ((rc = c->fbp_sino.ensure(c->geo.views * (size_t)c->geo.width)) || (rc = c->fbp_img.ensure(nimg))) return rc;
+  VCT_CUDA(cudaMemcpyAsync(c->fbp_sino.p, proj, nproj * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  if ((rc = vct_lengthproj_dev(c, c->fbp_sino.p, z, couch_speed, c->fbp_img.p))) return rc;
+  VCT_CUDA(cudaMemcpyAsync(npf, c->fbp_img.p, nimg * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  VCT_CUDA(cudaStreamSynchronize(c->stream));
+  return VCT_OK;
+}
+
 // Transpose of the FBP's linear part (no counterpart in the reference):
 // backprojection, filter and weight transposed, in reverse order.
 int vct_fbp_transpose_dev(vct_ctx* c, const float* d_u, int filter, float* d_lam) {

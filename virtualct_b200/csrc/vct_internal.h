@@ -105,6 +105,15 @@ int launch_fbp_filter_t(const float* d_q, const float* d_h0, const float* d_cm, 
 int launch_fbp_weight_t(const float* d_g, int V, int W, int start, int C, const double* d_coeff, float* d_lam,
                         cudaStream_t st);
 
+// lengthproj_TOMO (vct_lengthproj.cu): geometry of one slice.
+struct LpGeom {
+  int N, V, W, start_ch, end_ch;
+  int start, count, nrot;  // first view, views used, whole rotations before it
+  double s, sid, dsrc, diso, R, iso, dalpha;
+};
+int launch_lengthproj(const LpGeom& q, const double* d_cos, const double* d_sin, const float* d_proj, float* d_npf,
+                      cudaStream_t st);
+
 // Adjoint (vct_adjoint.cu).  Ray kinds of the per-ray walk record.
 constexpr int kAdjRayNone = 0;   // no segment
 constexpr int kAdjRayFast = 1;   // fast walk: lumped segment + chords in a major-index range

@@ -1,0 +1,100 @@
+// lengthproj_TOMO (MB/lengthproj_TOMO.cpp:14-185) on sm_100a: for every pixel
+// of the reconstruction mask, npf = sum over the views used of
+// (float)(lerp(proj, dj) * rr), accumulated in float in view order, where rr
+// is the pixel-width chord of the line from the source to the pixel centre
+// and dj the channel where that line meets the curved detector.  One thread
+// per pixel, the views in order; the geometry in FP64 (compiled with
+// --fmad=false, as the reference's x86-64 build rounds every operation), so
+// the per-view terms follow the reference's expressions.  The side tables
+// the reference writes (chord and detector position per pixel and view,
+// [N][N][V] floats each) are not kept: every term is recomputed.
+#include <cuda_runtime.h>
+#include <math.h>
+
+#include "vct_internal.h"
+
+namespace vct {
+
+__global__ void lengthproj_kernel(LpGeom q, const double* __restrict__ cos_t, const double* __restrict__ sin_t,
+                                  const float* __restrict__ proj, float* __restrict__ npf) {
+  const int jx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int jy = blockIdx.y;
+  const int N = q.N;
+  if (jx >= N) return;
+  // reconstruction mask, MB/misc_TOMO.cpp:10-39
+  const double r = (double)(N - 1) / 2.0;
+  if (!(((double)jy - r) * ((double)jy - r) + ((double)jx - r) * ((double)jx - r) <= r * r)) {
+    npf[(size_t)jy * N + jx] = 0.0f;
+    return;
+  }
+  const double s = q.s;
+  const double ry = N * s * 0.5 - (jy + 0.5) * s;
+  const double rx = -N * s * 0.5 + (jx + 0.5) * s;
+  float acc = 0.0f;
+  for (int k = 0; k < q.count; k++) {
+    int v = q.start + k - q.nrot * q.V;
+    if (v >= q.V) v -= q.V;
+    if (v < 0) v += q.V;  // the reference reads its tables out of range here
+    const double cb = cos_t[v], sb = sin_t[v];
+    const double sx = q.sid * sb, sy = q.sid * cb;
+    double len;
+    if (fabs(rx - sx) > fabs(ry - sy)) {
+      const double x0 = rx - 0.5 * s, x1 = rx + 0.5 * s;
+      const double y0 = (x0 - sx) / (rx - sx) * (ry - sy) + sy;
+      const double y1 = (x1 - sx) / (rx - sx) * (ry - sy) + sy;
+      len = sqrt((x0 - x1) * (x0 - x1) + (y0 - y1) * (y0 - y1));
+    } else {
+      // y-major: the reference evaluates both ends of x at y0, leaving only
+      // the pixel's y extent (:95-101)
+      const double y0 = ry - 0.5 * s, y1 = ry + 0.5 * s;
+      len = sqrt((y0 - y1) * (y0 - y1));
+    }
+    // the line meets the detector circle (centre on the source, radius R):
+    // the root nearer the origin (:110-134)
+    const double dx = q.dsrc * sb, dy = q.dsrc * cb;
+    const double a = (sy - ry) / (sx - rx);
+    const double b = -sx * (sy - ry) / (sx - rx) + sy;
+    const double qa = 1.0 + a * a;
+    const double qb = 2.0 * a * b - 2.0 * a * dy - 2.0 * dx;
+    const double qc = dx * dx + b * b + dy * dy - 2.0 * b * dy - q.R * q.R;
+    const double disc = sqrt(qb * qb - 4.0 * qa * qc);
+    const double x1 = (-qb + disc) / (2.0 * qa), y1 = a * x1 + b;
+    const double x2 = (-qb - disc) / (2.0 * qa), y2 = a * x2 + b;
+    double px, py;
+    if (x1 * x1 + y1 * y1 > x2 * x2 + y2 * y2) {
+      px = x2;
+      py = y2;
+    } else {
+      px = x1;
+      py = y1;
+    }
+    // angle along the detector from its centre point (:136-150)
+    const double ox = -q.diso * sb, oy = -q.diso * cb;
+    const double d2 = (px - ox) * (px - ox) + (py - oy) * (py - oy);
+    const double ang = acos(1.0 - d2 / (2.0 * q.R * q.R));
+    const double rpx = px * cb - py * sb;
+    const double dj = rpx > 0.0 ? q.iso - ang / q.dalpha : q.iso + ang / q.dalpha;
+    const float* row = proj + (size_t)k * q.W;
+    // three explicit tests, as :158-172 (a NaN channel adds nothing)
+    if (q.start_ch <= dj && dj < q.end_ch - 1) {
+      const int ij = (int)dj;
+      const double f = dj - (double)ij;
+      acc += (float)(((1.0 - f) * row[ij] + f * row[ij + 1]) * len);
+    } else if (q.start_ch > dj) {
+      acc += (float)(row[q.start_ch] * len);
+    } else if (dj >= q.end_ch - 1) {
+      acc += (float)(row[q.end_ch - 1] * len);
+    }
+  }
+  npf[(size_t)jy * N + jx] = acc;
+}
+
+int launch_lengthproj(const LpGeom& q, const double* d_cos, const double* d_sin, const float* d_proj, float* d_npf,
+                      cudaStream_t st) {
+  dim3 grid((q.N + 127) / 128, q.N);
+  lengthproj_kernel<<<grid, 128, 0, st>>>(q, d_cos, d_sin, d_proj, d_npf);
+  VCT_CUDA(cudaGetLastError());
+  return VCT_OK;
+}
+
+}  // namespace vct

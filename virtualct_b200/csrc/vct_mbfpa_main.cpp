@@ -6,8 +6,9 @@
 // Reads the reference's 31-field input txt, the int16 element maps (the
 // reference hard-codes Weight_input_ICRU110.raw and six elements,
 // MB/main.cpp:240,422) and the spectrum txt; writes reprojection_float.raw
-// (float32 [views][width]) and npf_float.raw (the reference's lengthproj_TOMO
-// output for its all-zero measured sinogram: zeros, MB/main.cpp:407-419).
+// (float32 [views][width]) and npf_float.raw (lengthproj_TOMO of the measured
+// sinogram, MB/main.cpp:407-419, on the GPU; the virtual path has no
+// measured sinogram, so, as in the reference, it is all zeros).
 // The energy loop, spectral sum, normalisation and noise of
 // MB/main.cpp:492-530 are one call to vct_mbfpa() on the GPU.
 #include <stdio.h>
@@ -100,9 +101,6 @@ int main(int argc, char* argv[]) {
   printf("%d energy bins, %d elements\n", NE, M);
 
   const size_t n2 = (size_t)g.recon_size * g.recon_size;
-  std::vector<float> npf(n2, 0.0f);
-  vct_write_raw("npf_float.raw", npf.data(), n2 * sizeof(float));
-
   std::vector<int16_t> maps((size_t)M * n2);
   if (vct_read_raw(weights.c_str(), 0, maps.data(), maps.size() * sizeof(int16_t), nullptr) != VCT_OK) {
     fprintf(stderr, "%s\n", vct_last_error());
@@ -113,6 +111,15 @@ int main(int argc, char* argv[]) {
   if (rc == VCT_OK) rc = vct_set_sum_mode(ctx, sum_mode);
   if (rc == VCT_OK) rc = vct_set_maps(ctx, maps.data(), M);
   if (rc == VCT_OK) rc = vct_set_spectrum(ctx, mu.data(), pdf.data(), M, NE);
+  if (rc == VCT_OK) {
+    // lengthproj_TOMO at the first slice's z with the measured sinogram the
+    // reference builds (MB/main.cpp:346-370); the virtual path reads none,
+    // so its rows are zeros.
+    std::vector<float> proj((size_t)(g.views / 2 * 2) * g.width, 0.0f);
+    std::vector<float> npf(n2, 0.0f);
+    rc = vct_lengthproj(ctx, proj.data(), cfg.recon_offset, cfg.couch_speed, npf.data());
+    if (rc == VCT_OK) rc = vct_write_raw("npf_float.raw", npf.data(), n2 * sizeof(float));
+  }
   std::vector<float> sino((size_t)g.views * g.width);
   float stats[3] = {0, 0, 0};
   if (rc == VCT_OK) rc = vct_mbfpa(ctx, cfg.photon_noise, seed, sino.data(), stats);

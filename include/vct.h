@@ -194,6 +194,19 @@ int vct_fbp_dev(vct_ctx* ctx, const float* d_sino, int filter, int in_mode, floa
  * on the GPU -- on different streams, or from several threads -- race. */
 int vct_fbp_noalloc(const vct_geometry* g, const float* d_sino, int filter, int in_mode, float* d_img,
                     void* stream);
+/* Beam-hardening correction, MB/beam_hardening_correction.cpp:21-69 (the
+ * reference's separate program on reprojection_float.raw): every
+ * transmission p becomes exp(-(|y| + alpha |y|^beta)), y = -ln p (logarithm
+ * in single precision, as the reference's C++ resolves log() of a float),
+ * stored as float.  vct_beam_hardening works on [views][width] host buffers
+ * (sino and out may alias), vct_beam_hardening_dev in place on the device.
+ * vct_set_beam_hardening(ctx, alpha, beta) makes every later vct_fbp* apply
+ * the same correction to its line integrals on the way into the filter (one
+ * pass fewer over the sinogram; alpha 0 turns it off, the default). */
+int vct_beam_hardening(vct_ctx* ctx, const float* sino, double alpha, double beta, float* out);
+int vct_beam_hardening_dev(vct_ctx* ctx, float* d_sino, double alpha, double beta);
+int vct_set_beam_hardening(vct_ctx* ctx, double alpha, double beta);
+
 /* Transpose of the FBP (no counterpart in the reference).  With in_mode 0
  * the FBP image is linear in lam = -ln p: img = B F W lam (weight W,
  * filter F, backprojection B).  vct_fbp_transpose returns

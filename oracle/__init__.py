@@ -95,6 +95,7 @@ def lib():
         L.orc_siddon.restype = C.c_int
         L.orc_walk_project.argtypes = [C.POINTER(OrcGeom), _dp, _dp, _dp, C.c_int, _dp, C.c_int]
         L.orc_walk_backproject.argtypes = [C.POINTER(OrcGeom), _dp, _dp, _dp, C.c_int, _dp, C.c_int]
+        L.orc_beam_hardening.argtypes = [_fp, C.c_longlong, C.c_double, C.c_double, _dp]
         L.orc_lengthproj.argtypes = [C.POINTER(OrcGeom), _dp, _dp, _fp, C.c_double, C.c_double, _fp]
         L.orc_walk_project_rays.argtypes = [C.POINTER(OrcGeom), _dp, _dp, _dp, C.c_int, _ip, C.c_int, _dp, C.c_int]
         L.orc_siddon_project.argtypes = [C.POINTER(OrcGeom), _dp, _dp, _dp, C.c_int, _dp, C.c_int]
@@ -379,6 +380,30 @@ def ref_lengthproj(N, pixel_cm, proj, V, cos_t, sin_t, z, couch_speed):
     if rc:
         raise RuntimeError(f"vctref_lengthproj failed ({rc})")
     return out, secs.value
+
+
+def beam_hardening(p, alpha, beta):
+    """Beam-hardening correction of transmissions p (float32); returns the
+    corrected copy and the (before, after) minima."""
+    out = np.array(p, np.float32, copy=True)
+    mins = np.zeros(2, np.float64)
+    lib().orc_beam_hardening(out.reshape(-1), out.size, float(alpha), float(beta), mins)
+    return out, (float(mins[0]), float(mins[1]))
+
+
+def ref_beam_hardening(p, alpha, beta):
+    """The reference's own program (oracle/_ref/bhc) on an 800 x 609
+    reprojection_float.raw in a scratch directory: (corrected, printed line)."""
+    import subprocess
+    import tempfile
+
+    exe = os.path.join(HERE, "_ref", "bhc")
+    with tempfile.TemporaryDirectory() as d:
+        np.ascontiguousarray(p, np.float32).tofile(os.path.join(d, "reprojection_float.raw"))
+        r = subprocess.run([exe, repr(float(alpha)), repr(float(beta))], cwd=d, capture_output=True, text=True,
+                           check=True)
+        out = np.fromfile(os.path.join(d, "reprojection_float_cor.raw"), np.float32).reshape(np.shape(p))
+    return out, r.stdout.strip()
 
 
 def lengthproj(g, cos_t, sin_t, proj, z=0.0, couch_speed=0.0):

@@ -973,3 +973,24 @@ void orc_lengthproj(const orc_geom* g, const double* cos_t, const double* sin_t,
   }
   free(mask);
 }
+
+/* ------------------------------------------------- beam-hardening correction */
+/* MB/beam_hardening_correction.cpp:49-56, elementwise: y = -ln p,
+ * y' = |y| + alpha |y|^beta, p' = (float)exp(-y'); mins[0], mins[1] receive
+ * the minima before and after, as the program prints them.  The reference is
+ * C++: log() of its float sample resolves to the float overload, so the
+ * logarithm is taken in single precision (logf) and widened. */
+void orc_beam_hardening(float* p, long long n, double alpha, double beta, double* mins) {
+  double min_org = 1000000, min_new = 1000000;
+  for (long long i = 0; i < n; i++) {
+    if (min_org > p[i]) min_org = p[i];
+    double y = -(double)logf(p[i]);
+    y = fabs(y) + (alpha * pow(fabs(y), beta));
+    p[i] = (float)exp(-y);
+    if (min_new > p[i]) min_new = p[i];
+  }
+  if (mins) {
+    mins[0] = min_org;
+    mins[1] = min_new;
+  }
+}

@@ -123,6 +123,10 @@ void orc_walk_backproject(const orc_geom* g, const double* cos_t, const double* 
 void orc_lengthproj(const orc_geom* g, const double* cos_t, const double* sin_t, const float* proj, double z,
                     double couch_speed, float* npf);
 
+/* Beam-hardening correction, MB/beam_hardening_correction.cpp:49-56, in place
+ * (mins: the minima before and after, may be NULL). */
+void orc_beam_hardening(float* p, long long n, double alpha, double beta, double* mins);
+
 /* Max-normalisation (MB/main.cpp:511-522) followed by gaussiannoise0
  * (MB/main.cpp:42-76) with glibc rand() after srand(seed) (the reference
  * never seeds: seed 1).  order selects which Uniform0() call in rand_gauss0

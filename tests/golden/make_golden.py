@@ -21,6 +21,9 @@ Fixtures
                   spectrum, seeded ellipse phantom seed 0): every 20th view of
                   the reference's un-normalised spectral sum, its global max
                   and min, and the total segment count.
+  beam_hardening.npz  the beam-hardening correction program's output
+                  (reprojection_float_cor.raw, every 32nd row) and printed
+                  minima on a seeded 800 x 609 sinogram, kV and MV parameters.
   lengthproj.npz  lengthproj_TOMO on seeded sinograms (uniform(0.1, 1) from
                   numpy's default_rng(seed), regenerated by the tests): small
                   helical cases in full, and the 512^2 x 800-view case as
@@ -119,7 +122,7 @@ def c1_subset(tabs):
 
 
 sys.path.insert(0, os.path.join(ROOT, "tests"))
-from golden_cases import LP_C1, LP_C1_STEP, LP_CASES, lp_proj  # noqa: E402
+from golden_cases import BH_PARAMS, BH_ROW_STEP, LP_C1, LP_C1_STEP, LP_CASES, bh_sino, lp_proj  # noqa: E402
 
 
 def lengthproj():
@@ -135,10 +138,19 @@ def lengthproj():
     np.savez_compressed(os.path.join(OUT, "lengthproj.npz"), **out)
 
 
+def beam_hardening():
+    out = {}
+    for k, (a, b) in enumerate(BH_PARAMS):
+        cor, line = O.ref_beam_hardening(bh_sino(), a, b)
+        out[f"rows_{k}"] = cor[::BH_ROW_STEP]
+        out[f"line_{k}"] = np.array(line)
+    np.savez_compressed(os.path.join(OUT, "beam_hardening.npz"), **out)
+
+
 def main():
     if not O.ref_available():
         raise SystemExit("reference harness not built: make -C oracle ref")
-    want = set(sys.argv[1:]) or {"mu_tables", "mb_small", "fbp_small", "c1_subset", "lengthproj"}
+    want = set(sys.argv[1:]) or {"mu_tables", "mb_small", "fbp_small", "c1_subset", "lengthproj", "beam_hardening"}
     tabs = None
     if want & {"mu_tables", "mb_small", "c1_subset"}:
         with tempfile.TemporaryDirectory() as tmp:
@@ -151,6 +163,8 @@ def main():
         c1_subset(tabs)
     if "lengthproj" in want:
         lengthproj()
+    if "beam_hardening" in want:
+        beam_hardening()
     for f in sorted(os.listdir(OUT)):
         print(f, os.path.getsize(os.path.join(OUT, f)))
 

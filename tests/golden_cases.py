@@ -12,3 +12,14 @@ LP_C1_STEP = 16
 
 def lp_proj(views, seed, width=609):
     return np.random.default_rng(seed).uniform(0.1, 1.0, (views // 2 * 2, width)).astype(np.float32)
+
+
+# Beam-hardening correction: a seeded 800 x 609 transmission sinogram, the
+# (alpha, beta) pairs of the reference program's usage line (kV, MV), and
+# the rows the fixture keeps.
+BH_PARAMS = [(0.01, 2.00), (0.01, 3.70)]
+BH_ROW_STEP = 32
+
+
+def bh_sino(seed=1):
+    return np.random.default_rng(seed).uniform(1e-3, 1.0, (800, 609)).astype(np.float32)

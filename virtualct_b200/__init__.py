@@ -50,6 +50,7 @@ EXPORTED_SYMBOLS = (
     "vct_normalize_noise_dev", "vct_fbp", "vct_fbp_dev", "vct_fbp_noalloc", "vct_fbp_filtered_dev",
     "vct_fbp_transpose", "vct_fbp_transpose_dev",
     "vct_set_density_scale", "vct_descent_step_dev", "vct_lengthproj", "vct_lengthproj_dev",
+    "vct_beam_hardening", "vct_beam_hardening_dev", "vct_set_beam_hardening",
     "vct_forward_adjoint", "vct_forward_adjoint_dev", "vct_forward_vjp_dev", "vct_adjoint_rays_dev",
     "vct_batch_create", "vct_batch_run", "vct_batch_synchronize", "vct_batch_config", "vct_batch_destroy",
     "vct_forward_batched",
@@ -161,6 +162,9 @@ def lib():
     L.vct_fbp_noalloc.argtypes = [C.POINTER(_CGeometry), vp, C.c_int, C.c_int, vp, vp]
     L.vct_set_density_scale.argtypes = [vp, C.c_double]
     L.vct_lengthproj.argtypes = [vp, vp, C.c_double, C.c_double, vp]
+    L.vct_beam_hardening.argtypes = [vp, vp, C.c_double, C.c_double, vp]
+    L.vct_beam_hardening_dev.argtypes = [vp, vp, C.c_double, C.c_double]
+    L.vct_set_beam_hardening.argtypes = [vp, C.c_double, C.c_double]
     L.vct_lengthproj_dev.argtypes = [vp, vp, C.c_double, C.c_double, vp]
     L.vct_descent_step_dev.argtypes = [vp, vp, vp, C.c_double, C.c_double, vp, C.c_longlong, vp]
     L.vct_forward_adjoint.argtypes = [vp, vp, vp, vp, C.POINTER(C.c_double)]
@@ -335,6 +339,23 @@ class Context:
     def normalize_noise_dev(self, sino, sigma: float, seed: int) -> None:
         _check(lib().vct_normalize_noise_dev(self._h, sino.data_ptr(), float(sigma), int(seed)),
                "vct_normalize_noise_dev")
+
+    def beam_hardening(self, sino, alpha: float, beta: float) -> np.ndarray:
+        """Beam-hardening correction of a [views][width] transmission sinogram."""
+        s = np.ascontiguousarray(sino, np.float32)
+        if s.shape != (self.geometry.views, self.geometry.width):
+            raise ValueError("sinogram must be [views][width]")
+        out = np.empty_like(s)
+        _check(lib().vct_beam_hardening(self._h, _ptr(s), float(alpha), float(beta), _ptr(out)), "vct_beam_hardening")
+        return out
+
+    def beam_hardening_dev(self, sino, alpha: float, beta: float) -> None:
+        _check(lib().vct_beam_hardening_dev(self._h, sino.data_ptr(), float(alpha), float(beta)),
+               "vct_beam_hardening_dev")
+
+    def set_beam_hardening(self, alpha: float, beta: float) -> None:
+        """Apply the correction inside every later FBP (alpha 0: off)."""
+        _check(lib().vct_set_beam_hardening(self._h, float(alpha), float(beta)), "vct_set_beam_hardening")
 
     def lengthproj(self, proj, z: float = 0.0, couch_speed: float = 0.0) -> np.ndarray:
         """lengthproj_TOMO: npf [N][N] from proj [views/2*2][width]."""

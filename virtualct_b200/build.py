@@ -40,7 +40,7 @@ CU_SOURCES = {
     "vct_lengthproj.cu": ["--fmad=false"],
 }
 CPP_SOURCES = ["vct_host.cpp", "vct_io.cpp", "vct_batch.cpp"]
-APPS = {"vct_mbfpa": "vct_mbfpa_main.cpp", "vct_fbp": "vct_fbp_main.cpp"}
+APPS = {"vct_mbfpa": "vct_mbfpa_main.cpp", "vct_fbp": "vct_fbp_main.cpp", "vct_bhc": "vct_bhc_main.cpp"}
 HEADERS = ["vct_internal.h", "vct_philox.h", "vct_walk.cuh", "vct_fastmath.cuh", "vct_ctx.h"]
 
 

@@ -57,6 +57,7 @@ struct vct_ctx {
   vct::DBuf<double> fbp_coeff;  // SID*cos((k-cw)*dbeta)*dbeta
   vct::DBuf<float> fbp_h[3];    // per filter (1 Ram-Lak, 2 Shepp-Logan): h0[2C-1] + row factors[C]
   vct::DBuf<float> fbp_g, fbp_q, fbp_sino, fbp_img;
+  double bh_alpha = 0.0, bh_beta = 0.0;  // beam-hardening correction in the FBP (alpha 0: off)
   // Adjoint: per-ray walk plans (geometry only), ray factors, fixed-point
   // accumulator of the exact-walk rays, loss partials.
   int adj_ready = 0, adj_nspecial = 0, adj_tile = -1;

@@ -19,21 +19,54 @@
 namespace vct {
 
 // ------------------------------------------------------------------ weight
+// With bh_alpha != 0 the beam-hardening correction of
+// MB/beam_hardening_correction.cpp:49-56 is applied on the way: the
+// line integral y = -ln p becomes |y| + alpha |y|^beta (the reference program
+// takes the logarithm in single precision, logf, and stores exp(-y') as float
+// for the FBP to take -ln again; here y' goes straight into the weight).
 __global__ void fbp_weight_kernel(const float* __restrict__ sino, int V, int W, int start, int C,
-                                  const double* __restrict__ coeff, float* __restrict__ g) {
+                                  const double* __restrict__ coeff, double bh_alpha, double bh_beta,
+                                  float* __restrict__ g) {
   const long long n = (long long)V * C;
   const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   if (i >= n) return;
   const int v = (int)(i / C);
   const int k = (int)(i - (long long)v * C);
-  const double p = (double)sino[(size_t)v * W + start + k];
-  g[i] = (float)(-log(p) * coeff[k]);
+  const float pf = sino[(size_t)v * W + start + k];
+  double y;
+  if (bh_alpha != 0.0) {
+    y = -(double)logf(pf);
+    y = fabs(y) + bh_alpha * pow(fabs(y), bh_beta);
+  } else {
+    y = -log((double)pf);
+  }
+  g[i] = (float)(y * coeff[k]);
 }
 
 int launch_fbp_weight(const float* d_sino, int V, int W, int start, int C, const double* d_coeff,
-                        float* d_g, cudaStream_t st) {
+                        float* d_g, cudaStream_t st, double bh_alpha, double bh_beta) {
   const long long n = (long long)V * C;
-  fbp_weight_kernel<<<(int)((n + 255) / 256), 256, 0, st>>>(d_sino, V, W, start, C, d_coeff, d_g);
+  fbp_weight_kernel<<<(int)((n + 255) / 256), 256, 0, st>>>(d_sino, V, W, start, C, d_coeff, bh_alpha, bh_beta,
+                                                             d_g);
+  VCT_CUDA(cudaGetLastError());
+  return VCT_OK;
+}
+
+// The correction on its own, in place: p <- (float)exp(-(|y| + alpha |y|^beta)),
+// y = -logf(p), as MB/beam_hardening_correction.cpp:49-56.
+__global__ void beam_hardening_kernel(float* __restrict__ p, long long n, double alpha, double beta) {
+  for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+    double y = -(double)logf(p[i]);
+    y = fabs(y) + alpha * pow(fabs(y), beta);
+    p[i] = (float)exp(-y);
+  }
+}
+
+int launch_beam_hardening(float* d_p, long long n, double alpha, double beta, cudaStream_t st) {
+  if (n <= 0) return VCT_OK;
+  long long blocks = (n + 255) / 256;
+  if (blocks > 148 * 64) blocks = 148 * 64;
+  beam_hardening_kernel<<<(unsigned)blocks, 256, 0, st>>>(d_p, n, alpha, beta);
   VCT_CUDA(cudaGetLastError());
   return VCT_OK;
 }

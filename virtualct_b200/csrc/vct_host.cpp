@@ -524,7 +524,7 @@ static int fbp_into(vct_ctx* c, const float* d_sino, int filter, int in_mode, fl
   if ((rc = build_filter(c, filter))) return rc;
   if ((rc = c->fbp_g.ensure((size_t)V * C)) || (rc = c->fbp_q.ensure((size_t)V * C))) return rc;
   if ((rc = launch_fbp_weight(d_sino, V, c->geo.width, c->geo.start_channel, C, c->fbp_coeff.p, c->fbp_g.p,
-                              c->stream)))
+                              c->stream, c->bh_alpha, c->bh_beta)))
     return rc;
   if ((rc = launch_fbp_filter(c->fbp_g.p, c->fbp_h[filter].p, c->fbp_h[filter].p + 2 * C - 1, V, C, in_mode,
                               c->fbp_q.p, c->stream)))
@@ -550,6 +550,39 @@ int vct_fbp(vct_ctx* c, const float* sino, int filter, int in_mode, float* img) 
   VCT_CUDA(cudaMemcpyAsync(c->fbp_sino.p, sino, nsino * sizeof(float), cudaMemcpyHostToDevice, c->stream));
   if ((rc = vct_fbp_dev(c, c->fbp_sino.p, filter, in_mode, c->fbp_img.p))) return rc;
   VCT_CUDA(cudaMemcpyAsync(img, c->fbp_img.p, nimg * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  VCT_CUDA(cudaStreamSynchronize(c->stream));
+  return VCT_OK;
+}
+
+// Beam-hardening correction, MB/beam_hardening_correction.cpp:21-69.
+int vct_set_beam_hardening(vct_ctx* c, double alpha, double beta) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!(alpha == alpha) || !(beta == beta)) return fail(VCT_E_ARG, "vct_set_beam_hardening: NaN");
+  c->bh_alpha = alpha;
+  c->bh_beta = beta;
+  return VCT_OK;
+}
+
+int vct_beam_hardening_dev(vct_ctx* c, float* d_sino, double alpha, double beta) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!d_sino) return fail(VCT_E_ARG, "vct_beam_hardening_dev: null buffer");
+  if ((rc = launch_beam_hardening(d_sino, (long long)c->geo.views * c->geo.width, alpha, beta, c->stream)))
+    return rc;
+  c->launches++;
+  return VCT_OK;
+}
+
+int vct_beam_hardening(vct_ctx* c, const float* sino, double alpha, double beta, float* out) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!sino || !out) return fail(VCT_E_ARG, "vct_beam_hardening: null buffer");
+  const size_t n = (size_t)c->geo.views * c->geo.width;
+  if ((rc = c->fbp_sino.ensure(n))) return rc;
+  VCT_CUDA(cudaMemcpyAsync(c->fbp_sino.p, sino, n * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  if ((rc = vct_beam_hardening_dev(c, c->fbp_sino.p, alpha, beta))) return rc;
+  VCT_CUDA(cudaMemcpyAsync(out, c->fbp_sino.p, n * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
   VCT_CUDA(cudaStreamSynchronize(c->stream));
   return VCT_OK;
 }

@@ -88,8 +88,10 @@ int launch_forward_batch(const FwdJob* d_jobs, int njobs, int M, int tile_rays, 
 int forward_batch_occupancy(int M, int ne_max, int* blocks_per_sm);
 int launch_normalize_noise(const DevGeom& g, const float* d_in, float* d_out, const FwdStats* d_stats,
                            int pad_zero, double sigma, uint64_t seed, cudaStream_t st);
+// bh_alpha != 0: beam-hardening correction of the line integrals on the way.
 int launch_fbp_weight(const float* d_sino, int V, int W, int start, int C, const double* d_coeff,
-                      float* d_g, cudaStream_t st);
+                      float* d_g, cudaStream_t st, double bh_alpha = 0.0, double bh_beta = 0.0);
+int launch_beam_hardening(float* d_p, long long n, double alpha, double beta, cudaStream_t st);
 int launch_fbp_filter(const float* d_g, const float* d_h0, const float* d_cm, int V, int C, int in_mode,
                       float* d_q, cudaStream_t st);
 // view_groups: how many warp groups split the views of the quarter-turn

@@ -165,6 +165,42 @@ int vct_mbfpa_dev(vct_ctx* ctx, double sigma, uint64_t seed, float* d_sino_out);
 int vct_lengthproj(vct_ctx* ctx, const float* proj, double z, double couch_speed, float* npf);
 int vct_lengthproj_dev(vct_ctx* ctx, const float* d_proj, double z, double couch_speed, float* d_npf);
 
+/* The reference's iterative step (MB/main.cpp:432-600):
+ *  - vct_lengthproj2: lengthproj_TOMO_2 (MB/lengthproj_TOMO.cpp:188-276), the
+ *    same sum over the rows (ite-1)%thinout + k*thinout, k < (views/2*2)/
+ *    thinout, with chord and channel rounded to float as the reference's
+ *    side tables hold them (recomputed here, never stored);
+ *  - vct_ir_update_dev: IR_ImageTOMO (MB/IR_ImageTOMO.cpp:19-72) on one
+ *    N x N map: per mask pixel lambda = w_tv TV + w_prior TV(image - prior)
+ *    + 1e-6, after = max(0, before + w (npf_re - npf/thinout + lambda)),
+ *    w = wbefore (before / (npf/thinout - lambda) past iteration 300);
+ *    d_prior may be NULL (zeros); pixels outside the mask are not written;
+ *  - vct_squdiff_dev: calc_squdiff_quad (MB/main.cpp:111-134): d_out2[0] =
+ *    sum (p - r)^2 and d_out2[1] = sum 0.5 p ln(p/r)^2 (only when
+ *    ite == num_ite, else 0) over the rows of iteration ite, channels
+ *    [start, end). */
+int vct_lengthproj2(vct_ctx* ctx, const float* proj, double z, double couch_speed, int ite, int thinout, float* npf);
+int vct_lengthproj2_dev(vct_ctx* ctx, const float* d_proj, double z, double couch_speed, int ite, int thinout,
+                        float* d_npf);
+int vct_ir_update_dev(vct_ctx* ctx, const float* d_before, const float* d_prior, const float* d_npf,
+                      const float* d_npf_re, double wbefore, double w_tv, double w_prior, int ite, int thinout,
+                      float* d_after);
+int vct_squdiff_dev(vct_ctx* ctx, const float* d_proj, const float* d_reproj, int ite, int thinout, int num_ite,
+                    double* d_out2);
+/* One pass of the iterative step (MB/main.cpp:432-600, ite >= 1), host
+ * buffers: the context's last energy bin alone projected (the un-normalised,
+ * per-bin float sinogram the reference's step reads), calc_squdiff_quad
+ * against proj ([views/2*2][width], the measured sinogram; *objective holds
+ * the previous value on entry and the new one on return, *quadratic
+ * optional), update_wbefore (MB/main.cpp:136-150) on *wbefore,
+ * lengthproj_TOMO_2 of the projected bin, and IR_ImageTOMO from `before`
+ * (the first element's map, g/cm^3) into `after` ([N][N]; values outside the
+ * mask are kept).  npf: lengthproj_TOMO of the measured sinogram; prior may
+ * be NULL. */
+int vct_ir_step(vct_ctx* ctx, const float* proj, const float* npf, const float* before, const float* prior, double z,
+                double couch_speed, int ite, int thinout, int num_ite, double w_tv, double w_prior, double* wbefore,
+                double* objective, double* quadratic, float* after);
+
 /* Only the normalisation + noise step on a device sinogram (in place). */
 int vct_normalize_noise_dev(vct_ctx* ctx, float* d_sino, double sigma, uint64_t seed);
 

@@ -97,6 +97,10 @@ def lib():
         L.orc_walk_backproject.argtypes = [C.POINTER(OrcGeom), _dp, _dp, _dp, C.c_int, _dp, C.c_int]
         L.orc_beam_hardening.argtypes = [_fp, C.c_longlong, C.c_double, C.c_double, _dp]
         L.orc_lengthproj.argtypes = [C.POINTER(OrcGeom), _dp, _dp, _fp, C.c_double, C.c_double, _fp]
+        L.orc_lengthproj2.argtypes = [C.POINTER(OrcGeom), _dp, _dp, _fp, C.c_double, C.c_double, C.c_int, C.c_int,
+                                      _fp]
+        L.orc_ir_update.argtypes = [C.c_int, _fp, C.c_void_p, _fp, _fp, C.c_double, C.c_double, C.c_double, C.c_int,
+                                    C.c_int, _fp]
         L.orc_walk_project_rays.argtypes = [C.POINTER(OrcGeom), _dp, _dp, _dp, C.c_int, _ip, C.c_int, _dp, C.c_int]
         L.orc_siddon_project.argtypes = [C.POINTER(OrcGeom), _dp, _dp, _dp, C.c_int, _dp, C.c_int]
         L.orc_normalize_noise.argtypes = [_fp, C.c_int, C.c_double, C.c_uint, C.c_int]
@@ -406,6 +410,52 @@ def ref_beam_hardening(p, alpha, beta):
     return out, r.stdout.strip()
 
 
+def lengthproj2(g, cos_t, sin_t, proj, ite, thinout, z=0.0, couch_speed=0.0):
+    """lengthproj_TOMO_2 restated (side tables recomputed, rounded to float)."""
+    proj = np.ascontiguousarray(proj, np.float32)
+    out = np.zeros((g.recon_size, g.recon_size), np.float32)
+    lib().orc_lengthproj2(C.byref(g), cos_t, sin_t, proj, float(z), float(couch_speed), int(ite), int(thinout), out)
+    return out
+
+
+def ref_lengthproj2(N, pixel_cm, proj0, proj, V, cos_t, sin_t, z, couch_speed, ite, thinout):
+    """The reference: lengthproj_TOMO on proj0 (fills its side tables), then
+    lengthproj_TOMO_2 on proj for iteration ite."""
+    proj0 = np.ascontiguousarray(proj0, np.float32)
+    proj = np.ascontiguousarray(proj, np.float32)
+    out = np.zeros((N, N), np.float32)
+    rc = ref_mb().vctref_lengthproj2(N, pixel_cm, proj0, proj, proj.shape[1], V, np.ascontiguousarray(cos_t),
+                                     np.ascontiguousarray(sin_t), float(z), float(couch_speed), int(ite), int(thinout),
+                                     out)
+    if rc:
+        raise RuntimeError(f"vctref_lengthproj2 failed ({rc})")
+    return out
+
+
+def ir_update(before, npf, npf_re, wbefore, w_tv, w_prior=0.0, ite=1, thinout=1, prior=None, after=None):
+    before = np.ascontiguousarray(before, np.float32)
+    N = before.shape[0]
+    out = np.array(before if after is None else after, np.float32, copy=True)
+    pr = None if prior is None else np.ascontiguousarray(prior, np.float32)
+    lib().orc_ir_update(N, before, None if pr is None else pr.ctypes.data, np.ascontiguousarray(npf, np.float32),
+                        np.ascontiguousarray(npf_re, np.float32), float(wbefore), float(w_tv), float(w_prior),
+                        int(ite), int(thinout), out)
+    return out
+
+
+def ref_ir_update(before, npf, npf_re, wbefore, w_tv, w_prior=0.0, ite=1, thinout=1, prior=None, after=None):
+    before = np.ascontiguousarray(before, np.float32)
+    N = before.shape[0]
+    out = np.array(before if after is None else after, np.float32, copy=True)
+    pr = np.zeros_like(before) if prior is None else np.ascontiguousarray(prior, np.float32)
+    rc = ref_mb().vctref_ir_update(N, before, pr, np.ascontiguousarray(npf, np.float32),
+                                   np.ascontiguousarray(npf_re, np.float32), float(wbefore), float(w_tv),
+                                   float(w_prior), int(ite), int(thinout), out)
+    if rc:
+        raise RuntimeError(f"vctref_ir_update failed ({rc})")
+    return out
+
+
 def lengthproj(g, cos_t, sin_t, proj, z=0.0, couch_speed=0.0):
     """lengthproj_TOMO restated: npf [N][N] from proj [views used][width]."""
     proj = np.ascontiguousarray(proj, np.float32)
@@ -436,6 +486,10 @@ def ref_mb():
         L.vctref_lengthproj.argtypes = [C.c_int, C.c_double, _fp, C.c_int, C.c_int, _dp, _dp, C.c_double, C.c_double,
                                         _fp, C.POINTER(C.c_double)]
         L.vctref_lengthproj.restype = C.c_int
+        L.vctref_lengthproj2.argtypes = [C.c_int, C.c_double, _fp, _fp, C.c_int, C.c_int, _dp, _dp, C.c_double,
+                                         C.c_double, C.c_int, C.c_int, _fp]
+        L.vctref_ir_update.argtypes = [C.c_int, _fp, _fp, _fp, _fp, C.c_double, C.c_double, C.c_double, C.c_int,
+                                       C.c_int, _fp]
         L.vctref_reprojection_bins.argtypes = [C.c_int, C.c_double, _fp, C.c_int, C.c_int, _dp, _dp, C.c_int,
                                                _fp, _fp, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
                                                C.c_void_p, C.POINTER(C.c_double)]

@@ -9,6 +9,8 @@
 //   energy loop + sum        Release_MBFPA_CPU_human/main.cpp:492-506
 //   lengthproj_TOMO          Release_MBFPA_CPU_human/lengthproj_TOMO.cpp:14
 //   prepareMaskData          Release_MBFPA_CPU_human/misc_TOMO.cpp:10
+//   lengthproj_TOMO_2        Release_MBFPA_CPU_human/lengthproj_TOMO.cpp:188
+//   IR_ImageTOMO             Release_MBFPA_CPU_human/IR_ImageTOMO.cpp:19
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -24,6 +26,7 @@
 #include "reprojection_TOMO.h"
 #include "lengthproj_TOMO.h"
 #include "misc_TOMO.h"
+#include "IR_ImageTOMO.h"
 #include "virtual_projection.h"
 
 static double now_s() {
@@ -147,6 +150,42 @@ int vctref_lengthproj(int N, double pixel_cm, const float* proj, int W, int V, c
                   sysmat, tracedet, 1);
   if (seconds) *seconds = now_s() - t0;
   free(sysmat); free(tracedet);
+  delete1DArray(mask);
+  return 0;
+}
+
+// The iterative step's backprojection: lengthproj_TOMO (ite 0) fills the side
+// tables as the reference's main does, then lengthproj_TOMO_2 reads them for
+// iteration `ite` with `thinout` on the sinogram proj.
+int vctref_lengthproj2(int N, double pixel_cm, const float* proj0, const float* proj, int W, int V,
+                       const double* cosT, const double* sinT, double z, double couch_speed, int ite, int thinout,
+                       float* npf) {
+  if (W < End_Channel) return -1;
+  size_t n2 = (size_t)N * N;
+  float* sysmat = (float*)malloc(sizeof(float) * n2 * V);
+  float* tracedet = (float*)malloc(sizeof(float) * n2 * V);
+  float* npf0 = (float*)calloc(n2, sizeof(float));
+  char* mask = prepareMaskData(N);
+  if (!sysmat || !tracedet || !mask || !npf0) {
+    free(sysmat); free(tracedet); free(npf0);
+    return -2;
+  }
+  lengthproj_TOMO(0, N, npf0, (float*)proj0, pixel_cm, W, V, (double*)cosT, (double*)sinT, z, couch_speed, mask,
+                  sysmat, tracedet, 1);
+  memset(npf, 0, sizeof(float) * n2);
+  lengthproj_TOMO_2(ite, N, npf, (float*)proj, pixel_cm, W, V, z, couch_speed, mask, sysmat, tracedet, thinout);
+  free(sysmat); free(tracedet); free(npf0);
+  delete1DArray(mask);
+  return 0;
+}
+
+// IR_ImageTOMO on one N x N map; `after` keeps its values outside the mask.
+int vctref_ir_update(int N, const float* before, const float* prior, const float* npf, const float* npf_re,
+                     double wbefore, double w_tv, double w_prior, int ite, int thinout, float* after) {
+  char* mask = prepareMaskData(N);
+  if (!mask) return -2;
+  IR_ImageTOMO(ite, N, (float*)before, after, (float*)prior, (float*)npf, (float*)npf_re, wbefore, w_tv, w_prior,
+               mask, thinout);
   delete1DArray(mask);
   return 0;
 }

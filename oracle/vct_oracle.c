@@ -887,8 +887,8 @@ static void orc_lp_views(const orc_geom* g, double z, double couch_speed, int* s
   *nrot = s0 / V;
 }
 
-void orc_lengthproj(const orc_geom* g, const double* cos_t, const double* sin_t, const float* proj, double z,
-                    double couch_speed, float* npf) {
+static void orc_lengthproj_rows(const orc_geom* g, const double* cos_t, const double* sin_t, const float* proj,
+                                double z, double couch_speed, int first, int stride, int tables, float* npf) {
   const int N = g->recon_size, V = g->views, W = g->width;
   const double s = g->pixel_cm;
   const int C = g->end_channel - g->start_channel;
@@ -899,6 +899,7 @@ void orc_lengthproj(const orc_geom* g, const double* cos_t, const double* sin_t,
   const double diso = g->det_radius - g->sid; /* DIST_BTWN_ISO_AND_DETECTOR_CM (142.6 - 85) */
   int start, count, nrot;
   orc_lp_views(g, z, couch_speed, &start, &count, &nrot);
+  count /= stride;
   unsigned char* mask = (unsigned char*)malloc((size_t)N * N);
   orc_mask(N, mask);
   memset(npf, 0, sizeof(float) * (size_t)N * N);
@@ -912,7 +913,8 @@ void orc_lengthproj(const orc_geom* g, const double* cos_t, const double* sin_t,
       const double rx = -N * s * 0.5 + (jx + 0.5) * s;
       float acc = 0.0f;
       for (int k = 0; k < count; k++) {
-        int v = start + k - nrot * V;
+        const int rk = first + k * stride; /* sinogram row j_one */
+        int v = start + rk - nrot * V;
         if (v >= V) v -= V;
         if (v < 0) v += V; /* the reference reads its tables out of range here */
         const double cb = cos_t[v], sb = sin_t[v];
@@ -954,10 +956,14 @@ void orc_lengthproj(const orc_geom* g, const double* cos_t, const double* sin_t,
         const double d2 = (px - ox) * (px - ox) + (py - oy) * (py - oy);
         const double ang = acos(1.0 - d2 / (2.0 * R * R));
         const double rpx = px * cb - py * sb;
-        const double dj = rpx > 0.0 ? g->iso_channel - ang / dalpha : g->iso_channel + ang / dalpha;
+        double dj = rpx > 0.0 ? g->iso_channel - ang / dalpha : g->iso_channel + ang / dalpha;
+        if (tables) { /* the side tables hold float (:76, :153) */
+          len = (double)(float)len;
+          dj = (double)(float)dj;
+        }
         const int ij = dj == dj ? (int)dj : 0;
         const double f = dj - (double)ij;
-        const float* row = proj + (size_t)k * W;
+        const float* row = proj + (size_t)rk * W;
         /* three explicit tests, as :158-172: a NaN channel (a source on the
          * pixel's vertical, 0/0 in the line slope) matches none and adds
          * nothing */
@@ -993,4 +999,57 @@ void orc_beam_hardening(float* p, long long n, double alpha, double beta, double
     mins[0] = min_org;
     mins[1] = min_new;
   }
+}
+
+void orc_lengthproj(const orc_geom* g, const double* cos_t, const double* sin_t, const float* proj, double z,
+                    double couch_speed, float* npf) {
+  orc_lengthproj_rows(g, cos_t, sin_t, proj, z, couch_speed, 0, 1, 0, npf);
+}
+
+void orc_lengthproj2(const orc_geom* g, const double* cos_t, const double* sin_t, const float* proj, double z,
+                     double couch_speed, int ite, int thinout, float* npf) {
+  orc_lengthproj_rows(g, cos_t, sin_t, proj, z, couch_speed, (ite - 1) % thinout, thinout, 1, npf);
+}
+
+/* ------------------------------------------------------ IR image update */
+/* The total-variation derivative of MB/IR_ImageTOMO.cpp:10-17: differences
+ * and squares in float, roots and the quotients in double. */
+static double orc_tv(float a, float a1, float a2, float a3, float a4, float a7, float a8) {
+  const float s1 = (a - a2) * (a - a2) + (a - a4) * (a - a4);
+  const float s2 = (a - a1) * (a - a1) + (a1 - a7) * (a1 - a7);
+  const float s3 = (a3 - a8) * (a3 - a8) + (a - a3) * (a - a3);
+  const double d1 = sqrt((double)s1) + 0.00000001;
+  const double d2 = sqrt((double)s2) + 0.00000001;
+  const double d3 = sqrt((double)s3) + 0.00000001;
+  const float t1 = (a - a2) + (a - a4);
+  return t1 / d1 + (a - a1) / d2 + (a - a3) / d3;
+}
+
+void orc_ir_update(int N, const float* before, const float* prior, const float* npf, const float* npf_re,
+                   double wbefore, double w_tv, double w_prior, int ite, int thinout, float* after) {
+  unsigned char* mask = (unsigned char*)malloc((size_t)N * N);
+  orc_mask(N, mask);
+  for (int y = 0; y < N; y++)
+    for (int x = 0; x < N; x++) {
+      const int k = y * N + x;
+      if (!mask[k]) continue;
+      double cost_tv = 0.0, cost_prior = 0.0;
+      if (y < N - 1 && x < N - 1 && x > 0 && y > 0) {
+        const int k1 = k - 1, k2 = k + 1, k3 = k - N, k4 = k + N, k7 = k + N - 1, k8 = k - N + 1;
+        cost_tv = -orc_tv(before[k], before[k1], before[k2], before[k3], before[k4], before[k7], before[k8]);
+#define ORC_PR(i) (prior ? prior[i] : 0.0f)
+        cost_prior = -orc_tv(before[k] - ORC_PR(k), before[k1] - ORC_PR(k1), before[k2] - ORC_PR(k2),
+                             before[k3] - ORC_PR(k3), before[k4] - ORC_PR(k4), before[k7] - ORC_PR(k7),
+                             before[k8] - ORC_PR(k8));
+#undef ORC_PR
+      }
+      const double lambda = w_tv * cost_tv + w_prior * cost_prior + 0.000001;
+      const double del_F = (float)(npf_re[k] - npf[k] / (float)thinout) + lambda;
+      double w = wbefore;
+      if (ite > 300) w = before[k] / (npf[k] / (float)thinout - lambda);
+      float v = (float)(before[k] + w * del_F);
+      if (v < 0.0f) v = 0.0f;
+      after[k] = v;
+    }
+  free(mask);
 }

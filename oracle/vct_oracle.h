@@ -127,6 +127,16 @@ void orc_lengthproj(const orc_geom* g, const double* cos_t, const double* sin_t,
  * (mins: the minima before and after, may be NULL). */
 void orc_beam_hardening(float* p, long long n, double alpha, double beta, double* mins);
 
+/* lengthproj_TOMO_2 (MB/lengthproj_TOMO.cpp:188-276): orc_lengthproj over the
+ * rows (ite-1)%thinout + k*thinout, k < (views/2*2)/thinout, with the chord
+ * and channel rounded to float as the reference's side tables hold them. */
+void orc_lengthproj2(const orc_geom* g, const double* cos_t, const double* sin_t, const float* proj, double z,
+                     double couch_speed, int ite, int thinout, float* npf);
+/* IR_ImageTOMO (MB/IR_ImageTOMO.cpp:19-72) on one N x N map (prior may be
+ * NULL); `after` keeps its values outside the mask. */
+void orc_ir_update(int N, const float* before, const float* prior, const float* npf, const float* npf_re,
+                   double wbefore, double w_tv, double w_prior, int ite, int thinout, float* after);
+
 /* Max-normalisation (MB/main.cpp:511-522) followed by gaussiannoise0
  * (MB/main.cpp:42-76) with glibc rand() after srand(seed) (the reference
  * never seeds: seed 1).  order selects which Uniform0() call in rand_gauss0

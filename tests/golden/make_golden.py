@@ -24,6 +24,9 @@ Fixtures
   beam_hardening.npz  the beam-hardening correction program's output
                   (reprojection_float_cor.raw, every 32nd row) and printed
                   minima on a seeded 800 x 609 sinogram, kV and MV parameters.
+  ir_step.npz     the iterative step's lengthproj_TOMO_2 (side tables from
+                  lengthproj_TOMO on a first sinogram) and IR_ImageTOMO on
+                  seeded inputs (tests/golden_cases.py).
   lengthproj.npz  lengthproj_TOMO on seeded sinograms (uniform(0.1, 1) from
                   numpy's default_rng(seed), regenerated by the tests): small
                   helical cases in full, and the 512^2 x 800-view case as
@@ -122,7 +125,8 @@ def c1_subset(tabs):
 
 
 sys.path.insert(0, os.path.join(ROOT, "tests"))
-from golden_cases import BH_PARAMS, BH_ROW_STEP, LP_C1, LP_C1_STEP, LP_CASES, bh_sino, lp_proj  # noqa: E402
+from golden_cases import (BH_PARAMS, BH_ROW_STEP, IR_CASES, LP2_CASES, LP_C1, LP_C1_STEP, LP_CASES,  # noqa: E402
+                          bh_sino, ir_inputs, lp2_inputs, lp_proj)
 
 
 def lengthproj():
@@ -147,10 +151,23 @@ def beam_hardening():
     np.savez_compressed(os.path.join(OUT, "beam_hardening.npz"), **out)
 
 
+def ir_step():
+    out = {}
+    for k, (N, V, pix, z, cs, ite, th, seed) in enumerate(LP2_CASES):
+        c, s = O.trig_tables(V)
+        p0, p = lp2_inputs(V, seed)
+        out[f"lp2_{k}"] = O.ref_lengthproj2(N, pix, p0, p, V, c, s, z, cs, ite, th)
+    for k, (N, ite, th, wb, wtv, wpr, seed) in enumerate(IR_CASES):
+        before, npf, npf_re, prior, after = ir_inputs(N, seed)
+        out[f"ir_{k}"] = O.ref_ir_update(before, npf, npf_re, wb, wtv, wpr, ite, th, prior, after)
+    np.savez_compressed(os.path.join(OUT, "ir_step.npz"), **out)
+
+
 def main():
     if not O.ref_available():
         raise SystemExit("reference harness not built: make -C oracle ref")
-    want = set(sys.argv[1:]) or {"mu_tables", "mb_small", "fbp_small", "c1_subset", "lengthproj", "beam_hardening"}
+    want = set(sys.argv[1:]) or {"mu_tables", "mb_small", "fbp_small", "c1_subset", "lengthproj", "beam_hardening",
+                                   "ir_step"}
     tabs = None
     if want & {"mu_tables", "mb_small", "c1_subset"}:
         with tempfile.TemporaryDirectory() as tmp:
@@ -165,6 +182,8 @@ def main():
         lengthproj()
     if "beam_hardening" in want:
         beam_hardening()
+    if "ir_step" in want:
+        ir_step()
     for f in sorted(os.listdir(OUT)):
         print(f, os.path.getsize(os.path.join(OUT, f)))
 

@@ -51,6 +51,7 @@ EXPORTED_SYMBOLS = (
     "vct_fbp_transpose", "vct_fbp_transpose_dev",
     "vct_set_density_scale", "vct_descent_step_dev", "vct_lengthproj", "vct_lengthproj_dev",
     "vct_beam_hardening", "vct_beam_hardening_dev", "vct_set_beam_hardening",
+    "vct_lengthproj2", "vct_lengthproj2_dev", "vct_ir_update_dev", "vct_squdiff_dev", "vct_ir_step",
     "vct_forward_adjoint", "vct_forward_adjoint_dev", "vct_forward_vjp_dev", "vct_adjoint_rays_dev",
     "vct_batch_create", "vct_batch_run", "vct_batch_synchronize", "vct_batch_config", "vct_batch_destroy",
     "vct_forward_batched",
@@ -163,6 +164,12 @@ def lib():
     L.vct_set_density_scale.argtypes = [vp, C.c_double]
     L.vct_lengthproj.argtypes = [vp, vp, C.c_double, C.c_double, vp]
     L.vct_beam_hardening.argtypes = [vp, vp, C.c_double, C.c_double, vp]
+    L.vct_lengthproj2.argtypes = [vp, vp, C.c_double, C.c_double, C.c_int, C.c_int, vp]
+    L.vct_lengthproj2_dev.argtypes = [vp, vp, C.c_double, C.c_double, C.c_int, C.c_int, vp]
+    L.vct_ir_update_dev.argtypes = [vp, vp, vp, vp, vp, C.c_double, C.c_double, C.c_double, C.c_int, C.c_int, vp]
+    L.vct_squdiff_dev.argtypes = [vp, vp, vp, C.c_int, C.c_int, C.c_int, vp]
+    L.vct_ir_step.argtypes = [vp, vp, vp, vp, vp, C.c_double, C.c_double, C.c_int, C.c_int, C.c_int, C.c_double,
+                              C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double), vp]
     L.vct_beam_hardening_dev.argtypes = [vp, vp, C.c_double, C.c_double]
     L.vct_set_beam_hardening.argtypes = [vp, C.c_double, C.c_double]
     L.vct_lengthproj_dev.argtypes = [vp, vp, C.c_double, C.c_double, vp]
@@ -366,6 +373,40 @@ class Context:
         out = np.zeros((g.recon_size, g.recon_size), np.float32)
         _check(lib().vct_lengthproj(self._h, _ptr(p), float(z), float(couch_speed), _ptr(out)), "vct_lengthproj")
         return out
+
+    def lengthproj2(self, proj, ite: int, thinout: int, z: float = 0.0, couch_speed: float = 0.0) -> np.ndarray:
+        """lengthproj_TOMO_2 of the iterative step: npf [N][N]."""
+        g = self.geometry
+        p = np.ascontiguousarray(proj, np.float32)
+        out = np.zeros((g.recon_size, g.recon_size), np.float32)
+        _check(lib().vct_lengthproj2(self._h, _ptr(p), float(z), float(couch_speed), int(ite), int(thinout), _ptr(out)),
+               "vct_lengthproj2")
+        return out
+
+    def ir_update_dev(self, before, npf, npf_re, after, wbefore, w_tv, w_prior=0.0, ite=1, thinout=1,
+                      prior=None) -> None:
+        _check(lib().vct_ir_update_dev(self._h, before.data_ptr(), _dp(prior), npf.data_ptr(), npf_re.data_ptr(),
+                                       float(wbefore), float(w_tv), float(w_prior), int(ite), int(thinout),
+                                       after.data_ptr()), "vct_ir_update_dev")
+
+    def ir_step(self, proj, npf, before, *, ite=1, thinout=10, num_ite=500, w_tv=1e-4, w_prior=0.0, wbefore=0.0105,
+                objective=1e7, z=0.0, couch_speed=0.0, prior=None, after=None):
+        """One pass of the reference's iterative step; returns (after, wbefore,
+        objective, quadratic)."""
+        N = self.geometry.recon_size
+        p = np.ascontiguousarray(proj, np.float32)
+        out = np.zeros((N, N), np.float32) if after is None else np.array(after, np.float32, copy=True)
+        wb, ob, qd = C.c_double(wbefore), C.c_double(objective), C.c_double(0.0)
+        pr = None if prior is None else np.ascontiguousarray(prior, np.float32)
+        _check(lib().vct_ir_step(self._h, _ptr(p), _ptr(np.ascontiguousarray(npf, np.float32)),
+                                 _ptr(np.ascontiguousarray(before, np.float32)), None if pr is None else _ptr(pr),
+                                 float(z), float(couch_speed), int(ite), int(thinout), int(num_ite), float(w_tv),
+                                 float(w_prior), C.byref(wb), C.byref(ob), C.byref(qd), _ptr(out)), "vct_ir_step")
+        return out, wb.value, ob.value, qd.value
+
+    def squdiff_dev(self, proj, reproj, out2, ite: int, thinout: int, num_ite: int) -> None:
+        _check(lib().vct_squdiff_dev(self._h, proj.data_ptr(), reproj.data_ptr(), int(ite), int(thinout), int(num_ite),
+                                     out2.data_ptr()), "vct_squdiff_dev")
 
     def lengthproj_dev(self, proj, npf, z: float = 0.0, couch_speed: float = 0.0) -> None:
         _check(lib().vct_lengthproj_dev(self._h, proj.data_ptr(), float(z), float(couch_speed), npf.data_ptr()),

@@ -57,7 +57,10 @@ struct vct_ctx {
   vct::DBuf<double> fbp_coeff;  // SID*cos((k-cw)*dbeta)*dbeta
   vct::DBuf<float> fbp_h[3];    // per filter (1 Ram-Lak, 2 Shepp-Logan): h0[2C-1] + row factors[C]
   vct::DBuf<float> fbp_g, fbp_q, fbp_sino, fbp_img;
-  double bh_alpha = 0.0, bh_beta = 0.0;  // beam-hardening correction in the FBP (alpha 0: off)
+  double bh_alpha = 0.0, bh_beta = 0.0;
+  vct::DBuf<double> sq_part;  // calc_squdiff_quad block partials
+  vct::DBuf<float> ir_proj, ir_reproj, ir_img;  // iterative step: sinograms [V][W], images 5 x [N][N]
+  vct::DBuf<double> ir_out;  // beam-hardening correction in the FBP (alpha 0: off)
   // Adjoint: per-ray walk plans (geometry only), ray factors, fixed-point
   // accumulator of the exact-walk rays, loss partials.
   int adj_ready = 0, adj_nspecial = 0, adj_tile = -1;

@@ -191,6 +191,8 @@ void vct_destroy(vct_ctx* c) {
   c->adj_g.release(); c->adj_part.release(); c->adj_loss.release(); c->adj_gmax.release();
   c->adj_sacc.release(); c->adj_meas.release(); c->adj_wts.release(); c->adj_grad.release();
   c->adj_ext.release();
+  c->sq_part.release();
+  c->ir_proj.release(); c->ir_reproj.release(); c->ir_img.release(); c->ir_out.release();
   if (c->h_stats) cudaFreeHost(c->h_stats);
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
@@ -554,6 +556,110 @@ int vct_fbp(vct_ctx* c, const float* sino, int filter, int in_mode, float* img) 
   return VCT_OK;
 }
 
+int vct_lengthproj2(vct_ctx* c, const float* proj, double z, double couch_speed, int ite, int thinout, float* npf) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!proj || !npf) return fail(VCT_E_ARG, "vct_lengthproj2: null buffer");
+  const size_t nproj = (size_t)(c->geo.views / 2 * 2) * c->geo.width;
+  const size_t nimg = (size_t)c->dg.N * c->dg.N;
+  if ((rc = c->fbp_sino.ensure(c->geo.views * (size_t)c->geo.width)) || (rc = c->fbp_img.ensure(nimg))) return rc;
+  VCT_CUDA(cudaMemcpyAsync(c->fbp_sino.p, proj, nproj * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  if ((rc = vct_lengthproj2_dev(c, c->fbp_sino.p, z, couch_speed, ite, thinout, c->fbp_img.p))) return rc;
+  VCT_CUDA(cudaMemcpyAsync(npf, c->fbp_img.p, nimg * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  VCT_CUDA(cudaStreamSynchronize(c->stream));
+  return VCT_OK;
+}
+
+// The image update of IR_ImageTOMO, MB/IR_ImageTOMO.cpp:19-72.
+int vct_ir_update_dev(vct_ctx* c, const float* d_before, const float* d_prior, const float* d_npf,
+                      const float* d_npf_re, double wbefore, double w_tv, double w_prior, int ite, int thinout,
+                      float* d_after) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!d_before || !d_npf || !d_npf_re || !d_after || thinout < 1) return fail(VCT_E_ARG, "vct_ir_update_dev: bad argument");
+  if ((rc = launch_ir_update(c->dg.N, d_before, d_prior, d_npf, d_npf_re, wbefore, w_tv, w_prior, ite, thinout, d_after,
+                             c->stream)))
+    return rc;
+  c->launches++;
+  return VCT_OK;
+}
+
+// calc_squdiff_quad, MB/main.cpp:111-134: objective (and, at ite == num_ite,
+// the quadratic) over the rows of iteration `ite`; d_out2 is 2 device doubles.
+int vct_squdiff_dev(vct_ctx* c, const float* d_proj, const float* d_reproj, int ite, int thinout, int num_ite,
+                    double* d_out2) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!d_proj || !d_reproj || !d_out2 || thinout < 1 || ite < 1) return fail(VCT_E_ARG, "vct_squdiff_dev: bad argument");
+  if ((rc = c->sq_part.ensure(squdiff_scratch_doubles()))) return rc;
+  const int used = c->geo.views / 2 * 2;
+  if ((rc = launch_squdiff(d_proj, d_reproj, c->geo.width, c->geo.start_channel, c->dg.C, (ite - 1) % thinout, thinout,
+                           used / thinout, ite == num_ite, c->sq_part.p, d_out2, c->stream)))
+    return rc;
+  c->launches += 2;
+  return VCT_OK;
+}
+
+// One pass of the iterative step, MB/main.cpp:432-600 for ite >= 1: the
+// last energy bin's sinogram (the reprojection_float buffer the reference's
+// step reads after its energy loop, un-normalised, float per bin), the
+// squared difference to the measured sinogram, update_wbefore
+// (MB/main.cpp:136-150), lengthproj_TOMO_2 of that sinogram and the
+// IR_ImageTOMO update of the first element's map.
+int vct_ir_step(vct_ctx* c, const float* proj, const float* npf, const float* before, const float* prior, double z,
+                double couch_speed, int ite, int thinout, int num_ite, double w_tv, double w_prior, double* wbefore,
+                double* objective, double* quadratic, float* after) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!proj || !npf || !before || !wbefore || !objective || !after || ite < 1 || thinout < 1)
+    return fail(VCT_E_ARG, "vct_ir_step: bad argument");
+  if (!c->maps_ready || !c->spectrum_ready) return fail(VCT_E_STATE, "vct_ir_step: maps or spectrum not set");
+  const size_t nsino = (size_t)c->geo.views * c->geo.width, n2 = (size_t)c->dg.N * c->dg.N;
+  const size_t nused = (size_t)(c->geo.views / 2 * 2) * c->geo.width;
+  if ((rc = c->ir_proj.ensure(nsino)) || (rc = c->ir_reproj.ensure(nsino)) || (rc = c->ir_img.ensure(5 * n2)) ||
+      (rc = c->ir_out.ensure(2)))
+    return rc;
+  float* d_npf = c->ir_img.p;
+  float* d_npf_re = d_npf + n2;
+  float* d_before = d_npf + 2 * n2;
+  float* d_prior = d_npf + 3 * n2;
+  float* d_after = d_npf + 4 * n2;
+  VCT_CUDA(cudaMemsetAsync(c->ir_proj.p, 0, nsino * sizeof(float), c->stream));
+  VCT_CUDA(cudaMemcpyAsync(c->ir_proj.p, proj, nused * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  VCT_CUDA(cudaMemcpyAsync(d_npf, npf, n2 * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  VCT_CUDA(cudaMemcpyAsync(d_before, before, n2 * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  if (prior) VCT_CUDA(cudaMemcpyAsync(d_prior, prior, n2 * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  VCT_CUDA(cudaMemcpyAsync(d_after, after, n2 * sizeof(float), cudaMemcpyHostToDevice, c->stream));
+  // the last bin alone: its row of the reference-summation table, one bin
+  VCT_CUDA(cudaMemsetAsync(c->ir_reproj.p, 0, nsino * sizeof(float), c->stream));
+  VCT_CUDA(cudaMemcpyAsync(c->stats.p, c->stats.p + 1, sizeof(FwdStats), cudaMemcpyDeviceToDevice, c->stream));
+  if ((rc = launch_forward(c->dg, c->maps.p, c->M, c->mu_scaled.p + (size_t)(c->NE - 1) * c->M, c->pdf.p + c->NE - 1,
+                           1, c->cos_t.p, c->sin_t.p, c->det_px0.p, c->det_py0.p, VCT_SUM_REFERENCE,
+                           c->walk_mode == VCT_WALK_FAST, c->ir_reproj.p, nullptr, c->stats.p, c->stream)))
+    return rc;
+  c->launches++;
+  // calc_squdiff_quad over the measured rows used (the measured sinogram
+  // holds the views used, row k = view k).
+  if ((rc = vct_squdiff_dev(c, c->ir_proj.p, c->ir_reproj.p, ite, thinout, num_ite, c->ir_out.p))) return rc;
+  double h_out[2];
+  VCT_CUDA(cudaMemcpyAsync(h_out, c->ir_out.p, 2 * sizeof(double), cudaMemcpyDeviceToHost, c->stream));
+  VCT_CUDA(cudaStreamSynchronize(c->stream));
+  const double obj_before = *objective;
+  *objective = h_out[0];
+  if (quadratic) *quadratic = h_out[1];
+  // update_wbefore, MB/main.cpp:136-150
+  if (*objective < obj_before) *wbefore += 0.0001;
+  else if (ite > 1) *wbefore -= 0.0002;
+  if (*wbefore <= 0.0) *wbefore = 0.0001;
+  if ((rc = vct_lengthproj2_dev(c, c->ir_reproj.p, z, couch_speed, ite, thinout, d_npf_re))) return rc;
+  if ((rc = vct_ir_update_dev(c, d_before, prior ? d_prior : nullptr, d_npf, d_npf_re, *wbefore, w_tv, w_prior, ite,
+                              thinout, d_after)))
+    return rc;
+  VCT_CUDA(cudaMemcpyAsync(after, d_after, n2 * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
+  VCT_CUDA(cudaStreamSynchronize(c->stream));
+  return VCT_OK;
+}
+
 // Beam-hardening correction, MB/beam_hardening_correction.cpp:21-69.
 int vct_set_beam_hardening(vct_ctx* c, double alpha, double beta) {
   int rc = check_ctx(c);
@@ -592,10 +698,12 @@ int vct_beam_hardening(vct_ctx* c, const float* sino, double alpha, double beta,
 // a rotation); with no couch motion the reference divides 0/0 there and reads
 // its trig tables out of range, and this build starts at view 0, as the
 // reference's main does for the sinogram it passes in (MB/main.cpp:350).
-int vct_lengthproj_dev(vct_ctx* c, const float* d_proj, double z, double couch_speed, float* d_npf) {
+static int lengthproj_into(vct_ctx* c, const float* d_proj, double z, double couch_speed, int ite, int thinout,
+                           int tables, float* d_npf) {
   int rc = check_ctx(c);
   if (rc) return rc;
-  if (!d_proj || !d_npf) return fail(VCT_E_ARG, "vct_lengthproj_dev: null buffer");
+  if (!d_proj || !d_npf) return fail(VCT_E_ARG, "vct_lengthproj: null buffer");
+  if (thinout < 1 || ite < 1 - (tables ? 0 : 1)) return fail(VCT_E_ARG, "vct_lengthproj: bad ite/thinout");
   const vct_geometry& g = c->geo;
   LpGeom q{};
   q.N = c->dg.N;
@@ -612,6 +720,10 @@ int vct_lengthproj_dev(vct_ctx* c, const float* d_proj, double z, double couch_s
     q.start = (int)sv;
   }
   q.nrot = q.start / g.views;
+  q.first = tables ? (ite - 1) % thinout : 0;  // thinnumb, :195-196
+  q.stride = thinout;
+  q.count = tables ? q.count / thinout : q.count;
+  q.round_tables = tables;
   q.s = g.pixel_cm;
   q.sid = g.sid_cm;
   q.dsrc = g.det_src_iso_cm;
@@ -622,6 +734,15 @@ int vct_lengthproj_dev(vct_ctx* c, const float* d_proj, double z, double couch_s
   if ((rc = launch_lengthproj(q, c->cos_t.p, c->sin_t.p, d_proj, d_npf, c->stream))) return rc;
   c->launches++;
   return VCT_OK;
+}
+
+int vct_lengthproj_dev(vct_ctx* c, const float* d_proj, double z, double couch_speed, float* d_npf) {
+  return lengthproj_into(c, d_proj, z, couch_speed, 0, 1, 0, d_npf);
+}
+
+int vct_lengthproj2_dev(vct_ctx* c, const float* d_proj, double z, double couch_speed, int ite, int thinout,
+                        float* d_npf) {
+  return lengthproj_into(c, d_proj, z, couch_speed, ite, thinout, 1, d_npf);
 }
 
 int vct_lengthproj(vct_ctx* c, const float* proj, double z, double couch_speed, float* npf) {

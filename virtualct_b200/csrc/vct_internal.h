@@ -111,10 +111,20 @@ int launch_fbp_weight_t(const float* d_g, int V, int W, int start, int C, const 
 struct LpGeom {
   int N, V, W, start_ch, end_ch;
   int start, count, nrot;  // first view, views used, whole rotations before it
+  int first, stride;       // rows first + k*stride, k < count (lengthproj_TOMO: 0, 1)
+  int round_tables;        // 1: chord and channel rounded to float (lengthproj_TOMO_2)
   double s, sid, dsrc, diso, R, iso, dalpha;
 };
 int launch_lengthproj(const LpGeom& q, const double* d_cos, const double* d_sin, const float* d_proj, float* d_npf,
                       cudaStream_t st);
+
+// The reference's iterative step (vct_ir.cu).
+int launch_ir_update(int N, const float* d_before, const float* d_prior, const float* d_npf, const float* d_npf_re,
+                     double wbefore, double w_tv, double w_prior, int ite, int thinout, float* d_after,
+                     cudaStream_t st);
+int squdiff_scratch_doubles();
+int launch_squdiff(const float* d_p, const float* d_r, int W, int start, int C, int first, int stride, int rows,
+                   int quad, double* d_part, double* d_out, cudaStream_t st);
 
 // Adjoint (vct_adjoint.cu).  Ray kinds of the per-ray walk record.
 constexpr int kAdjRayNone = 0;   // no segment

@@ -8,6 +8,9 @@
 // the per-view terms follow the reference's expressions.  The side tables
 // the reference writes (chord and detector position per pixel and view,
 // [N][N][V] floats each) are not kept: every term is recomputed.
+// lengthproj_TOMO_2 (:188-276, the iterative step) reads those tables back
+// for every `stride`-th view from `first` on; with round_tables the chord and
+// the channel are rounded to float, as the tables store them.
 #include <cuda_runtime.h>
 #include <math.h>
 
@@ -32,7 +35,8 @@ __global__ void lengthproj_kernel(LpGeom q, const double* __restrict__ cos_t, co
   const double rx = -N * s * 0.5 + (jx + 0.5) * s;
   float acc = 0.0f;
   for (int k = 0; k < q.count; k++) {
-    int v = q.start + k - q.nrot * q.V;
+    const int row_k = q.first + k * q.stride;  // sinogram row (j_one)
+    int v = q.start + row_k - q.nrot * q.V;
     if (v >= q.V) v -= q.V;
     if (v < 0) v += q.V;  // the reference reads its tables out of range here
     const double cb = cos_t[v], sb = sin_t[v];
@@ -73,8 +77,12 @@ __global__ void lengthproj_kernel(LpGeom q, const double* __restrict__ cos_t, co
     const double d2 = (px - ox) * (px - ox) + (py - oy) * (py - oy);
     const double ang = acos(1.0 - d2 / (2.0 * q.R * q.R));
     const double rpx = px * cb - py * sb;
-    const double dj = rpx > 0.0 ? q.iso - ang / q.dalpha : q.iso + ang / q.dalpha;
-    const float* row = proj + (size_t)k * q.W;
+    double dj = rpx > 0.0 ? q.iso - ang / q.dalpha : q.iso + ang / q.dalpha;
+    if (q.round_tables) {
+      len = (double)(float)len;
+      dj = (double)(float)dj;
+    }
+    const float* row = proj + (size_t)row_k * q.W;
     // three explicit tests, as :158-172 (a NaN channel adds nothing)
     if (q.start_ch <= dj && dj < q.end_ch - 1) {
       const int ij = (int)dj;

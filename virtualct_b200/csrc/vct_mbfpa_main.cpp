@@ -17,6 +17,7 @@
 #include <sys/stat.h>
 #include <sys/types.h>
 
+#include <algorithm>
 #include <string>
 #include <vector>
 
@@ -130,6 +131,39 @@ int main(int argc, char* argv[]) {
   }
   printf("projection_min = %lf, used noise = %lf\n", (double)stats[1], cfg.photon_noise);
   rc = vct_write_raw("reprojection_float.raw", sino.data(), sino.size() * sizeof(float));
+  // The iterative step (MB/main.cpp:432-600 at ite 1, after the energy loop):
+  // first element's map updated by IR_ImageTOMO, written per slice as
+  // ReconImageRaw/Reconstruction_ite0001_zNNNN.raw, and as int16
+  // 1024*(x - 0.0716)/0.0716 of the best image to Reconstruction_512x512x<slices>.raw.
+  if (rc == VCT_OK) {
+    char name[256];
+    snprintf(name, sizeof name, "ReconImageRaw/Reconstruction_512x512x%d.raw", cfg.recon_slices);
+    FILE* fprecon = fopen(name, "wb");
+    const int thinout = cfg.osemset > 0 ? cfg.osemset : 1;
+    std::vector<float> proj((size_t)(g.views / 2 * 2) * g.width, 0.0f);  // no measured sinogram
+    std::vector<float> npf(n2, 0.0f), before(n2), after(n2), best(n2, 0.0f);
+    std::vector<int16_t> img16(n2);
+    for (int rz = 0; rz < cfg.recon_slices && rc == VCT_OK; rz++) {
+      const double zpos = cfg.recon_offset + rz * cfg.recon_step;
+      rc = vct_lengthproj(ctx, proj.data(), zpos, cfg.couch_speed, npf.data());
+      for (size_t i = 0; i < n2; i++) before[i] = (float)maps[i] / 1000;  // initial_image_def
+      std::fill(after.begin(), after.end(), 0.0f);
+      double wbefore = cfg.gradient_decent_const + 0.0005, objective = 10000000.0, quadratic = 0.0;
+      double min_squdiff = 10000000.0;
+      if (rc == VCT_OK)
+        rc = vct_ir_step(ctx, proj.data(), npf.data(), before.data(), nullptr, zpos, cfg.couch_speed, 1, thinout,
+                         cfg.num_ite, cfg.total_variation, cfg.prior_const, &wbefore, &objective, &quadratic,
+                         after.data());
+      if (rc != VCT_OK) break;
+      snprintf(name, sizeof name, "ReconImageRaw/Reconstruction_ite%04d_z%04d.raw", 1, rz);
+      rc = vct_write_raw(name, after.data(), n2 * sizeof(float));
+      if (min_squdiff > objective) best = after;  // calc_reconImagefloat_min
+      else std::fill(best.begin(), best.end(), 0.0f);
+      for (size_t i = 0; i < n2; i++) img16[i] = (short)(1024 * (best[i] - 0.0716) / 0.0716);
+      if (fprecon) fwrite(img16.data(), sizeof(int16_t), n2, fprecon);
+    }
+    if (fprecon) fclose(fprecon);
+  }
   vct_destroy(ctx);
   if (rc != VCT_OK) {
     fprintf(stderr, "%s\n", vct_last_error());

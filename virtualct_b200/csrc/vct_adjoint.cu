@@ -368,8 +368,8 @@ adj_gather_kernel(AdjGeom a, const double* __restrict__ cos_t, const double* __r
   __shared__ float4 s_A[kAdjCap];
   __shared__ float4 s_B[kAdjCap];
   __shared__ int2 s_K[kAdjCap];
-  __shared__ __align__(16) float s_g[kAdjCap * MG];
-  __shared__ int s_jlo[kAdjVB], s_jn[kAdjVB], s_base[kAdjVB + 1];
+  __shared__ float4 s_g4[(MG / 4) * kAdjCap];  // ray factors, quad q of ray k at q * kAdjCap + k
+  __shared__ int s_jlo[kAdjVB], s_jn[kAdjVB], s_base[kAdjVB + 1], s_cplx[kAdjVB];
   __shared__ float s_cb[kAdjVB], s_sb[kAdjVB], s_dtx[kAdjVB], s_dty[kAdjVB];
 
   const int N = a.N, NE1 = N + 1;
@@ -425,6 +425,7 @@ adj_gather_kernel(AdjGeom a, const double* __restrict__ cos_t, const double* __r
       }
       s_jlo[threadIdx.x] = jlo;
       s_jn[threadIdx.x] = jn;
+      s_cplx[threadIdx.x] = 0;
       s_cb[threadIdx.x] = (float)cb;
       s_sb[threadIdx.x] = (float)sb;
       s_dtx[threadIdx.x] = (float)(Tx - Sx);
@@ -462,7 +463,27 @@ adj_gather_kernel(AdjGeom a, const double* __restrict__ cos_t, const double* __r
                            __int_as_float(fast ? r.z : -1));
       s_K[k] = make_int2(r.x >> 2, r.y);
 #pragma unroll
-      for (int m = 0; m < MG; m++) s_g[k * MG + m] = m < M ? gr[ray * M + m] : 0.0f;
+      for (int q = 0; q < MG / 4; q++) {
+        float4 gq;
+        gq.x = 4 * q + 0 < M ? gr[ray * M + 4 * q + 0] : 0.0f;
+        gq.y = 4 * q + 1 < M ? gr[ray * M + 4 * q + 1] : 0.0f;
+        gq.z = 4 * q + 2 < M ? gr[ray * M + 4 * q + 2] : 0.0f;
+        gq.w = 4 * q + 3 < M ? gr[ray * M + 4 * q + 3] : 0.0f;
+        s_g4[q * kAdjCap + k] = gq;
+      }
+      // Does the ray's walk end or lump inside this tile?  If no staged ray
+      // of the view does, the whole block takes the plain chord path.
+      if (fast) {
+        const int lo = (r.y & 0xffff) - 1, hi = (r.y >> 16) - 1;
+        const int c0 = (r.x >> 2) ? e0 - 1 : f0 - 1;  // the tile's first cell on the ray's major axis
+        const int c1 = c0 + ((r.x >> 2) ? TX : TY) - 1;
+        bool cplx = c0 < lo || c1 > hi;
+        if (r.z >= 0) {
+          const int lc = r.z % a.N, lr = r.z / a.N;
+          cplx = cplx || (lc >= e0 - 1 && lc <= e0 + TX - 2 && lr >= f0 - 1 && lr <= f0 + TY - 2);
+        }
+        if (cplx) atomicOr(&s_cplx[vb], 1);
+      }
     }
     __syncthreads();
 
@@ -481,20 +502,45 @@ adj_gather_kernel(AdjGeom a, const double* __restrict__ cos_t, const double* __r
       const float dj = fmaf((fabsf(qx) + fabsf(qy)) * iq * iq, kdj, 0.05f);
       const int j0 = max((int)ceilf(jc - dj) - a.start - jlo, 0);
       const int j1 = min((int)floorf(jc + dj) - a.start - jlo, jn - 1);
-      for (int j = j0; j <= j1; j++) {
-        const int k = base + j;
-        const float4 A = s_A[k];
-        const float4 B = s_B[k];
-        const int2 K = s_K[k];
-        const float b = fmaf(A.x, ly, fmaf(-A.y, lx, A.z));
-        const float num = A.w - fabsf(b);
-        float len = num > 0.0f ? fminf(B.x, num * B.y) : 0.0f;
-        const int mi = K.x ? colx : rowx;
-        if (mi < (K.y & 0xffff) || mi > (K.y >> 16)) len = 0.0f;
-        if (__float_as_int(B.w) == pix) len += B.z;
-        const float* g = s_g + k * MG;
+      if (!s_cplx[vb]) {
+        // every candidate's walk covers the whole tile: chord only
+        for (int j = j0; j <= j1; j++) {
+          const int k = base + j;
+          const float4 A = s_A[k];
+          const float4 B = s_B[k];
+          const float b = fmaf(A.x, ly, fmaf(-A.y, lx, A.z));
+          const float num = A.w - fabsf(b);
+          const float len = num > 0.0f ? fminf(B.x, num * B.y) : 0.0f;
 #pragma unroll
-        for (int m = 0; m < M; m++) acc[m] = fmaf(len, g[m], acc[m]);
+          for (int q = 0; q < MG / 4; q++) {
+            const float4 g = s_g4[q * kAdjCap + k];
+            if (4 * q + 0 < M) acc[4 * q + 0] = fmaf(len, g.x, acc[4 * q + 0]);
+            if (4 * q + 1 < M) acc[4 * q + 1] = fmaf(len, g.y, acc[4 * q + 1]);
+            if (4 * q + 2 < M) acc[4 * q + 2] = fmaf(len, g.z, acc[4 * q + 2]);
+            if (4 * q + 3 < M) acc[4 * q + 3] = fmaf(len, g.w, acc[4 * q + 3]);
+          }
+        }
+      } else {
+        for (int j = j0; j <= j1; j++) {
+          const int k = base + j;
+          const float4 A = s_A[k];
+          const float4 B = s_B[k];
+          const int2 K = s_K[k];
+          const float b = fmaf(A.x, ly, fmaf(-A.y, lx, A.z));
+          const float num = A.w - fabsf(b);
+          float len = num > 0.0f ? fminf(B.x, num * B.y) : 0.0f;
+          const int mi = K.x ? colx : rowx;
+          if (mi < (K.y & 0xffff) || mi > (K.y >> 16)) len = 0.0f;
+          if (__float_as_int(B.w) == pix) len += B.z;
+#pragma unroll
+          for (int q = 0; q < MG / 4; q++) {
+            const float4 g = s_g4[q * kAdjCap + k];
+            if (4 * q + 0 < M) acc[4 * q + 0] = fmaf(len, g.x, acc[4 * q + 0]);
+            if (4 * q + 1 < M) acc[4 * q + 1] = fmaf(len, g.y, acc[4 * q + 1]);
+            if (4 * q + 2 < M) acc[4 * q + 2] = fmaf(len, g.z, acc[4 * q + 2]);
+            if (4 * q + 3 < M) acc[4 * q + 3] = fmaf(len, g.w, acc[4 * q + 3]);
+          }
+        }
       }
     }
 #pragma unroll

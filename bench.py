@@ -103,6 +103,23 @@ class ClockSampler:
 
 
 # ----------------------------------------------------------------- our arm
+def reduce_max(x: float, dist, device) -> float:
+    """Largest x over the ranks (every rank gets it); x itself without a
+    process group.  The elapsed times of a multi-rank run are taken this way."""
+    if dist is None:
+        return x
+    import torch
+
+    t = torch.tensor([x], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def replica_inputs(rank: int):
+    """Each rank projects its own slice: the phantom seed is the rank."""
+    return load_inputs(seed=rank)
+
+
 def run_ours(args, rank, world, dist):
     import torch
 
@@ -112,7 +129,7 @@ def run_ours(args, rank, world, dist):
     torch.cuda.set_device(dev)
     stream = torch.cuda.Stream()
     torch.cuda.set_stream(stream)
-    maps, mu, pdf = load_inputs(seed=rank)
+    maps, mu, pdf = replica_inputs(rank)
     NE = len(pdf)
     geo = vct.Geometry()
     ctx = vct.Context(geo, device=dev)
@@ -141,11 +158,7 @@ def run_ours(args, rank, world, dist):
         return sum(a.elapsed_time(b) for a, b in ev) / 1e3  # seconds
 
     def max_over_ranks(x):
-        if dist is None:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device="cuda")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+        return reduce_max(x, dist, "cuda")
 
     step = lambda: ctx.mbfpa_dev(SIGMA, 1 + rank, d_sino)  # noqa: E731
     fbp_step = lambda: ctx.fbp_dev(d_sino, d_img, 1)  # noqa: E731

@@ -184,6 +184,8 @@ def run_ours(args, rank, world, dist):
     barrier()
     t_fwd = max_over_ranks(timed(lambda: ctx.forward_dev(d_sino), args.steps)) / args.steps
     extras = {}
+    if rank == 0:
+        extras["parity"] = parity_vs_reference(ctx, d_sino)
     want = set() if args.no_extras or world > 1 else set(args.extras.split(","))
     if "adjoint" in want:
         extras["adjoint"] = bench_adjoint(ctx, d_maps, mu, pdf, stream, timed, args.steps, args.warmup)
@@ -292,6 +294,30 @@ def run_ours(args, rank, world, dist):
     if world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(maps, mu, pdf)
     return line
+
+
+# ------------------------------------------------------------------ parity
+def parity_vs_reference(ctx, d_sino):
+    """The device forward of the rank-0 slice (phantom seed 0, the bench
+    spectrum) against the reference's un-normalised spectral sum on every
+    20th view (tests/golden/c1_subset.npz)."""
+    import torch
+
+    path = os.path.join(ROOT, "tests", "golden", "c1_subset.npz")
+    if not os.path.exists(path):
+        return {"unavailable": "c1_subset fixture missing"}
+    d = np.load(path)
+    if int(d["seed"]) != 0:
+        return {"unavailable": "c1_subset fixture is not the seed-0 slice"}
+    ctx.forward_dev(d_sino)
+    torch.cuda.synchronize()
+    out = d_sino.cpu().numpy()[d["rows"]].astype(np.float64)
+    ref = d["full_rows"].astype(np.float64)
+    ok = ref > 0
+    return {"vs_reference_max_rel": float(np.max(np.abs(out[ok] - ref[ok]) / ref[ok])),
+            "tolerance": 1e-5, "rows": int(len(d["rows"])), "channels": int(ref.shape[1]),
+            "what": "un-normalised polyenergetic sinogram on every 20th view vs reprojection_TOMO summed over "
+                    "110 bins in reference order (pinned oracle, cross-checked against the compiled reference)"}
 
 
 # ------------------------------------------------ adjoint and batched lines

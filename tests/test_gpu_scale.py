@@ -95,3 +95,33 @@ def test_scale_geometry_gradient_vs_fp64(cuda_device):
     d = grad - ref
     assert np.abs(d).max() <= 1e-5 * np.abs(ref).max()
     assert np.linalg.norm(d) <= 1e-5 * np.linalg.norm(ref)
+
+
+def test_decomposition_checkpoint_resume(cuda_device, tmp_path):
+    """save() after three iterations and load() into a fresh decomposition:
+    the next iteration equals the uninterrupted run's bit for bit."""
+    import torch
+
+    el = phantoms.ELEMENTS8
+    tabs = [phantoms.kramers_tables(k, el) for k in (80, 140)]
+    geo = vct.Geometry(views=80, recon_size=64, pixel_cm=0.1)
+    true = [phantoms.ellipse_phantom(60 + s, 64, elements=el, border_px=2) for s in range(2)]
+    meas = [_measured(geo, m, tabs, 0.0, 10 * s) for s, m in enumerate(true)]
+    start = np.stack([m.astype(np.float32) / 1000.0 * 0.9 for m in true])
+    a = Decomposition(geo, tabs, meas, torch.from_numpy(start.copy()).cuda(), units=UNITS, tune=False)
+    b = Decomposition(geo, tabs, meas, torch.from_numpy(start.copy()).cuda(), units=UNITS, tune=False)
+    c = Decomposition(geo, tabs, meas, torch.from_numpy(np.zeros_like(start)).cuda(), units=UNITS, tune=False)
+    try:
+        a.iterate(4)
+        b.iterate(3)
+        b.save(tmp_path / "ckpt")
+        c.load(tmp_path / "ckpt")
+        c.iterate(1)
+        assert c.history == a.history
+        assert torch.equal(c.rho, a.rho)
+        assert torch.equal(c.maps, a.maps)
+        assert np.array_equal(c.step_size, a.step_size)
+    finally:
+        a.close()
+        b.close()
+        c.close()

@@ -20,6 +20,8 @@
 #include <algorithm>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "vct_ctx.h"
 
 using namespace vct;
@@ -305,6 +307,10 @@ int vct_batch_create(const vct_job* jobs, int n, int M, int device, int tune, vc
 
 int vct_batch_run(vct_batch* b, void* stream) {
   if (!b) return fail(VCT_E_ARG, "vct_batch_run: null batch");
+  nvtxRangePushA("vct_batch_run");
+  struct Pop {
+    ~Pop() { nvtxRangePop(); }
+  } pop;
   VCT_CUDA(cudaSetDevice(b->device));
   VCT_CUDA(cudaGraphLaunch(b->exec, stream ? (cudaStream_t)stream : b->stream));
   return VCT_OK;

@@ -9,6 +9,8 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "vct_internal.h"
 #include "vct_philox.h"
 
@@ -34,6 +36,13 @@ static const double kPI = 3.141592653589793238462643383279;
 using namespace vct;
 
 #include "vct_ctx.h"
+
+// An NVTX range over a host entry point (visible to ncu --nvtx and to any
+// NVTX-aware profiler; free when none is attached).
+struct NvtxScope {
+  explicit NvtxScope(const char* name) { nvtxRangePushA(name); }
+  ~NvtxScope() { nvtxRangePop(); }
+};
 
 static int check_ctx(vct_ctx* c) {
   if (!c) return fail(VCT_E_ARG, "null context");
@@ -399,6 +408,7 @@ static int fetch_stats(vct_ctx* c) {
 }
 
 int vct_forward_dev(vct_ctx* c, float* d_out) {
+  NvtxScope nvtx_scope("vct_forward_dev");
   int rc = check_ctx(c);
   if (rc) return rc;
   if (!d_out) return fail(VCT_E_ARG, "null output");
@@ -406,6 +416,7 @@ int vct_forward_dev(vct_ctx* c, float* d_out) {
 }
 
 int vct_forward(vct_ctx* c, float* out) {
+  NvtxScope nvtx_scope("vct_forward");
   int rc = check_ctx(c);
   if (rc) return rc;
   if (!out) return fail(VCT_E_ARG, "null output");
@@ -417,6 +428,7 @@ int vct_forward(vct_ctx* c, float* out) {
 }
 
 int vct_line_integrals_dev(vct_ctx* c, double* d_lint) {
+  NvtxScope nvtx_scope("vct_line_integrals_dev");
   int rc = check_ctx(c);
   if (rc) return rc;
   if (!d_lint) return fail(VCT_E_ARG, "null output");
@@ -439,6 +451,7 @@ int vct_normalize_noise_dev(vct_ctx* c, float* d_sino, double sigma, uint64_t se
 }
 
 int vct_mbfpa_dev(vct_ctx* c, double sigma, uint64_t seed, float* d_out) {
+  NvtxScope nvtx_scope("vct_mbfpa_dev");
   int rc = check_ctx(c);
   if (rc) return rc;
   if (!d_out) return fail(VCT_E_ARG, "null output");
@@ -451,6 +464,7 @@ int vct_mbfpa_dev(vct_ctx* c, double sigma, uint64_t seed, float* d_out) {
 }
 
 int vct_mbfpa(vct_ctx* c, double sigma, uint64_t seed, float* out, float* stats3) {
+  NvtxScope nvtx_scope("vct_mbfpa");
   int rc = check_ctx(c);
   if (rc) return rc;
   if (!out) return fail(VCT_E_ARG, "null output");
@@ -539,10 +553,12 @@ static int fbp_into(vct_ctx* c, const float* d_sino, int filter, int in_mode, fl
 }
 
 int vct_fbp_dev(vct_ctx* c, const float* d_sino, int filter, int in_mode, float* d_img) {
+  NvtxScope nvtx_scope("vct_fbp_dev");
   return fbp_into(c, d_sino, filter, in_mode, d_img, 4);
 }
 
 int vct_fbp(vct_ctx* c, const float* sino, int filter, int in_mode, float* img) {
+  NvtxScope nvtx_scope("vct_fbp");
   int rc = check_ctx(c);
   if (rc) return rc;
   if (!sino || !img) return fail(VCT_E_ARG, "null buffer");
@@ -609,6 +625,7 @@ int vct_squdiff_dev(vct_ctx* c, const float* d_proj, const float* d_reproj, int 
 int vct_ir_step(vct_ctx* c, const float* proj, const float* npf, const float* before, const float* prior, double z,
                 double couch_speed, int ite, int thinout, int num_ite, double w_tv, double w_prior, double* wbefore,
                 double* objective, double* quadratic, float* after) {
+  NvtxScope nvtx_scope("vct_ir_step");
   int rc = check_ctx(c);
   if (rc) return rc;
   if (!proj || !npf || !before || !wbefore || !objective || !after || ite < 1 || thinout < 1)
@@ -671,6 +688,7 @@ int vct_set_beam_hardening(vct_ctx* c, double alpha, double beta) {
 }
 
 int vct_beam_hardening_dev(vct_ctx* c, float* d_sino, double alpha, double beta) {
+  NvtxScope nvtx_scope("vct_beam_hardening_dev");
   int rc = check_ctx(c);
   if (rc) return rc;
   if (!d_sino) return fail(VCT_E_ARG, "vct_beam_hardening_dev: null buffer");
@@ -737,6 +755,7 @@ static int lengthproj_into(vct_ctx* c, const float* d_proj, double z, double cou
 }
 
 int vct_lengthproj_dev(vct_ctx* c, const float* d_proj, double z, double couch_speed, float* d_npf) {
+  NvtxScope nvtx_scope("vct_lengthproj_dev");
   return lengthproj_into(c, d_proj, z, couch_speed, 0, 1, 0, d_npf);
 }
 
@@ -762,6 +781,7 @@ int vct_lengthproj(vct_ctx* c, const float* proj, double z, double couch_speed, 
 // Transpose of the FBP's linear part (no counterpart in the reference):
 // backprojection, filter and weight transposed, in reverse order.
 int vct_fbp_transpose_dev(vct_ctx* c, const float* d_u, int filter, float* d_lam) {
+  NvtxScope nvtx_scope("vct_fbp_transpose_dev");
   int rc = check_ctx(c);
   if (rc) return rc;
   if (!d_u || !d_lam) return fail(VCT_E_ARG, "null buffer");
@@ -923,6 +943,7 @@ static int adj_run(vct_ctx* c, int mode, const float* d_meas, const float* d_wts
 extern "C" {
 
 int vct_forward_adjoint_dev(vct_ctx* c, const float* d_meas, const float* d_weights, float* d_grad, double* d_loss) {
+  NvtxScope nvtx_scope("vct_forward_adjoint_dev");
   int rc = check_ctx(c);
   if (rc) return rc;
   if (!d_meas || !d_grad) return fail(VCT_E_ARG, "vct_forward_adjoint_dev: null buffer");
@@ -930,6 +951,7 @@ int vct_forward_adjoint_dev(vct_ctx* c, const float* d_meas, const float* d_weig
 }
 
 int vct_forward_vjp_dev(vct_ctx* c, const float* d_dy, float* d_grad) {
+  NvtxScope nvtx_scope("vct_forward_vjp_dev");
   int rc = check_ctx(c);
   if (rc) return rc;
   if (!d_dy || !d_grad) return fail(VCT_E_ARG, "vct_forward_vjp_dev: null buffer");
@@ -937,6 +959,7 @@ int vct_forward_vjp_dev(vct_ctx* c, const float* d_dy, float* d_grad) {
 }
 
 int vct_adjoint_rays_dev(vct_ctx* c, const float* d_g, float* d_out) {
+  NvtxScope nvtx_scope("vct_adjoint_rays_dev");
   int rc = check_ctx(c);
   if (rc) return rc;
   if (!d_g || !d_out) return fail(VCT_E_ARG, "vct_adjoint_rays_dev: null buffer");
@@ -945,6 +968,7 @@ int vct_adjoint_rays_dev(vct_ctx* c, const float* d_g, float* d_out) {
 }
 
 int vct_forward_adjoint(vct_ctx* c, const float* meas, const float* weights, float* grad, double* loss) {
+  NvtxScope nvtx_scope("vct_forward_adjoint");
   int rc = check_ctx(c);
   if (rc) return rc;
   if (!meas || !grad) return fail(VCT_E_ARG, "vct_forward_adjoint: null buffer");

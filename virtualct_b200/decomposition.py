@@ -117,6 +117,59 @@ class Decomposition:
         for s in range(self.S):
             self._requantize(s, stream_ptr)
 
+    # checkpoint / resume ------------------------------------------------------
+    def save(self, directory) -> None:
+        """Densities of every slice as float32 [M][N][N] raw files
+        (rho_sNNNN.raw, the reference's raw layout) and the descent state
+        (state.json).  The gradient at the accepted point is not stored: the
+        kernels are deterministic, so load() recomputes it bit for bit (its
+        squared norm is stored, as the reduction order that made it varies)."""
+        import json
+        import os
+
+        import torch
+
+        torch.cuda.synchronize()
+        os.makedirs(directory, exist_ok=True)
+        for s in range(self.S):
+            self.rho[s].cpu().numpy().astype(np.float32).tofile(os.path.join(directory, f"rho_s{s:04d}.raw"))
+        state = {"slices": self.S, "elements": self.M, "units": self.units,
+                 "step_size": [float(x) for x in self.step_size],
+                 "cur_loss": None if self.cur_loss is None else [float(x) for x in self.cur_loss],
+                 "gnorm2": [float(x) for x in self.gnorm2],
+                 "history": self.history, "accepted": self.accepted, "rejected": self.rejected}
+        with open(os.path.join(directory, "state.json"), "w") as f:
+            json.dump(state, f)
+
+    def load(self, directory, stream_ptr: int | None = None) -> None:
+        """Continue from save(): the next iterate() takes the step the saved
+        run would have taken."""
+        import json
+        import os
+
+        import torch
+
+        with open(os.path.join(directory, "state.json")) as f:
+            state = json.load(f)
+        if state["slices"] != self.S or state["elements"] != self.M or state["units"] != self.units:
+            raise ValueError("checkpoint does not match this decomposition")
+        N = self.geometry.recon_size
+        for s in range(self.S):
+            a = np.fromfile(os.path.join(directory, f"rho_s{s:04d}.raw"), np.float32).reshape(self.M, N, N)
+            self.rho[s].copy_(torch.from_numpy(a))
+        self._requantize_all(stream_ptr)
+        self.step_size = np.array(state["step_size"], np.float64)
+        self.history = list(state["history"])
+        self.accepted, self.rejected = state["accepted"], state["rejected"]
+        if state["cur_loss"] is None:
+            self.cur_loss = None
+            return
+        self.cur_loss = np.array(state["cur_loss"], np.float64)
+        self.gnorm2 = np.array(state["gnorm2"], np.float64)
+        self.gradients(stream_ptr)
+        torch.cuda.synchronize()
+        torch.sum(self.grads, 1, out=self.g)
+
     def total_loss(self) -> float:
         """Total loss at the accepted points."""
         return float(self.cur_loss.sum()) if self.cur_loss is not None else float("nan")

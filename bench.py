@@ -564,7 +564,9 @@ def bench_scale(stream, slices=64, iters=2):
             "ms_per_iteration": t, "value": units / t * 1e3, "unit": "rays*bins/s (forward + adjoint)",
             "iterations_timed": iters, "projected_50_iterations_s": 50 * t / 1e3,
             "loss_first": dec.history[0], "loss_last": dec.history[-1], "accepted": dec.accepted,
-            "rejected": dec.rejected, "setup_s": setup_s}
+            "rejected": dec.rejected, "unchanged": dec.unchanged,
+            "step_rule": "SQS-diagonal-scaled projected gradient, adaptive Barzilai-Borwein steps, Armijo test",
+            "setup_s": setup_s}
     dec.close()
     return line
 

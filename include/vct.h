@@ -294,6 +294,12 @@ int vct_adjoint_rays_dev(vct_ctx* ctx, const float* d_g, float* d_out);
  * default stream); allocates nothing. */
 int vct_descent_step_dev(float* d_rho, const float* d_grad_a, const float* d_grad_b, double step, double units,
                          int16_t* d_maps, long long count, void* stream);
+/* The same step with a diagonal scale (a preconditioner, no counterpart in
+ * the reference): rho[i] = max(0, rho[i] - step * grad[i] * scale[i % period]),
+ * then maps[i] as above.  period is the scale table's length (M*N*N for one
+ * table shared by every slice of a [S][M][N][N] block).  Allocates nothing. */
+int vct_descent_step_scaled_dev(float* d_rho, const float* d_grad, const float* d_scale, long long period,
+                                double step, double units, int16_t* d_maps, long long count, void* stream);
 
 /* ------------------------------------------------------------------ batch
  * Many slices of uneven size (geometry, grid, spectrum) in one captured CUDA

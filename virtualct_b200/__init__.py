@@ -49,7 +49,7 @@ EXPORTED_SYMBOLS = (
     "vct_set_sum_mode", "vct_set_walk_mode", "vct_forward", "vct_forward_dev", "vct_line_integrals_dev", "vct_mbfpa", "vct_mbfpa_dev",
     "vct_normalize_noise_dev", "vct_fbp", "vct_fbp_dev", "vct_fbp_noalloc", "vct_fbp_filtered_dev",
     "vct_fbp_transpose", "vct_fbp_transpose_dev",
-    "vct_set_density_scale", "vct_descent_step_dev", "vct_lengthproj", "vct_lengthproj_dev",
+    "vct_set_density_scale", "vct_descent_step_dev", "vct_descent_step_scaled_dev", "vct_lengthproj", "vct_lengthproj_dev",
     "vct_beam_hardening", "vct_beam_hardening_dev", "vct_set_beam_hardening",
     "vct_lengthproj2", "vct_lengthproj2_dev", "vct_ir_update_dev", "vct_squdiff_dev", "vct_ir_step",
     "vct_forward_adjoint", "vct_forward_adjoint_dev", "vct_forward_vjp_dev", "vct_adjoint_rays_dev",
@@ -174,6 +174,8 @@ def lib():
     L.vct_set_beam_hardening.argtypes = [vp, C.c_double, C.c_double]
     L.vct_lengthproj_dev.argtypes = [vp, vp, C.c_double, C.c_double, vp]
     L.vct_descent_step_dev.argtypes = [vp, vp, vp, C.c_double, C.c_double, vp, C.c_longlong, vp]
+    L.vct_descent_step_scaled_dev.argtypes = [vp, vp, vp, C.c_longlong, C.c_double, C.c_double, vp, C.c_longlong,
+                                              vp]
     L.vct_forward_adjoint.argtypes = [vp, vp, vp, vp, C.POINTER(C.c_double)]
     L.vct_forward_adjoint_dev.argtypes = [vp, vp, vp, vp, vp]
     L.vct_forward_vjp_dev.argtypes = [vp, vp, vp]
@@ -542,6 +544,16 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def descent_step_scaled_dev(rho, grad, scale, step: float, units: float, maps, stream_ptr: int | None = None) -> None:
+    """rho -= step * grad * scale (scale broadcast over leading dimensions),
+    clamped at 0; maps = round(rho * units)."""
+    if rho.numel() % scale.numel():
+        raise ValueError("the scale table must tile rho")
+    _check(lib().vct_descent_step_scaled_dev(rho.data_ptr(), grad.data_ptr(), scale.data_ptr(), scale.numel(),
+                                             float(step), float(units), maps.data_ptr(), rho.numel(), stream_ptr),
+           "vct_descent_step_scaled_dev")
 
 
 def descent_step_dev(rho, grad_a, grad_b, step: float, units: float, maps, stream_ptr: int | None = None) -> None:

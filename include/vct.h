@@ -37,6 +37,7 @@ extern "C" {
 #define VCT_E_IO (-5)          /* file missing, short or malformed */
 #define VCT_E_STATE (-6)       /* call order: e.g. forward before maps are set */
 #define VCT_E_UNSUPPORTED (-7) /* configuration outside this build's limits */
+#define VCT_E_RANGE (-8)       /* a measured value outside the range the reference accepts */
 
 #define VCT_MAX_MATERIALS 8
 #define VCT_MAX_BINS 1024 /* the reference's spectrum buffers hold 1024 bins (MB/main.cpp:338-339) */
@@ -285,6 +286,19 @@ int vct_forward_vjp_dev(vct_ctx* ctx, const float* d_dy, float* d_grad);
  * per-ray, per-element weights d_g [views/2*2][end-start][M] (float), M the
  * maps' element count; the transpose of vct_line_integrals_dev. */
 int vct_adjoint_rays_dev(vct_ctx* ctx, const float* d_g, float* d_out);
+
+/* Helical z-interpolation, MB/main.cpp:347-371 (start_angle_num 0,
+ * UsedReconAngle 2): from a measured volume [rotations][views][width]
+ * (vct_load_measured), the sinogram [views][width] of one reconstruction z.
+ * View j < (views/2*2)/2 is blended with view j of the next rotation,
+ * (1 - w) a + w b in FP64 with w = 0.5 |j - views/2| / (views/2), where the
+ * next rotation exists within the volume (j + views <= (rotations-1)*views);
+ * every other view is (1 - w) a + w a.  Rows from views/2*2 on are left as
+ * they are in out.  _dev: device buffers, enqueued on stream (NULL: legacy
+ * default stream); the host form copies through the given device. */
+int vct_helical_sinogram(const float* volume, int rotations, int views, int width, float* out, int device);
+int vct_helical_sinogram_dev(const float* d_volume, int rotations, int views, int width, float* d_out,
+                             void* stream);
 
 /* One projected gradient-descent step on device densities (no counterpart in
  * the reference): rho[i] = max(0, rho[i] - step * (grad_a[i] + grad_b[i]))

@@ -96,6 +96,51 @@ void vct_fbp_geometry(const vct_fbp_config* cfg, vct_geometry* g);
 int vct_read_raw(const char* path, long offset, void* buf, size_t bytes, size_t* got);
 int vct_write_raw(const char* path, const void* buf, size_t bytes);
 
+/* ------------------------------------------------- measured-data ingestion
+ * The raw detector layout of a measured sinogram and its air scan: the
+ * NumberOfChannels, NumberOfSkips, AirScn_Sinogram_Height,
+ * AirScn_Sinogram_Number, Start_Channel and End_Channel constants of
+ * MB/physParamsTOMO.h:32-65 as runtime fields. */
+typedef struct vct_raw_layout {
+  int raw_channels;   /* floats per raw detector row (609) */
+  int skip_channels;  /* raw channels before the first used one (27) */
+  int air_rows;       /* rows per air-scan block and per PR rotation (800) */
+  int air_blocks;     /* air-scan blocks averaged after the first, unused one (5) */
+  int start_channel;  /* raw-channel window of the IN-mode maximum check */
+  int end_channel;    /*   [start_channel, end_channel): 0 and 609 */
+} vct_raw_layout;
+void vct_raw_layout_default(vct_raw_layout* layout);
+
+/* loadProjectionData, MB/projectionDataTOMO.cpp:324-508: reads
+ * cfg->air_scan_file and cfg->proj_file and writes the normalised volume
+ * [cfg->total_proj_number][cfg->proj_height][cfg->proj_width] and its mask
+ * (1 = usable).  The air scan's first block is skipped and the next
+ * air_blocks are averaged in float, block by block.
+ *   PR (cfg->in_pr_class "PR"): each rotation is an [air_rows][raw_channels]
+ *      plane; volume = plane / air mean over channels skip_channels.., rows
+ *      thinned by cfg->sino_fact; mask 1.
+ *   IN: rows of raw_channels floats per view (5 per view when
+ *      cfg->data_sampling_rate_orig >= 200, the first used); volume =
+ *      row / (2 * air mean of air row 0), values below 0.1 set to 0 with
+ *      mask 0.  As in the reference's loop, only view 0 of each rotation
+ *      reads the file's row; views >= 1 read rows of its buffer that no read
+ *      fills, so they are 0 (or NaN where the air mean is 0).
+ * Files are read with the reference's byte counts into buffers that persist
+ * between reads: a short file repeats the previous read's tail.  Returns
+ * VCT_E_IO when a file is missing (the reference then keeps a zero volume),
+ * VCT_E_RANGE when an IN-mode value in [start_channel, end_channel) exceeds 1
+ * (the reference prints it and stops; *max_value = that value),
+ * VCT_E_UNSUPPORTED for layouts that would take the reference past its own
+ * buffers (PR: skip_channels + width > raw_channels or kept air rows !=
+ * proj_height; IN: rows read past one air block).  *rotations receives the
+ * rotations read, *max_value the IN-mode maximum in the window (0 for PR).
+ * The normalisation runs on `device`; _dev writes device buffers on stream
+ * and returns after it has finished with its host copies. */
+int vct_load_measured(const vct_mb_config* cfg, const vct_raw_layout* layout, int device, float* volume,
+                      unsigned char* mask, int* rotations, double* max_value);
+int vct_load_measured_dev(const vct_mb_config* cfg, const vct_raw_layout* layout, float* d_volume,
+                          unsigned char* d_mask, int* rotations, double* max_value, void* stream);
+
 #ifdef __cplusplus
 }
 #endif

@@ -103,6 +103,11 @@ def lib():
                                     C.c_int, _fp]
         L.orc_walk_project_rays.argtypes = [C.POINTER(OrcGeom), _dp, _dp, _dp, C.c_int, _ip, C.c_int, _dp, C.c_int]
         L.orc_siddon_project.argtypes = [C.POINTER(OrcGeom), _dp, _dp, _dp, C.c_int, _dp, C.c_int]
+        L.orc_load_measured.argtypes = [C.c_char_p, C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int,
+                                        C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, C.c_int, _fp, _u8p,
+                                        C.POINTER(C.c_double)]
+        L.orc_load_measured.restype = C.c_int
+        L.orc_helical.argtypes = [_fp, C.c_int, C.c_int, C.c_int, _fp]
         L.orc_normalize_noise.argtypes = [_fp, C.c_int, C.c_double, C.c_uint, C.c_int]
         L.orc_normalize_noise.restype = C.c_double
         L.orc_fbp_constmap.argtypes = [C.POINTER(OrcGeom), C.c_int, _dp]
@@ -475,6 +480,43 @@ def ref_available() -> bool:
     return all(os.path.exists(os.path.join(HERE, "_ref", f)) for f in ("libvct_ref_mb.so", "libvct_ref_fbp.so"))
 
 
+# The raw layout constants of MB/physParamsTOMO.h:32-33,43-46,64-65.
+RAW_LAYOUT = dict(ch=609, skip=27, air_rows=800, air_blocks=5, start_ch=0, end_ch=609)
+
+
+def load_measured(proj_file, air_file, in_mode, width, views, nskip, rotations, rate_orig, layout=None):
+    """orc_load_measured: (code, volume [rotations][views][width], mask, max)."""
+    lay = dict(RAW_LAYOUT, **(layout or {}))
+    vol = np.zeros((max(rotations, 0), views, width), np.float32)
+    mask = np.zeros(vol.shape, np.uint8)
+    mx = C.c_double(0.0)
+    rpv = 5 if rate_orig >= 200 else 1
+    rc = lib().orc_load_measured(str(proj_file).encode(), str(air_file).encode(), int(in_mode), width, views, nskip,
+                                 rotations, rpv, lay["ch"], lay["skip"], lay["air_rows"], lay["air_blocks"],
+                                 lay["start_ch"], lay["end_ch"], vol, mask, C.byref(mx))
+    return rc, vol, mask, mx.value
+
+
+def helical(vol):
+    """orc_helical: the z-interpolated [views][width] sinogram."""
+    vol = np.ascontiguousarray(vol, np.float32)
+    R, V, W = vol.shape
+    out = np.zeros((V, W), np.float32)
+    lib().orc_helical(vol, R, V, W, out)
+    return out
+
+
+def ref_load_measured(proj_file, air_file, in_pr, width, height_raw, nskip, rotations, rate_orig):
+    """The reference's loadProjectionData (run in the current directory, where
+    it writes projections.raw): (return value, volume, mask)."""
+    views = height_raw // nskip
+    vol = np.zeros((max(rotations, 0), views, width), np.float32)
+    mask = np.zeros(vol.shape, np.uint8)
+    rc = ref_mb().vctref_load_measured(str(proj_file).encode(), str(air_file).encode(), in_pr.encode(), width,
+                                       height_raw, nskip, rotations, float(rate_orig), vol, mask)
+    return rc, vol, mask
+
+
 def ref_mb():
     global _REF_MB
     if _REF_MB is None:
@@ -494,6 +536,9 @@ def ref_mb():
                                                _fp, _fp, C.c_int, C.c_int, C.c_int, C.c_void_p, C.c_void_p,
                                                C.c_void_p, C.POINTER(C.c_double)]
         L.vctref_reprojection_bins.restype = C.c_int
+        L.vctref_load_measured.argtypes = [C.c_char_p, C.c_char_p, C.c_char_p, C.c_int, C.c_int, C.c_int, C.c_int,
+                                           C.c_double, _fp, _u8p]
+        L.vctref_load_measured.restype = C.c_int
         _REF_MB = L
     return _REF_MB
 

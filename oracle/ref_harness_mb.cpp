@@ -11,6 +11,7 @@
 //   prepareMaskData          Release_MBFPA_CPU_human/misc_TOMO.cpp:10
 //   lengthproj_TOMO_2        Release_MBFPA_CPU_human/lengthproj_TOMO.cpp:188
 //   IR_ImageTOMO             Release_MBFPA_CPU_human/IR_ImageTOMO.cpp:19
+//   loadProjectionData       Release_MBFPA_CPU_human/projectionDataTOMO.cpp:324
 #include <stdio.h>
 #include <stdlib.h>
 #include <string.h>
@@ -27,6 +28,7 @@
 #include "lengthproj_TOMO.h"
 #include "misc_TOMO.h"
 #include "IR_ImageTOMO.h"
+#include "projectionDataTOMO.h"
 #include "virtual_projection.h"
 
 static double now_s() {
@@ -190,4 +192,35 @@ int vctref_ir_update(int N, const float* before, const float* prior, const float
   return 0;
 }
 
+}  // extern "C"
+
+extern "C" {
+// loadProjectionData on a PROJECTION_DATA holding the fields it reads.  It
+// writes projections.raw into the current directory (the caller picks it).
+// height_raw is projImgHeight before the sino_fact thinning.  Returns what
+// loadProjectionData returns; vol/mask receive projVolume/mask_projVolume
+// ([rotations][height_raw/nskip][width]) when it returned >= 0.
+int vctref_load_measured(const char* proj_file, const char* air_file, const char* in_pr, int width, int height_raw,
+                         int nskip, int rotations, double rate_orig, float* vol, unsigned char* mask) {
+  PROJECTION_DATA* pd = newProjectionData();
+  memset(pd, 0, sizeof *pd);
+  snprintf(pd->projImgFileName, sizeof pd->projImgFileName, "%s", proj_file);
+  snprintf(pd->AirScanImgFileName, sizeof pd->AirScanImgFileName, "%s", air_file);
+  snprintf(pd->InPrClassString, sizeof pd->InPrClassString, "%s", in_pr);
+  pd->projImgWidth = width;
+  pd->projImgHeight = height_raw;
+  pd->sino_fact = nskip;
+  pd->totalProjNumber = rotations;
+  pd->datatype = UNIT_FLOAT32;
+  pd->datasize = 4;
+  pd->DataSamplingRateOrig = rate_orig;
+  const int ret = loadProjectionData(pd);
+  if (ret >= 0) {
+    const size_t n = (size_t)width * pd->projImgHeight * pd->usedProjNumber;
+    memcpy(vol, pd->projVolume, n * sizeof(float));
+    memcpy(mask, pd->mask_projVolume, n);
+  }
+  deleteProjectionData(pd);
+  return ret;
+}
 }  // extern "C"

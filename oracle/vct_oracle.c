@@ -1053,3 +1053,113 @@ void orc_ir_update(int N, const float* before, const float* prior, const float* 
     }
   free(mask);
 }
+
+
+/* ------------------------------------------------- measured-data ingestion */
+/* MB/projectionDataTOMO.cpp:324-508.  Each fread below fills the same
+ * buffer the reference fills, with the same byte count, so a short read
+ * leaves the previous contents in the tail just as it does there. */
+int orc_load_measured(const char* proj_file, const char* air_file, int in_mode, int width, int views, int nskip,
+                      int rotations, int rows_per_view, int ch, int skip, int air_rows, int air_blocks,
+                      int start_ch, int end_ch, float* vol, unsigned char* mask, double* maxv) {
+  *maxv = 0.0;
+  const long long plane = (long long)ch * air_rows;
+  if (in_mode) {
+    if ((long long)(views - 1) * ch + skip + width > plane) return -3;  /* air rows read past a block */
+  } else {
+    if ((long long)(air_rows - 1) * ch + skip + width > plane) return -3;
+    if ((air_rows + nskip - 1) / nskip != views) return -3;  /* kept rows per rotation != views */
+  }
+  FILE* fp = fopen(proj_file, "rb");
+  if (!fp) return -1;
+  FILE* fa = fopen(air_file, "rb");
+  if (!fa) {
+    fclose(fp);
+    return -1;
+  }
+  float* air = (float*)calloc((size_t)plane, sizeof(float));
+  float* sum_air = (float*)calloc((size_t)plane, sizeof(float));
+  float* proj = (float*)calloc((size_t)plane, sizeof(float));
+  size_t got;
+  /* the first air block is read and not used (:385, :401) */
+  got = fread(air, 1, (size_t)plane * sizeof(float), fa);
+  for (int b = 0; b < air_blocks; b++) {
+    got = fread(air, 1, (size_t)plane * sizeof(float), fa);
+    if (!in_mode) {
+      for (long long k = 0; k < plane; k++) sum_air[k] += air[k] / air_blocks;  /* :389-393 */
+    } else {
+      long long k = 0; /* :404-412 */
+      for (int k1 = 0; k1 < views; k1++)
+        for (int k2 = skip; k2 < skip + width; k2++) sum_air[k++] += air[(long long)k1 * ch + k2] / air_blocks;
+    }
+  }
+  (void)got;
+  fclose(fa);
+  int ret = rotations;
+  if (!in_mode) {
+    long long out = 0; /* :435-455 */
+    for (int t = 0; t < rotations; t++) {
+      got = fread(proj, 1, (size_t)plane * sizeof(float), fp);
+      for (int k1 = 0; k1 < air_rows; k1++)
+        for (int k2 = skip; k2 < skip + width; k2++) {
+          const long long kk = (long long)k1 * ch + k2;
+          const float d = proj[kk] / sum_air[kk];
+          if (k1 / nskip * nskip == k1) {
+            vol[out] = d;
+            mask[out] = 1;
+            out++;
+          }
+        }
+    }
+  } else {
+    double pmax = 0.0; /* :458-500 */
+    for (int t = 0; t < rotations && ret >= 0; t++)
+      for (int j = 0; j < views && ret >= 0; j++) {
+        got = fread(proj, 1, (size_t)ch * sizeof(float), fp);
+        int k = 0;
+        for (int i = skip; i < skip + width; i++) {
+          const long long kk = (long long)j * ch + i;
+          float d = proj[kk] / (sum_air[k] * 2);
+          if (pmax < d && i >= start_ch && i < end_ch) {
+            pmax = d;
+            if (pmax > 1.0) {
+              ret = -2;
+              break;
+            }
+          }
+          const long long o = ((long long)t * views + j) * width + k;
+          mask[o] = 1;
+          if (d < 0.1) {
+            d = 0.0f;
+            mask[o] = 0;
+          }
+          vol[o] = d;
+          k++;
+        }
+        for (int r = 1; r < rows_per_view && ret >= 0; r++) got = fread(proj, 1, (size_t)ch * sizeof(float), fp);
+      }
+    *maxv = pmax;
+  }
+  fclose(fp);
+  free(air);
+  free(sum_air);
+  free(proj);
+  return ret;
+}
+
+/* MB/main.cpp:347-371 with start_angle_num = 0 and UsedReconAngle = 2. */
+void orc_helical(const float* vol, int rotations, int views, int width, float* out) {
+  const int use = views / 2 * 2;
+  for (int j = 0; j < use; j++) {
+    const int num_pro = j;
+    int iphase = 0;
+    if (num_pro < use / 2) iphase = 1;
+    else if (num_pro > use / 2) iphase = -1;
+    if (j + iphase * views < views) iphase = 0;
+    if (j + iphase * views > (rotations - 1) * views) iphase = 0;
+    const double zw = 0.5 * fabs(num_pro - (views / 2.0)) / (views / 2.0);
+    for (int c = 0; c < width; c++)
+      out[(long long)num_pro * width + c] =
+          (float)((1.0 - zw) * vol[(long long)j * width + c] + zw * vol[(long long)(j + iphase * views) * width + c]);
+  }
+}

@@ -160,6 +160,26 @@ void orc_fbp_transpose(const orc_geom* g, const double* h, const double* cos_t, 
 void orc_fbp_backproject(const orc_geom* g, const float* fltd, const double* cos_t,
                          const double* sin_t, float* img);
 
+/* Measured-data ingestion, MB/projectionDataTOMO.cpp:324-508.  The raw
+ * layout constants of MB/physParamsTOMO.h: ch = NumberOfChannels (609),
+ * skip = NumberOfSkips (27), air_rows = AirScn_Sinogram_Height (800),
+ * air_blocks = AirScn_Sinogram_Number (5), [start_ch, end_ch) =
+ * [Start_Channel, End_Channel).  views is projImgHeight after the sino_fact
+ * thinning (nskip); rows_per_view 5 when DataSamplingRateOrig >= 200, else 1.
+ * Files are read with fread into buffers that persist between reads, as the
+ * reference reads them.  Returns -1 when either file is missing, -2 when an
+ * IN-mode value in the channel window exceeds 1 (*maxv = that value: the
+ * reference stops there), -3 when the sizes would take the reference outside
+ * its buffers, else the rotations read (*maxv = IN-mode maximum, 0 for PR).
+ * vol and mask are [rotations][views][width]. */
+int orc_load_measured(const char* proj_file, const char* air_file, int in_mode, int width, int views, int nskip,
+                      int rotations, int rows_per_view, int ch, int skip, int air_rows, int air_blocks,
+                      int start_ch, int end_ch, float* vol, unsigned char* mask, double* maxv);
+/* Helical z-interpolation of MB/main.cpp:347-371 (start_angle_num 0,
+ * UsedReconAngle 2): out [views][width] from vol [rotations][views][width];
+ * rows from views/2*2 on are left as they are. */
+void orc_helical(const float* vol, int rotations, int views, int width, float* out);
+
 /* Inscribed-circle mask: MB/misc_TOMO.cpp:10-39, FBP/misc.cpp:9-37. */
 void orc_mask(int N, unsigned char* mask);
 

@@ -31,6 +31,16 @@ Fixtures
                   numpy's default_rng(seed), regenerated by the tests): small
                   helical cases in full, and the 512^2 x 800-view case as
                   every 16th row of npf.
+  measured.npz    loadProjectionData on seeded measured sinograms and air
+                  scans (tests/golden_cases.py MEAS_CASES, regenerated by the
+                  tests): return value and SHA-256 of the volume and mask per
+                  case, a sample of each volume, and the line the reference
+                  prints when an IN-mode value exceeds 1 (MEAS_STOP).
+  measured_e2e.npz  the reference's MBFPA program on measured IN-mode input
+                  (MEAS_E2E): projections.raw (SHA-256 and nonzero indices),
+                  npf_float.raw, the iterative step's two ReconImageRaw
+                  files, every 10th view of reprojection_float.raw and the
+                  printed maximum.
 
     python tests/golden/make_golden.py [fixture ...]   (default: all)
 """
@@ -126,7 +136,8 @@ def c1_subset(tabs):
 
 sys.path.insert(0, os.path.join(ROOT, "tests"))
 from golden_cases import (BH_PARAMS, BH_ROW_STEP, IR_CASES, LP2_CASES, LP_C1, LP_C1_STEP, LP_CASES,  # noqa: E402
-                          bh_sino, ir_inputs, lp2_inputs, lp_proj)
+                          MEAS_CASES, MEAS_E2E_N, MEAS_STOP, bh_sino, ir_inputs, lp2_inputs, lp_proj,
+                          write_e2e_inputs, write_measured)
 
 
 def lengthproj():
@@ -163,11 +174,77 @@ def ir_step():
     np.savez_compressed(os.path.join(OUT, "ir_step.npz"), **out)
 
 
+def _sha(a):
+    import hashlib
+
+    return np.frombuffer(hashlib.sha256(np.ascontiguousarray(a).tobytes()).digest(), np.uint8)
+
+
+def measured():
+    """loadProjectionData of the reference (the harness in a scratch
+    directory) on every MEAS_CASES input: its return value and the SHA-256 of
+    the volume and mask it leaves; and, from a child process (the reference
+    exits there), the line it prints when an IN-mode value exceeds 1."""
+    import subprocess
+
+    out = {}
+    cwd = os.getcwd()
+    for name, case in MEAS_CASES.items():
+        cls, width, views, nskip, rotations, rate = case[:6]
+        with tempfile.TemporaryDirectory() as d:
+            write_measured(d, case)
+            os.chdir(d)
+            try:
+                rc, vol, mask = O.ref_load_measured("proj.raw", "air.raw", cls, width, views * nskip, nskip,
+                                                    rotations, rate)
+            finally:
+                os.chdir(cwd)
+        out[f"{name}_rc"] = np.int32(rc)
+        out[f"{name}_vol_sha"] = _sha(vol)
+        out[f"{name}_mask_sha"] = _sha(mask)
+        out[f"{name}_vol_sample"] = vol[:, ::37, ::41]
+    cls, width, views, nskip, rotations, rate = MEAS_STOP[:6]
+    with tempfile.TemporaryDirectory() as d:
+        write_measured(d, MEAS_STOP)
+        code = ("import sys; sys.path.insert(0, %r); import oracle as O; "
+                "O.ref_load_measured('proj.raw', 'air.raw', %r, %d, %d, %d, %d, %r)"
+                % (ROOT, cls, width, views * nskip, nskip, rotations, rate))
+        r = subprocess.run([sys.executable, "-c", code], cwd=d, capture_output=True, text=True, timeout=300)
+    line = [x for x in r.stderr.splitlines() if "STOP" in x]
+    assert r.returncode == 0 and len(line) == 1, r.stderr[-500:]
+    out["stop_line"] = np.array(line[0].strip())
+    np.savez_compressed(os.path.join(OUT, "measured.npz"), **out)
+
+
+def measured_e2e():
+    """The reference's MBFPA program (oracle/_ref/mb_mvct) on measured input
+    (golden_cases.MEAS_E2E): projections.raw, npf_float.raw, the iterative
+    step's ReconImageRaw outputs and the reprojection."""
+    import subprocess
+
+    exe = os.path.join(ROOT, "oracle", "_ref", "mb_mvct")
+    N = MEAS_E2E_N
+    with tempfile.TemporaryDirectory() as d:
+        write_e2e_inputs(d)
+        r = subprocess.run([exe, "mb.txt"], cwd=d, capture_output=True, text=True, timeout=600)
+        assert r.returncode == 0, r.stderr[-500:]
+        proj = np.fromfile(os.path.join(d, "projections.raw"), np.float32)
+        np.savez_compressed(
+            os.path.join(OUT, "measured_e2e.npz"),
+            projections_sha=_sha(proj), projections_nonzero=np.flatnonzero(proj).astype(np.int32),
+            npf=np.fromfile(os.path.join(d, "npf_float.raw"), np.float32).reshape(N, N),
+            ite1=np.fromfile(os.path.join(d, "ReconImageRaw", "Reconstruction_ite0001_z0000.raw"),
+                             np.float32).reshape(N, N),
+            recon16=np.fromfile(os.path.join(d, "ReconImageRaw", f"Reconstruction_512x512x1.raw"), np.int16),
+            reprojection_rows=np.fromfile(os.path.join(d, "reprojection_float.raw"), np.float32).reshape(-1, 609)[::10],
+            max_line=np.array([x for x in r.stderr.splitlines() if x.startswith("Maximum projection")][0].strip()))
+
+
 def main():
     if not O.ref_available():
         raise SystemExit("reference harness not built: make -C oracle ref")
     want = set(sys.argv[1:]) or {"mu_tables", "mb_small", "fbp_small", "c1_subset", "lengthproj", "beam_hardening",
-                                   "ir_step"}
+                                   "ir_step", "measured", "measured_e2e"}
     tabs = None
     if want & {"mu_tables", "mb_small", "c1_subset"}:
         with tempfile.TemporaryDirectory() as tmp:
@@ -184,6 +261,10 @@ def main():
         beam_hardening()
     if "ir_step" in want:
         ir_step()
+    if "measured" in want:
+        measured()
+    if "measured_e2e" in want:
+        measured_e2e()
     for f in sorted(os.listdir(OUT)):
         print(f, os.path.getsize(os.path.join(OUT, f)))
 

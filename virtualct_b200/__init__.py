@@ -32,6 +32,7 @@ VCT_E_NOMEM = -4
 VCT_E_IO = -5
 VCT_E_STATE = -6
 VCT_E_UNSUPPORTED = -7
+VCT_E_RANGE = -8
 SUM_COMPENSATED = 0
 SUM_REFERENCE = 1
 WALK_FAST = 0
@@ -58,7 +59,8 @@ EXPORTED_SYMBOLS = (
     "vct_last_segment_count",
     "vct_kernel_launches", "vct_version", "vct_philox4x32_10", "vct_probe_peaks",
     "vct_load_mb_config", "vct_load_fbp_config", "vct_mb_geometry", "vct_fbp_geometry", "vct_read_raw",
-    "vct_write_raw",
+    "vct_write_raw", "vct_raw_layout_default", "vct_load_measured", "vct_load_measured_dev",
+    "vct_helical_sinogram", "vct_helical_sinogram_dev",
 )
 
 
@@ -66,6 +68,44 @@ class VctError(RuntimeError):
     def __init__(self, code: int, where: str, msg: str):
         super().__init__(f"{where}: {msg} (code {code})")
         self.code = code
+
+
+class MbConfig(C.Structure):
+    """vct_mb_config: the MBFPA input txt's fields (include/vct_io.h)."""
+    _fields_ = [
+        ("in_pr_class", C.c_char * 16), ("prior_image_onoff", C.c_int), ("proj_width", C.c_int),
+        ("proj_height", C.c_int), ("proj_data_type", C.c_char * 16), ("proj_file_offset", C.c_int),
+        ("proj_file", C.c_char * 256), ("air_scan_file", C.c_char * 256), ("gantry_rotation_period", C.c_double),
+        ("data_sampling_rate", C.c_double), ("data_sampling_rate_orig", C.c_double),
+        ("start_view_angle", C.c_double), ("couch_speed", C.c_double), ("start_couch_position", C.c_double),
+        ("recon_size", C.c_int), ("recon_pix_size", C.c_double), ("recon_tgt_class", C.c_char * 16),
+        ("recon_offset", C.c_double), ("recon_step", C.c_double), ("recon_slices", C.c_int), ("xfactor", C.c_int),
+        ("recon_data_file", C.c_char * 256), ("fbp_slice", C.c_int), ("x_reg", C.c_double), ("y_reg", C.c_double),
+        ("z_reg", C.c_double), ("scan_list_z", C.c_double), ("osemset", C.c_int), ("total_variation", C.c_double),
+        ("prior_const", C.c_double), ("markov_const", C.c_double), ("gradient_decent_const", C.c_double),
+        ("num_ite", C.c_int), ("sino_fact", C.c_int), ("spectrum_file", C.c_char * 256),
+        ("photon_noise", C.c_double), ("total_proj_number", C.c_int),
+    ]
+
+    @classmethod
+    def load(cls, path: str) -> "MbConfig":
+        cfg = cls()
+        _check(lib().vct_load_mb_config(str(path).encode(), C.byref(cfg)), "vct_load_mb_config")
+        return cfg
+
+
+class RawLayout(C.Structure):
+    """vct_raw_layout: the raw detector layout of a measured sinogram."""
+    _fields_ = [("raw_channels", C.c_int), ("skip_channels", C.c_int), ("air_rows", C.c_int),
+                ("air_blocks", C.c_int), ("start_channel", C.c_int), ("end_channel", C.c_int)]
+
+    @classmethod
+    def default(cls, **kw) -> "RawLayout":
+        lay = cls()
+        lib().vct_raw_layout_default(C.byref(lay))
+        for k, v in kw.items():
+            setattr(lay, k, v)
+        return lay
 
 
 class _CGeometry(C.Structure):
@@ -194,6 +234,13 @@ def lib():
     L.vct_philox4x32_10.argtypes = [vp, vp, vp]
     L.vct_philox4x32_10.restype = None
     L.vct_probe_peaks.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.vct_load_mb_config.argtypes = [C.c_char_p, vp]
+    L.vct_raw_layout_default.argtypes = [vp]
+    L.vct_raw_layout_default.restype = None
+    L.vct_load_measured.argtypes = [vp, vp, C.c_int, vp, vp, C.POINTER(C.c_int), C.POINTER(C.c_double)]
+    L.vct_load_measured_dev.argtypes = [vp, vp, vp, vp, C.POINTER(C.c_int), C.POINTER(C.c_double), vp]
+    L.vct_helical_sinogram.argtypes = [vp, C.c_int, C.c_int, C.c_int, vp, C.c_int]
+    L.vct_helical_sinogram_dev.argtypes = [vp, C.c_int, C.c_int, C.c_int, vp, vp]
     _lib = L
     return L
 
@@ -544,6 +591,35 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def load_measured(cfg: MbConfig, layout: RawLayout | None = None, device: int = 0):
+    """vct_load_measured: (volume [rotations][views][width], mask, rotations,
+    max_value).  Raises VctError (code VCT_E_IO for a missing file,
+    VCT_E_RANGE for the IN-mode stop)."""
+    lay = layout or RawLayout.default()
+    shape = (cfg.total_proj_number, cfg.proj_height, cfg.proj_width)
+    vol = np.zeros(shape, np.float32)
+    mask = np.zeros(shape, np.uint8)
+    rot, mx = C.c_int(0), C.c_double(0.0)
+    _check(lib().vct_load_measured(C.byref(cfg), C.byref(lay), device, _ptr(vol), _ptr(mask), C.byref(rot),
+                                   C.byref(mx)), "vct_load_measured")
+    return vol, mask, rot.value, mx.value
+
+
+def helical_sinogram(volume, device: int = 0, out=None) -> np.ndarray:
+    """vct_helical_sinogram: [views][width] from [rotations][views][width]."""
+    v = np.ascontiguousarray(volume, np.float32)
+    R, V, W = v.shape
+    o = np.zeros((V, W), np.float32) if out is None else out
+    _check(lib().vct_helical_sinogram(_ptr(v), R, V, W, _ptr(o), device), "vct_helical_sinogram")
+    return o
+
+
+def helical_sinogram_dev(volume, out, stream_ptr: int | None = None) -> None:
+    R, V, W = volume.shape
+    _check(lib().vct_helical_sinogram_dev(volume.data_ptr(), R, V, W, out.data_ptr(), stream_ptr),
+           "vct_helical_sinogram_dev")
 
 
 def descent_step_scaled_dev(rho, grad, scale, step: float, units: float, maps, stream_ptr: int | None = None) -> None:

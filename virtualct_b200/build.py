@@ -39,6 +39,7 @@ CU_SOURCES = {
     "vct_descent.cu": [],
     "vct_lengthproj.cu": ["--fmad=false"],
     "vct_ir.cu": ["--fmad=false"],
+    "vct_measured.cu": ["--fmad=false"],
 }
 CPP_SOURCES = ["vct_host.cpp", "vct_io.cpp", "vct_batch.cpp"]
 APPS = {"vct_mbfpa": "vct_mbfpa_main.cpp", "vct_fbp": "vct_fbp_main.cpp", "vct_bhc": "vct_bhc_main.cpp"}

@@ -83,6 +83,7 @@ const char* vct_strerror(int code) {
     case VCT_E_IO: return "I/O error";
     case VCT_E_STATE: return "invalid call order";
     case VCT_E_UNSUPPORTED: return "unsupported configuration";
+    case VCT_E_RANGE: return "measured value out of range";
     default: return "unknown error";
   }
 }

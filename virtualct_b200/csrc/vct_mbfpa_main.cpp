@@ -7,8 +7,13 @@
 // reference hard-codes Weight_input_ICRU110.raw and six elements,
 // MB/main.cpp:240,422) and the spectrum txt; writes reprojection_float.raw
 // (float32 [views][width]) and npf_float.raw (lengthproj_TOMO of the measured
-// sinogram, MB/main.cpp:407-419, on the GPU; the virtual path has no
-// measured sinogram, so, as in the reference, it is all zeros).
+// sinogram, MB/main.cpp:407-419, on the GPU).
+// The measured sinogram: when the txt names a sinogram and an air scan that
+// exist, vct_load_measured normalises them (loadProjectionData,
+// MB/projectionDataTOMO.cpp:324-508; the volume is also written to
+// projections.raw, as there) and vct_helical_sinogram interpolates the
+// slice's sinogram (MB/main.cpp:347-371).  The virtual path names none ("*"),
+// so, as in the reference, the measured sinogram and npf are all zeros.
 // The energy loop, spectral sum, normalisation and noise of
 // MB/main.cpp:492-530 are one call to vct_mbfpa() on the GPU.
 #include <stdio.h>
@@ -107,18 +112,49 @@ int main(int argc, char* argv[]) {
     fprintf(stderr, "%s\n", vct_last_error());
     return 1;
   }
+  // loadProjectionData (MB/projectionDataTOMO.cpp:324-508), reached from
+  // loadData before the prior-image message.
+  const size_t proj2 = (size_t)g.views * g.width;
+  std::vector<float> measured(proj2, 0.0f);  // projection_float of MB/main.cpp:248
+  {
+    fprintf(stderr, strcmp(cfg.in_pr_class, "PR") == 0 ? "Pre-treatment CT \n" : "In-treatment CT \n");
+    vct_raw_layout lay;
+    vct_raw_layout_default(&lay);
+    const int R = cfg.total_proj_number;
+    std::vector<float> volume((size_t)(R > 0 ? R : 0) * proj2);
+    std::vector<unsigned char> vmask(volume.size());
+    int got = 0;
+    double pmax = 0.0;
+    const int rc = vct_load_measured(&cfg, &lay, device, volume.data(), vmask.data(), &got, &pmax);
+    if (rc == VCT_E_IO) {
+      fprintf(stderr, "%s\n", vct_last_error());  // the reference goes on with a zero volume
+    } else if (rc == VCT_E_RANGE) {
+      fprintf(stderr, "%s \n", vct_last_error());
+      return 0;  // :474-477
+    } else if (rc != VCT_OK) {
+      fprintf(stderr, "%s\n", vct_last_error());
+      return 1;
+    } else {
+      fprintf(stderr, "Maximum projection: %lf \n", pmax);
+      if (vct_write_raw("projections.raw", volume.data(), volume.size() * sizeof(float)) != VCT_OK)
+        fprintf(stderr, "%s\n", vct_last_error());
+      if (got == 0) return 0;  // loadData returned 0: main exits (MB/main.cpp:225-228)
+      if (vct_helical_sinogram(volume.data(), got, g.views, g.width, measured.data(), device) != VCT_OK) {
+        fprintf(stderr, "%s\n", vct_last_error());
+        return 1;
+      }
+    }
+  }
   vct_ctx* ctx = nullptr;
   int rc = vct_create(&g, device, &ctx);
   if (rc == VCT_OK) rc = vct_set_sum_mode(ctx, sum_mode);
   if (rc == VCT_OK) rc = vct_set_maps(ctx, maps.data(), M);
   if (rc == VCT_OK) rc = vct_set_spectrum(ctx, mu.data(), pdf.data(), M, NE);
   if (rc == VCT_OK) {
-    // lengthproj_TOMO at the first slice's z with the measured sinogram the
-    // reference builds (MB/main.cpp:346-370); the virtual path reads none,
-    // so its rows are zeros.
-    std::vector<float> proj((size_t)(g.views / 2 * 2) * g.width, 0.0f);
+    // lengthproj_TOMO at the first slice's z with the measured sinogram
+    // (MB/main.cpp:346-370, zeros on the virtual path).
     std::vector<float> npf(n2, 0.0f);
-    rc = vct_lengthproj(ctx, proj.data(), cfg.recon_offset, cfg.couch_speed, npf.data());
+    rc = vct_lengthproj(ctx, measured.data(), cfg.recon_offset, cfg.couch_speed, npf.data());
     if (rc == VCT_OK) rc = vct_write_raw("npf_float.raw", npf.data(), n2 * sizeof(float));
   }
   std::vector<float> sino((size_t)g.views * g.width);
@@ -132,26 +168,27 @@ int main(int argc, char* argv[]) {
   printf("projection_min = %lf, used noise = %lf\n", (double)stats[1], cfg.photon_noise);
   rc = vct_write_raw("reprojection_float.raw", sino.data(), sino.size() * sizeof(float));
   // The iterative step (MB/main.cpp:432-600 at ite 1, after the energy loop):
-  // first element's map updated by IR_ImageTOMO, written per slice as
-  // ReconImageRaw/Reconstruction_ite0001_zNNNN.raw, and as int16
+  // first element's map updated by IR_ImageTOMO, written as
+  // ReconImageRaw/Reconstruction_ite0001_z0000.raw, and as int16
   // 1024*(x - 0.0716)/0.0716 of the best image to Reconstruction_512x512x<slices>.raw.
+  // The reference's slice loop runs for slice 0 only, whatever the txt's
+  // slice count (MB/main.cpp:322-323).
   if (rc == VCT_OK) {
     char name[256];
     snprintf(name, sizeof name, "ReconImageRaw/Reconstruction_512x512x%d.raw", cfg.recon_slices);
     FILE* fprecon = fopen(name, "wb");
     const int thinout = cfg.osemset > 0 ? cfg.osemset : 1;
-    std::vector<float> proj((size_t)(g.views / 2 * 2) * g.width, 0.0f);  // no measured sinogram
     std::vector<float> npf(n2, 0.0f), before(n2), after(n2), best(n2, 0.0f);
     std::vector<int16_t> img16(n2);
-    for (int rz = 0; rz < cfg.recon_slices && rc == VCT_OK; rz++) {
+    for (int rz = 0; rz < 1 && rc == VCT_OK; rz++) {
       const double zpos = cfg.recon_offset + rz * cfg.recon_step;
-      rc = vct_lengthproj(ctx, proj.data(), zpos, cfg.couch_speed, npf.data());
+      rc = vct_lengthproj(ctx, measured.data(), zpos, cfg.couch_speed, npf.data());
       for (size_t i = 0; i < n2; i++) before[i] = (float)maps[i] / 1000;  // initial_image_def
       std::fill(after.begin(), after.end(), 0.0f);
       double wbefore = cfg.gradient_decent_const + 0.0005, objective = 10000000.0, quadratic = 0.0;
       double min_squdiff = 10000000.0;
       if (rc == VCT_OK)
-        rc = vct_ir_step(ctx, proj.data(), npf.data(), before.data(), nullptr, zpos, cfg.couch_speed, 1, thinout,
+        rc = vct_ir_step(ctx, measured.data(), npf.data(), before.data(), nullptr, zpos, cfg.couch_speed, 1, thinout,
                          cfg.num_ite, cfg.total_variation, cfg.prior_const, &wbefore, &objective, &quadratic,
                          after.data());
       if (rc != VCT_OK) break;

@@ -152,23 +152,23 @@ def write_spectrum_txt(path, rows: np.ndarray) -> None:
 
 # --------------------------------------------------------------- input txts
 _MB_FIELDS = [
-    ("Energy Label (IN (for treatment beam) or PR (for CT))", "PR"),
+    ("Energy Label (IN (for treatment beam) or PR (for CT))", "{cls}"),
     ("Prior image ON/OFF (0: no prior, 1: planCT, 2: MVCT)", "0"),
     ("sinogram width ", "{width}"),
     ("sinogram height ", "{height}"),
     ("Data type", "float"),
     ("projection image file header bytes ", "0"),
-    ("sinogram image data for input ", "*"),
-    ("Air scan image data for input // parameters are fixed", "*"),
+    ("sinogram image data for input ", "{sino}"),
+    ("Air scan image data for input // parameters are fixed", "{air}"),
     ("Gantry rotation period [s]", "{period}"),
     ("Data sampling rate [Hz]", "{rate}"),
     ("Starting view angle [degree]", "{start_angle}"),
-    ("Couch speed [cm/rotation]", "0.0"),
-    ("Start couch position [cm]", "0.0"),
+    ("Couch speed [cm/rotation]", "{couch_speed}"),
+    ("Start couch position [cm]", "{couch_start}"),
     ("reconstruction size (square format) ", "{N}"),
     ("reconstruction pixel size [cm]", "{pixel}"),
     ("reconstruction target class string ", "*"),
-    ("reconstruction start z [cm]", "0.0"),
+    ("reconstruction start z [cm]", "{z0}"),
     ("reconstruction z step [cm]", "0.1"),
     ("reconstruction slices ", "1"),
     ("Factor for output CT value ", "{xfactor}"),
@@ -180,7 +180,7 @@ _MB_FIELDS = [
     ("Constants for regularization terms' weight // TV, Prior, Other (NOT used)", "0.0001 0.0 0.0"),
     ("Gradient Decent constant (NOT used)", "0.01"),
     ("Number of iteration (NOT used)", "500"),
-    ("Sinogram factor (NOT used)", "1"),
+    ("Sinogram factor (NOT used)", "{sino_fact}"),
     ("Spectrum data name", "{spectrum}"),
     ("Photon noise in detector", "{noise}"),
 ]
@@ -222,10 +222,19 @@ def _write_txt(path, fields, values) -> None:
 
 
 def write_mb_txt(path, *, spectrum: str, width: int = 609, views: int = 800, N: int = 512, pixel_cm: float = 0.1,
-                 noise: float = 0.0, xfactor: int = 1, start_angle: float = 0.0, period: float = 10.0) -> None:
-    rate = views / period
-    _write_txt(path, _MB_FIELDS, dict(width=width, height=views, period=f"{period:g}", rate=f"{rate:g}",
-                                      start_angle=f"{start_angle:g}", N=N, pixel=f"{pixel_cm:g}", xfactor=xfactor,
+                 noise: float = 0.0, xfactor: int = 1, start_angle: float = 0.0, period: float = 10.0,
+                 cls: str = "PR", sino: str = "*", air: str = "*", rotations: int = 1, rate: float | None = None,
+                 sino_fact: int = 1, couch_speed: float = 0.0, couch_start: float = 0.0, z0: float = 0.0) -> None:
+    """The 31-field MBFPA txt.  The sampling rate defaults to views / period;
+    the txt's sinogram height is period * rate raw rows per rotation (5 per
+    view at 200 Hz and above), times `rotations`, from which the reader
+    derives the rotation count."""
+    rate = views / period if rate is None else rate
+    height = int(round(period * rate)) * rotations
+    _write_txt(path, _MB_FIELDS, dict(cls=cls, width=width, height=height, sino=sino, air=air,
+                                      period=f"{period:g}", rate=f"{rate:g}", start_angle=f"{start_angle:g}",
+                                      couch_speed=f"{couch_speed:g}", couch_start=f"{couch_start:g}", z0=f"{z0:g}",
+                                      N=N, pixel=f"{pixel_cm:g}", xfactor=xfactor, sino_fact=sino_fact,
                                       spectrum=spectrum, noise=f"{noise:.10g}"))
 
 

@@ -151,6 +151,19 @@ int vct_line_integrals_dev(vct_ctx* ctx, double* d_lint_out);
 int vct_mbfpa(vct_ctx* ctx, double sigma, uint64_t seed, float* sino_out, float* stats);
 int vct_mbfpa_dev(vct_ctx* ctx, double sigma, uint64_t seed, float* d_sino_out);
 
+/* vct_set_maps + vct_mbfpa for n slices of this context's geometry and
+ * spectrum, pipelined (no counterpart in the reference, which projects one
+ * slice per process): slice i's maps ([M][N][N] int16 at maps[i]) go
+ * host->device on one copy stream while slice i-1 is projected and slice
+ * i-2's sinogram ([views][width] float to out[i]) comes back on another, so
+ * with pinned host buffers the copies hide behind the projections (pageable
+ * buffers give the same results, with the copies serialised).  Slice i's
+ * noise uses seed + i.  stats (optional): [n][3] as vct_mbfpa's.  Returns
+ * when every sinogram is in host memory; the context keeps the last slice's
+ * maps. */
+int vct_mbfpa_many(vct_ctx* ctx, int n, const int16_t* const* maps, int M, double sigma, uint64_t seed,
+                   float* const* out, float* stats);
+
 /* lengthproj_TOMO (MB/lengthproj_TOMO.cpp:14-185; the reference's main calls
  * it at MB/main.cpp:407 and writes npf_float.raw): for every pixel of the
  * reconstruction circle, npf = sum over the views/2*2 views used of

@@ -48,7 +48,7 @@ EXPORTED_SYMBOLS = (
     "vct_geometry_default", "vct_strerror", "vct_last_error", "vct_create", "vct_destroy", "vct_set_stream",
     "vct_synchronize", "vct_attenuation_coefficient", "vct_set_maps", "vct_set_maps_dev", "vct_set_spectrum",
     "vct_set_sum_mode", "vct_set_walk_mode", "vct_forward", "vct_forward_dev", "vct_line_integrals_dev", "vct_mbfpa", "vct_mbfpa_dev",
-    "vct_normalize_noise_dev", "vct_fbp", "vct_fbp_dev", "vct_fbp_noalloc", "vct_fbp_filtered_dev",
+    "vct_normalize_noise_dev", "vct_mbfpa_many", "vct_fbp", "vct_fbp_dev", "vct_fbp_noalloc", "vct_fbp_filtered_dev",
     "vct_fbp_transpose", "vct_fbp_transpose_dev",
     "vct_set_density_scale", "vct_descent_step_dev", "vct_descent_step_scaled_dev", "vct_lengthproj", "vct_lengthproj_dev",
     "vct_beam_hardening", "vct_beam_hardening_dev", "vct_set_beam_hardening",
@@ -234,6 +234,7 @@ def lib():
     L.vct_philox4x32_10.argtypes = [vp, vp, vp]
     L.vct_philox4x32_10.restype = None
     L.vct_probe_peaks.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    L.vct_mbfpa_many.argtypes = [vp, C.c_int, vp, C.c_int, C.c_double, C.c_uint64, vp, vp]
     L.vct_load_mb_config.argtypes = [C.c_char_p, vp]
     L.vct_raw_layout_default.argtypes = [vp]
     L.vct_raw_layout_default.restype = None
@@ -388,6 +389,28 @@ class Context:
         st = np.zeros(3, np.float32)
         _check(lib().vct_mbfpa(self._h, float(sigma), int(seed), _ptr(out), _ptr(st)), "vct_mbfpa")
         return (out, st) if return_stats else out
+
+    def mbfpa_many(self, maps, sigma: float = 0.0, seed: int = 1, out=None, return_stats: bool = False):
+        """vct_mbfpa_many: a list of host int16 [M][N][N] arrays (pinned ones,
+        e.g. torch pin_memory().numpy(), overlap the copies); returns the
+        [n][views][width] sinograms (or writes the given list of arrays)."""
+        g = self.geometry
+        arrs = [np.ascontiguousarray(m, np.int16) for m in maps]
+        n = len(arrs)
+        if out is None:
+            out = [np.empty((g.views, g.width), np.float32) for _ in range(n)]
+        if len(out) != n or any(o.dtype != np.float32 or o.size != g.views * g.width or not o.flags.c_contiguous
+                                for o in out):
+            raise ValueError("out must hold n contiguous float32 [views][width] arrays")
+        M = arrs[0].shape[0] if n else self._M or 1
+        pin = (C.c_void_p * max(n, 1))(*[a.ctypes.data for a in arrs])
+        pout = (C.c_void_p * max(n, 1))(*[o.ctypes.data for o in out])
+        st = np.zeros((max(n, 1), 3), np.float32)
+        _check(lib().vct_mbfpa_many(self._h, n, pin, M, float(sigma), int(seed), pout,
+                                    _ptr(st) if return_stats else None), "vct_mbfpa_many")
+        if n:
+            self._M = M
+        return (out, st[:n]) if return_stats else out
 
     def mbfpa_dev(self, sigma: float, seed: int, out) -> None:
         _check(lib().vct_mbfpa_dev(self._h, float(sigma), int(seed), out.data_ptr()), "vct_mbfpa_dev")

@@ -26,6 +26,25 @@ struct DBuf {
     n = 0;
   }
 };
+// Copy streams, events and double buffers of vct_mbfpa_many, made on its
+// first call.
+struct Pipe {
+  cudaStream_t in = nullptr, out = nullptr;
+  cudaEvent_t start = nullptr, ev_in[2] = {}, ev_packed[2] = {}, ev_done[2] = {}, ev_out[2] = {};
+  DBuf<int16_t> stage[2];
+  DBuf<float> sino[2];
+  ~Pipe() {
+    for (int s = 0; s < 2; s++) {
+      stage[s].release();
+      sino[s].release();
+      for (cudaEvent_t e : {ev_in[s], ev_packed[s], ev_done[s], ev_out[s]})
+        if (e) cudaEventDestroy(e);
+    }
+    if (start) cudaEventDestroy(start);
+    if (in) cudaStreamDestroy(in);
+    if (out) cudaStreamDestroy(out);
+  }
+};
 }  // namespace vct
 
 struct vct_ctx {
@@ -74,6 +93,7 @@ struct vct_ctx {
   vct::DBuf<unsigned long long> adj_sacc;
   vct::DBuf<float> adj_meas, adj_wts, adj_grad;
   vct::DBuf<float> adj_ext;  // [M][N+1][N+1] gather output before the fold
+  vct::Pipe* pipe = nullptr;  // vct_mbfpa_many
 };
 
 

@@ -204,6 +204,10 @@ void vct_destroy(vct_ctx* c) {
   c->sq_part.release();
   c->ir_proj.release(); c->ir_reproj.release(); c->ir_img.release(); c->ir_out.release();
   if (c->h_stats) cudaFreeHost(c->h_stats);
+  if (c->pipe) {
+    cudaStreamSynchronize(c->pipe->out);
+    delete c->pipe;
+  }
   if (c->own_stream) cudaStreamDestroy(c->own_stream);
   delete c;
 }
@@ -482,6 +486,94 @@ int vct_mbfpa(vct_ctx* c, double sigma, uint64_t seed, float* out, float* stats3
     stats3[0] = mx;
     stats3[1] = mn / mx;
     stats3[2] = (float)c->h_stats->segments;
+  }
+  return VCT_OK;
+}
+
+// Many slices from host buffers: slice i's maps go host->device on pipe->in
+// while slice i-1 projects on the context's stream and slice i-2's sinogram
+// goes device->host on pipe->out.  Two staging and two sinogram buffers; the
+// events order each buffer's reuse.
+static int ensure_pipe(vct_ctx* c) {
+  if (c->pipe) return VCT_OK;
+  vct::Pipe* p = new vct::Pipe();
+  c->pipe = p;
+  VCT_CUDA(cudaStreamCreateWithFlags(&p->in, cudaStreamNonBlocking));
+  VCT_CUDA(cudaStreamCreateWithFlags(&p->out, cudaStreamNonBlocking));
+  VCT_CUDA(cudaEventCreateWithFlags(&p->start, cudaEventDisableTiming));
+  for (int s = 0; s < 2; s++)
+    for (cudaEvent_t* e : {&p->ev_in[s], &p->ev_packed[s], &p->ev_done[s], &p->ev_out[s]})
+      VCT_CUDA(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+  return VCT_OK;
+}
+
+int vct_mbfpa_many(vct_ctx* c, int n, const int16_t* const* maps, int M, double sigma, uint64_t seed,
+                   float* const* out, float* stats3) {
+  NvtxScope nvtx_scope("vct_mbfpa_many");
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (n < 0 || (n > 0 && (!maps || !out)) || M < 1 || M > VCT_MAX_MATERIALS)
+    return fail(VCT_E_ARG, "vct_mbfpa_many: bad argument");
+  if (n == 0) return VCT_OK;
+  if (!c->spectrum_ready) return fail(VCT_E_STATE, "vct_mbfpa_many: spectrum not set");
+  if (M != c->M) return fail(VCT_E_ARG, "vct_mbfpa_many: M differs from the spectrum's");
+  for (int i = 0; i < n; i++)
+    if (!maps[i] || !out[i]) return fail(VCT_E_ARG, "vct_mbfpa_many: null slice buffer");
+  const size_t n2 = (size_t)c->dg.N * c->dg.N, nsino = (size_t)c->geo.views * c->geo.width;
+  if ((rc = ensure_pipe(c))) return rc;
+  vct::Pipe* p = c->pipe;
+  for (int s = 0; s < 2; s++)
+    if ((rc = p->stage[s].ensure(n2 * M)) || (rc = p->sino[s].ensure(nsino))) return rc;
+  if ((rc = c->maps.ensure(map_records(c->dg.N))) || (rc = c->full.ensure(nsino))) return rc;
+  vct::FwdStats* h = nullptr;  // per-slice statistics, pinned
+  if (stats3) VCT_CUDA(cudaMallocHost((void**)&h, (size_t)n * sizeof(vct::FwdStats)));
+  struct FreeHost {
+    void* p;
+    ~FreeHost() {
+      if (p) cudaFreeHost(p);
+    }
+  } free_h{h};
+  // everything below comes after the work already queued on the context's stream
+  VCT_CUDA(cudaEventRecord(p->start, c->stream));
+  VCT_CUDA(cudaStreamWaitEvent(p->in, p->start, 0));
+  VCT_CUDA(cudaStreamWaitEvent(p->out, p->start, 0));
+  const int pad = pad_zero_of(c);
+  for (int i = 0; i < n; i++) {
+    const int s = i & 1;
+    if (i >= 2) VCT_CUDA(cudaStreamWaitEvent(p->in, p->ev_packed[s], 0));  // slice i-2 left stage[s]
+    VCT_CUDA(cudaMemcpyAsync(p->stage[s].p, maps[i], n2 * M * sizeof(int16_t), cudaMemcpyHostToDevice, p->in));
+    VCT_CUDA(cudaEventRecord(p->ev_in[s], p->in));
+    VCT_CUDA(cudaStreamWaitEvent(c->stream, p->ev_in[s], 0));
+    if ((rc = launch_pack_maps(p->stage[s].p, M, c->dg.N, c->maps.p, c->stream))) return rc;
+    c->launches++;
+    VCT_CUDA(cudaEventRecord(p->ev_packed[s], c->stream));
+    c->maps_ready = 1;
+    if ((rc = forward_into(c, c->full.p, nullptr))) return rc;
+    if (i >= 2) VCT_CUDA(cudaStreamWaitEvent(c->stream, p->ev_out[s], 0));  // slice i-2 left sino[s]
+    if ((rc = launch_normalize_noise(c->dg, c->full.p, p->sino[s].p, c->stats.p, pad, sigma, seed + (uint64_t)i,
+                                     c->stream)))
+      return rc;
+    c->launches++;
+    if (h) VCT_CUDA(cudaMemcpyAsync(h + i, c->stats.p, sizeof(vct::FwdStats), cudaMemcpyDeviceToHost, c->stream));
+    VCT_CUDA(cudaEventRecord(p->ev_done[s], c->stream));
+    VCT_CUDA(cudaStreamWaitEvent(p->out, p->ev_done[s], 0));
+    VCT_CUDA(cudaMemcpyAsync(out[i], p->sino[s].p, nsino * sizeof(float), cudaMemcpyDeviceToHost, p->out));
+    VCT_CUDA(cudaEventRecord(p->ev_out[s], p->out));
+  }
+  VCT_CUDA(cudaStreamWaitEvent(c->stream, p->ev_out[(n - 1) & 1], 0));
+  VCT_CUDA(cudaStreamSynchronize(c->stream));
+  VCT_CUDA(cudaStreamSynchronize(p->out));
+  if (h) {
+    for (int i = 0; i < n; i++) {
+      float mx = 0, mn = 0;
+      memcpy(&mx, &h[i].max_bits, 4);
+      memcpy(&mn, &h[i].min_bits, 4);
+      if (pad) mn = fminf(mn, 0.0f);
+      stats3[3 * i] = mx;
+      stats3[3 * i + 1] = mn / mx;
+      stats3[3 * i + 2] = (float)h[i].segments;
+    }
+    c->last_segments = (long long)h[n - 1].segments;
   }
   return VCT_OK;
 }

@@ -185,7 +185,7 @@ def run_ours(args, rank, world, dist):
     t_fwd = max_over_ranks(timed(lambda: ctx.forward_dev(d_sino), args.steps)) / args.steps
     extras = {}
     if rank == 0:
-        extras["parity"] = parity_vs_reference(ctx, d_sino)
+        extras["parity"] = parity_vs_reference(ctx, d_sino, d_img)
     want = set() if args.no_extras or world > 1 else set(args.extras.split(","))
     if "adjoint" in want:
         extras["adjoint"] = bench_adjoint(ctx, d_maps, mu, pdf, stream, timed, args.steps, args.warmup)
@@ -302,10 +302,13 @@ def run_ours(args, rank, world, dist):
 
 
 # ------------------------------------------------------------------ parity
-def parity_vs_reference(ctx, d_sino):
-    """The device forward of the rank-0 slice (phantom seed 0, the bench
-    spectrum) against the reference's un-normalised spectral sum on every
-    20th view (tests/golden/c1_subset.npz)."""
+def parity_vs_reference(ctx, d_sino, d_img):
+    """Errors of this rank-0 slice (phantom seed 0, the bench spectrum) against
+    tests/golden/c1_subset.npz: the un-normalised forward on every 20th view
+    against the reference's spectral sum (reprojection_TOMO over 110 bins in
+    its order) and against the FP64 sum; and the Ram-Lak FBP of the
+    max-normalised, noise-free sinogram against the reference's FBP on every
+    16th image row."""
     import torch
 
     path = os.path.join(ROOT, "tests", "golden", "c1_subset.npz")
@@ -314,15 +317,30 @@ def parity_vs_reference(ctx, d_sino):
     d = np.load(path)
     if int(d["seed"]) != 0:
         return {"unavailable": "c1_subset fixture is not the seed-0 slice"}
+    rows = d["rows"]
     ctx.forward_dev(d_sino)
     torch.cuda.synchronize()
-    out = d_sino.cpu().numpy()[d["rows"]].astype(np.float64)
-    ref = d["full_rows"].astype(np.float64)
+    out = d_sino.cpu().numpy()[rows].astype(np.float64)
+    ref, f64 = d["full_rows"].astype(np.float64), d["fp64_rows"]
     ok = ref > 0
-    return {"vs_reference_max_rel": float(np.max(np.abs(out[ok] - ref[ok]) / ref[ok])),
-            "tolerance": 1e-5, "rows": int(len(d["rows"])), "channels": int(ref.shape[1]),
-            "what": "un-normalised polyenergetic sinogram on every 20th view vs reprojection_TOMO summed over "
-                    "110 bins in reference order (pinned oracle, cross-checked against the compiled reference)"}
+    ctx.mbfpa_dev(0.0, 1, d_sino)  # sigma 0: max-normalisation only
+    ctx.fbp_dev(d_sino, d_img, 1)
+    torch.cuda.synchronize()
+    step = N // d["fbp_ramlak_rows"].shape[0]
+    img = d_img.cpu().numpy()[::step].astype(np.float64)
+    fref = d["fbp_ramlak_rows"].astype(np.float64)
+    return {
+        "forward_vs_reference_max_rel": float(np.max(np.abs(out[ok] - ref[ok]) / ref[ok])),
+        "forward_vs_fp64_max_rel": float(np.max(np.abs(out - f64) / f64)),
+        "reference_vs_fp64_max_rel": float(np.max(np.abs(ref - f64) / f64)),
+        "forward_tolerance": 1e-5,
+        "fbp_vs_reference_max_abs_over_max": float(np.abs(img - fref).max() / np.abs(fref).max()),
+        "fbp_vs_reference_l2_rel": float(np.linalg.norm(img - fref) / np.linalg.norm(fref)),
+        "fbp_tolerance": 1e-4,
+        "what": "forward: un-normalised polyenergetic sinogram, every 20th view (40 x 609); fbp: Ram-Lak image of "
+                "the noise-free normalised sinogram, every 16th row (32 x 512); references from the reference "
+                "compiled from its sources and the FP64 oracle",
+    }
 
 
 # ------------------------------------------------ adjoint and batched lines

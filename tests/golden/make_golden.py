@@ -19,8 +19,10 @@ Fixtures
                   64^2, Ram-Lak and Shepp-Logan.
   c1_subset.npz   full-size C1 (512^2, 800 x 609, 6 elements, 110-bin Kramers
                   spectrum, seeded ellipse phantom seed 0): every 20th view of
-                  the reference's un-normalised spectral sum, its global max
-                  and min, and the total segment count.
+                  the reference's un-normalised spectral sum and the FP64
+                  oracle's, its global max and min, the total segment count,
+                  and every 16th row of the reference's Ram-Lak FBP of the
+                  max-normalised, noise-free sinogram.
   beam_hardening.npz  the beam-hardening correction program's output
                   (reprojection_float_cor.raw, every 32nd row) and printed
                   minima on a seeded 800 x 609 sinogram, kV and MV parameters.
@@ -63,6 +65,7 @@ MB = os.path.join(REF, "Release_MBFPA_CPU_human")
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 C1_SEED = 0
+C1_FBP_ROW_STEP = 16
 C1_SUBSET_STEP = 20
 
 
@@ -128,7 +131,12 @@ def c1_subset(tabs):
     ora2 = O.forward_exact(g, c, s, rho, np.ascontiguousarray(mu[:, 50:52]), pdf[50:52].copy())
     assert np.array_equal(ora2, ref2), "oracle and reference disagree on bins 50-51"
     rows = np.arange(0, 800, C1_SUBSET_STEP)
+    f64 = O.forward_fp64(g, c, s, rho, mu, pdf)
+    # the reference's FBP (Ram-Lak) of the max-normalised, noise-free sinogram
+    # (MB/main.cpp:511-522 in float, then FBP/main.cpp:137-167)
+    img, _, _, _ = O.ref_fbp(1, (full / full.max()).astype(np.float32), 512, 0.1, 1, c, s)
     np.savez_compressed(os.path.join(OUT, "c1_subset.npz"), rows=rows, full_rows=full[rows],
+                        fp64_rows=f64[rows], fbp_ramlak_rows=img[::C1_FBP_ROW_STEP],
                         max=np.float32(full.max()), min=np.float32(full.min()),
                         segments=np.int64(nseg.sum()), seed=C1_SEED,
                         maps_sha=np.frombuffer(__import__("hashlib").sha256(maps.tobytes()).digest(), np.uint8))

@@ -7,7 +7,7 @@ import pytest
 
 import oracle as O
 import virtualct_b200 as vct
-from conftest import GOLDEN, SINO_RTOL, golden, max_rel
+from conftest import GOLDEN, SINO_RTOL, fbp_errors, golden, max_rel
 from virtualct_b200 import phantoms
 
 pytestmark = pytest.mark.gpu
@@ -90,6 +90,25 @@ def test_c1_full_size_matches_reference(cuda_device, walk):
     assert abs(float(out.max()) / float(d["max"]) - 1) < SINO_RTOL
     ref_norm = d["full_rows"] / d["max"]
     assert max_rel(norm[rows], ref_norm) < 2 * SINO_RTOL
+
+
+def test_c1_fbp_and_fp64_rows(cuda_device):
+    """C1 end to end: the device forward within 1e-5 of the FP64 sum, and the
+    Ram-Lak FBP of its max-normalised, noise-free sinogram within 1e-4 of the
+    reference's FBP of the reference's sinogram (every 16th row)."""
+    d = golden("c1_subset.npz")
+    t = golden("mu_tables.npz")
+    maps = phantoms.ellipse_phantom(int(d["seed"]), 512)
+    with vct.Context(vct.Geometry()) as ctx:
+        ctx.set_maps(maps)
+        ctx.set_spectrum(t["kramers120_mu"], t["kramers120_pdf"])
+        out = ctx.forward()
+        norm = ctx.mbfpa(0.0, 1)
+        img = ctx.fbp(norm, filter=1)
+    assert max_rel(out[d["rows"]], d["fp64_rows"]) < SINO_RTOL
+    step = 512 // d["fbp_ramlak_rows"].shape[0]
+    mx, l2 = fbp_errors(img[::step], d["fbp_ramlak_rows"])
+    assert mx < 1e-4 and l2 < 1e-4, (mx, l2)
 
 
 def test_eight_elements_and_6mv(cuda_device):

@@ -333,11 +333,14 @@ int launch_adj_gmax(int M, const int* d_special, const int* d_nspecial, int nspe
 }
 
 // ------------------------------------------------------ pixel-driven gather
-// Views staged per round and the largest channel window one tile needs per
-// view (the host picks the tile so the window fits; see adj_pick_tile).
-constexpr int kAdjVB = 4;
+// Largest channel window one tile needs per view (the host picks the tile so
+// the window fits; see adj_pick_tile), rays staged per round, and the views a
+// round considers: it takes as many as fit in the staging space (at least
+// kAdjCap / kAdjWMax), so each barrier serves more views when windows are
+// narrow.
 constexpr int kAdjWMax = 128;
-constexpr int kAdjCap = kAdjVB * kAdjWMax;
+constexpr int kAdjCap = 4 * kAdjWMax;
+constexpr int kAdjVB = 8;
 
 // Angle of the direction (u, v) from the source, measured like the channel
 // angle theta = (iso - jj) * dalpha: (sin theta, -cos theta) is channel jj's
@@ -369,7 +372,7 @@ adj_gather_kernel(AdjGeom a, const double* __restrict__ cos_t, const double* __r
   __shared__ float4 s_B[kAdjCap];
   __shared__ int2 s_K[kAdjCap];
   __shared__ float4 s_g4[(MG / 4) * kAdjCap];  // ray factors, quad q of ray k at q * kAdjCap + k
-  __shared__ int s_jlo[kAdjVB], s_jn[kAdjVB], s_base[kAdjVB + 1], s_cplx[kAdjVB];
+  __shared__ int s_jlo[kAdjVB], s_jn[kAdjVB], s_base[kAdjVB + 1], s_cplx[kAdjVB], s_nvb;
   __shared__ float s_cb[kAdjVB], s_sb[kAdjVB], s_dtx[kAdjVB], s_dty[kAdjVB];
 
   const int N = a.N, NE1 = N + 1;
@@ -394,11 +397,11 @@ adj_gather_kernel(AdjGeom a, const double* __restrict__ cos_t, const double* __r
   for (int m = 0; m < M; m++) dacc[m] = 0.0;
 
   const int V = a.views_used;
-  for (int v0 = 0; v0 < V; v0 += kAdjVB) {
-    const int nvb = min(kAdjVB, V - v0);
+  for (int v0 = 0; v0 < V;) {
+    const int nvc = min(kAdjVB, V - v0);  // views considered this round
     // Channel window of the tile for each view: the angles of the tile's
     // corners grown by one cell, plus two channels.
-    if (threadIdx.x < nvb) {
+    if (threadIdx.x < nvc) {
       const int v = v0 + threadIdx.x;
       const double cb = cos_t[v], sb = sin_t[v];
       const double Sx = a.sid * sb, Sy = a.sid * cb;
@@ -432,15 +435,17 @@ adj_gather_kernel(AdjGeom a, const double* __restrict__ cos_t, const double* __r
       s_dty[threadIdx.x] = (float)(Ty - Sy);
     }
     __syncthreads();
-    if (threadIdx.x == 0) {
-      int b = 0;
-      for (int k = 0; k < nvb; k++) {
+    if (threadIdx.x == 0) {  // the views whose windows fit the staging space
+      int b = 0, k = 0;
+      for (; k < nvc && b + s_jn[k] <= kAdjCap; k++) {
         s_base[k] = b;
         b += s_jn[k];
       }
-      s_base[nvb] = b;
+      s_base[k] = b;
+      s_nvb = k;
     }
     __syncthreads();
+    const int nvb = s_nvb;
     // Stage the window's rays: direction and offset from the tile centre in
     // FP64, then float (small for every ray that can reach the tile).
     const int total = s_base[nvb];
@@ -546,6 +551,7 @@ adj_gather_kernel(AdjGeom a, const double* __restrict__ cos_t, const double* __r
 #pragma unroll
     for (int m = 0; m < M; m++) dacc[m] += (double)acc[m];
     __syncthreads();
+    v0 += nvb;
   }
   if (!live) return;
   const size_t n2 = (size_t)NE1 * NE1;

@@ -19,12 +19,14 @@ constexpr int kPad = kMapPad;
 VCT_HD int pad_index(int col, int row, int N) { return (col + kPad) + (row + kPad) * (N + 2 * kPad); }
 
 // Resident blocks per SM the register allocation is held to, and the number
-// of walk segments whose gathers are issued together (chosen by measurement).
+// of walk segments whose gathers are issued together (chosen by measurement:
+// at C1, 2 / 4 / 5 / 6 / 8 / 12 segments gave 0.85 / 0.77 / 0.75 / 0.73 / 0.76 /
+// 0.75 ms, with no spills).
 #ifndef VCT_FWD_MINBLOCKS
 #define VCT_FWD_MINBLOCKS 0
 #endif
 #ifndef VCT_FWD_UNROLL
-#define VCT_FWD_UNROLL 4
+#define VCT_FWD_UNROLL 6
 #endif
 // 1: a transposed copy of the padded map follows the row-major one; walks
 // with x as the major axis read it.

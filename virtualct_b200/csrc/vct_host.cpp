@@ -196,7 +196,7 @@ void vct_destroy(vct_ctx* c) {
   c->full.release(); c->out.release(); c->stats.release();
   c->fbp_coeff.release();
   for (auto& h : c->fbp_h) h.release();
-  c->fbp_g.release(); c->fbp_q.release(); c->fbp_sino.release(); c->fbp_img.release();
+  c->fbp_g.release(); c->fbp_q.release(); c->fbp_sino.release(); c->fbp_img.release(); c->fbp_tacc.release();
   c->adj_rec.release(); c->adj_special.release(); c->adj_ints.release(); c->adj_dir.release();
   c->adj_g.release(); c->adj_part.release(); c->adj_loss.release(); c->adj_gmax.release();
   c->adj_sacc.release(); c->adj_meas.release(); c->adj_wts.release(); c->adj_grad.release();
@@ -881,9 +881,11 @@ int vct_fbp_transpose_dev(vct_ctx* c, const float* d_u, int filter, float* d_lam
   if (filter != 1 && filter != 2) return fail(VCT_E_ARG, "filter must be 1 (Ram-Lak) or 2 (Shepp-Logan)");
   const int V = c->geo.views, C = c->dg.C;
   if ((rc = build_filter(c, filter))) return rc;
-  if ((rc = c->fbp_g.ensure((size_t)V * C)) || (rc = c->fbp_q.ensure((size_t)V * C))) return rc;
+  if ((rc = c->fbp_g.ensure((size_t)V * C)) || (rc = c->fbp_q.ensure((size_t)V * C)) ||
+      (rc = c->fbp_tacc.ensure(fbp_backproject_t_scratch(V, C, c->dg.N))))
+    return rc;
   if ((rc = launch_fbp_backproject_t(d_u, V, C, c->dg.N, c->geo.pixel_cm, c->geo.sid_cm, c->geo.max_beta,
-                                     c->geo.xfactor, c->cs_f.p, c->fbp_q.p, c->stream)))
+                                     c->geo.xfactor, c->cs_f.p, c->fbp_tacc.p, c->fbp_q.p, c->stream)))
     return rc;
   if ((rc = launch_fbp_filter_t(c->fbp_q.p, c->fbp_h[filter].p, c->fbp_h[filter].p + 2 * C - 1, V, C, c->fbp_g.p,
                                 c->stream)))

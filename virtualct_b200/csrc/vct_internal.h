@@ -100,8 +100,10 @@ int launch_fbp_backproject(const float* d_q, int V, int C, int N, double pixel_c
                            double max_beta, int xfactor, const float* d_cs, float* d_img,
                            cudaStream_t st, int view_groups = 4);
 // Transposes of the three FBP steps (vct_fbp.cu).
+size_t fbp_backproject_t_scratch(int V, int C, int N);  // 64-bit words of d_acc
 int launch_fbp_backproject_t(const float* d_u, int V, int C, int N, double pixel_cm, double sid, double max_beta,
-                             int xfactor, const float* d_cs, float* d_qb, cudaStream_t st);
+                             int xfactor, const float* d_cs, unsigned long long* d_acc, float* d_qb,
+                             cudaStream_t st);
 int launch_fbp_filter_t(const float* d_q, const float* d_h0, const float* d_cm, int V, int C, float* d_g,
                         cudaStream_t st);
 int launch_fbp_weight_t(const float* d_g, int V, int W, int start, int C, const double* d_coeff, float* d_lam,

@@ -319,6 +319,16 @@ int vct_helical_sinogram_dev(const float* d_volume, int rotations, int views, in
  * rho[i] * units rounded to nearest and clamped to [0, 32767], ready for
  * vct_set_maps_dev.  Enqueued on stream (a cudaStream_t, NULL: legacy
  * default stream); allocates nothing. */
+/* Index checks (no counterpart in the reference).  libvct_bounds.so, built
+ * beside libvct.so with -DVCT_BOUNDS=1, checks the kernels' computed indices
+ * (the walks' map gathers, the adjoint's staged rays, the backprojector's
+ * rows, lengthproj's views and channels, the measured-data planes); an access
+ * whose check fails is skipped and counted.  Returns the count since the last
+ * call on the current device (and clears it) and, in *where, unit * 100000 +
+ * source line of a failing check (units: 1 forward, 2 adjoint, 3 FBP,
+ * 4 lengthproj, 5 measured data).  libvct.so returns VCT_E_UNSUPPORTED. */
+int vct_bounds_violations(unsigned long long* hits, int* where);
+
 int vct_descent_step_dev(float* d_rho, const float* d_grad_a, const float* d_grad_b, double step, double units,
                          int16_t* d_maps, long long count, void* stream);
 /* The same step with a diagonal scale (a preconditioner, no counterpart in

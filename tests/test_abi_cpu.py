@@ -29,6 +29,20 @@ def test_library_exports_every_declared_symbol():
         assert hasattr(L, name), name
 
 
+def test_index_checked_library_exports_the_same_symbols():
+    import ctypes
+
+    path = os.path.join(ROOT, "virtualct_b200", "lib", "libvct_bounds.so")
+    assert os.path.exists(path), "libvct_bounds.so not built"
+    B = ctypes.CDLL(path)
+    for name in declared_symbols():
+        assert hasattr(B, name), name
+    # the product library carries no index checks and says so
+    with pytest.raises(vct.VctError) as e:
+        vct.bounds_violations()
+    assert e.value.code == vct.VCT_E_UNSUPPORTED
+
+
 def test_attenuation_matches_reference_tables():
     t = golden("mu_tables.npz")
     mu, pdf = vct.attenuation_coefficient(os.path.join(GOLDEN, "kramers_120kvp.txt"))

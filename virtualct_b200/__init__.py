@@ -22,7 +22,8 @@ from dataclasses import dataclass, fields
 import numpy as np
 
 PKG = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(PKG, "lib", "libvct.so")
+# VCT_LIB=bounds loads the index-checked build (lib/libvct_bounds.so).
+LIB_PATH = os.path.join(PKG, "lib", "libvct_bounds.so" if os.environ.get("VCT_LIB") == "bounds" else "libvct.so")
 
 VCT_OK = 0
 VCT_E_ARG = -1
@@ -57,7 +58,7 @@ EXPORTED_SYMBOLS = (
     "vct_batch_create", "vct_batch_run", "vct_batch_synchronize", "vct_batch_config", "vct_batch_destroy",
     "vct_forward_batched",
     "vct_last_segment_count",
-    "vct_kernel_launches", "vct_version", "vct_philox4x32_10", "vct_probe_peaks",
+    "vct_kernel_launches", "vct_bounds_violations", "vct_version", "vct_philox4x32_10", "vct_probe_peaks",
     "vct_load_mb_config", "vct_load_fbp_config", "vct_mb_geometry", "vct_fbp_geometry", "vct_read_raw",
     "vct_write_raw", "vct_raw_layout_default", "vct_load_measured", "vct_load_measured_dev",
     "vct_helical_sinogram", "vct_helical_sinogram_dev",
@@ -235,6 +236,7 @@ def lib():
     L.vct_philox4x32_10.restype = None
     L.vct_probe_peaks.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.vct_mbfpa_many.argtypes = [vp, C.c_int, vp, C.c_int, C.c_double, C.c_uint64, vp, vp]
+    L.vct_bounds_violations.argtypes = [C.POINTER(C.c_ulonglong), C.POINTER(C.c_int)]
     L.vct_load_mb_config.argtypes = [C.c_char_p, vp]
     L.vct_raw_layout_default.argtypes = [vp]
     L.vct_raw_layout_default.restype = None
@@ -614,6 +616,14 @@ class Batch:
             self.close()
         except Exception:
             pass
+
+
+def bounds_violations() -> tuple[int, int]:
+    """(failed index checks since the last call, unit * 100000 + line of one);
+    only the index-checked build (VCT_LIB=bounds) has them."""
+    h, w = C.c_ulonglong(0), C.c_int(0)
+    _check(lib().vct_bounds_violations(C.byref(h), C.byref(w)), "vct_bounds_violations")
+    return h.value, w.value
 
 
 def load_measured(cfg: MbConfig, layout: RawLayout | None = None, device: int = 0):

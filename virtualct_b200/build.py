@@ -3,9 +3,14 @@
 Usage: python -m virtualct_b200.build [--force]
 
 Outputs, all in-tree so they travel with the repository snapshot:
-  virtualct_b200/lib/libvct.so     C-ABI library (include/vct.h)
-  virtualct_b200/bin/vct_mbfpa     drop-in for Release_MBFPA_CPU_human/mvct.exe
-  virtualct_b200/bin/vct_fbp       drop-in for Release_FBP_CPU/mvct.exe
+  virtualct_b200/lib/libvct.so         C-ABI library (include/vct.h)
+  virtualct_b200/lib/libvct_bounds.so  the same library with index checks in the
+                                       kernels (-DVCT_BOUNDS=1): a failed check
+                                       skips its access and is counted
+                                       (vct_bounds_violations); for tests
+  virtualct_b200/bin/vct_mbfpa         drop-in for Release_MBFPA_CPU_human/mvct.exe
+  virtualct_b200/bin/vct_fbp           drop-in for Release_FBP_CPU/mvct.exe
+  virtualct_b200/bin/vct_bhc           drop-in for the beam-hardening correction
 """
 from __future__ import annotations
 
@@ -13,6 +18,7 @@ import os
 import shutil
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 PKG = os.path.dirname(os.path.abspath(__file__))
 ROOT = os.path.dirname(PKG)
@@ -22,6 +28,7 @@ BUILD = os.path.join(PKG, "_build")
 LIBDIR = os.path.join(PKG, "lib")
 BINDIR = os.path.join(PKG, "bin")
 LIB = os.path.join(LIBDIR, "libvct.so")
+LIB_BOUNDS = os.path.join(LIBDIR, "libvct_bounds.so")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", INC, "-I", CSRC]
@@ -67,32 +74,34 @@ def _run(cmd: list[str]) -> None:
         raise RuntimeError(f"build step failed: {os.path.basename(cmd[-1])}")
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
-    os.makedirs(BUILD, exist_ok=True)
+def _library(lib: str, objdir: str, defines: list[str], force: bool, verbose: bool, hdrs: list[str]) -> str:
+    """Compile every translation unit (in parallel) and link `lib`."""
+    os.makedirs(objdir, exist_ok=True)
+    jobs, objs = [], []
+    for src, extra in list(CU_SOURCES.items()) + [(c, None) for c in CPP_SOURCES]:
+        s = os.path.join(CSRC, src)
+        o = os.path.join(objdir, src + ".o")
+        objs.append(o)
+        if force or not _newer(o, [s] + hdrs + [__file__]):
+            arch = ARCH if extra is not None else []
+            jobs.append([nvcc(), *arch, *NVCC_COMMON, *defines, *(extra or []), "-c", s, "-o", o])
+    with ThreadPoolExecutor(max_workers=min(len(jobs), os.cpu_count() or 4) or 1) as pool:
+        for cmd in jobs:
+            if verbose:
+                print(" ".join(cmd))
+        list(pool.map(_run, jobs))
+    if force or not _newer(lib, objs):
+        _run([nvcc(), *ARCH, "-shared", "-Xcompiler", "-fPIC", *objs, "-o", lib, "-cudart", "static"])
+    return lib
+
+
+def build(force: bool = False, verbose: bool = False, bounds: bool = True) -> str:
     os.makedirs(LIBDIR, exist_ok=True)
     os.makedirs(BINDIR, exist_ok=True)
     hdrs = [os.path.join(CSRC, h) for h in HEADERS] + [os.path.join(INC, h) for h in ("vct.h", "vct_io.h")]
-    objs = []
-    for src, extra in CU_SOURCES.items():
-        s = os.path.join(CSRC, src)
-        o = os.path.join(BUILD, src + ".o")
-        if force or not _newer(o, [s] + hdrs + [__file__]):
-            cmd = [nvcc(), *ARCH, *NVCC_COMMON, *extra, "-c", s, "-o", o]
-            if verbose:
-                print(" ".join(cmd))
-            _run(cmd)
-        objs.append(o)
-    for src in CPP_SOURCES:
-        s = os.path.join(CSRC, src)
-        o = os.path.join(BUILD, src + ".o")
-        if force or not _newer(o, [s] + hdrs + [__file__]):
-            cmd = [nvcc(), *NVCC_COMMON, "-c", s, "-o", o]
-            if verbose:
-                print(" ".join(cmd))
-            _run(cmd)
-        objs.append(o)
-    if force or not _newer(LIB, objs):
-        _run([nvcc(), *ARCH, "-shared", "-Xcompiler", "-fPIC", *objs, "-o", LIB, "-cudart", "static"])
+    _library(LIB, BUILD, [], force, verbose, hdrs)
+    if bounds:
+        _library(LIB_BOUNDS, os.path.join(BUILD, "bounds"), ["-DVCT_BOUNDS=1"], force, verbose, hdrs)
     for app, src in APPS.items():
         s = os.path.join(CSRC, src)
         exe = os.path.join(BINDIR, app)

@@ -455,6 +455,7 @@ adj_gather_kernel(AdjGeom a, const double* __restrict__ cos_t, const double* __r
       const int v = v0 + vb;
       const int c = s_jlo[vb] + (k - s_base[vb]);
       const long long ray = (long long)v * a.C + c;
+      if (!VCT_INDEX_OK(v < a.views_used && c >= 0 && c < a.C && k < kAdjCap)) continue;
       const double cb = cos_t[v], sb = sin_t[v];
       const double2 e = dir[c];
       const double dx = e.x * cb + e.y * sb, dy = -e.x * sb + e.y * cb;
@@ -511,6 +512,7 @@ adj_gather_kernel(AdjGeom a, const double* __restrict__ cos_t, const double* __r
         // every candidate's walk covers the whole tile: chord only
         for (int j = j0; j <= j1; j++) {
           const int k = base + j;
+          if (!VCT_INDEX_OK(k >= 0 && k < kAdjCap)) continue;
           const float4 A = s_A[k];
           const float4 B = s_B[k];
           const float b = fmaf(A.x, ly, fmaf(-A.y, lx, A.z));
@@ -528,6 +530,7 @@ adj_gather_kernel(AdjGeom a, const double* __restrict__ cos_t, const double* __r
       } else {
         for (int j = j0; j <= j1; j++) {
           const int k = base + j;
+          if (!VCT_INDEX_OK(k >= 0 && k < kAdjCap)) continue;
           const float4 A = s_A[k];
           const float4 B = s_B[k];
           const int2 K = s_K[k];
@@ -636,5 +639,7 @@ int launch_adj_gather(const AdjGeom& a, int M, int tile, const double* d_cos, co
   VCT_CUDA(cudaGetLastError());
   return VCT_OK;
 }
+
+VCT_BOUNDS_READER(bounds_adjoint)
 
 }  // namespace vct

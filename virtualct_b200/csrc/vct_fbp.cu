@@ -315,6 +315,7 @@ __device__ __forceinline__ void bp_orbit_view(const float* __restrict__ Q, int V
     for (int q = 0; q < 4; q++) {
       int row = j + q * V4;
       row = row >= V ? row - V : row;
+      if (!VCT_INDEX_OK(row >= 0 && row < V)) continue;
       const float* qr = Q + (size_t)row * C + gi;
       const float q0 = __ldg(qr), q1 = __ldg(qr + 1);
       acc[q] = fmaf(fmaf(w, q1 - q0, q0), iL2, acc[q]);
@@ -659,5 +660,7 @@ int launch_fbp_backproject(const float* d_q, int V, int C, int N, double pixel_c
   VCT_CUDA(cudaGetLastError());
   return VCT_OK;
 }
+
+VCT_BOUNDS_READER(bounds_fbp)
 
 }  // namespace vct

@@ -416,4 +416,6 @@ int launch_normalize_noise(const DevGeom& g, const float* d_in, float* d_out, co
   return VCT_OK;
 }
 
+VCT_BOUNDS_READER(bounds_forward)
+
 }  // namespace vct

@@ -90,6 +90,29 @@ const char* vct_strerror(int code) {
 
 const char* vct_last_error(void) { return g_last_error.c_str(); }
 
+int vct_bounds_violations(unsigned long long* hits, int* where) {
+  if (!hits || !where) return fail(VCT_E_ARG, "vct_bounds_violations: null argument");
+#if VCT_BOUNDS
+  int (*readers[])(unsigned int*, int*) = {bounds_forward, bounds_adjoint, bounds_fbp, bounds_lengthproj,
+                                          bounds_measured};
+  *hits = 0;
+  *where = 0;
+  for (int u = 0; u < (int)(sizeof readers / sizeof readers[0]); u++) {
+    unsigned int h = 0;
+    int line = 0;
+    const int rc = readers[u](&h, &line);
+    if (rc) return rc;
+    if (h && !*where) *where = (u + 1) * 100000 + line;
+    *hits += h;
+  }
+  return VCT_OK;
+#else
+  *hits = 0;
+  *where = 0;
+  return fail(VCT_E_UNSUPPORTED, "this library has no index checks; libvct_bounds.so has");
+#endif
+}
+
 int vct_create(const vct_geometry* g, int device, vct_ctx** out) {
   if (!g || !out) return fail(VCT_E_ARG, "vct_create: null argument");
   *out = nullptr;

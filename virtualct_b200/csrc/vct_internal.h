@@ -20,6 +20,55 @@ int cuda_fail(cudaError_t e, const char* what);
     if (e_ != cudaSuccess) return vct::cuda_fail(e_, #call); \
   } while (0)
 
+// Index checks of the bounds build (libvct_bounds.so, -DVCT_BOUNDS=1): an
+// access whose check fails is skipped and counted, with the largest failing
+// source line, in its translation unit's counters, which
+// vct_bounds_violations reads and clears.  Nothing traps.  In the product
+// build VCT_INDEX_OK(c) is `true` and the checks compile away.
+#ifndef VCT_BOUNDS
+#define VCT_BOUNDS 0
+#endif
+#if defined(__CUDACC__)
+#if VCT_BOUNDS
+static __device__ unsigned int vct_bounds_hits_;
+static __device__ int vct_bounds_line_;
+static __host__ __device__ __forceinline__ bool vct_index_ok_(bool ok, int line) {
+#if defined(__CUDA_ARCH__)
+  if (!ok) {
+    atomicAdd(&vct_bounds_hits_, 1u);
+    atomicMax(&vct_bounds_line_, line);
+  }
+#endif
+  return ok;
+}
+#define VCT_INDEX_OK(cond) vct::vct_index_ok_((cond), __LINE__)
+// Defines the translation unit's reader: (hits, largest line), then clears.
+#define VCT_BOUNDS_READER(name)                                                        \
+  int name(unsigned int* hits, int* line) {                                            \
+    VCT_CUDA(cudaMemcpyFromSymbol(hits, vct_bounds_hits_, sizeof(unsigned int)));      \
+    VCT_CUDA(cudaMemcpyFromSymbol(line, vct_bounds_line_, sizeof(int)));              \
+    const unsigned int z = 0;                                                          \
+    VCT_CUDA(cudaMemcpyToSymbol(vct_bounds_hits_, &z, sizeof z));                      \
+    VCT_CUDA(cudaMemcpyToSymbol(vct_bounds_line_, &z, sizeof z));                      \
+    return VCT_OK;                                                                     \
+  }
+#else
+#define VCT_INDEX_OK(cond) true
+#define VCT_BOUNDS_READER(name)              \
+  int name(unsigned int* hits, int* line) { \
+    *hits = 0;                               \
+    *line = 0;                               \
+    return VCT_OK;                           \
+  }
+#endif
+#endif
+// The readers, one per instrumented translation unit.
+int bounds_forward(unsigned int* hits, int* line);
+int bounds_adjoint(unsigned int* hits, int* line);
+int bounds_fbp(unsigned int* hits, int* line);
+int bounds_lengthproj(unsigned int* hits, int* line);
+int bounds_measured(unsigned int* hits, int* line);
+
 // Geometry constants derived once per context; every field is computed on the
 // host with the reference's own expression order so the device walk sees
 // bit-identical inputs.

@@ -39,6 +39,7 @@ __global__ void lengthproj_kernel(LpGeom q, const double* __restrict__ cos_t, co
     int v = q.start + row_k - q.nrot * q.V;
     if (v >= q.V) v -= q.V;
     if (v < 0) v += q.V;  // the reference reads its tables out of range here
+    if (!VCT_INDEX_OK(v >= 0 && v < q.V)) continue;
     const double cb = cos_t[v], sb = sin_t[v];
     const double sx = q.sid * sb, sy = q.sid * cb;
     double len;
@@ -86,6 +87,7 @@ __global__ void lengthproj_kernel(LpGeom q, const double* __restrict__ cos_t, co
     // three explicit tests, as :158-172 (a NaN channel adds nothing)
     if (q.start_ch <= dj && dj < q.end_ch - 1) {
       const int ij = (int)dj;
+      if (!VCT_INDEX_OK(ij >= 0 && ij + 1 < q.W)) continue;
       const double f = dj - (double)ij;
       acc += (float)(((1.0 - f) * row[ij] + f * row[ij + 1]) * len);
     } else if (q.start_ch > dj) {
@@ -104,5 +106,7 @@ int launch_lengthproj(const LpGeom& q, const double* d_cos, const double* d_sin,
   VCT_CUDA(cudaGetLastError());
   return VCT_OK;
 }
+
+VCT_BOUNDS_READER(bounds_lengthproj)
 
 }  // namespace vct

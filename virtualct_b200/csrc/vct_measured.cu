@@ -56,6 +56,7 @@ __global__ void normalize_pr_kernel(const float* __restrict__ raw, const float* 
     const int r = (int)(tr % views);
     const int t = (int)(tr / views);
     const long long kk = (long long)r * nskip * ch + skip + k;
+    if (!VCT_INDEX_OK(kk >= 0 && kk < plane)) continue;
     vol[o] = raw[t * plane + kk] / air[kk];
     mask[o] = 1;
   }
@@ -111,6 +112,7 @@ __global__ void helical_kernel(const float* __restrict__ vol, int rotations, int
     if (j + iphase * views < views) iphase = 0;
     if (j + iphase * views > (rotations - 1) * views) iphase = 0;
     const double zw = 0.5 * fabs(j - (views / 2.0)) / (views / 2.0);
+    if (!VCT_INDEX_OK(j + iphase * views >= 0 && j + iphase * views < rotations * views)) continue;
     out[o] = (float)((1.0 - zw) * (double)vol[(long long)j * width + c] +
                      zw * (double)vol[(long long)(j + iphase * views) * width + c]);
   }
@@ -220,6 +222,8 @@ static int check_measured(const vct_mb_config* cfg, const vct_raw_layout* l, int
   }
   return VCT_OK;
 }
+
+VCT_BOUNDS_READER(bounds_measured)
 
 }  // namespace vct
 

@@ -500,7 +500,8 @@ VCT_HD bool walk_fast(const DevGeom& g, const PixelRec* __restrict__ maps, const
     }
     int4 wv[kUnroll];
 #pragma unroll
-    for (int u = 0; u < kUnroll; u++) wv[u] = ldg4(m4 + px[u]);
+    for (int u = 0; u < kUnroll; u++)
+      wv[u] = VCT_INDEX_OK(px[u] >= 0 && px[u] < P * P) ? ldg4(m4 + px[u]) : make_int4(0, 0, 0, 0);
 #pragma unroll
     for (int u = 0; u < kUnroll; u++)
 #pragma unroll
@@ -509,7 +510,7 @@ VCT_HD bool walk_fast(const DevGeom& g, const PixelRec* __restrict__ maps, const
 #pragma unroll
   for (int m = 0; m < M; m++) a.Lq[m] += acc[m];
   a.nseg += nseg;
-  if (pix_lumped >= 0) gather_add_exact<M>(maps, pix_lumped, rr_first, a);
+  if (pix_lumped >= 0 && VCT_INDEX_OK(pix_lumped < P * P)) gather_add_exact<M>(maps, pix_lumped, rr_first, a);
   return true;
 }
 

@@ -76,7 +76,9 @@ typedef struct vct_ctx vct_ctx;
  * and detector tables on the host and uploads them. */
 int vct_create(const vct_geometry* g, int device, vct_ctx** out);
 void vct_destroy(vct_ctx* ctx);
-/* cudaStream_t passed as an opaque pointer; NULL = the context's own stream. */
+/* cudaStream_t passed as an opaque pointer; NULL = the context's own stream
+ * (so the legacy default stream, whose handle is also NULL, is named by
+ * cudaStreamLegacy, (void*)1). */
 int vct_set_stream(vct_ctx* ctx, void* stream);
 int vct_synchronize(vct_ctx* ctx);
 
@@ -163,6 +165,31 @@ int vct_mbfpa_dev(vct_ctx* ctx, double sigma, uint64_t seed, float* d_sino_out);
  * maps. */
 int vct_mbfpa_many(vct_ctx* ctx, int n, const int16_t* const* maps, int M, double sigma, uint64_t seed,
                    float* const* out, float* stats);
+
+/* One slice over several GPUs (no counterpart in the reference): each rank
+ * projects some views, the ranks combine (max, min) and normalise their own
+ * rows, and each backprojects one band of the image; virtualct_b200.sharded
+ * does the collectives.  Pieced together, the results are bit-identical to
+ * vct_mbfpa_dev and vct_fbp_dev on one GPU.
+ *   vct_forward_views_dev: the un-normalised forward of views [v0, v1) of
+ *     the views/2*2 used into those rows of d_out ([views][width]; other
+ *     rows untouched), and the rows' (max, min) into d_maxmin (2 device
+ *     floats, 8-byte aligned).
+ *   vct_normalize_noise_rows_dev: max-normalisation and noise of rows
+ *     [r0, r1) of [0, views) in place, with the global (max, min) in
+ *     d_maxmin (the element-wise max of the ranks' max, min of their min);
+ *     slice-wide noise keyed by (seed, view, channel) as vct_mbfpa_dev's.
+ *   vct_fbp_band_count: the bands vct_fbp_band_dev splits the image into
+ *     (N/2 orbit rows of the quarter-turn backprojector when views % 4 == 0
+ *     and N is even, else N image rows).
+ *   vct_fbp_band_dev: vct_fbp_dev's image for bands [band0, band1) only;
+ *     other pixels are not written. */
+int vct_forward_views_dev(vct_ctx* ctx, int v0, int v1, float* d_out, float* d_maxmin);
+int vct_normalize_noise_rows_dev(vct_ctx* ctx, float* d_sino, int r0, int r1, const float* d_maxmin, double sigma,
+                                 uint64_t seed);
+int vct_fbp_band_count(vct_ctx* ctx, int* count);
+int vct_fbp_band_dev(vct_ctx* ctx, const float* d_sino, int filter, int in_mode, int band0, int band1,
+                     float* d_img);
 
 /* lengthproj_TOMO (MB/lengthproj_TOMO.cpp:14-185; the reference's main calls
  * it at MB/main.cpp:407 and writes npf_float.raw): for every pixel of the

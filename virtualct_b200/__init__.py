@@ -49,7 +49,8 @@ EXPORTED_SYMBOLS = (
     "vct_geometry_default", "vct_strerror", "vct_last_error", "vct_create", "vct_destroy", "vct_set_stream",
     "vct_synchronize", "vct_attenuation_coefficient", "vct_set_maps", "vct_set_maps_dev", "vct_set_spectrum",
     "vct_set_sum_mode", "vct_set_walk_mode", "vct_forward", "vct_forward_dev", "vct_line_integrals_dev", "vct_mbfpa", "vct_mbfpa_dev",
-    "vct_normalize_noise_dev", "vct_mbfpa_many", "vct_fbp", "vct_fbp_dev", "vct_fbp_noalloc", "vct_fbp_filtered_dev",
+    "vct_normalize_noise_dev", "vct_mbfpa_many", "vct_forward_views_dev", "vct_normalize_noise_rows_dev",
+    "vct_fbp_band_count", "vct_fbp_band_dev", "vct_fbp", "vct_fbp_dev", "vct_fbp_noalloc", "vct_fbp_filtered_dev",
     "vct_fbp_transpose", "vct_fbp_transpose_dev",
     "vct_set_density_scale", "vct_descent_step_dev", "vct_descent_step_scaled_dev", "vct_lengthproj", "vct_lengthproj_dev",
     "vct_beam_hardening", "vct_beam_hardening_dev", "vct_set_beam_hardening",
@@ -236,6 +237,10 @@ def lib():
     L.vct_philox4x32_10.restype = None
     L.vct_probe_peaks.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.vct_mbfpa_many.argtypes = [vp, C.c_int, vp, C.c_int, C.c_double, C.c_uint64, vp, vp]
+    L.vct_forward_views_dev.argtypes = [vp, C.c_int, C.c_int, vp, vp]
+    L.vct_normalize_noise_rows_dev.argtypes = [vp, vp, C.c_int, C.c_int, vp, C.c_double, C.c_uint64]
+    L.vct_fbp_band_count.argtypes = [vp, C.POINTER(C.c_int)]
+    L.vct_fbp_band_dev.argtypes = [vp, vp, C.c_int, C.c_int, C.c_int, C.c_int, vp]
     L.vct_bounds_violations.argtypes = [C.POINTER(C.c_ulonglong), C.POINTER(C.c_int)]
     L.vct_load_mb_config.argtypes = [C.c_char_p, vp]
     L.vct_raw_layout_default.argtypes = [vp]
@@ -413,6 +418,24 @@ class Context:
         if n:
             self._M = M
         return (out, st[:n]) if return_stats else out
+
+    # one slice over several ranks (virtualct_b200.sharded)
+    def forward_views_dev(self, v0: int, v1: int, out, maxmin) -> None:
+        _check(lib().vct_forward_views_dev(self._h, int(v0), int(v1), out.data_ptr(), maxmin.data_ptr()),
+               "vct_forward_views_dev")
+
+    def normalize_noise_rows_dev(self, sino, r0: int, r1: int, maxmin, sigma: float, seed: int) -> None:
+        _check(lib().vct_normalize_noise_rows_dev(self._h, sino.data_ptr(), int(r0), int(r1), maxmin.data_ptr(),
+                                                  float(sigma), int(seed)), "vct_normalize_noise_rows_dev")
+
+    def fbp_band_count(self) -> int:
+        n = C.c_int(0)
+        _check(lib().vct_fbp_band_count(self._h, C.byref(n)), "vct_fbp_band_count")
+        return n.value
+
+    def fbp_band_dev(self, sino, b0: int, b1: int, img, filter: int = 1, in_mode: bool = False) -> None:
+        _check(lib().vct_fbp_band_dev(self._h, sino.data_ptr(), filter, int(in_mode), int(b0), int(b1),
+                                      img.data_ptr()), "vct_fbp_band_dev")
 
     def mbfpa_dev(self, sigma: float, seed: int, out) -> None:
         _check(lib().vct_mbfpa_dev(self._h, float(sigma), int(seed), out.data_ptr()), "vct_mbfpa_dev")

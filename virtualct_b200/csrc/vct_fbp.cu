@@ -190,13 +190,13 @@ constexpr int BP_TX = 32, BP_TY = 8, BP_PIX = 2, BP_VC = 32;
 __global__ void __launch_bounds__(BP_TX * BP_TY, 4)
 fbp_bp_kernel(const float* __restrict__ Q, int V, int C, int N, int win, float scale, float sid,
               float inv_dbeta, float center, float out_scale, const float2* __restrict__ cs,
-              float* __restrict__ img) {
+              float* __restrict__ img, int row0, int row1) {
   extern __shared__ float2 sm2[];
   float2* sQ = sm2;                                        // [BP_VC][win] pairs
   float2* sCS = sQ + BP_VC * win;                          // [BP_VC]
   int* sOff = reinterpret_cast<int*>(sCS + BP_VC);         // [BP_VC]
   const int tid = threadIdx.y * BP_TX + threadIdx.x;
-  const int x0 = blockIdx.x * BP_TX, y0 = blockIdx.y * (BP_TY * BP_PIX);
+  const int x0 = blockIdx.x * BP_TX, y0 = row0 + blockIdx.y * (BP_TY * BP_PIX);
   const int x = x0 + threadIdx.x;
   const float cp = (float)N / 2.0f - 0.5f;
   // Inscribed-circle mask (FBP/misc.cpp:20-36): (y-r)^2 + (x-r)^2 <= r^2.
@@ -208,14 +208,14 @@ fbp_bp_kernel(const float* __restrict__ Q, int V, int C, int N, int win, float s
   for (int k = 0; k < BP_PIX; k++) {
     const int y = y0 + threadIdx.y + BP_TY * k;
     yy[k] = -((float)y - cp) * scale;
-    in[k] = x < N && y < N && ((double)y - r) * ((double)y - r) + ((double)x - r) * ((double)x - r) <= r * r;
+    in[k] = x < N && y < row1 && ((double)y - r) * ((double)y - r) + ((double)x - r) * ((double)x - r) <= r * r;
     acc[k] = 0.0f;
   }
   // A tile with no pixel inside the circle only writes zeros.
   const bool any = __syncthreads_or(in[0] || in[1]);
   const int use = any ? V / 2 * 2 : 0;  // usesinogram, :30
   // Tile corners (pixel centres) for the per-view windows.
-  const int xe = min(x0 + BP_TX - 1, N - 1), ye = min(y0 + BP_TY * BP_PIX - 1, N - 1);
+  const int xe = min(x0 + BP_TX - 1, N - 1), ye = min(y0 + BP_TY * BP_PIX - 1, row1 - 1);
   const float cx0 = -((float)x0 - cp) * scale, cx1 = -((float)xe - cp) * scale;
   const float cy0 = -((float)y0 - cp) * scale, cy1 = -((float)ye - cp) * scale;
   for (int v0 = 0; v0 < use; v0 += BP_VC) {
@@ -271,7 +271,7 @@ fbp_bp_kernel(const float* __restrict__ Q, int V, int C, int N, int win, float s
 #pragma unroll
   for (int k = 0; k < BP_PIX; k++) {
     const int y = y0 + threadIdx.y + BP_TY * k;
-    if (x < N && y < N) img[(size_t)y * N + x] = in[k] ? acc[k] * out_scale : 0.0f;
+    if (x < N && y < row1) img[(size_t)y * N + x] = in[k] ? acc[k] * out_scale : 0.0f;
   }
 }
 
@@ -326,16 +326,17 @@ __device__ __forceinline__ void bp_orbit_view(const float* __restrict__ Q, int V
 template <int VS>
 __global__ void __launch_bounds__(BS_TX * BS_TY * VS)
 fbp_bp_sym_kernel(const float* __restrict__ Q, int V, int C, int N, float scale, float sid, float inv_dbeta,
-                  float center, float out_scale, const float2* __restrict__ cs, float* __restrict__ img) {
+                  float center, float out_scale, const float2* __restrict__ cs, float* __restrict__ img, int y_lo,
+                  int y_hi) {
   __shared__ float part[VS - 1][4][BS_TX * BS_TY];
   const int H = N / 2, V4 = V / 4;
   const int x = blockIdx.x * BS_TX + threadIdx.x;
-  const int y = blockIdx.y * BS_TY + threadIdx.y;
+  const int y = y_lo + blockIdx.y * BS_TY + threadIdx.y;  // orbit rows [y_lo, y_hi) of [0, N/2)
   const int lt = threadIdx.y * BS_TX + threadIdx.x;
   const int z = threadIdx.z;
   const double r = (double)(N - 1) / 2.0;
   // The circle mask (FBP/misc.cpp:20-36) is invariant under the quarter turn.
-  const bool in = x < H && y < H &&
+  const bool in = x < H && y < y_hi &&
                   ((double)y - r) * ((double)y - r) + ((double)x - r) * ((double)x - r) <= r * r;
   float acc[4] = {0.0f, 0.0f, 0.0f, 0.0f};
   if (in) {
@@ -356,7 +357,7 @@ fbp_bp_sym_kernel(const float* __restrict__ Q, int V, int C, int N, float scale,
     for (int q = 0; q < 4; q++) part[z - 1][q][lt] = acc[q];
   }
   __syncthreads();
-  if (z == 0 && x < H && y < H) {
+  if (z == 0 && x < H && y < y_hi) {
     const int px[4] = {x, N - 1 - y, N - 1 - x, y};
     const int py[4] = {y, x, N - 1 - y, N - 1 - x};
 #pragma unroll
@@ -621,9 +622,15 @@ int launch_fbp_backproject_t(const float* d_u, int V, int C, int N, double pixel
   return VCT_OK;
 }
 
+int fbp_band_count(int V, int N) { return (V % 4 == 0 && N % 2 == 0) ? N / 2 : N; }
+
 int launch_fbp_backproject(const float* d_q, int V, int C, int N, double pixel_cm, double sid,
                            double max_beta, int xfactor, const float* d_cs, float* d_img,
-                           cudaStream_t st, int view_groups) {
+                           cudaStream_t st, int view_groups, int band0, int band1) {
+  if (band1 < 0) band1 = fbp_band_count(V, N);
+  if (band0 < 0 || band0 > band1 || band1 > fbp_band_count(V, N))
+    return fail(VCT_E_ARG, "fbp: band outside the image");
+  if (band0 == band1) return VCT_OK;
   const int half = (C - 1) / 2;
   const double dbeta_det = max_beta / half;
   const double dbeta = 2.0 * 3.141592653589793 / V;
@@ -637,26 +644,26 @@ int launch_fbp_backproject(const float* d_q, int V, int C, int N, double pixel_c
   if (win > C + 4) win = C + 4;
   if (V % 4 == 0 && N % 2 == 0) {
     const int H = N / 2;
-    dim3 grid((H + BS_TX - 1) / BS_TX, (H + BS_TY - 1) / BS_TY);
+    dim3 grid((H + BS_TX - 1) / BS_TX, (band1 - band0 + BS_TY - 1) / BS_TY);
     const float a_sc = (float)pixel_cm, a_sid = (float)sid, a_ib = (float)(1.0 / dbeta_det), a_c = (float)(C / 2),
                 a_os = (float)(dbeta * xfactor);
     const float2* cs2 = reinterpret_cast<const float2*>(d_cs);
     switch (view_groups) {
-      case 2: fbp_bp_sym_kernel<2><<<grid, dim3(BS_TX, BS_TY, 2), 0, st>>>(d_q, V, C, N, a_sc, a_sid, a_ib, a_c, a_os, cs2, d_img); break;
-      case 8: fbp_bp_sym_kernel<8><<<grid, dim3(BS_TX, BS_TY, 8), 0, st>>>(d_q, V, C, N, a_sc, a_sid, a_ib, a_c, a_os, cs2, d_img); break;
-      default: fbp_bp_sym_kernel<BS_VS><<<grid, dim3(BS_TX, BS_TY, BS_VS), 0, st>>>(d_q, V, C, N, a_sc, a_sid, a_ib, a_c, a_os, cs2, d_img); break;
+      case 2: fbp_bp_sym_kernel<2><<<grid, dim3(BS_TX, BS_TY, 2), 0, st>>>(d_q, V, C, N, a_sc, a_sid, a_ib, a_c, a_os, cs2, d_img, band0, band1); break;
+      case 8: fbp_bp_sym_kernel<8><<<grid, dim3(BS_TX, BS_TY, 8), 0, st>>>(d_q, V, C, N, a_sc, a_sid, a_ib, a_c, a_os, cs2, d_img, band0, band1); break;
+      default: fbp_bp_sym_kernel<BS_VS><<<grid, dim3(BS_TX, BS_TY, BS_VS), 0, st>>>(d_q, V, C, N, a_sc, a_sid, a_ib, a_c, a_os, cs2, d_img, band0, band1); break;
     }
     VCT_CUDA(cudaGetLastError());
     return VCT_OK;
   }
-  dim3 grid((N + BP_TX - 1) / BP_TX, (N + BP_TY * BP_PIX - 1) / (BP_TY * BP_PIX));
+  dim3 grid((N + BP_TX - 1) / BP_TX, (band1 - band0 + BP_TY * BP_PIX - 1) / (BP_TY * BP_PIX));
   dim3 block(BP_TX, BP_TY);
   const size_t smem = (size_t)BP_VC * win * sizeof(float2) + BP_VC * (sizeof(float2) + sizeof(int));
   VCT_CUDA(cudaFuncSetAttribute(fbp_bp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   fbp_bp_kernel<<<grid, block, smem, st>>>(d_q, V, C, N, win, (float)pixel_cm, (float)sid,
                                            (float)(1.0 / dbeta_det), (float)(C / 2),
                                            (float)(dbeta * xfactor),
-                                           reinterpret_cast<const float2*>(d_cs), d_img);
+                                           reinterpret_cast<const float2*>(d_cs), d_img, band0, band1);
   VCT_CUDA(cudaGetLastError());
   return VCT_OK;
 }

@@ -120,7 +120,7 @@ forward_kernel(DevGeom g, const PixelRec* __restrict__ maps, const double* __res
                const float* __restrict__ pdf, int NE, const double* __restrict__ cos_t,
                const double* __restrict__ sin_t, const double* __restrict__ det_px0,
                const double* __restrict__ det_py0, int fast, float* __restrict__ out,
-               double* __restrict__ lint, FwdStats* __restrict__ stats) {
+               double* __restrict__ lint, FwdStats* __restrict__ stats, long long ray0, long long ray1) {
   extern __shared__ double smem[];
   double* s_mu = smem;                                             // [NE][M]
   float* s_pdf = reinterpret_cast<float*>(smem + (size_t)NE * M);  // [NE]
@@ -128,9 +128,9 @@ forward_kernel(DevGeom g, const PixelRec* __restrict__ maps, const double* __res
   for (int i = threadIdx.x; i < NE; i += blockDim.x) s_pdf[i] = pdf[i];
   __syncthreads();
 
-  const long long nrays = (long long)g.views_used * g.C;
-  const long long ray = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const bool active = ray < nrays;
+  // rays [ray0, ray1) of the views_used * C
+  const long long ray = ray0 + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  const bool active = ray < ray1;
   float val = 0.0f;
   int nseg = 0;
   if (active) {
@@ -184,21 +184,21 @@ template <int M>
 static int launch_forward_m(const DevGeom& g, const PixelRec* d_maps, const double* d_mu,
                             const float* d_pdf, int NE, const double* d_cos, const double* d_sin,
                             const double* d_px0, const double* d_py0, int sum_mode, int fast,
-                            float* d_out, double* d_lint, FwdStats* d_stats, cudaStream_t st) {
-  const long long nrays = (long long)g.views_used * g.C;
-  const int blocks = (int)((nrays + kFwdThreads - 1) / kFwdThreads);
+                            float* d_out, double* d_lint, FwdStats* d_stats, cudaStream_t st, int v0, int v1) {
+  const long long ray0 = (long long)v0 * g.C, ray1 = (long long)v1 * g.C;
+  const int blocks = (int)((ray1 - ray0 + kFwdThreads - 1) / kFwdThreads);
   const size_t smem = (size_t)NE * M * sizeof(double) + (size_t)NE * sizeof(float);
   if (blocks == 0) return VCT_OK;
   if (sum_mode == VCT_SUM_REFERENCE) {
     auto k = forward_kernel<M, VCT_SUM_REFERENCE>;
     VCT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k<<<blocks, kFwdThreads, smem, st>>>(g, d_maps, d_mu, d_pdf, NE, d_cos, d_sin, d_px0, d_py0, fast,
-                                          d_out, d_lint, d_stats);
+                                          d_out, d_lint, d_stats, ray0, ray1);
   } else {
     auto k = forward_kernel<M, VCT_SUM_COMPENSATED>;
     VCT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     k<<<blocks, kFwdThreads, smem, st>>>(g, d_maps, d_mu, d_pdf, NE, d_cos, d_sin, d_px0, d_py0, fast,
-                                          d_out, d_lint, d_stats);
+                                          d_out, d_lint, d_stats, ray0, ray1);
   }
   VCT_CUDA(cudaGetLastError());
   return VCT_OK;
@@ -207,12 +207,14 @@ static int launch_forward_m(const DevGeom& g, const PixelRec* d_maps, const doub
 int launch_forward(const DevGeom& g, const PixelRec* d_maps, int M, const double* d_mu_tab,
                    const float* d_pdf, int NE, const double* d_cos, const double* d_sin,
                    const double* d_det_ox, const double* d_det_oy, int sum_mode, int fast, float* d_out,
-                   double* d_lint, FwdStats* d_stats, cudaStream_t st) {
+                   double* d_lint, FwdStats* d_stats, cudaStream_t st, int v0, int v1) {
   fast = fast && !g.rmax_active;
+  if (v1 < 0) v1 = g.views_used;
+  if (v0 < 0 || v0 > v1 || v1 > g.views_used) return fail(VCT_E_ARG, "forward: view range outside the views used");
   switch (M) {
 #define VCT_CASE(mm) \
   case mm:           \
-    return launch_forward_m<mm>(g, d_maps, d_mu_tab, d_pdf, NE, d_cos, d_sin, d_det_ox, d_det_oy, sum_mode, fast, d_out, d_lint, d_stats, st);
+    return launch_forward_m<mm>(g, d_maps, d_mu_tab, d_pdf, NE, d_cos, d_sin, d_det_ox, d_det_oy, sum_mode, fast, d_out, d_lint, d_stats, st, v0, v1);
     VCT_CASE(1) VCT_CASE(2) VCT_CASE(3) VCT_CASE(4) VCT_CASE(5) VCT_CASE(6) VCT_CASE(7) VCT_CASE(8)
 #undef VCT_CASE
     default:
@@ -374,10 +376,9 @@ int forward_batch_occupancy(int M, int ne_max, int* blocks_per_sm) {
 // keyed by the 64-bit seed, counter (channel, view, 0, 0).
 __global__ void normalize_noise_kernel(const float* __restrict__ in, float* __restrict__ out, int V,
                                        int W, const FwdStats* __restrict__ stats, int pad_zero,
-                                       double sigma, uint32_t k0, uint32_t k1) {
-  const long long n = (long long)V * W;
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+                                       double sigma, uint32_t k0, uint32_t k1, long long i0, long long i1) {
+  const long long i = i0 + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= i1) return;
   const float pmax = __uint_as_float(stats->max_bits);
   float pmin_raw = __uint_as_float(stats->min_bits);
   if (pad_zero) pmin_raw = fminf(pmin_raw, 0.0f);
@@ -406,12 +407,15 @@ __global__ void normalize_noise_kernel(const float* __restrict__ in, float* __re
 }
 
 int launch_normalize_noise(const DevGeom& g, const float* d_in, float* d_out, const FwdStats* d_stats,
-                           int pad_zero, double sigma, uint64_t seed, cudaStream_t st) {
-  const long long n = (long long)g.views * g.width;
+                           int pad_zero, double sigma, uint64_t seed, cudaStream_t st, int r0, int r1) {
+  if (r1 < 0) r1 = g.views;
+  if (r0 < 0 || r0 > r1 || r1 > g.views) return fail(VCT_E_ARG, "normalise: row range outside the sinogram");
+  const long long i0 = (long long)r0 * g.width, i1 = (long long)r1 * g.width;
   const int threads = 256;
-  const int blocks = (int)((n + threads - 1) / threads);
+  const int blocks = (int)((i1 - i0 + threads - 1) / threads);
+  if (blocks == 0) return VCT_OK;
   normalize_noise_kernel<<<blocks, threads, 0, st>>>(d_in, d_out, g.views, g.width, d_stats, pad_zero,
-                                                     sigma, (uint32_t)seed, (uint32_t)(seed >> 32));
+                                                     sigma, (uint32_t)seed, (uint32_t)(seed >> 32), i0, i1);
   VCT_CUDA(cudaGetLastError());
   return VCT_OK;
 }

@@ -647,7 +647,8 @@ static int build_filter(vct_ctx* c, int filter) {
   return VCT_OK;
 }
 
-static int fbp_into(vct_ctx* c, const float* d_sino, int filter, int in_mode, float* d_img, int view_groups) {
+static int fbp_into(vct_ctx* c, const float* d_sino, int filter, int in_mode, float* d_img, int view_groups,
+                    int band0 = 0, int band1 = -1) {
   int rc = check_ctx(c);
   if (rc) return rc;
   if (!d_sino || !d_img) return fail(VCT_E_ARG, "null buffer");
@@ -662,10 +663,59 @@ static int fbp_into(vct_ctx* c, const float* d_sino, int filter, int in_mode, fl
                               c->fbp_q.p, c->stream)))
     return rc;
   if ((rc = launch_fbp_backproject(c->fbp_q.p, V, C, c->dg.N, c->geo.pixel_cm, c->geo.sid_cm, c->geo.max_beta,
-                                   c->geo.xfactor, c->cs_f.p, d_img, c->stream, view_groups)))
+                                   c->geo.xfactor, c->cs_f.p, d_img, c->stream, view_groups, band0, band1)))
     return rc;
   c->launches += 3;
   return VCT_OK;
+}
+
+// ------------------------------------------------------ one slice, sharded
+int vct_forward_views_dev(vct_ctx* c, int v0, int v1, float* d_out, float* d_maxmin) {
+  NvtxScope nvtx_scope("vct_forward_views_dev");
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!d_out || !d_maxmin) return fail(VCT_E_ARG, "vct_forward_views_dev: null buffer");
+  if (v0 < 0 || v0 > v1 || v1 > c->dg.views_used) return fail(VCT_E_ARG, "vct_forward_views_dev: bad view range");
+  if (!c->maps_ready || !c->spectrum_ready) return fail(VCT_E_STATE, "forward: maps or spectrum not set");
+  const size_t row = (size_t)c->geo.width;
+  VCT_CUDA(cudaMemcpyAsync(c->stats.p, c->stats.p + 1, sizeof(FwdStats), cudaMemcpyDeviceToDevice, c->stream));
+  if (v1 > v0) VCT_CUDA(cudaMemsetAsync(d_out + v0 * row, 0, (size_t)(v1 - v0) * row * sizeof(float), c->stream));
+  const double* mu_tab = c->sum_mode == VCT_SUM_REFERENCE ? c->mu_scaled.p : c->mu_log2.p;
+  if (v1 > v0) {
+    rc = launch_forward(c->dg, c->maps.p, c->M, mu_tab, c->pdf.p, c->NE, c->cos_t.p, c->sin_t.p, c->det_px0.p,
+                        c->det_py0.p, c->sum_mode, c->walk_mode == VCT_WALK_FAST, d_out, nullptr, c->stats.p,
+                        c->stream, v0, v1);
+    if (rc) return rc;
+    c->launches++;
+  }
+  // (max, min) of the rows as two floats: FwdStats begins with their bits
+  VCT_CUDA(cudaMemcpyAsync(d_maxmin, c->stats.p, 2 * sizeof(float), cudaMemcpyDeviceToDevice, c->stream));
+  return VCT_OK;
+}
+
+int vct_normalize_noise_rows_dev(vct_ctx* c, float* d_sino, int r0, int r1, const float* d_maxmin, double sigma,
+                                 uint64_t seed) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!d_sino || !d_maxmin) return fail(VCT_E_ARG, "vct_normalize_noise_rows_dev: null buffer");
+  if (((uintptr_t)d_maxmin & 7) != 0) return fail(VCT_E_ARG, "vct_normalize_noise_rows_dev: d_maxmin not 8-byte aligned");
+  rc = launch_normalize_noise(c->dg, d_sino, d_sino, reinterpret_cast<const FwdStats*>(d_maxmin), pad_zero_of(c),
+                              sigma, seed, c->stream, r0, r1);
+  if (!rc) c->launches++;
+  return rc;
+}
+
+int vct_fbp_band_count(vct_ctx* c, int* count) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!count) return fail(VCT_E_ARG, "vct_fbp_band_count: null argument");
+  *count = fbp_band_count(c->geo.views, c->dg.N);
+  return VCT_OK;
+}
+
+int vct_fbp_band_dev(vct_ctx* c, const float* d_sino, int filter, int in_mode, int band0, int band1, float* d_img) {
+  NvtxScope nvtx_scope("vct_fbp_band_dev");
+  return fbp_into(c, d_sino, filter, in_mode, d_img, 4, band0, band1);
 }
 
 int vct_fbp_dev(vct_ctx* c, const float* d_sino, int filter, int in_mode, float* d_img) {

@@ -115,7 +115,7 @@ int launch_pack_maps(const int16_t* d_maps, int M, int N, PixelRec* d_packed, cu
 int launch_forward(const DevGeom& g, const PixelRec* d_maps, int M, const double* d_mu_tab,
                    const float* d_pdf, int NE, const double* d_cos, const double* d_sin,
                    const double* d_det_ox, const double* d_det_oy, int sum_mode, int fast, float* d_out,
-                   double* d_lint, FwdStats* d_stats, cudaStream_t st);
+                   double* d_lint, FwdStats* d_stats, cudaStream_t st, int v0 = 0, int v1 = -1);
 // One slice of a batched forward (vct_batch.cpp): its geometry, device
 // tables and outputs.  tile0 is the index of its first ray tile.
 struct FwdJob {
@@ -136,7 +136,7 @@ int launch_forward_batch(const FwdJob* d_jobs, int njobs, int M, int tile_rays, 
                          int grid, unsigned int* d_counter, cudaStream_t st);
 int forward_batch_occupancy(int M, int ne_max, int* blocks_per_sm);
 int launch_normalize_noise(const DevGeom& g, const float* d_in, float* d_out, const FwdStats* d_stats,
-                           int pad_zero, double sigma, uint64_t seed, cudaStream_t st);
+                           int pad_zero, double sigma, uint64_t seed, cudaStream_t st, int r0 = 0, int r1 = -1);
 // bh_alpha != 0: beam-hardening correction of the line integrals on the way.
 int launch_fbp_weight(const float* d_sino, int V, int W, int start, int C, const double* d_coeff,
                       float* d_g, cudaStream_t st, double bh_alpha = 0.0, double bh_beta = 0.0);
@@ -145,9 +145,13 @@ int launch_fbp_filter(const float* d_g, const float* d_h0, const float* d_cm, in
                       float* d_q, cudaStream_t st);
 // view_groups: how many warp groups split the views of the quarter-turn
 // backprojector (2, 4 or 8; other values mean 4).
+// band0..band1: the image rows [band0, band1) of the general backprojector,
+// or the orbit rows [band0, band1) of [0, N/2) of the quarter-turn one
+// (fbp_band_count); pixels outside the band are not written.
+int fbp_band_count(int V, int N);
 int launch_fbp_backproject(const float* d_q, int V, int C, int N, double pixel_cm, double sid,
                            double max_beta, int xfactor, const float* d_cs, float* d_img,
-                           cudaStream_t st, int view_groups = 4);
+                           cudaStream_t st, int view_groups = 4, int band0 = 0, int band1 = -1);
 // Transposes of the three FBP steps (vct_fbp.cu).
 size_t fbp_backproject_t_scratch(int V, int C, int N);  // 64-bit words of d_acc
 int launch_fbp_backproject_t(const float* d_u, int V, int C, int N, double pixel_cm, double sid, double max_beta,

@@ -16,15 +16,27 @@ constexpr int kLineBuf = 512;  // LINEBUF_SIZE, MB/projectionDataTOMO.cpp:11
 struct TxtReader {
   FILE* fp;
   char line[kLineBuf];
+  int field = 0;     // fields read so far
+  int missing = -1;  // the first field whose value line is past the end of the file
   void skip(int n) {
     for (int i = 0; i < n; i++)
       if (!fgets(line, kLineBuf, fp)) line[0] = 0;
   }
   // One field = two skipped lines + one value line (:24-64).  A value line
-  // that sscanf cannot parse leaves the field unchanged, as in the reference.
+  // that sscanf cannot parse leaves the field unchanged, as in the reference;
+  // a file that ends before a value line is refused (the reference would read
+  // on with the field uninitialised).
   void next() {
     skip(2);
-    if (!fgets(line, kLineBuf, fp)) line[0] = 0;
+    if (!fgets(line, kLineBuf, fp)) {
+      line[0] = 0;
+      if (missing < 0) missing = field;
+    }
+    field++;
+  }
+  int check(const char* path) const {
+    if (missing < 0) return VCT_OK;
+    return fail(VCT_E_IO, std::string("info file: ") + path + " ends before field " + std::to_string(missing + 1));
   }
   void i(int* v) { next(); sscanf(line, "%d", v); }
   void d(double* v) { next(); sscanf(line, "%lf", v); }
@@ -83,6 +95,7 @@ int vct_load_mb_config(const char* path, vct_mb_config* c) {
   r.s(c->spectrum_file, sizeof c->spectrum_file);
   r.d(&c->photon_noise);
   fclose(fp);
+  if (int rc = r.check(path)) return rc;
   // :125-134
   c->data_sampling_rate_orig = c->data_sampling_rate;
   if (c->data_sampling_rate >= 200) c->data_sampling_rate = c->data_sampling_rate / 5;
@@ -122,6 +135,7 @@ int vct_load_fbp_config(const char* path, vct_fbp_config* c) {
   r.i(&c->xfactor);
   r.s(c->output_file, sizeof c->output_file);
   fclose(fp);
+  if (int rc = r.check(path)) return rc;
   // FBP/projectionDataTOMO.cpp:94-96
   c->total_proj_number = (int)(c->proj_height / (c->gantry_rotation_period * c->data_sampling_rate));
   c->proj_height = (int)(c->gantry_rotation_period * c->data_sampling_rate);

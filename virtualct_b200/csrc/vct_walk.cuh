@@ -478,7 +478,40 @@ VCT_HD bool walk_fast(const DevGeom& g, const PixelRec* __restrict__ maps, const
   // segment's pixel with weight 0; the indices stay inside the padded border
   // because the walk ends within one step of the square.
   constexpr int kUnroll = VCT_FWD_UNROLL;
-  for (int it = 0; it < (8 * N + 128) / kUnroll && t < tend; it++) {
+  const int it_max = (8 * N + 128) / kUnroll;
+  int it = 0;
+  // Bulk iterations, with no per-slot end test.  A segment ends at the next
+  // major gridline at the latest, so t < tmaj always holds and tmaj grows by
+  // at most one per segment: while tmaj + kUnroll - 1 <= tend (integers held
+  // in doubles, exact), every slot of the iteration starts before tend.  The
+  // integer sums do not depend on how the segments are grouped, so the
+  // result is the same as the checked loop's alone.
+  for (; it < it_max && tmaj + (double)(kUnroll - 1) <= tend; it++) {
+    int px[kUnroll];
+    unsigned int wq[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; u++) {
+      const bool mj = tmaj <= tmin;
+      const double tn = mj ? tmaj : tmin;
+      wq[u] = lo32((tn - t) + 4194304.0);
+      px[u] = pix;
+      t = tn;
+      tmaj = mj ? tmaj + 1.0 : tmaj;
+      tmin = mj ? tmin : tmin + dt;
+      pix += mj ? dpix_maj : dpix_min;
+    }
+    nseg += kUnroll;
+    int4 wv[kUnroll];
+#pragma unroll
+    for (int u = 0; u < kUnroll; u++)
+      wv[u] = VCT_INDEX_OK(px[u] >= 0 && px[u] < P * P) ? ldg4(m4 + px[u]) : make_int4(0, 0, 0, 0);
+#pragma unroll
+    for (int u = 0; u < kUnroll; u++)
+#pragma unroll
+      for (int m = 0; m < M; m++) acc[m] += (unsigned long long)mat_of(wv[u], m) * wq[u];
+  }
+  // The last iterations, each slot tested against the end.
+  for (; it < it_max && t < tend; it++) {
     int px[kUnroll];
     unsigned int wq[kUnroll];
 #pragma unroll

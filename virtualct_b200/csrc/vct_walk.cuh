@@ -433,6 +433,25 @@ VCT_HD void fast_plan(const DevGeom& g, const Ray& r, FastPlan& p) {
   p.dt = dt;
 }
 
+// Fixed-point accumulation of one segment, two elements per 32-bit record
+// word u = s_lo | s_hi << 16: P += u * w adds s_lo * w + 2^16 * s_hi * w and
+// H += s_hi * w, so sum(s_lo * w) = P - 2^16 * H modulo 2^64, which is exact
+// because that sum itself fits in 64 bits (three integer instructions per
+// pair instead of four).  A word with one element in use takes its low half.
+template <int M>
+VCT_HD void acc_words(const int4& w, unsigned int q, unsigned long long* P, unsigned long long* H) {
+#pragma unroll
+  for (int i = 0; i < (M + 1) / 2; i++) {
+    const unsigned int u = i == 0 ? (unsigned)w.x : i == 1 ? (unsigned)w.y : i == 2 ? (unsigned)w.z : (unsigned)w.w;
+    if (2 * i + 1 < M) {
+      P[i] += (unsigned long long)u * q;
+      H[i] += (unsigned long long)(u >> 16) * q;
+    } else {
+      P[i] += (unsigned long long)(u & 0xffffu) * q;
+    }
+  }
+}
+
 // Returns false when the ray needs the exact walk.
 template <int M>
 VCT_HD bool walk_fast(const DevGeom& g, const PixelRec* __restrict__ maps, const Ray& r, RayAcc& a) {
@@ -470,9 +489,10 @@ VCT_HD bool walk_fast(const DevGeom& g, const PixelRec* __restrict__ maps, const
   double t = 0.0;
   const double tend = (double)pl.K;
   const int4* __restrict__ m4 = reinterpret_cast<const int4*>(mp);
-  unsigned long long acc[M];
+  constexpr int kWords = (M + 1) / 2;
+  unsigned long long accP[kWords], accH[kWords];
 #pragma unroll
-  for (int m = 0; m < M; m++) acc[m] = 0ull;
+  for (int i = 0; i < kWords; i++) accP[i] = accH[i] = 0ull;
   int nseg = 0;
   // Every iteration closes one segment.  The event logic does not depend on
   // the map, so kUnroll segments are laid out first and their gathers issued
@@ -508,9 +528,7 @@ VCT_HD bool walk_fast(const DevGeom& g, const PixelRec* __restrict__ maps, const
     for (int u = 0; u < kUnroll; u++)
       wv[u] = VCT_INDEX_OK(px[u] >= 0 && px[u] < P * P) ? ldg4(m4 + px[u]) : make_int4(0, 0, 0, 0);
 #pragma unroll
-    for (int u = 0; u < kUnroll; u++)
-#pragma unroll
-      for (int m = 0; m < M; m++) acc[m] += (unsigned long long)mat_of(wv[u], m) * wq[u];
+    for (int u = 0; u < kUnroll; u++) acc_words<M>(wv[u], wq[u], accP, accH);
   }
   // The last iterations, each slot tested against the end.
   for (; it < it_max && t < tend; it++) {
@@ -538,12 +556,13 @@ VCT_HD bool walk_fast(const DevGeom& g, const PixelRec* __restrict__ maps, const
     for (int u = 0; u < kUnroll; u++)
       wv[u] = VCT_INDEX_OK(px[u] >= 0 && px[u] < P * P) ? ldg4(m4 + px[u]) : make_int4(0, 0, 0, 0);
 #pragma unroll
-    for (int u = 0; u < kUnroll; u++)
-#pragma unroll
-      for (int m = 0; m < M; m++) acc[m] += (unsigned long long)mat_of(wv[u], m) * wq[u];
+    for (int u = 0; u < kUnroll; u++) acc_words<M>(wv[u], wq[u], accP, accH);
   }
 #pragma unroll
-  for (int m = 0; m < M; m++) a.Lq[m] += acc[m];
+  for (int i = 0; i < kWords; i++) {
+    a.Lq[2 * i] += accP[i] - (accH[i] << 16);
+    if (2 * i + 1 < M) a.Lq[2 * i + 1] += accH[i];
+  }
   a.nseg += nseg;
   if (pix_lumped >= 0 && VCT_INDEX_OK(pix_lumped < P * P)) gather_add_exact<M>(maps, pix_lumped, rr_first, a);
   return true;

@@ -54,3 +54,25 @@ def test_fast_walk_matches_exact_walk(walk_check, tmp_path, N, pix, views, seed,
         # every first step is a pixel boundary at 0.1 cm; only rays through
         # the origin (even channel counts) take the exact walk
         assert fallback <= (0 if channels % 2 else views)
+
+
+@pytest.fixture(scope="module")
+def acc_check(tmp_path_factory):
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(nvcc):
+        pytest.skip("nvcc not available")
+    exe = tmp_path_factory.mktemp("acc") / "acc_check"
+    src = os.path.join(ROOT, "tests", "host", "acc_check.cu")
+    subprocess.run([nvcc, "-O2", "-std=c++17", "-Wno-deprecated-gpu-targets", "-I", os.path.join(ROOT, "include"),
+                    "-I", os.path.join(ROOT, "virtualct_b200", "csrc"), src, "-o", str(exe)],
+                   check=True, capture_output=True)
+    return exe
+
+
+@pytest.mark.parametrize("M", [1, 2, 3, 4, 5, 6, 7, 8])
+def test_paired_word_accumulation_is_exact(acc_check, M):
+    """Two elements per 64-bit multiply-add, the low sum recovered modulo 2^64:
+    equal to the per-element sums at the extremes (65535 densities, 2^30
+    weights, 20,000 segments, so the packed sums wrap many times)."""
+    r = subprocess.run([str(acc_check), str(M), "20000", str(M + 100)], capture_output=True, text=True)
+    assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout

@@ -39,7 +39,7 @@ SPECTRUM = os.path.join(ROOT, "tests", "golden", "kramers_120kvp.txt")
 METRIC = "MBFPA rays*bins/s (FBP slices/s alongside)"
 # DRAM bytes (read + write) of one forward_kernel launch on this workload,
 # from one ncu capture: the two map copies once; the gathers hit L1/L2.
-FWD_DRAM_BYTES = 8579584
+FWD_DRAM_BYTES = 8581888
 CONFIG_NAME = "plain MBFPA+FBP single slice: 512^2, 6 elements, 800 views x 609 channels, 120 kVp Kramers 110 bins"
 
 

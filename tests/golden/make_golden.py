@@ -17,7 +17,7 @@ Fixtures
                   for a seeded 64^2 ellipse phantom, 40 and 41 views.
   fbp_small.npz   filterSinogram + reconstructImage of a 40-view sinogram onto
                   64^2, Ram-Lak and Shepp-Logan.
-  c1_subset.npz   full-size C1 (512^2, 800 x 609, 6 elements, 110-bin Kramers
+  c1_subset.npz   full-size single slice (512^2, 800 x 609, 6 elements, 110-bin Kramers
                   spectrum, seeded ellipse phantom seed 0): every 20th view of
                   the reference's un-normalised spectral sum and the FP64
                   oracle's, its global max and min, the total segment count,

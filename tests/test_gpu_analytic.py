@@ -67,7 +67,7 @@ def _line_integrals(geo, maps, walk):
         return L.cpu().numpy()
 
 
-# (N, pixel cm, views, channels): the C1 grid; coarser grids; even channel
+# (N, pixel cm, views, channels): the 512^2 grid at 0.1 cm; coarser grids; even channel
 # counts, whose central ray passes through the origin; view counts whose views
 # include 0, 45, 90 ... degrees exactly.  The pixel sizes divide 1 cm: the
 # walk steps from the first whole-cm gridline, so for sizes that do not (say

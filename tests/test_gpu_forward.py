@@ -93,7 +93,7 @@ def test_c1_full_size_matches_reference(cuda_device, walk):
 
 
 def test_c1_fbp_and_fp64_rows(cuda_device):
-    """C1 end to end: the device forward within 1e-5 of the FP64 sum, and the
+    """The 512^2, 800 x 609, 6-element slice end to end: the device forward within 1e-5 of the FP64 sum, and the
     Ram-Lak FBP of its max-normalised, noise-free sinogram within 1e-4 of the
     reference's FBP of the reference's sinogram (every 16th row)."""
     d = golden("c1_subset.npz")
@@ -112,7 +112,7 @@ def test_c1_fbp_and_fp64_rows(cuda_device):
 
 
 def test_eight_elements_and_6mv(cuda_device):
-    """C2-style: 8 elements (Mg, Si added), MV spectrum; against the FP64 oracle."""
+    """6 MV style: 8 elements (Mg, Si added), MV spectrum; against the FP64 oracle."""
     rows = phantoms.mv_spectrum()
     import tempfile
 

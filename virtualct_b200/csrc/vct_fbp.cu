@@ -482,7 +482,7 @@ constexpr int BT_PARTS = 8;
 // low word's carry is read from the value it held before the add, and the
 // high word is touched only when it changes.  Low and high words live in
 // separate arrays, so neighbouring bins are neighbouring banks.  (Measured:
-// 0.85 ms for the C1 transpose against 1.86 ms with 64-bit atomics and
+// 0.85 ms for the 512^2, 800 x 609 transpose against 1.86 ms with 64-bit atomics and
 // 1.50 ms with float ones.)
 __device__ __forceinline__ void add64_split(unsigned int* lo, unsigned int* hi, unsigned long long v) {
   const unsigned int vlo = (unsigned int)v, vhi = (unsigned int)(v >> 32);

@@ -19,11 +19,12 @@ constexpr int kPad = kMapPad;
 VCT_HD int pad_index(int col, int row, int N) { return (col + kPad) + (row + kPad) * (N + 2 * kPad); }
 
 // Resident blocks per SM the register allocation is held to, and the number
-// of walk segments whose gathers are issued together (chosen by measurement:
-// at C1, 2 / 4 / 5 / 6 / 8 / 12 segments gave 0.85 / 0.77 / 0.75 / 0.73 / 0.76 /
-// 0.75 ms, with no spills).  Capping registers for 6 / 7 / 8 blocks per SM
-// (small spills) gave 0.734 / 0.738 / 0.800 ms against 0.738 ms uncapped: the
-// walk is issue-bound, so no cap is set.
+// of walk segments whose gathers are issued together (chosen by measurement
+// on the 512^2 slice with 800 x 609 rays: 2 / 4 / 5 / 6 / 8 / 12 segments gave
+// 0.85 / 0.77 / 0.75 / 0.73 / 0.76 / 0.75 ms, with no spills).  Capping
+// registers for 6 / 7 / 8 blocks per SM (small spills) gave 0.734 / 0.738 /
+// 0.800 ms against 0.738 ms uncapped: the walk is issue-bound, so no cap is
+// set.
 #ifndef VCT_FWD_MINBLOCKS
 #define VCT_FWD_MINBLOCKS 0
 #endif

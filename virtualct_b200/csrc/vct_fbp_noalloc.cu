@@ -9,10 +9,16 @@
 // vct_fbp_dev without any allocation: the caller passes the sinogram and the
 // image (device pointers); the intermediate buffers (weighted and filtered
 // sinograms) and the small per-call tables live in the file-scope device
-// arrays below, which every GPU that loads the library holds until the
-// process exits.
+// arrays below.  A device holds them from the first call on it until the
+// process exits: with CUDA's lazy module loading (the default) the driver
+// allocates them when that first call loads this file's module, so make it at
+// start-up, where an allocation may still fail safely.  Every call shares
+// the arrays, so calls that overlap on the GPU race.
+#include <cuda.h>  // CUresult and CUcontext only: the driver call is looked up through the runtime
 #include <cuda_runtime.h>
 #include <math.h>
+
+#include <mutex>
 
 #include "vct_internal.h"
 
@@ -29,31 +35,74 @@ static __device__ __align__(256) float g_noalloc_kernel[3 * kNoAllocMaxC];  // h
 static __device__ __align__(256) double g_noalloc_coeff[kNoAllocMaxC];     // SID*cos((k-cw)*db)*db
 static __device__ __align__(256) float g_noalloc_cs[2 * kNoAllocMaxV];     // (cos, sin) per view
 
+// Device addresses of the arrays above on one device, valid in the CUDA
+// context whose unique id is ctx_id.
 struct NoAllocPtrs {
   float* weighted;
   float* filtered;
   float* kernel;
   double* coeff;
   float* cs;
+  unsigned long long ctx_id;
   int ready;
 };
-static NoAllocPtrs g_ptrs[64];  // per device; host-side addresses of the arrays above
+static NoAllocPtrs g_ptrs[64];  // per device
+static std::mutex g_ptrs_mutex;  // guards g_ptrs and g_ctx_get_id
+
+// cuCtxGetId (CUDA 12.0+), reached through the runtime so that libvct needs
+// no link against the driver library.
+typedef CUresult (*CtxGetIdFn)(CUcontext, unsigned long long*);
+static CtxGetIdFn g_ctx_get_id = nullptr;
+
+// Unique id of the calling thread's current CUDA context; 0 when none is
+// current yet (the runtime creates the device's primary context at its first
+// call that needs one).
+static int current_context_id(unsigned long long* id) {
+  *id = 0;
+  if (!g_ctx_get_id) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+    cudaError_t e = cudaGetDriverEntryPointByVersion("cuCtxGetId", &fn, 12000, cudaEnableDefault, &q);
+    if (e != cudaSuccess) return cuda_fail(e, "vct_fbp_noalloc: cudaGetDriverEntryPointByVersion(cuCtxGetId)");
+    if (q != cudaDriverEntryPointSuccess || !fn)
+      return fail(VCT_E_CUDA, "vct_fbp_noalloc: the driver has no cuCtxGetId");
+    g_ctx_get_id = (CtxGetIdFn)fn;
+  }
+  if (g_ctx_get_id(nullptr, id) != CUDA_SUCCESS) *id = 0;
+  return VCT_OK;
+}
 
 // Host code cannot use the arrays' names as device addresses; their device
-// addresses come from cudaGetSymbolAddress, once per device, with that device
-// current.
-static int noalloc_setup(int device) {
+// addresses come from cudaGetSymbolAddress, called with the device current.
+// They are looked up at the first call on a device and again whenever the
+// current context is not the one they were looked up in (after
+// cudaDeviceReset, say, when the module is loaded anew at other addresses).
+// The lookup also makes the runtime load this file's module on the device,
+// which is when the driver allocates the arrays.  One lock serialises the
+// set-up of all devices, so concurrent first calls cannot see a half-written
+// entry.
+static int noalloc_setup(int device, NoAllocPtrs* out) {
   if (device < 0 || device >= 64) return fail(VCT_E_ARG, "vct_fbp_noalloc: device index out of range");
+  std::lock_guard<std::mutex> lock(g_ptrs_mutex);
   NoAllocPtrs& p = g_ptrs[device];
-  if (p.ready) return VCT_OK;
-  cudaError_t e;
-  if ((e = cudaGetSymbolAddress((void**)&p.weighted, g_noalloc_weighted)) != cudaSuccess ||
-      (e = cudaGetSymbolAddress((void**)&p.filtered, g_noalloc_filtered)) != cudaSuccess ||
-      (e = cudaGetSymbolAddress((void**)&p.kernel, g_noalloc_kernel)) != cudaSuccess ||
-      (e = cudaGetSymbolAddress((void**)&p.coeff, g_noalloc_coeff)) != cudaSuccess ||
-      (e = cudaGetSymbolAddress((void**)&p.cs, g_noalloc_cs)) != cudaSuccess)
-    return cuda_fail(e, "vct_fbp_noalloc: cudaGetSymbolAddress");
-  p.ready = 1;
+  unsigned long long id = 0;
+  if (int rc = current_context_id(&id)) return rc;
+  if (!p.ready || id == 0 || p.ctx_id != id) {
+    NoAllocPtrs n = {};
+    cudaError_t e;
+    if ((e = cudaGetSymbolAddress((void**)&n.weighted, g_noalloc_weighted)) != cudaSuccess ||
+        (e = cudaGetSymbolAddress((void**)&n.filtered, g_noalloc_filtered)) != cudaSuccess ||
+        (e = cudaGetSymbolAddress((void**)&n.kernel, g_noalloc_kernel)) != cudaSuccess ||
+        (e = cudaGetSymbolAddress((void**)&n.coeff, g_noalloc_coeff)) != cudaSuccess ||
+        (e = cudaGetSymbolAddress((void**)&n.cs, g_noalloc_cs)) != cudaSuccess)
+      return cuda_fail(e, "vct_fbp_noalloc: cudaGetSymbolAddress");
+    // The lookups bound a context to this thread if none was.
+    if (int rc = current_context_id(&n.ctx_id)) return rc;
+    if (n.ctx_id == 0) return fail(VCT_E_CUDA, "vct_fbp_noalloc: no current CUDA context after set-up");
+    n.ready = 1;
+    p = n;
+  }
+  *out = p;
   return VCT_OK;
 }
 
@@ -118,26 +167,25 @@ __global__ void noalloc_tables_kernel(int V, int C, double start_deg, double sid
 
 using namespace vct;
 
-// See include/vct.h.  The first call on a device looks up the scratch
-// arrays' device addresses for it (cudaGetSymbolAddress); make that first
-// call before any stream capture.
+// See include/vct.h.  The first call on a device (and the first after its
+// context was reset) looks up the scratch arrays' device addresses there and
+// may make the driver allocate them; make that call at start-up, before any
+// stream capture.
 extern "C" int vct_fbp_noalloc(const vct_geometry* g, const float* d_sino, int filter, int in_mode, float* d_img,
                                void* stream) {
   if (!g || !d_sino || !d_img) return fail(VCT_E_ARG, "vct_fbp_noalloc: null argument");
   if (filter != 1 && filter != 2) return fail(VCT_E_ARG, "vct_fbp_noalloc: filter must be 1 or 2");
+  if (int rc = check_geometry(g, "vct_fbp_noalloc")) return rc;
   const int C = g->end_channel - g->start_channel, V = g->views, N = g->recon_size;
-  if (C < 3 || g->start_channel < 0 || g->width < g->end_channel || V < 2 || N < 2 || !(g->pixel_cm > 0) ||
-      g->xfactor == 0)
-    return fail(VCT_E_ARG, "vct_fbp_noalloc: geometry out of range");
   if (C > kNoAllocMaxC || V > kNoAllocMaxV || (long long)V * C > kNoAllocMaxVC)
     return fail(VCT_E_ARG,
                 "vct_fbp_noalloc: views*channels above the static scratch limit (views <= 4096, "
                 "channels <= 2048, views*channels <= 1048576)");
   int device = 0;
   VCT_CUDA(cudaGetDevice(&device));
-  int rc = noalloc_setup(device);
+  NoAllocPtrs p;
+  int rc = noalloc_setup(device, &p);
   if (rc) return rc;
-  const NoAllocPtrs& p = g_ptrs[device];
   cudaStream_t st = (cudaStream_t)stream;
   const int n = 2 * C - 1 > V ? 2 * C - 1 : V;
   noalloc_tables_kernel<<<(n + 127) / 128, 128, 0, st>>>(V, C, g->start_view_deg, g->sid_cm, g->max_beta, filter,

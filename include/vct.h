@@ -257,18 +257,23 @@ int vct_fbp_dev(vct_ctx* ctx, const float* d_sino, int filter, int in_mode, floa
  * that cannot allocate device memory at the point where they reconstruct: a
  * process whose device memory is owned by another allocator or a fixed
  * budget, a real-time loop that must not wait on an allocation, library code
- * that may not fail on one.  Same result as vct_fbp_dev, without a context:
- * g gives the geometry, d_sino [views][width] and d_img [N][N] are the
- * caller's device buffers on the current device, stream is a cudaStream_t
- * (NULL: the legacy default stream); the call returns once the work is
- * enqueued.  The intermediate buffers are static device arrays of libvct
- * (about 8 MB, held on every GPU that loads the library until the process
- * exits), limited to views <= 4096, channels <= 2048 and
- * views*channels <= 1048576; larger sizes return
- * VCT_E_ARG.  The first call on a device looks up those arrays' device
- * addresses for it; make it before any stream capture.  All calls share the
- * arrays (each call rewrites every element it reads), so calls that overlap
- * on the GPU -- on different streams, or from several threads -- race. */
+ * that may not fail on one.  The result equals vct_fbp_dev's within the FBP
+ * tolerance (its filter and trig tables are built on the device, in double,
+ * where vct_fbp_dev uploads host-built ones), without a context: g gives the
+ * geometry (the limits of vct_create apply), d_sino [views][width] and d_img
+ * [N][N] are the caller's device buffers on the current device, stream is a
+ * cudaStream_t (NULL: the legacy default stream); the call returns once the
+ * work is enqueued.  The intermediate buffers are static device arrays of
+ * libvct, about 8 MB, limited to views <= 4096, channels <= 2048 and
+ * views*channels <= 1048576; larger sizes return VCT_E_ARG.  The first call
+ * on a device looks up those arrays' device addresses there, and with CUDA's
+ * lazy module loading (the default) that is when the driver allocates them,
+ * so it can fail with VCT_E_NOMEM: make it at start-up, before any stream
+ * capture.  Later calls allocate nothing.  A call made after the device's
+ * context was reset (cudaDeviceReset) repeats that set-up.  All calls share
+ * the arrays (each call rewrites every element it reads), so calls that
+ * overlap on the GPU -- on different streams, or from several threads --
+ * race. */
 int vct_fbp_noalloc(const vct_geometry* g, const float* d_sino, int filter, int in_mode, float* d_img,
                     void* stream);
 /* Beam-hardening correction, MB/beam_hardening_correction.cpp:21-69 (the
@@ -412,16 +417,21 @@ void vct_batch_destroy(vct_batch* b);
 int vct_forward_batched(const vct_job* jobs, int n, int M, int device);
 
 /* ------------------------------------------------------------ inspection */
+/* Per-stage device times (no counterpart in the reference, whose only timers
+ * are the clock() laps of FBP/misc.cpp:196-215).  With on != 0, every later
+ * forward, FBP, FBP transpose and adjoint call on ctx records a CUDA event on
+ * its stream before its first kernel stage and after each stage;
+ * vct_stage_times waits for the last such call's events and returns, for up
+ * to cap stages, the stage names (static strings) and milliseconds, with the
+ * stage count in *n.  Off (the default), nothing is recorded. */
+int vct_set_stage_timing(vct_ctx* ctx, int on);
+int vct_stage_times(vct_ctx* ctx, int cap, const char** names, float* ms, int* n);
 /* Number of in-grid walk segments of the last forward (the algorithmic work
  * unit of the forward kernel). */
 int vct_last_segment_count(vct_ctx* ctx, long long* segments);
 /* Number of kernels this context has launched since creation. */
 long long vct_kernel_launches(vct_ctx* ctx);
 int vct_version(void);
-/* Roofline denominators measured on `device`: L2 read bandwidth (GB/s,
- * ld.global.cg over a 16 MB L2-resident buffer), FP64 and FP32 FMA
- * throughput (TFLOP/s).  Any output pointer may be NULL. */
-int vct_probe_peaks(int device, double* l2_read_gbs, double* fp64_tflops, double* fp32_tflops);
 /* Philox4x32-10 (the noise generator of vct_mbfpa) evaluated on the host,
  * for known-answer tests. */
 void vct_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]);

@@ -27,6 +27,13 @@ int cuda_fail(cudaError_t e, const char* what) {
   set_error(std::string(what) + ": " + cudaGetErrorString(e));
   return e == cudaErrorMemoryAllocation ? VCT_E_NOMEM : VCT_E_CUDA;
 }
+int check_geometry(const vct_geometry* g, const char* who) {
+  const int C = g->end_channel - g->start_channel;
+  if (g->views < 2 || g->views > 100000 || C < 3 || g->start_channel < 0 || g->width < g->end_channel ||
+      g->recon_size < 2 || g->recon_size > 8192 || !(g->pixel_cm > 0) || g->xfactor == 0)
+    return fail(VCT_E_ARG, std::string(who) + ": geometry out of range");
+  return VCT_OK;
+}
 
 // PI as the reference spells it (MB/physParamsTOMO.h:1); rounds to M_PI.
 static const double kPI = 3.141592653589793238462643383279;
@@ -117,9 +124,7 @@ int vct_create(const vct_geometry* g, int device, vct_ctx** out) {
   if (!g || !out) return fail(VCT_E_ARG, "vct_create: null argument");
   *out = nullptr;
   const int C = g->end_channel - g->start_channel;
-  if (g->views < 2 || g->views > 100000 || C < 3 || g->start_channel < 0 || g->width < g->end_channel ||
-      g->recon_size < 2 || g->recon_size > 8192 || !(g->pixel_cm > 0) || g->xfactor == 0)
-    return fail(VCT_E_ARG, "vct_create: geometry out of range");
+  if (int rc = check_geometry(g, "vct_create")) return rc;
   if ((C - 1) / 2 == 0) return fail(VCT_E_ARG, "vct_create: too few channels");
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0)
@@ -420,10 +425,12 @@ static int forward_into(vct_ctx* c, float* d_out, double* d_lint) {
   VCT_CUDA(cudaMemcpyAsync(c->stats.p, c->stats.p + 1, sizeof(FwdStats), cudaMemcpyDeviceToDevice, c->stream));
   if (d_out) VCT_CUDA(cudaMemsetAsync(d_out, 0, nsino * sizeof(float), c->stream));
   const double* mu_tab = c->sum_mode == VCT_SUM_REFERENCE ? c->mu_scaled.p : c->mu_log2.p;
+  c->timer.begin(c->stream);
   int rc = launch_forward(c->dg, c->maps.p, c->M, mu_tab, c->pdf.p, c->NE, c->cos_t.p, c->sin_t.p,
                           c->det_px0.p, c->det_py0.p, c->sum_mode, c->walk_mode == VCT_WALK_FAST, d_out,
                           d_lint, c->stats.p, c->stream);
   if (rc) return rc;
+  c->timer.mark("forward_kernel", c->stream);
   c->launches++;
   return VCT_OK;
 }
@@ -656,15 +663,19 @@ static int fbp_into(vct_ctx* c, const float* d_sino, int filter, int in_mode, fl
   const int V = c->geo.views, C = c->dg.C;
   if ((rc = build_filter(c, filter))) return rc;
   if ((rc = c->fbp_g.ensure((size_t)V * C)) || (rc = c->fbp_q.ensure((size_t)V * C))) return rc;
+  c->timer.begin(c->stream);
   if ((rc = launch_fbp_weight(d_sino, V, c->geo.width, c->geo.start_channel, C, c->fbp_coeff.p, c->fbp_g.p,
                               c->stream, c->bh_alpha, c->bh_beta)))
     return rc;
+  c->timer.mark("fbp_weight_kernel", c->stream);
   if ((rc = launch_fbp_filter(c->fbp_g.p, c->fbp_h[filter].p, c->fbp_h[filter].p + 2 * C - 1, V, C, in_mode,
                               c->fbp_q.p, c->stream)))
     return rc;
+  c->timer.mark("fbp_filter_kernel", c->stream);
   if ((rc = launch_fbp_backproject(c->fbp_q.p, V, C, c->dg.N, c->geo.pixel_cm, c->geo.sid_cm, c->geo.max_beta,
                                    c->geo.xfactor, c->cs_f.p, d_img, c->stream, view_groups, band0, band1)))
     return rc;
+  c->timer.mark("fbp_backproject", c->stream);
   c->launches += 3;
   return VCT_OK;
 }
@@ -957,15 +968,19 @@ int vct_fbp_transpose_dev(vct_ctx* c, const float* d_u, int filter, float* d_lam
   if ((rc = c->fbp_g.ensure((size_t)V * C)) || (rc = c->fbp_q.ensure((size_t)V * C)) ||
       (rc = c->fbp_tacc.ensure(fbp_backproject_t_scratch(V, C, c->dg.N))))
     return rc;
+  c->timer.begin(c->stream);
   if ((rc = launch_fbp_backproject_t(d_u, V, C, c->dg.N, c->geo.pixel_cm, c->geo.sid_cm, c->geo.max_beta,
                                      c->geo.xfactor, c->cs_f.p, c->fbp_tacc.p, c->fbp_q.p, c->stream)))
     return rc;
+  c->timer.mark("fbp_backproject_t", c->stream);
   if ((rc = launch_fbp_filter_t(c->fbp_q.p, c->fbp_h[filter].p, c->fbp_h[filter].p + 2 * C - 1, V, C, c->fbp_g.p,
                                 c->stream)))
     return rc;
+  c->timer.mark("fbp_filter_t", c->stream);
   if ((rc = launch_fbp_weight_t(c->fbp_g.p, V, c->geo.width, c->geo.start_channel, C, c->fbp_coeff.p, d_lam,
                                 c->stream)))
     return rc;
+  c->timer.mark("fbp_weight_t", c->stream);
   c->launches += 3;
   return VCT_OK;
 }
@@ -981,6 +996,30 @@ int vct_fbp_transpose(vct_ctx* c, const float* u, int filter, float* lam) {
   if ((rc = vct_fbp_transpose_dev(c, c->fbp_img.p, filter, c->fbp_sino.p))) return rc;
   VCT_CUDA(cudaMemcpyAsync(lam, c->fbp_sino.p, nsino * sizeof(float), cudaMemcpyDeviceToHost, c->stream));
   VCT_CUDA(cudaStreamSynchronize(c->stream));
+  return VCT_OK;
+}
+
+int vct_set_stage_timing(vct_ctx* c, int on) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (on && !c->timer.ev[0])
+    for (cudaEvent_t& e : c->timer.ev) VCT_CUDA(cudaEventCreate(&e));
+  c->timer.on = on != 0;
+  c->timer.n = 0;
+  return VCT_OK;
+}
+
+int vct_stage_times(vct_ctx* c, int cap, const char** names, float* ms, int* n) {
+  int rc = check_ctx(c);
+  if (rc) return rc;
+  if (!n || (cap > 0 && (!names || !ms))) return fail(VCT_E_ARG, "vct_stage_times: null argument");
+  if (!c->timer.on) return fail(VCT_E_STATE, "vct_stage_times: stage timing is off (vct_set_stage_timing)");
+  *n = c->timer.n;
+  if (c->timer.n > 0) VCT_CUDA(cudaEventSynchronize(c->timer.ev[c->timer.n]));
+  for (int i = 0; i < c->timer.n && i < cap; i++) {
+    names[i] = c->timer.name[i];
+    VCT_CUDA(cudaEventElapsedTime(&ms[i], c->timer.ev[i], c->timer.ev[i + 1]));
+  }
   return VCT_OK;
 }
 
@@ -1066,6 +1105,7 @@ static int adj_run(vct_ctx* c, int mode, const float* d_meas, const float* d_wts
   const long long nrays = (long long)dg.views_used * dg.C;
   const size_t n2 = (size_t)dg.N * dg.N;
   const float* d_g = d_g_in;
+  c->timer.begin(c->stream);
   VCT_CUDA(cudaMemsetAsync(c->adj_gmax.p, 0, sizeof(unsigned int), c->stream));
   if (!d_g) {
     if (!c->maps_ready || !c->spectrum_ready) return fail(VCT_E_STATE, "adjoint: maps or spectrum not set");
@@ -1074,12 +1114,14 @@ static int adj_run(vct_ctx* c, int mode, const float* d_meas, const float* d_wts
                                  c->det_px0.p, c->det_py0.p, c->adj_rec.p, mode, d_meas, d_wts, c->adj_g.p,
                                  c->adj_part.p, c->adj_gmax.p, c->stream)))
       return rc;
+    c->timer.mark("adj_forward_kernel", c->stream);
     c->launches++;
     d_g = c->adj_g.p;
     if (mode == 0) {
       if ((rc = launch_adj_loss(c->adj_part.p, adj_forward_blocks(dg), d_loss ? d_loss : c->adj_loss.p,
                                 c->stream)))
         return rc;
+      c->timer.mark("adj_loss_kernel", c->stream);
       c->launches++;
     }
   } else if (c->adj_nspecial > 0) {
@@ -1097,13 +1139,17 @@ static int adj_run(vct_ctx* c, int mode, const float* d_meas, const float* d_wts
                                  c->adj_ints.p, c->adj_nspecial, d_g, c->adj_gmax.p, c->ag.lmax, c->ag.log2_terms,
                                  c->adj_sacc.p, c->stream)))
       return rc;
+    c->timer.mark("adj_special_kernel", c->stream);
     c->launches++;
     sacc = c->adj_sacc.p;
   }
   if ((rc = c->adj_ext.ensure((size_t)M * (dg.N + 1) * (dg.N + 1)))) return rc;
-  if ((rc = launch_adj_gather(c->ag, M, c->adj_tile, c->cos_t.p, c->sin_t.p, c->adj_dir.p, c->adj_rec.p, d_g, sacc,
-                              c->adj_gmax.p, c->adj_ext.p, d_grad, c->adj_ints.p + 1, c->stream)))
+  if ((rc = launch_adj_gather(c->ag, M, c->adj_tile, c->cos_t.p, c->sin_t.p, c->adj_dir.p, c->adj_rec.p, d_g,
+                              c->adj_ext.p, c->adj_ints.p + 1, c->stream)))
     return rc;
+  c->timer.mark("adj_gather_kernel", c->stream);
+  if ((rc = launch_adj_fold(c->ag, M, sacc, c->adj_gmax.p, c->adj_ext.p, d_grad, c->stream))) return rc;
+  c->timer.mark("adj_fold_kernel", c->stream);
   c->launches += 2;
   return VCT_OK;
 }

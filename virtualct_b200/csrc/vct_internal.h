@@ -13,6 +13,10 @@ namespace vct {
 void set_error(const std::string& msg);
 int fail(int code, const std::string& msg);
 int cuda_fail(cudaError_t e, const char* what);
+// The geometry limits every entry point that takes a vct_geometry applies
+// (views, channels, grid size, pixel size, xfactor); `who` prefixes the
+// error message.  Returns VCT_OK or VCT_E_ARG.
+int check_geometry(const vct_geometry* g, const char* who);
 
 #define VCT_CUDA(call)                                     \
   do {                                                     \
@@ -212,7 +216,11 @@ int adj_pick_tile(const AdjGeom& a, double lim);
 // [M][N][N] together with the exact-walk rays' fixed-point sums (d_sacc may
 // be NULL).  Two launches.
 int launch_adj_gather(const AdjGeom& a, int M, int tile, const double* d_cos, const double* d_sin,
-                      const double2* d_dir, const int4* d_rec, const float* d_g, const unsigned long long* d_sacc,
-                      const unsigned int* d_gmax, float* d_ext, float* d_grad, int* d_status, cudaStream_t st);
+                      const double2* d_dir, const int4* d_rec, const float* d_g, float* d_ext, int* d_status,
+                      cudaStream_t st);
+// Cells at index -1 onto index 0 and the exact-walk rays' fixed-point sums
+// added: d_ext [M][N+1][N+1] -> d_grad [M][N][N].
+int launch_adj_fold(const AdjGeom& a, int M, const unsigned long long* d_sacc, const unsigned int* d_gmax,
+                    const float* d_ext, float* d_grad, cudaStream_t st);
 
 }  // namespace vct

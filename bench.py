@@ -37,10 +37,22 @@ V, C, N, PIX = 800, 609, 512, 0.1
 SIGMA = 0.0000537  # txt field "Photon noise in detector" of the shipped 120 kV input
 SPECTRUM = os.path.join(ROOT, "tests", "golden", "kramers_120kvp.txt")
 METRIC = "MBFPA rays*bins/s (FBP slices/s alongside)"
-# DRAM bytes (read + write) of one forward_kernel launch on this workload,
-# from one ncu capture: the two map copies once; the gathers hit L1/L2.
-FWD_DRAM_BYTES = 8581888
+# From one ncu capture of forward_kernel<6, COMPENSATED> on this workload
+# (C1, 512^2, 800 x 609, 110 bins; `ncu --set full --clock-control none -k
+# regex:forward_kernel -s 3 -c 1` of `python bench.py --steps 2 --warmup 3
+# --no-cpu-baseline --no-extras`): DRAM bytes read + written per launch (the two
+# map copies once; the gathers hit L1/L2) and warp instructions executed per
+# launch.  Not measured by the run that prints them.
+FWD_CAPTURE = {"dram_bytes": 8581888, "warp_instructions": 3.24e8,
+               "source": "ncu capture of forward_kernel<6,0> (Siddon event loop in FP64, 6 gathers in flight), "
+                         "commit 104c45c"}
 CONFIG_NAME = "plain MBFPA+FBP single slice: 512^2, 6 elements, 800 views x 609 channels, 120 kVp Kramers 110 bins"
+# mask pixels of the 512^2 reconstruction circle (FBP/misc.cpp:9-37)
+MASK_PX = 205012
+# FP32 operations per backprojection update (rotation 6, L^2 4, fan angle 3,
+# channel 2, interpolation 3, weight and sum 4; plus one arctangent and one
+# reciprocal), FBP/reconstructImageTOMO.cpp:67-93
+BP_FLOP_PER_UPDATE = 22
 
 
 def load_inputs(seed: int):
@@ -50,6 +62,44 @@ def load_inputs(seed: int):
     mu, pdf = vct.attenuation_coefficient(SPECTRUM)
     maps = phantoms.ellipse_phantom(seed, N)
     return maps, mu, pdf
+
+
+def phantoms_module():
+    """virtualct_b200/phantoms.py (numpy only) loaded on its own, so that the
+    reference arm never loads the package or its library."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("vct_phantoms_standalone",
+                                                  os.path.join(ROOT, "virtualct_b200", "phantoms.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def cpu_model() -> str:
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
+def probe_peaks(device: int) -> dict:
+    """Live roofline denominators from lib/libvct_peaks.so (bench-only probes,
+    not the product library): L2 read bandwidth, FP64 and FP32 FMA rate."""
+    import ctypes
+
+    L = ctypes.CDLL(os.path.join(ROOT, "virtualct_b200", "lib", "libvct_peaks.so"))
+    L.vct_probe_peaks.argtypes = [ctypes.c_int] + [ctypes.POINTER(ctypes.c_double)] * 3
+    L.vct_peaks_error.restype = ctypes.c_char_p
+    l2, f64, f32 = ctypes.c_double(0), ctypes.c_double(0), ctypes.c_double(0)
+    rc = L.vct_probe_peaks(device, ctypes.byref(l2), ctypes.byref(f64), ctypes.byref(f32))
+    if rc != 0:
+        raise RuntimeError(f"vct_probe_peaks: {L.vct_peaks_error().decode()}")
+    return {"l2_read_gbs": l2.value, "fp64_tflops": f64.value, "fp32_tflops": f32.value}
 
 
 class ClockSampler:
@@ -115,6 +165,59 @@ def reduce_max(x: float, dist, device) -> float:
     return float(t.item())
 
 
+def stage_medians(ctx, fn, reps):
+    """Per-stage device times of fn() (vct_set_stage_timing: CUDA events on the
+    context's stream around each kernel stage), median over reps calls made
+    after the timed regions."""
+    ctx.set_stage_timing(True)
+    runs = []
+    for _ in range(reps):
+        fn()
+        runs.append(ctx.stage_times())
+    ctx.set_stage_timing(False)
+    names = [n for n, _ in runs[-1]]
+    return {n: statistics.median(r[i][1] for r in runs if len(r) > i) for i, n in enumerate(names)}
+
+
+def issue_roofline(warp_inst, t_launch, clocks, dev):
+    """Instruction-issue axis of a kernel: warp instructions per launch (from
+    an ncu capture) over the launch time, against one warp instruction per
+    clock per SM sub-partition (4 per SM) at the median SM clock sampled under
+    load."""
+    import torch
+
+    sms = torch.cuda.get_device_properties(dev).multi_processor_count
+    mhz = clocks.get("sm_mhz") or clocks.get("sm_max_mhz") or 1965.0
+    peak = 4.0 * sms * mhz * 1e6
+    achieved = warp_inst / t_launch
+    return {"achieved": achieved, "peak": peak, "unit": "warp instructions/s", "frac": achieved / peak,
+            "warp_instructions_per_launch": warp_inst, "sm_mhz": mhz,
+            "source": "warp instructions: " + FWD_CAPTURE["source"]}
+
+
+def fbp_roofline(stages, views, channels, mask_px, peaks):
+    """Rooflines of the FBP's two compute kernels from their live stage times:
+    the filter against the FP32 FMA peak (2 V C^2 FLOP, the reference's dense
+    609-tap convolution per sample) and the backprojection against the same
+    peak at BP_FLOP_PER_UPDATE per (mask pixel, view) update."""
+    used = views // 2 * 2
+    out = {"stages_ms": stages}
+    t_f = stages.get("fbp_filter_kernel")
+    t_b = stages.get("fbp_backproject")
+    if t_f:
+        fl = 2.0 * views * channels * channels
+        out["filter"] = {"bound": "fp32", "achieved": fl / t_f / 1e9, "peak": peaks["fp32_tflops"], "unit": "TFLOP/s",
+                         "frac": fl / t_f / 1e9 / peaks["fp32_tflops"], "flop_per_launch": fl, "launch_ms": t_f}
+    if t_b:
+        upd = float(mask_px) * used
+        fl = upd * BP_FLOP_PER_UPDATE
+        out["backprojection"] = {"bound": "fp32", "achieved": fl / t_b / 1e9, "peak": peaks["fp32_tflops"],
+                                 "unit": "TFLOP/s", "frac": fl / t_b / 1e9 / peaks["fp32_tflops"],
+                                 "updates_per_launch": upd, "updates_per_s": upd / t_b * 1e3,
+                                 "flop_per_update": BP_FLOP_PER_UPDATE, "launch_ms": t_b}
+    return out
+
+
 def replica_inputs(rank: int):
     """Each rank projects its own slice: the phantom seed is the rank."""
     return load_inputs(seed=rank)
@@ -178,21 +281,31 @@ def run_ours(args, rank, world, dist):
 
     barrier()
     t_fbp = max_over_ranks(timed(fbp_step, args.steps))
+    fbp_stages = stage_medians(ctx, fbp_step, max(args.warmup, 5))
 
     # Dominant kernel alone (forward walk + spectral epilogue): per-launch
     # device time for the roofline, same flush discipline.
     barrier()
     t_fwd = max_over_ranks(timed(lambda: ctx.forward_dev(d_sino), args.steps)) / args.steps
+    # Algorithmic work unit: the reference walk's in-grid segments, counted by
+    # one forward in exact-walk mode (outside every timed region).
+    ctx.set_walk_mode(vct.WALK_EXACT)
+    ctx.forward_dev(d_sino)
+    segments = ctx.last_segment_count
+    ctx.set_walk_mode(vct.WALK_FAST)
     extras = {}
     if rank == 0:
         extras["parity"] = parity_vs_reference(ctx, d_sino, d_img)
     want = set() if args.no_extras or world > 1 else set(args.extras.split(","))
+    if "c2" in want:
+        extras["c2"] = bench_c2(stream, timed, args.steps, args.warmup)
     if "adjoint" in want:
-        extras["adjoint"] = bench_adjoint(ctx, d_maps, mu, pdf, stream, timed, args.steps, args.warmup)
+        extras["adjoint"] = bench_adjoint(ctx, d_maps, mu, pdf, stream, timed, args.steps, args.warmup, segments,
+                                          dev)
     if "lengthproj" in want:
         extras["lengthproj"] = bench_lengthproj(ctx, stream, timed, args.steps, args.warmup)
     if "fbp_transpose" in want:
-        extras["fbp_transpose"] = bench_fbp_transpose(ctx, stream, timed, args.steps, args.warmup)
+        extras["fbp_transpose"] = bench_fbp_transpose(ctx, stream, timed, args.steps, args.warmup, dev)
     if "batched" in want:
         extras["batched"] = bench_batched(stream, args.warmup, n=args.batch_slices)
     if "scale" in want:
@@ -200,12 +313,6 @@ def run_ours(args, rank, world, dist):
     if "batched_adjoint" in want:
         extras["batched_adjoint"] = bench_batched_adjoint(stream, args.warmup, n=max(args.batch_slices // 4, 1))
     clk.__exit__(None, None, None)
-    # Algorithmic work unit: the reference walk's in-grid segments, counted by
-    # one forward in exact-walk mode (outside every timed region).
-    ctx.set_walk_mode(vct.WALK_EXACT)
-    ctx.forward_dev(d_sino)
-    segments = ctx.last_segment_count
-    ctx.set_walk_mode(vct.WALK_FAST)
 
     # End to end through the public API with host buffers: every step's maps
     # go host->device from pinned memory and every noisy sinogram comes back
@@ -239,7 +346,8 @@ def run_ours(args, rank, world, dist):
         return None
     units = V * C * NE  # rays * bins per slice
     value = units * world * args.steps / t_mb
-    peaks = vct.probe_peaks(dev)
+    peaks = probe_peaks(dev)
+    clocks = clk.summary()
     meas_path = os.path.join(ROOT, "MEASURED_PEAKS.json")
     measured = json.load(open(meas_path)) if os.path.exists(meas_path) else {}
     M = maps.shape[0]
@@ -266,7 +374,8 @@ def run_ours(args, rank, world, dist):
                    "parallelism": f"replicas x{world}" if world > 1 else "single GPU",
                    "l2": "flushed (256 MB write) before every timed step"},
         "fbp": {"metric": "FBP slices/s", "value": world * args.steps / t_fbp, "unit": "slices/s",
-                "ms_per_slice": t_fbp / args.steps * 1e3, "filter": "Ram-Lak"},
+                "ms_per_slice": t_fbp / args.steps * 1e3, "filter": "Ram-Lak",
+                "roofline": fbp_roofline(fbp_stages, V, C, MASK_PX, peaks)},
         "pipeline_ms_per_slice": (t_mb + t_fbp) / args.steps * 1e3,
         "e2e": {"value": units * world * args.steps / t_e2e, "unit": "rays*bins/s",
                 "h2d_bytes_per_step": int(maps.nbytes), "d2h_bytes_per_step": int(V * C * 4),
@@ -280,10 +389,10 @@ def run_ours(args, rank, world, dist):
             "peak": peaks["l2_read_gbs"],
             "unit": "GB/s",
             "frac": achieved / peaks["l2_read_gbs"],
-            "traffic": FWD_DRAM_BYTES,
-            "traffic_source": "ncu dram__bytes_read.sum + dram__bytes_write.sum, one forward_kernel launch "
-                              "(profiles/forward_kernel_c1_512_800x609.md)",
-            "peak_source": "measured live: vct_probe_peaks L2 read (ld.global.cg, 16 MB resident)",
+            "traffic": FWD_CAPTURE["dram_bytes"],
+            "traffic_source": "dram__bytes_read.sum + dram__bytes_write.sum per launch, " + FWD_CAPTURE["source"],
+            "peak_source": "measured live: libvct_peaks L2 read probe (ld.global.cg, 16 MB resident)",
+            "issue": issue_roofline(FWD_CAPTURE["warp_instructions"], t_fwd, clocks, dev),
             "algorithmic_bytes_per_launch": int(alg_bytes),
             "segments_per_launch": int(segments),
             "segments_visited_per_launch": int(segments_visited),
@@ -293,7 +402,7 @@ def run_ours(args, rank, world, dist):
                      "frac": fp64_flops / t_fwd / 1e12 / peaks["fp64_tflops"]},
             "fp32_peak_tflops": peaks["fp32_tflops"],
         },
-        "clocks": clk.summary(),
+        "clocks": clocks,
     }
     line.update(extras)
     if world == 1 and not args.no_cpu_baseline:
@@ -329,18 +438,75 @@ def parity_vs_reference(ctx, d_sino, d_img):
     step = N // d["fbp_ramlak_rows"].shape[0]
     img = d_img.cpu().numpy()[::step].astype(np.float64)
     fref = d["fbp_ramlak_rows"].astype(np.float64)
-    return {
+    f64img = d["fbp_ramlak_fp64_rows"].astype(np.float64)
+    out_line = {
         "forward_vs_reference_max_rel": float(np.max(np.abs(out[ok] - ref[ok]) / ref[ok])),
         "forward_vs_fp64_max_rel": float(np.max(np.abs(out - f64) / f64)),
         "reference_vs_fp64_max_rel": float(np.max(np.abs(ref - f64) / f64)),
         "forward_tolerance": 1e-5,
-        "fbp_vs_reference_max_abs_over_max": float(np.abs(img - fref).max() / np.abs(fref).max()),
-        "fbp_vs_reference_l2_rel": float(np.linalg.norm(img - fref) / np.linalg.norm(fref)),
+        "fbp_vs_reference_max_abs_over_max": _max_abs_over_max(img, fref),
+        "fbp_vs_reference_l2_rel": _l2_rel(img, fref),
+        "fbp_vs_fp64_max_abs_over_max": _max_abs_over_max(img, f64img),
+        "fbp_vs_fp64_l2_rel": _l2_rel(img, f64img),
+        "reference_fbp_vs_fp64_max_abs_over_max": _max_abs_over_max(fref, f64img),
         "fbp_tolerance": 1e-4,
         "what": "forward: un-normalised polyenergetic sinogram, every 20th view (40 x 609); fbp: Ram-Lak image of "
                 "the noise-free normalised sinogram, every 16th row (32 x 512); references from the reference "
-                "compiled from its sources and the FP64 oracle",
+                "compiled from its sources and the FP64 oracle (FBP with every sum in FP64)",
     }
+    out_line["shipped"] = parity_shipped()
+    return out_line
+
+
+def _max_abs_over_max(a, ref):
+    a, ref = np.asarray(a, np.float64), np.asarray(ref, np.float64)
+    return float(np.abs(a - ref).max() / np.abs(ref).max())
+
+
+def _l2_rel(a, ref):
+    a, ref = np.asarray(a, np.float64), np.asarray(ref, np.float64)
+    return float(np.linalg.norm(a - ref) / np.linalg.norm(ref))
+
+
+def parity_shipped():
+    """The device path on the reference's shipped inputs (fixtures from the
+    reference compiled from its sources): the ICRU-110 phantom with the
+    shipped 100-bin 120 kV and 650-bin 6 MV spectra (noise-free forward,
+    every 20th view) and the shipped human FBP case (Shepp-Logan, every 8th
+    row), each against the reference and the FP64 oracle."""
+    import torch
+
+    import virtualct_b200 as vct
+
+    res = {}
+    path = os.path.join(ROOT, "tests", "golden", "icru_shipped.npz")
+    if os.path.exists(path):
+        d = np.load(path)
+        rows = d["rows"]
+        with vct.Context(vct.Geometry()) as c2:
+            c2.set_maps(d["maps"])
+            for name in ("kv120", "mv6"):
+                c2.set_spectrum(d[f"{name}_mu"], d[f"{name}_pdf"])
+                out = c2.forward()[rows].astype(np.float64)
+                ref, f64 = d[f"{name}_rows"].astype(np.float64), d[f"{name}_fp64_rows"]
+                res[f"icru110_{name}"] = {
+                    "bins": int(len(d[f"{name}_pdf"])),
+                    "forward_vs_reference_max_rel": float(np.max(np.abs(out - ref) / ref)),
+                    "forward_vs_fp64_max_rel": float(np.max(np.abs(out - f64) / f64)),
+                    "reference_vs_fp64_max_rel": float(np.max(np.abs(ref - f64) / f64))}
+    path = os.path.join(ROOT, "tests", "golden", "fbp_human.npz")
+    if os.path.exists(path):
+        d = np.load(path)
+        with vct.Context(vct.Geometry()) as c2:
+            img = c2.fbp(d["sino"], int(d["filter"]))[d["rows"]]
+        res["human_fbp_shepp_logan"] = {
+            "vs_reference_max_abs_over_max": _max_abs_over_max(img, d["golden_rows"]),
+            "vs_reference_l2_rel": _l2_rel(img, d["golden_rows"]),
+            "vs_fp64_max_abs_over_max": _max_abs_over_max(img, d["fp64_rows"]),
+            "vs_fp64_l2_rel": _l2_rel(img, d["fp64_rows"]),
+            "reference_vs_fp64_max_abs_over_max": _max_abs_over_max(d["golden_rows"], d["fp64_rows"])}
+    torch.cuda.synchronize()
+    return res
 
 
 # ------------------------------------------------ adjoint and batched lines
@@ -360,7 +526,7 @@ def _event_ms(stream, fn, reps):
     return best
 
 
-def bench_adjoint(ctx, d_maps, mu, pdf, stream, timed, steps, warmup):
+def bench_adjoint(ctx, d_maps, mu, pdf, stream, timed, steps, warmup, segments, dev):
     """Loss + gradient at 512^2, 6 elements, 120 kVp, 800 x 609 (the adjoint
     configuration): measured sinogram = the noisy MBFPA of the phantom, the
     gradient taken at densities x 0.97.  One step = vct_forward_adjoint_dev
@@ -385,13 +551,81 @@ def bench_adjoint(ctx, d_maps, mu, pdf, stream, timed, steps, warmup):
     for _ in range(warmup):
         g_fn()
     t_g = timed(g_fn, steps) / steps
+    stages = stage_medians(ctx, fn, max(warmup, 5))
     ctx.set_maps(d_maps)
     NE = len(pdf)
+    peaks = probe_peaks(dev)
+    # A^T moves the forward's data the other way: one ray factor per
+    # (segment, element) meets one map cell.  Its unit is the forward's gather
+    # bytes, S*M*2 + V*C*4 per launch.
+    alg = segments * int(d_maps.shape[0]) * 2 + V * C * 4
+    t_gk = stages.get("adj_gather_kernel")
+    roof = {"stages_ms": stages}
+    if t_gk:
+        roof.update({"kernel": "adj_gather_kernel", "bound": "l2", "achieved": alg / t_gk / 1e6,
+                     "peak": peaks["l2_read_gbs"], "unit": "GB/s", "frac": alg / t_gk / 1e6 / peaks["l2_read_gbs"],
+                     "algorithmic_bytes_per_launch": int(alg), "launch_ms": t_gk,
+                     "unit_note": "the forward's gather bytes S*M*2 + V*C*4 (S: the walk's segments)"})
     return {"workload": "loss + dl/drho: 512^2, 6 elements, 120 kVp 110 bins, 800 views x 609 channels",
             "ms_per_gradient": t * 1e3, "rays_bins_per_s": V * C * NE / t,
             "gather_ms": t_g * 1e3, "gather_pixel_views_per_s": N * N * V / t_g,
-            "kernels_per_gradient": int(launches), "loss": float(loss.item()),
+            "kernels_per_gradient": int(launches), "loss": float(loss.item()), "roofline": roof,
             "notes": "deterministic: pixel-driven A^T, no float atomics"}
+
+
+def bench_c2(stream, timed, steps, warmup):
+    """The 6 MV configuration: 512^2 at 0.1 cm, 8 elements (H C N O P Ca Mg
+    Si), the seeded 33 cm cylinder with 16 inserts (tests/golden/c2_subset.npz's
+    slice), the synthetic 60-bin 6 MV spectrum, 800 x 609: MBFPA (noise) and
+    the Shepp-Logan FBP per slice, L2 flushed before every step; the forward
+    kernel's gather-byte roofline; parity against the fixture."""
+    import torch
+
+    import virtualct_b200 as vct
+    from virtualct_b200 import phantoms
+
+    d = np.load(os.path.join(ROOT, "tests", "golden", "c2_subset.npz"))
+    maps = phantoms.gammex_cylinder_phantom(int(d["seed"]), N)
+    mu, pdf = d["mu"], d["pdf"]
+    NE, M = len(pdf), maps.shape[0]
+    sino = torch.empty((V, C), dtype=torch.float32, device="cuda")
+    img = torch.empty((N, N), dtype=torch.float32, device="cuda")
+    with vct.Context(vct.Geometry()) as c2:
+        c2.set_stream(stream.cuda_stream)
+        c2.set_maps(torch.from_numpy(maps).cuda())
+        c2.set_spectrum(mu, pdf)
+        step = lambda: c2.mbfpa_dev(SIGMA, 3, sino)  # noqa: E731
+        fstep = lambda: c2.fbp_dev(sino, img, 2)  # noqa: E731
+        for _ in range(warmup):
+            step()
+            fstep()
+        t_mb = timed(step, steps) / steps
+        t_fbp = timed(fstep, steps) / steps
+        t_fwd = timed(lambda: c2.forward_dev(sino), steps) / steps
+        out = torch.empty_like(sino)
+        c2.forward_dev(out)
+        c2.synchronize()
+        rows = d["rows"]
+        o = out.cpu().numpy()[rows].astype(np.float64)
+        c2.set_walk_mode(vct.WALK_EXACT)
+        c2.forward_dev(out)
+        c2.synchronize()
+        segments = c2.last_segment_count
+        c2.set_walk_mode(vct.WALK_FAST)
+    peaks = probe_peaks(torch.cuda.current_device())
+    alg = segments * M * 2 + V * C * 4
+    ref, f64 = d["full_rows"].astype(np.float64), d["fp64_rows"]
+    return {"workload": "6 MV: 512^2, 8 elements, 16-insert cylinder (seed %d), 800 views x 609 channels, "
+                        "synthetic 6 MV 60 bins; MBFPA + noise, Shepp-Logan FBP" % int(d["seed"]),
+            "value": V * C * NE / t_mb, "unit": "rays*bins/s", "ms_per_slice": t_mb * 1e3,
+            "fbp_slices_per_s": 1.0 / t_fbp, "fbp_ms_per_slice": t_fbp * 1e3,
+            "roofline": {"kernel": "forward_kernel<8>", "bound": "l2", "achieved": alg / t_fwd / 1e9,
+                         "peak": peaks["l2_read_gbs"], "unit": "GB/s", "frac": alg / t_fwd / 1e9 / peaks["l2_read_gbs"],
+                         "algorithmic_bytes_per_launch": int(alg), "segments_per_launch": int(segments),
+                         "launch_ms": t_fwd * 1e3},
+            "parity": {"forward_vs_oracle_max_rel": float(np.max(np.abs(o - ref) / ref)),
+                       "forward_vs_fp64_max_rel": float(np.max(np.abs(o - f64) / f64))},
+            "l2": "flushed (256 MB write) before every timed step"}
 
 
 def bench_lengthproj(ctx, stream, timed, steps, warmup):
@@ -410,7 +644,7 @@ def bench_lengthproj(ctx, stream, timed, steps, warmup):
             "ms_per_slice": t * 1e3, "pixel_views_per_s": mask_px * V / t}
 
 
-def bench_fbp_transpose(ctx, stream, timed, steps, warmup):
+def bench_fbp_transpose(ctx, stream, timed, steps, warmup, dev):
     """The FBP transpose (backprojection gather, transposed filter and
     weight) of an image-space gradient at 512^2 -> 800 x 609."""
     import torch
@@ -421,8 +655,19 @@ def bench_fbp_transpose(ctx, stream, timed, steps, warmup):
     for _ in range(warmup):
         fn()
     t = timed(fn, steps) / steps
+    stages = stage_medians(ctx, fn, max(warmup, 5))
+    peaks = probe_peaks(dev)
+    roof = {"stages_ms": stages}
+    t_b = stages.get("fbp_backproject_t")
+    if t_b:
+        upd = float(MASK_PX) * (V // 2 * 2)
+        fl = upd * BP_FLOP_PER_UPDATE
+        roof.update({"kernel": "fbp_bp_t_scatter_kernel (+ max|u|, transpose, finish)", "bound": "fp32",
+                     "achieved": fl / t_b / 1e9, "peak": peaks["fp32_tflops"], "unit": "TFLOP/s",
+                     "frac": fl / t_b / 1e9 / peaks["fp32_tflops"], "updates_per_launch": upd,
+                     "updates_per_s": upd / t_b * 1e3, "flop_per_update": BP_FLOP_PER_UPDATE, "launch_ms": t_b})
     return {"workload": "W^T F^T B^T u: 512^2 image-space gradient -> 800 x 609 (Ram-Lak)",
-            "ms_per_slice": t * 1e3, "slices_per_s": 1.0 / t}
+            "ms_per_slice": t * 1e3, "slices_per_s": 1.0 / t, "roofline": roof}
 
 
 def _batch_inputs(n, seed, kvps_tabs):
@@ -606,19 +851,27 @@ def cpu_baseline(maps, mu, pdf):
     if O.ref_available():
         O.ref_reprojection(N, PIX, rho, V, C, c, s, 1, mu, pdf, ke0=0, ke1=1, threads=cores)  # cold tables
         _, secs = O.ref_reprojection(N, PIX, rho, V, C, c, s, 1, mu, pdf, ke0=50, ke1=52, threads=cores)
-        return {"value": V * C * 2 / secs, "unit": "rays*bins/s", "cores": cores, "kind": "reference",
-                "sample": "reprojection_TOMO for 2 energy bins x 800 views x 609 channels", "seconds": secs}
+        return {"value": V * C * 2 / secs, "unit": "rays*bins/s", "cores": cores, "cpu_model": cpu_model(),
+                "kind": "reference", "sample": "reprojection_TOMO for 2 energy bins x 800 views x 609 channels",
+                "seconds": secs}
     g = O.geom()
     t0 = time.perf_counter()
     O.forward_exact(g, c, s, rho, np.ascontiguousarray(mu[:, 50:52]), pdf[50:52].copy(), nthreads=cores)
     secs = time.perf_counter() - t0
-    return {"value": V * C * 2 / secs, "unit": "rays*bins/s", "cores": cores, "kind": "port",
+    return {"value": V * C * 2 / secs, "unit": "rays*bins/s", "cores": cores, "cpu_model": cpu_model(), "kind": "port",
             "sample": "oracle forward (reference order) for 2 energy bins x 800 views x 609 channels",
             "seconds": secs}
 
 
 # ----------------------------------------------------------- reference arm
 def run_reference(args, rank):
+    """The reference's own CPU code on the host cores, for this arm's config:
+    reprojection_TOMO (MB/reprojection_TOMO.cpp:13, compiled from its sources
+    into oracle/_ref/libvct_ref_mb.so with its own OpenMP) with the reference's
+    own attenuation_coefficient (MB/prior_weight_production.cpp:180) for mu and
+    pdf, and filterSinogram + reconstructImage as shipped (single thread).  The
+    phantom comes from phantoms.py loaded on its own: nothing of the product
+    library is loaded in this process."""
     if rank != 0:
         return None
     import oracle as O
@@ -626,30 +879,29 @@ def run_reference(args, rank):
     if not O.ref_available():
         return {"impl": "reference", "unavailable": "oracle/_ref not built (reference sources absent at build time)"}
     cores = os.cpu_count() or 1
-    maps, mu, pdf = load_inputs(seed=0)
+    pdf, mu = O.ref_attenuation(SPECTRUM)
+    maps = phantoms_module().ellipse_phantom(0, N)
     NE = len(pdf)
     rho = O.rho_from_maps(maps)
     c, s = O.trig_tables(V)
-    # One step = reprojection_TOMO (the reference walks every ray once per
-    # energy bin, MB/main.cpp:492-506) for one bin over one block of 40 of the
-    # 800 views, cycling through blocks and bins; the per-ray work is that of
-    # the full sinogram.
-    VB = 40
 
+    # One step = one reprojection_TOMO call: one energy bin over the whole
+    # 800 x 609 sinogram (the reference walks every ray once per bin,
+    # MB/main.cpp:492-506), cycling through the bins; a slice is NE steps.
     def ref_step(k):
-        b, ke = k % (V // VB), (50 + k) % NE
-        cs, sn = np.ascontiguousarray(c[b * VB:(b + 1) * VB]), np.ascontiguousarray(s[b * VB:(b + 1) * VB])
-        _, secs = O.ref_reprojection(N, PIX, rho, VB, C, cs, sn, 1, mu, pdf, ke0=ke, ke1=ke + 1, threads=cores)
+        ke = (50 + k) % NE
+        _, secs = O.ref_reprojection(N, PIX, rho, V, C, c, s, 1, mu, pdf, ke0=ke, ke1=ke + 1, threads=cores)
         return secs
 
     for w in range(max(args.warmup, 1)):
         ref_step(w)
     total = sum(ref_step(k) for k in range(args.steps))
-    value = VB * C * args.steps / total
+    value = V * C * args.steps / total
     # FBP as shipped: single-threaded filterSinogram + reconstructImage, once.
     full, _ = O.ref_reprojection(N, PIX, rho, V, C, c, s, 1, mu, pdf, ke0=0, ke1=1, threads=cores)
     sino = (full / full.max()).astype(np.float32)
     _, _, tf, tb = O.ref_fbp(1, sino, N, PIX, 1, c, s)
+    sample = f"reprojection_TOMO, one energy bin x {V} views x {C} channels per step ({NE} steps per slice)"
     return {
         "impl": "reference",
         "metric": METRIC,
@@ -659,7 +911,7 @@ def run_reference(args, rank):
         "steps": args.steps,
         "warmup": args.warmup,
         "ms_per_step": total / args.steps * 1e3,
-        "ms_per_slice_all_bins": total / args.steps * (V // VB) * NE * 1e3,
+        "ms_per_slice_all_bins": total / args.steps * NE * 1e3,
         "higher_is_better": True,
         "scaling": "weak",
         "vs_baseline": None,
@@ -668,8 +920,8 @@ def run_reference(args, rank):
         "config": {"workload": CONFIG_NAME, "views": V, "channels": C, "grid": N, "elements": 6, "energy_bins": NE},
         "fbp": {"metric": "FBP slices/s", "value": 1.0 / (tf + tb), "unit": "slices/s",
                 "filter_s": tf, "backprojection_s": tb, "threads": 1},
-        "cpu_baseline": {"value": value, "unit": "rays*bins/s", "cores": cores, "kind": "reference",
-                         "sample": "reprojection_TOMO, one energy bin x 40 views x 609 channels per step"},
+        "cpu_baseline": {"value": value, "unit": "rays*bins/s", "cores": cores, "cpu_model": cpu_model(),
+                         "kind": "reference", "sample": sample},
         "e2e": {"value": value, "unit": "rays*bins/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
 
@@ -684,8 +936,8 @@ def main():
     ap.add_argument("--no-extras", action="store_true", help="skip the adjoint and batched lines")
     ap.add_argument("--batch-slices", type=int, default=256,
                     help="slices of the batched line (the batched adjoint line takes a quarter)")
-    ap.add_argument("--extras", default="adjoint,lengthproj,fbp_transpose,batched,batched_adjoint,scale",
-                    help="comma list of extra lines (1 GPU): adjoint, lengthproj, fbp_transpose, batched, "
+    ap.add_argument("--extras", default="c2,adjoint,lengthproj,fbp_transpose,batched,batched_adjoint,scale",
+                    help="comma list of extra lines (1 GPU): c2, adjoint, lengthproj, fbp_transpose, batched, "
                          "batched_adjoint, scale")
     ap.add_argument("--scale-slices", type=int, default=64, help="slices of the scale line")
     ap.add_argument("--scale-iters", type=int, default=2,

@@ -70,6 +70,22 @@ def geom(views=800, channels=609, recon_size=512, pixel_cm=0.1, xfactor=1, **kw)
     return g
 
 
+def reference_root():
+    """Where the reference's sources are: $REF if set, else the default the
+    build recipe (oracle/Makefile) holds.  Only test and fixture code reads
+    them; the GPU tests and the bench never do."""
+    ref = os.environ.get("REF")
+    if ref:
+        return ref
+    import subprocess
+
+    try:
+        r = subprocess.run(["make", "-s", "-C", HERE, "print-ref"], capture_output=True, text=True, timeout=30)
+    except (OSError, subprocess.TimeoutExpired):
+        return ""
+    return r.stdout.strip() if r.returncode == 0 else ""
+
+
 def lib():
     global _LIB
     if _LIB is None:
@@ -114,6 +130,7 @@ def lib():
         L.orc_fbp_filter.argtypes = [C.POINTER(OrcGeom), _fp, _dp, C.c_int, _fp]
         L.orc_fbp_backproject.argtypes = [C.POINTER(OrcGeom), _fp, _dp, _dp, _fp]
         L.orc_fbp_transpose.argtypes = [C.POINTER(OrcGeom), _dp, _dp, _dp, _dp, _dp]
+        L.orc_fbp_fp64.argtypes = [C.POINTER(OrcGeom), _fp, _dp, _dp, _dp, _dp]
         L.orc_mask.argtypes = [C.c_int, _u8p]
         _LIB = L
     return _LIB
@@ -368,6 +385,15 @@ def fbp(g, sino, filt, cos_t, sin_t, in_mode=0):
     h = fbp_constmap(g, filt)
     q = fbp_filter(g, sino, h, in_mode)
     return fbp_backproject(g, q, cos_t, sin_t), q
+
+
+def fbp_fp64(g, sino, filt, cos_t, sin_t):
+    """The FBP with every sum in double (the FP64 denominator): [N][N]."""
+    h = fbp_constmap(g, filt)
+    img = np.zeros((g.recon_size, g.recon_size), np.float64)
+    lib().orc_fbp_fp64(C.byref(g), np.ascontiguousarray(sino, np.float32), np.ascontiguousarray(h), cos_t, sin_t,
+                       img)
+    return img
 
 
 def fbp_transpose(g, u, filt, cos_t, sin_t):

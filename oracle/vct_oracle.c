@@ -599,6 +599,70 @@ void orc_fbp_backproject(const orc_geom* g, const float* fltd, const double* cos
   free(mask);
 }
 
+/* The FBP of orc_fbp_filter + orc_fbp_backproject with every accumulation
+ * and intermediate in double (the "error against FP64" denominator; the
+ * reference accumulates both sums in float, FBP/filterSinogramTOMO.cpp:233-242
+ * and FBP/reconstructImageTOMO.cpp:93).  img is [N][N]. */
+void orc_fbp_fp64(const orc_geom* g, const float* sino, const double* h, const double* cos_t,
+                  const double* sin_t, double* img) {
+  const int C = g->end_channel - g->start_channel;
+  const int half = (C - 1) / 2;
+  const int cw = C / 2;
+  const int V = g->views, W = g->width, N = g->recon_size;
+  double* coeff = (double*)malloc(sizeof(double) * C);
+  double* q = (double*)malloc(sizeof(double) * (size_t)V * C);
+  for (int k = 0; k < C; k++) coeff[k] = g->sid * cos((k - cw) * (g->max_beta / half));
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static)
+#endif
+  for (int n = 0; n < V; n++) {
+    for (int m = 0; m < C; m++) {
+      double acc = 0.0;
+      for (int k = 0; k < C; k++) {
+        double projdat = sino[(size_t)n * W + k + g->start_channel];
+        acc += h[(size_t)m * C + k] * (-log(projdat) * coeff[k]) * g->max_beta / half;
+      }
+      q[(size_t)n * C + m] = acc;
+    }
+  }
+  const double scale = g->pixel_cm;
+  const double centerPos = (double)N / 2.0 - 0.5;
+  const int use = V / 2 * 2;
+  const double xfactor = (double)g->xfactor;
+  unsigned char* mask = (unsigned char*)malloc((size_t)N * N);
+  orc_mask(N, mask);
+#ifdef _OPENMP
+#pragma omp parallel for schedule(static)
+#endif
+  for (int y = 0; y < N; y++) {
+    for (int x = 0; x < N; x++) {
+      double acc = 0.0;
+      if (mask[y * N + x]) {
+        double xx = -(x - centerPos) * scale;
+        double yy = -(y - centerPos) * scale;
+        for (int th = 0; th < use; th++) {
+          double dbeta = 2.0 * ORC_PI / (V);
+          double c = cos_t[th], s = sin_t[th];
+          double X = xx * c + yy * s;
+          double Y = -xx * s + yy * c;
+          double L2 = (-Y + g->sid) * (-Y + g->sid) + X * X;
+          double fGAM = atan(X / (g->sid - Y)) / (g->max_beta / half) + cw;
+          int GAM = (int)(fGAM);
+          double w = fGAM - GAM;
+          if (GAM >= 0 && GAM < C - 1) {
+            double sum = (1 - w) * q[(size_t)th * C + GAM] + w * q[(size_t)th * C + GAM + 1];
+            acc += 1.0 / L2 * sum * dbeta * xfactor;
+          }
+        }
+      }
+      img[(size_t)y * N + x] = acc;
+    }
+  }
+  free(mask);
+  free(q);
+  free(coeff);
+}
+
 void orc_fbp_transpose(const orc_geom* g, const double* h, const double* cos_t, const double* sin_t,
                        const double* u, double* out) {
   const int N = g->recon_size, V = g->views, W = g->width;

@@ -155,6 +155,8 @@ void orc_fbp_filter(const orc_geom* g, const float* sino, const double* h, int i
  * out = W^T F^T B^T u for u [N][N]; h is prepareConstMap's [C][C] matrix.
  * B^T follows orc_fbp_backproject's formula (FBP/reconstructImageTOMO.cpp:
  * 57-93), F^T the filter of FBP/filterSinogramTOMO.cpp:233-243. */
+void orc_fbp_fp64(const orc_geom* g, const float* sino, const double* h, const double* cos_t,
+                  const double* sin_t, double* img);
 void orc_fbp_transpose(const orc_geom* g, const double* h, const double* cos_t, const double* sin_t,
                        const double* u, double* out);
 void orc_fbp_backproject(const orc_geom* g, const float* fltd, const double* cos_t,

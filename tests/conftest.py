@@ -15,7 +15,11 @@ if ROOT not in sys.path:
     sys.path.insert(0, ROOT)
 
 GOLDEN = os.path.join(ROOT, "tests", "golden")
-REF = os.environ.get("REF", "/root/reference")
+# The reference's sources: $REF, else the oracle build recipe's default.  The
+# tests that read them skip where they are absent (as on a GPU box).
+from oracle import reference_root  # noqa: E402
+
+REF = reference_root()
 REF_MB = os.path.join(REF, "Release_MBFPA_CPU_human")
 REF_FBP = os.path.join(REF, "Release_FBP_CPU")
 

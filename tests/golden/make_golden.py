@@ -1,7 +1,7 @@
 """Generates the golden fixtures in tests/golden/ from the reference itself.
 
-Run in a checkout that has the reference sources (REF, default
-/root/reference) and `make -C oracle` done:
+Run in a checkout that has the reference sources ($REF, else the default
+written in oracle/Makefile) and `make -C oracle` done:
 
     python tests/golden/make_golden.py
 
@@ -22,7 +22,29 @@ Fixtures
                   the reference's un-normalised spectral sum and the FP64
                   oracle's, its global max and min, the total segment count,
                   and every 16th row of the reference's Ram-Lak FBP of the
-                  max-normalised, noise-free sinogram.
+                  max-normalised, noise-free sinogram and of the FBP with
+                  every sum in FP64.
+  icru_shipped.npz  the reference's shipped inputs: the ICRU-110 phantom
+                  (Weight_input_ICRU110.raw, 6 x 512^2 int16) with the shipped
+                  100-bin 120 kV and 650-bin 6 MV spectra, noise-free: every
+                  20th view of reprojection_TOMO's spectral sum over all bins
+                  (the reference run on those 40 views) and of the FP64
+                  oracle's; the 120 kV sum's global max and min (pinned
+                  oracle, bit-identical to the reference); and every 8th row
+                  of the shipped noisy sinogram (reprojection_float.raw,
+                  sigma 5.37e-5).
+  fbp_human.npz   the shipped FBP case: the input sinogram
+                  (Release_FBP_CPU/reprojection_float.raw, 800 x 609) and every
+                  8th row of the shipped Shepp-Logan image
+                  (FBP_virtual_projection_512x512_human.raw) and of the FBP
+                  with every sum in FP64.
+  c2_subset.npz   the 6 MV configuration at full size: 512^2, 8 elements, the
+                  seeded 33 cm cylinder with 16 inserts, the synthetic 60-bin
+                  6 MV spectrum (mu and pdf of the attenuation model),
+                  800 x 609: every 20th view of the pinned oracle's spectral
+                  sum in reference order and of the FP64 sum, its max and
+                  min, and every 16th row of the Shepp-Logan FBP of the
+                  normalised sinogram (reference arithmetic) and in FP64.
   beam_hardening.npz  the beam-hardening correction program's output
                   (reprojection_float_cor.raw, every 32nd row) and printed
                   minima on a seeded 800 x 609 sinogram, kV and MV parameters.
@@ -60,13 +82,18 @@ sys.path.insert(0, ROOT)
 import oracle as O  # noqa: E402
 from virtualct_b200 import phantoms  # noqa: E402
 
-REF = os.environ.get("REF", "/root/reference")
+REF = O.reference_root()
 MB = os.path.join(REF, "Release_MBFPA_CPU_human")
+FBP_DIR = os.path.join(REF, "Release_FBP_CPU")
 OUT = os.path.dirname(os.path.abspath(__file__))
 
 C1_SEED = 0
 C1_FBP_ROW_STEP = 16
 C1_SUBSET_STEP = 20
+SHIP_ROW_STEP = 20      # forward rows of the shipped-input fixture
+SHIP_NOISY_STEP = 8     # rows of the shipped noisy sinogram
+FBP_HUMAN_ROW_STEP = 8  # image rows of the shipped FBP case
+C2_SEED = 3
 
 
 def kramers_file(tmp, kvp=120):
@@ -134,12 +161,83 @@ def c1_subset(tabs):
     f64 = O.forward_fp64(g, c, s, rho, mu, pdf)
     # the reference's FBP (Ram-Lak) of the max-normalised, noise-free sinogram
     # (MB/main.cpp:511-522 in float, then FBP/main.cpp:137-167)
-    img, _, _, _ = O.ref_fbp(1, (full / full.max()).astype(np.float32), 512, 0.1, 1, c, s)
+    norm = (full / full.max()).astype(np.float32)
+    img, _, _, _ = O.ref_fbp(1, norm, 512, 0.1, 1, c, s)
+    img64 = O.fbp_fp64(g, norm, 1, c, s)
     np.savez_compressed(os.path.join(OUT, "c1_subset.npz"), rows=rows, full_rows=full[rows],
                         fp64_rows=f64[rows], fbp_ramlak_rows=img[::C1_FBP_ROW_STEP],
+                        fbp_ramlak_fp64_rows=img64[::C1_FBP_ROW_STEP],
                         max=np.float32(full.max()), min=np.float32(full.min()),
                         segments=np.int64(nseg.sum()), seed=C1_SEED,
                         maps_sha=np.frombuffer(__import__("hashlib").sha256(maps.tobytes()).digest(), np.uint8))
+
+
+def icru_shipped(tabs):
+    maps = np.fromfile(os.path.join(MB, "Weight_input_ICRU110.raw"), np.int16).reshape(6, 512, 512)
+    rho = O.rho_from_maps(maps)
+    c, s = O.trig_tables(800)
+    rows = np.arange(0, 800, SHIP_ROW_STEP)
+    cs, ss = np.ascontiguousarray(c[rows]), np.ascontiguousarray(s[rows])
+    gsub = O.geom(views=len(rows))
+    out = {"maps": maps, "rows": rows}
+    for name in ("kv120", "mv6"):
+        pdf, mu = tabs[f"{name}_pdf"], tabs[f"{name}_mu"]
+        # reprojection_TOMO over every bin on the 40 views (each view's rays
+        # are walked as in the full run: the walk reads only its cos/sin)
+        ref, _ = O.ref_reprojection(512, 0.1, rho, len(rows), 609, cs, ss, 1, mu, pdf)
+        out[f"{name}_rows"] = ref
+        out[f"{name}_fp64_rows"] = O.forward_fp64(gsub, cs, ss, rho, mu, pdf)
+        out[f"{name}_pdf"], out[f"{name}_mu"] = pdf, mu
+    # the full 120 kV sum's extremes (the pinned oracle reproduces the shipped
+    # noisy output from it bit for bit)
+    full = O.forward_exact(O.geom(), c, s, rho, tabs["kv120_mu"], tabs["kv120_pdf"])
+    out["kv120_max"], out["kv120_min"] = np.float32(full.max()), np.float32(full.min())
+    gold = np.fromfile(os.path.join(MB, "reprojection_float.raw"), np.float32).reshape(800, 609)
+    out["noisy_rows"] = np.arange(0, 800, SHIP_NOISY_STEP)
+    out["noisy"] = gold[::SHIP_NOISY_STEP]
+    out["sigma"] = np.float64(0.0000537)
+    np.savez_compressed(os.path.join(OUT, "icru_shipped.npz"), **out)
+
+
+def fbp_human():
+    sino = np.fromfile(os.path.join(FBP_DIR, "reprojection_float.raw"), np.float32).reshape(800, 609)
+    gold = np.fromfile(os.path.join(FBP_DIR, "FBP_virtual_projection_512x512_human.raw"), np.float32)
+    gold = gold.reshape(512, 512)
+    g = O.geom()
+    c, s = O.trig_tables(800)
+    img, _, _, _ = O.ref_fbp(2, sino, 512, 0.1, 1, c, s)
+    assert np.array_equal(img, gold), "the reference built here does not reproduce the shipped FBP image"
+    f64 = O.fbp_fp64(g, sino, 2, c, s)
+    np.savez_compressed(os.path.join(OUT, "fbp_human.npz"), sino=sino, rows=np.arange(0, 512, FBP_HUMAN_ROW_STEP),
+                        golden_rows=gold[::FBP_HUMAN_ROW_STEP], fp64_rows=f64[::FBP_HUMAN_ROW_STEP], filter=2)
+
+
+def c2_tables():
+    """mu [8][60] and pdf [60] of the synthetic 6 MV spectrum (through its
+    txt form) for H C N O P Ca Mg Si, by the oracle's attenuation model."""
+    with tempfile.TemporaryDirectory() as tmp:
+        p = os.path.join(tmp, "mv6_60.txt")
+        phantoms.write_spectrum_txt(p, phantoms.mv_spectrum())
+        pdf, e = O.spectrum(p)
+    return O.attenuation(e, phantoms.ELEMENTS8), pdf
+
+
+def c2_subset():
+    maps = phantoms.gammex_cylinder_phantom(C2_SEED, 512)
+    rho = O.rho_from_maps(maps)
+    mu, pdf = c2_tables()
+    c, s = O.trig_tables(800)
+    g = O.geom()
+    full = O.forward_exact(g, c, s, rho, mu, pdf)
+    f64 = O.forward_fp64(g, c, s, rho, mu, pdf)
+    rows = np.arange(0, 800, C1_SUBSET_STEP)
+    norm = (full / full.max()).astype(np.float32)
+    img, _ = O.fbp(g, norm, 2, c, s)
+    img64 = O.fbp_fp64(g, norm, 2, c, s)
+    np.savez_compressed(os.path.join(OUT, "c2_subset.npz"), rows=rows, full_rows=full[rows], fp64_rows=f64[rows],
+                        max=np.float32(full.max()), min=np.float32(full.min()), mu=mu, pdf=pdf, seed=C2_SEED,
+                        fbp_sl_rows=img[::C1_FBP_ROW_STEP], fbp_sl_fp64_rows=img64[::C1_FBP_ROW_STEP],
+                        maps_sha=_sha(maps))
 
 
 sys.path.insert(0, os.path.join(ROOT, "tests"))
@@ -252,9 +350,9 @@ def main():
     if not O.ref_available():
         raise SystemExit("reference harness not built: make -C oracle ref")
     want = set(sys.argv[1:]) or {"mu_tables", "mb_small", "fbp_small", "c1_subset", "lengthproj", "beam_hardening",
-                                   "ir_step", "measured", "measured_e2e"}
+                                   "ir_step", "measured", "measured_e2e", "icru_shipped", "fbp_human", "c2_subset"}
     tabs = None
-    if want & {"mu_tables", "mb_small", "c1_subset"}:
+    if want & {"mu_tables", "mb_small", "c1_subset", "icru_shipped"}:
         with tempfile.TemporaryDirectory() as tmp:
             tabs = mu_tables(tmp)
     if "mb_small" in want:
@@ -273,6 +371,12 @@ def main():
         measured()
     if "measured_e2e" in want:
         measured_e2e()
+    if "icru_shipped" in want:
+        icru_shipped(tabs)
+    if "fbp_human" in want:
+        fbp_human()
+    if "c2_subset" in want:
+        c2_subset()
     for f in sorted(os.listdir(OUT)):
         print(f, os.path.getsize(os.path.join(OUT, f)))
 

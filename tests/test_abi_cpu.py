@@ -64,6 +64,18 @@ def test_attenuation_eight_elements_extends_table():
     assert np.all(mu8[6] > 0) and np.all(mu8[7] > mu8[6])  # Si attenuates more than Mg
 
 
+def test_attenuation_c2_tables_match_fixture(tmp_path):
+    """The 60-bin 6 MV spectrum through its txt form, 8 elements: the product's
+    host model gives the C2 fixture's (oracle) mu and pdf bit for bit."""
+    from virtualct_b200 import phantoms
+
+    d = golden("c2_subset.npz")
+    p = str(tmp_path / "mv6_60.txt")
+    phantoms.write_spectrum_txt(p, phantoms.mv_spectrum())
+    mu, pdf = vct.attenuation_coefficient(p, vct.GAMMEX_ELEMENTS)
+    assert np.array_equal(pdf, d["pdf"]) and np.array_equal(mu, d["mu"])
+
+
 def test_attenuation_errors():
     with pytest.raises(vct.VctError) as e:
         vct.attenuation_coefficient("/nonexistent/spectrum.txt")

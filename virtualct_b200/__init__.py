@@ -58,8 +58,8 @@ EXPORTED_SYMBOLS = (
     "vct_forward_adjoint", "vct_forward_adjoint_dev", "vct_forward_vjp_dev", "vct_adjoint_rays_dev",
     "vct_batch_create", "vct_batch_run", "vct_batch_synchronize", "vct_batch_config", "vct_batch_destroy",
     "vct_forward_batched",
-    "vct_last_segment_count",
-    "vct_kernel_launches", "vct_bounds_violations", "vct_version", "vct_philox4x32_10", "vct_probe_peaks",
+    "vct_last_segment_count", "vct_set_stage_timing", "vct_stage_times",
+    "vct_kernel_launches", "vct_bounds_violations", "vct_version", "vct_philox4x32_10",
     "vct_load_mb_config", "vct_load_fbp_config", "vct_mb_geometry", "vct_fbp_geometry", "vct_read_raw",
     "vct_write_raw", "vct_raw_layout_default", "vct_load_measured", "vct_load_measured_dev",
     "vct_helical_sinogram", "vct_helical_sinogram_dev",
@@ -231,11 +231,12 @@ def lib():
     L.vct_batch_destroy.restype = None
     L.vct_forward_batched.argtypes = [C.POINTER(_CJob), C.c_int, C.c_int, C.c_int]
     L.vct_last_segment_count.argtypes = [vp, C.POINTER(C.c_longlong)]
+    L.vct_set_stage_timing.argtypes = [vp, C.c_int]
+    L.vct_stage_times.argtypes = [vp, C.c_int, C.POINTER(C.c_char_p), C.POINTER(C.c_float), C.POINTER(C.c_int)]
     L.vct_kernel_launches.argtypes = [vp]
     L.vct_kernel_launches.restype = C.c_longlong
     L.vct_philox4x32_10.argtypes = [vp, vp, vp]
     L.vct_philox4x32_10.restype = None
-    L.vct_probe_peaks.argtypes = [C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.vct_mbfpa_many.argtypes = [vp, C.c_int, vp, C.c_int, C.c_double, C.c_uint64, vp, vp]
     L.vct_forward_views_dev.argtypes = [vp, C.c_int, C.c_int, vp, vp]
     L.vct_normalize_noise_rows_dev.argtypes = [vp, vp, C.c_int, C.c_int, vp, C.c_double, C.c_uint64]
@@ -284,13 +285,6 @@ def philox4x32_10(ctr, key):
     return out
 
 
-def probe_peaks(device: int = 0) -> dict:
-    """Live roofline denominators on `device` (see vct_probe_peaks)."""
-    l2, f64, f32 = C.c_double(0), C.c_double(0), C.c_double(0)
-    _check(lib().vct_probe_peaks(device, C.byref(l2), C.byref(f64), C.byref(f32)), "vct_probe_peaks")
-    return {"l2_read_gbs": l2.value, "fp64_tflops": f64.value, "fp32_tflops": f32.value}
-
-
 class Context:
     """One device context (vct_ctx): geometry tables, maps, spectrum and
     scratch buffers live on the GPU between calls."""
@@ -334,6 +328,19 @@ class Context:
     @property
     def kernel_launches(self) -> int:
         return int(lib().vct_kernel_launches(self._h))
+
+    def set_stage_timing(self, on: bool = True) -> None:
+        """Record CUDA events around every kernel stage of later calls."""
+        _check(lib().vct_set_stage_timing(self._h, 1 if on else 0), "vct_set_stage_timing")
+
+    def stage_times(self) -> list:
+        """[(stage name, ms)] of the last timed call (waits for it)."""
+        cap = 16
+        names = (C.c_char_p * cap)()
+        ms = (C.c_float * cap)()
+        n = C.c_int(0)
+        _check(lib().vct_stage_times(self._h, cap, names, ms, C.byref(n)), "vct_stage_times")
+        return [(names[i].decode(), float(ms[i])) for i in range(min(n.value, cap))]
 
     @property
     def last_segment_count(self) -> int:

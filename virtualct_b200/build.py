@@ -11,6 +11,9 @@ Outputs, all in-tree so they travel with the repository snapshot:
   virtualct_b200/bin/vct_mbfpa         drop-in for Release_MBFPA_CPU_human/mvct.exe
   virtualct_b200/bin/vct_fbp           drop-in for Release_FBP_CPU/mvct.exe
   virtualct_b200/bin/vct_bhc           drop-in for the beam-hardening correction
+  virtualct_b200/lib/libvct_peaks.so   bench.py's roofline denominators (L2 read,
+                                       FP64 and FP32 FMA probes); not part of
+                                       the product library
 """
 from __future__ import annotations
 
@@ -29,6 +32,8 @@ LIBDIR = os.path.join(PKG, "lib")
 BINDIR = os.path.join(PKG, "bin")
 LIB = os.path.join(LIBDIR, "libvct.so")
 LIB_BOUNDS = os.path.join(LIBDIR, "libvct_bounds.so")
+LIB_PEAKS = os.path.join(LIBDIR, "libvct_peaks.so")
+PEAKS_SRC = os.path.join(CSRC, "probe", "vct_peaks.cu")
 
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVCC_COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", INC, "-I", CSRC]
@@ -40,7 +45,6 @@ NVCC_COMMON = ["-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-I", IN
 CU_SOURCES = {
     "vct_forward.cu": ["--fmad=false"],
     "vct_fbp.cu": [],
-    "vct_probe.cu": [],
     "vct_fbp_noalloc.cu": [],
     "vct_adjoint.cu": ["--fmad=false"],
     "vct_descent.cu": [],
@@ -102,6 +106,9 @@ def build(force: bool = False, verbose: bool = False, bounds: bool = True) -> st
     _library(LIB, BUILD, [], force, verbose, hdrs)
     if bounds:
         _library(LIB_BOUNDS, os.path.join(BUILD, "bounds"), ["-DVCT_BOUNDS=1"], force, verbose, hdrs)
+    if force or not _newer(LIB_PEAKS, [PEAKS_SRC, __file__]):
+        _run([nvcc(), *ARCH, "-O3", "-std=c++17", "-lineinfo", "-Xcompiler", "-fPIC", "-shared", PEAKS_SRC,
+              "-o", LIB_PEAKS, "-cudart", "static"])
     for app, src in APPS.items():
         s = os.path.join(CSRC, src)
         exe = os.path.join(BINDIR, app)

@@ -1,11 +1,25 @@
-// Peak probes used as roofline denominators: the B200 figures this path is
-// bound by (L2 read bandwidth for the map gathers, FP64 and FP32 FMA issue)
-// are not among the pool's measured peaks, so they are measured live.
+// Peak probes used by bench.py as roofline denominators: the B200 figures
+// this path is bound by (L2 read bandwidth for the map gathers, FP64 and FP32
+// FMA issue) are not among the measured HBM and GEMM peaks, so they are
+// measured live.  Built as its own library (lib/libvct_peaks.so), not part of
+// the product libvct.so.
 #include <cuda_runtime.h>
+#include <stdio.h>
 
-#include "vct_internal.h"
+namespace {
 
-namespace vct {
+thread_local char g_err[256];
+
+int probe_fail(cudaError_t e, const char* what) {
+  snprintf(g_err, sizeof g_err, "%s: %s", what, cudaGetErrorString(e));
+  return -2;
+}
+
+#define PROBE_CUDA(call)                                  \
+  do {                                                    \
+    cudaError_t e_ = (call);                              \
+    if (e_ != cudaSuccess) return probe_fail(e_, #call);  \
+  } while (0)
 
 // L2 read bandwidth: every block streams the same L2-resident buffer with
 // ld.global.cg (cached in L2, not L1), 16 B per thread per load.
@@ -41,16 +55,17 @@ __global__ void probe_fma_kernel(int iters, T seed, T* __restrict__ sink) {
   if (s == (T)-1.2345) sink[0] = s;
 }
 
-}  // namespace vct
+}  // namespace
 
-using namespace vct;
+extern "C" const char* vct_peaks_error(void) { return g_err; }
 
+// Returns 0, or a negative code with the message in vct_peaks_error().
 extern "C" int vct_probe_peaks(int device, double* l2_read_gbs, double* fp64_tflops, double* fp32_tflops) {
-  VCT_CUDA(cudaSetDevice(device));
+  PROBE_CUDA(cudaSetDevice(device));
   int sms = 0;
-  VCT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
+  PROBE_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device));
   cudaStream_t st;
-  VCT_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
+  PROBE_CUDA(cudaStreamCreateWithFlags(&st, cudaStreamNonBlocking));
   cudaEvent_t e0, e1;
   cudaEventCreate(&e0);
   cudaEventCreate(&e1);
@@ -59,13 +74,13 @@ extern "C" int vct_probe_peaks(int device, double* l2_read_gbs, double* fp64_tfl
   unsigned int* sink = nullptr;
   double* dsink = nullptr;
   float* fsink = nullptr;
-  int rc = VCT_OK;
+  int rc = 0;
   if (cudaMalloc((void**)&buf, bytes) != cudaSuccess || cudaMalloc((void**)&sink, 64) != cudaSuccess ||
       cudaMalloc((void**)&dsink, 64) != cudaSuccess || cudaMalloc((void**)&fsink, 64) != cudaSuccess) {
-    rc = fail(VCT_E_NOMEM, "vct_probe_peaks: allocation");
+    rc = probe_fail(cudaErrorMemoryAllocation, "vct_probe_peaks: allocation");
   }
   float ms = 0;
-  if (rc == VCT_OK) {
+  if (rc == 0) {
     cudaMemsetAsync(buf, 1, bytes, st);
     const int blocks = sms * 4, threads = 512, reps = 64;
     probe_l2_kernel<<<blocks, threads, 0, st>>>(buf, bytes / 16, 1, sink);  // warm L2
@@ -93,7 +108,7 @@ extern "C" int vct_probe_peaks(int device, double* l2_read_gbs, double* fp64_tfl
     cudaEventElapsedTime(&ms, e0, e1);
     if (fp32_tflops) *fp32_tflops = 2.0 * 32 * (double)iters * 4 * fthreads * fblocks / (ms * 1e-3) / 1e12;
     cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) rc = cuda_fail(e, "vct_probe_peaks");
+    if (e != cudaSuccess) rc = probe_fail(e, "vct_probe_peaks");
   }
   cudaFree(buf);
   cudaFree(sink);

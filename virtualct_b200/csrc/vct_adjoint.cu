@@ -621,18 +621,20 @@ static int launch_adj_gather_m(const AdjGeom& a, int tile, const double* d_cos, 
 }
 
 int launch_adj_gather(const AdjGeom& a, int M, int tile, const double* d_cos, const double* d_sin,
-                      const double2* d_dir, const int4* d_rec, const float* d_g, const unsigned long long* d_sacc,
-                      const unsigned int* d_gmax, float* d_ext, float* d_grad, int* d_status, cudaStream_t st) {
+                      const double2* d_dir, const int4* d_rec, const float* d_g, float* d_ext, int* d_status,
+                      cudaStream_t st) {
   if (tile < 0 || tile > 3) return fail(VCT_E_UNSUPPORTED, "adjoint: no tile fits the channel window");
-  int rc;
   switch (M) {
 #define VCT_CASE(mm) \
-  case mm: rc = launch_adj_gather_m<mm>(a, tile, d_cos, d_sin, d_dir, d_rec, d_g, d_ext, d_status, st); break;
+  case mm: return launch_adj_gather_m<mm>(a, tile, d_cos, d_sin, d_dir, d_rec, d_g, d_ext, d_status, st);
     VCT_CASE(1) VCT_CASE(2) VCT_CASE(3) VCT_CASE(4) VCT_CASE(5) VCT_CASE(6) VCT_CASE(7) VCT_CASE(8)
 #undef VCT_CASE
     default: return fail(VCT_E_ARG, "adjoint: 1..8 materials");
   }
-  if (rc) return rc;
+}
+
+int launch_adj_fold(const AdjGeom& a, int M, const unsigned long long* d_sacc, const unsigned int* d_gmax,
+                    const float* d_ext, float* d_grad, cudaStream_t st) {
   const long long n = (long long)M * a.N * a.N;
   adj_fold_kernel<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(M, a.N, d_ext, d_sacc, d_gmax, a.lmax, a.log2_terms,
                                                                 d_grad);

@@ -45,6 +45,29 @@ struct Pipe {
     if (out) cudaStreamDestroy(out);
   }
 };
+// Per-stage device times of one entry-point call (vct_set_stage_timing):
+// an event on the call's stream before its first stage and after each
+// stage.  Off by default; when off, begin() and mark() do nothing.
+struct StageTimer {
+  static constexpr int kMax = 16;
+  int on = 0;
+  int n = 0;
+  const char* name[kMax] = {};
+  cudaEvent_t ev[kMax + 1] = {};
+  void begin(cudaStream_t s) {
+    n = 0;
+    if (on) cudaEventRecord(ev[0], s);
+  }
+  void mark(const char* stage, cudaStream_t s) {
+    if (!on || n >= kMax) return;
+    name[n] = stage;
+    cudaEventRecord(ev[++n], s);
+  }
+  ~StageTimer() {
+    for (cudaEvent_t e : ev)
+      if (e) cudaEventDestroy(e);
+  }
+};
 }  // namespace vct
 
 struct vct_ctx {
@@ -95,6 +118,7 @@ struct vct_ctx {
   vct::DBuf<float> adj_meas, adj_wts, adj_grad;
   vct::DBuf<float> adj_ext;  // [M][N+1][N+1] gather output before the fold
   vct::Pipe* pipe = nullptr;  // vct_mbfpa_many
+  vct::StageTimer timer;      // vct_set_stage_timing
 };
 
 

@@ -122,7 +122,7 @@ int vct_set_sum_mode(vct_ctx* ctx, int mode);
  * expressions (divisions and square roots included), so segment boundaries
  * match it bit for bit.  VCT_WALK_FAST (default) advances the minor
  * coordinate incrementally, tracks the next gridline, uses one precomputed
- * step length and splits crossing steps in 30-bit fixed point; rays whose
+ * step length and splits crossing steps in 31-bit fixed point; rays whose
  * first major gridline is not a pixel boundary (pixel sizes that do not
  * divide 1 cm) and geometries where the rmax test can fire take the exact
  * walk.  Densities enter as s/1000 exactly in both modes. */

@@ -1,7 +1,7 @@
 // CPU check of the fast walk's paired-word accumulation (acc_words in
 // virtualct_b200/csrc/vct_walk.cuh, __host__ __device__): for seeded records
 // and weights, including the extremes (16-bit densities of 65535, weights of
-// 2^30) and enough segments that the packed 64-bit sums wrap, the recovered
+// 2^31, a whole major step) and enough segments that the packed 64-bit sums wrap, the recovered
 // per-element sums must equal the plain per-element 64-bit sums exactly.
 //   acc_check <M> <segments> <seed>   prints "ok" or the first mismatch
 #include "../../virtualct_b200/csrc/vct_walk.cuh"
@@ -31,7 +31,7 @@ static int run(long nseg, unsigned long long seed) {
       if (m >= M) v[m] = 0;
     }
     const unsigned long long rq = next();
-    const unsigned int q = (rq & 3) == 0 ? (1u << 30) : (unsigned int)((rq >> 20) & ((1u << 30) - 1));
+    const unsigned int q = (rq & 3) == 0 ? (1u << 31) : (unsigned int)((rq >> 20) & ((1u << 31) - 1));
     int4 w;
     w.x = (int)(v[0] | (unsigned)v[1] << 16);
     w.y = (int)(v[2] | (unsigned)v[3] << 16);

@@ -72,7 +72,7 @@ def acc_check(tmp_path_factory):
 @pytest.mark.parametrize("M", [1, 2, 3, 4, 5, 6, 7, 8])
 def test_paired_word_accumulation_is_exact(acc_check, M):
     """Two elements per 64-bit multiply-add, the low sum recovered modulo 2^64:
-    equal to the per-element sums at the extremes (65535 densities, 2^30
+    equal to the per-element sums at the extremes (65535 densities, 2^31
     weights, 20,000 segments, so the packed sums wrap many times)."""
     r = subprocess.run([str(acc_check), str(M), "20000", str(M + 100)], capture_output=True, text=True)
     assert r.returncode == 0 and r.stdout.strip() == "ok", r.stdout

@@ -13,9 +13,10 @@
 //               (compiled with --fmad=false, IEEE division and square root),
 //               so segment boundaries match it bit for bit;
 //   walk_fast   the same segments found by a Siddon-style event loop (major
-//               gridline / minor gridline, whichever comes first), one
-//               segment per iteration, weights in 30-bit fixed point and
-//               integer multiply-add accumulation; no per-step division.
+//               gridline / minor gridline, whichever comes first) with event
+//               times in integer fixed point, one segment per iteration,
+//               weights in 2^-31 steps and integer multiply-add
+//               accumulation; no per-step division or FP64 arithmetic.
 //
 // Maps are one 16-byte record (8 x int16) per pixel in a padded
 // (N+4) x (N+4) layout whose border reproduces the reference's truncating

@@ -62,14 +62,11 @@ VCT_HD int d2i_rz(double d) {
   return (int)d;
 #endif
 }
-// Low 32 bits of a double's bit pattern.
-VCT_HD unsigned int lo32(double d) {
+VCT_HD double dmul_rn(double a, double b) {
 #if defined(__CUDA_ARCH__)
-  return (unsigned int)__double2loint(d);
+  return __dmul_rn(a, b);
 #else
-  unsigned long long b;
-  memcpy(&b, &d, 8);
-  return (unsigned int)b;
+  return a * b;
 #endif
 }
 
@@ -92,7 +89,7 @@ VCT_HD unsigned int mat_of(const int4& w, int m) {
 // ----------------------------------------------------------------- accumulators
 // Ld: sum s*len (cm) of segments emitted one by one (the exact walk, and the
 // fast walk's first segment).  Lq: sum s*w_q of the fast walk's segments, w_q
-// the segment's share of one major step in units of 2^-30; one major step is
+// the segment's share of one major step in units of 2^-31; one major step is
 // `sec` cm long.
 struct RayAcc {
   double Ld[8];
@@ -117,7 +114,7 @@ template <int M>
 VCT_HD void finish_lines(const RayAcc& a, double L[8], double div) {
 #pragma unroll
   for (int m = 0; m < M; m++) {
-    const double steps = (double)a.Lq[m] * (1.0 / 1073741824.0);
+    const double steps = (double)a.Lq[m] * (1.0 / 2147483648.0);
     L[m] = (a.Ld[m] + steps * a.sec) / div;
   }
 }
@@ -312,7 +309,8 @@ VCT_HD void walk_exact(const DevGeom& g, const PixelRec* __restrict__ maps, cons
 //     steps are walked as a Siddon event loop in units of major steps t:
 //     major events at integer t, minor events at t_min, t_min + dt, ...;
 //     every iteration closes one segment [t, min(next events)] and adds
-//     s * w_q, w_q = its length in 2^-30 steps.
+//     s * w_q, w_q = its length in 2^-31 steps (event times in integer
+//     fixed point).
 // When uin/s is an integer, every major step spans exactly one pixel column
 // and every piece between events lies inside one pixel, so the reference's
 // midpoint rule picks the same pixel as the event bookkeeping.  Rays it does
@@ -484,11 +482,22 @@ VCT_HD bool walk_fast(const DevGeom& g, const PixelRec* __restrict__ maps, const
     dpix_min = dirw;
   }
   const int pix_first = pix;
-  const double dt = pl.dt;
-  double tmin = pl.tmin0;  // next minor event, in steps
-  double tmaj = 1.0;
-  double t = 0.0;
-  const double tend = (double)pl.K;
+  // Event times in fixed point, so the loop runs on the integer pipes:
+  //   kh  = k << 12, k the next major event (an integer step, 1..K);
+  //   T   = the next minor event in units of 2^-44 steps, 64 bits (its high
+  //         word is in units of 2^-12 steps, so k is due first iff kh <= T.hi);
+  //   t31 = the current time in units of 2^-31 steps, modulo 2^32.
+  // A segment's weight is the difference of its end and start times in
+  // 2^-31 steps (0..2^31), so the weights of a ray add up to exactly K steps.
+  // Minor events advance by DT = dt * 2^44 rounded (2^-45 steps per event at
+  // most; the reference's own crossing points are found afresh per step).
+  // Times beyond 2^18 steps (past every walk's end) are clamped there.
+  const double kTcap = 262144.0;                         // 2^18 steps
+  unsigned long long T = (unsigned long long)dmul_rn(fmin(pl.tmin0, kTcap), 17592186044416.0);  // 2^44
+  const unsigned long long DT = (unsigned long long)dmul_rn(fmin(pl.dt, kTcap), 17592186044416.0);
+  unsigned int kh = 1u << 12;                            // next major event: step 1
+  const unsigned int kend = (unsigned int)pl.K << 12;    // the last major event, step K
+  unsigned int t31 = 0u;
   const int4* __restrict__ m4 = reinterpret_cast<const int4*>(mp);
   constexpr int kWords = (M + 1) / 2;
   unsigned long long accP[kWords], accH[kWords];
@@ -504,23 +513,24 @@ VCT_HD bool walk_fast(const DevGeom& g, const PixelRec* __restrict__ maps, const
   const int it_max = (8 * N + 128) / kUnroll;
   int it = 0;
   // Bulk iterations, with no per-slot end test.  A segment ends at the next
-  // major gridline at the latest, so t < tmaj always holds and tmaj grows by
-  // at most one per segment: while tmaj + kUnroll - 1 <= tend (integers held
-  // in doubles, exact), every slot of the iteration starts before tend.  The
-  // integer sums do not depend on how the segments are grouped, so the
-  // result is the same as the checked loop's alone.
-  for (; it < it_max && tmaj + (double)(kUnroll - 1) <= tend; it++) {
+  // major event at the latest, so the next major event advances by at most
+  // one step per segment: while k + kUnroll - 1 <= K every slot of the
+  // iteration starts before step K.  The integer sums do not depend on how
+  // the segments are grouped, so the result is the same as the checked
+  // loop's alone.
+  const unsigned int kbulk = kend - ((unsigned int)(kUnroll - 1) << 12);
+  for (; it < it_max && kend >= ((unsigned int)(kUnroll - 1) << 12) && kh <= kbulk; it++) {
     int px[kUnroll];
     unsigned int wq[kUnroll];
 #pragma unroll
     for (int u = 0; u < kUnroll; u++) {
-      const bool mj = tmaj <= tmin;
-      const double tn = mj ? tmaj : tmin;
-      wq[u] = lo32((tn - t) + 4194304.0);
+      const bool mj = kh <= (unsigned int)(T >> 32);
+      const unsigned int e31 = mj ? kh << 19 : (unsigned int)(T >> 13);
+      wq[u] = e31 - t31;
       px[u] = pix;
-      t = tn;
-      tmaj = mj ? tmaj + 1.0 : tmaj;
-      tmin = mj ? tmin : tmin + dt;
+      t31 = e31;
+      if (mj) kh += 1u << 12;
+      else T += DT;
       pix += mj ? dpix_maj : dpix_min;
     }
     nseg += kUnroll;
@@ -531,24 +541,23 @@ VCT_HD bool walk_fast(const DevGeom& g, const PixelRec* __restrict__ maps, const
 #pragma unroll
     for (int u = 0; u < kUnroll; u++) acc_words<M>(wv[u], wq[u], accP, accH);
   }
-  // The last iterations, each slot tested against the end.
-  for (; it < it_max && t < tend; it++) {
+  // The last iterations, each slot tested against the end: a slot is live
+  // while major event K has not been passed.
+  for (; it < it_max && kh <= kend; it++) {
     int px[kUnroll];
     unsigned int wq[kUnroll];
 #pragma unroll
     for (int u = 0; u < kUnroll; u++) {
-      const bool live = t < tend;
-      const bool mj = tmaj <= tmin;
-      const double tn = mj ? tmaj : tmin;
-      // Segment weight in 2^-30 steps: adding 2^22 leaves round(w * 2^30)
-      // in the low mantissa bits (0 <= w <= 1).
-      wq[u] = live ? lo32((tn - t) + 4194304.0) : 0u;
+      const bool live = kh <= kend;
+      const bool mj = kh <= (unsigned int)(T >> 32);
+      const unsigned int e31 = mj ? kh << 19 : (unsigned int)(T >> 13);
+      wq[u] = live ? e31 - t31 : 0u;
       px[u] = live ? pix : pix_first;
       nseg += live;
       if (live) {
-        t = tn;
-        tmaj = mj ? tmaj + 1.0 : tmaj;
-        tmin = mj ? tmin : tmin + dt;
+        t31 = e31;
+        if (mj) kh += 1u << 12;
+        else T += DT;
         pix += mj ? dpix_maj : dpix_min;
       }
     }

@@ -30,7 +30,6 @@
 #include <cuda_runtime.h>
 #include <math.h>
 
-#include "vct_fastmath.cuh"
 #include "vct_internal.h"
 #include "vct_walk.cuh"
 
@@ -38,7 +37,7 @@ namespace vct {
 
 // ------------------------------------------------------------- walk plans
 // Per-ray record: x = kind | xmaj << 2; y = (maj_lo + 1) | (maj_hi + 1) << 16;
-// z = lumped pixel (col + row * N) or -1; w = lumped length (float bits, cm).
+// z = lumped pixel (col | row << 16) or -1; w = lumped length (float bits, cm).
 __global__ void adj_plan_kernel(DevGeom g, const double* __restrict__ cos_t, const double* __restrict__ sin_t,
                                 const double* __restrict__ det_px0, const double* __restrict__ det_py0,
                                 int4* __restrict__ rec, int* __restrict__ special, int* __restrict__ nspecial) {
@@ -65,7 +64,7 @@ __global__ void adj_plan_kernel(DevGeom g, const double* __restrict__ cos_t, con
       if (p.pix_lumped >= 0) {
         const int P = g.N + 2 * kPad;
         const int col = p.pix_lumped % P - kPad, row = p.pix_lumped / P - kPad;
-        o.z = col + row * g.N;
+        o.z = col | (row << 16);  // both in [0, N): no division to unpack
         o.w = __float_as_int((float)p.rr_first);
       }
     }
@@ -333,234 +332,277 @@ int launch_adj_gmax(int M, const int* d_special, const int* d_nspecial, int nspe
 }
 
 // ------------------------------------------------------ pixel-driven gather
-// Largest channel window one tile needs per view (the host picks the tile so
-// the window fits; see adj_pick_tile), rays staged per round, and the views a
-// round considers: it takes as many as fit in the staging space (at least
-// kAdjCap / kAdjWMax), so each barrier serves more views when windows are
-// narrow.
-constexpr int kAdjWMax = 128;
-constexpr int kAdjCap = 4 * kAdjWMax;
-constexpr int kAdjVB = 8;
+// Staged rays per view (the channel window of one tile; the host picks the
+// tile so the window fits).
+constexpr int kAdjW = 64;
 
-// Angle of the direction (u, v) from the source, measured like the channel
-// angle theta = (iso - jj) * dalpha: (sin theta, -cos theta) is channel jj's
-// unrotated direction.  Only v < 0 occurs (the grid lies below the source).
-// It only picks candidate channels, whose ranges carry a margin.
-__device__ __forceinline__ float fan_angle(float u, float v) {
-  const float t = u * rcp_approx(-v);
-  return fabsf(t) <= 0.5f ? atan_small(t) : atanf(t);
+// Per (tile, view), computed once per context from the geometry and the walk
+// plans (adj_tiles_kernel):
+//   a = (J0, Jx, Jy, Jxx), b = (Jxy, Jyy, dj, 0), c = (kmax, jlo, jn, cplx).
+// The channel coordinate of a cell centre at offset (lx, ly) from the tile
+// centre is modelled as jc = J0 + Jx lx + Jy ly + Jxx lx^2 + Jxy lx ly +
+// Jyy ly^2 (second-order Taylor expansion of the fan angle at the tile
+// centre, FP64, channels counted from jlo), and dj bounds a cell's angular
+// half-width in channels with the expansion's third-order remainder as
+// margin: every ray whose chord through the cell can be positive lies among
+// the integers in (jc - dj, jc + dj), at most kmax = floor(2 dj) + 1 of
+// them, inside the window of jn channels from jlo.  cplx = 1 when some ray of the window
+// ends its walk or lumps inside the tile (else every cell takes the plain
+// chord path for the view).
+struct AdjTileView {
+  float4 a, b;
+  int4 c;
+};
+
+template <int TX, int TY>
+__global__ void adj_tiles_kernel(AdjGeom a, const double* __restrict__ cos_t, const double* __restrict__ sin_t,
+                                 const int4* __restrict__ rec, AdjTileView* __restrict__ out,
+                                 int* __restrict__ status) {
+  const int NE1 = a.N + 1;
+  const int nbx = (NE1 + TX - 1) / TX, nby = (NE1 + TY - 1) / TY;
+  const int V = a.views_used;
+  const long long item = ((long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;  // one warp per (tile, view)
+  const int lane = threadIdx.x & 31;
+  if (item >= (long long)nbx * nby * V) return;
+  const int tile = (int)(item / V), v = (int)(item - (long long)tile * V);
+  const int e0 = (tile % nbx) * TX, f0 = (tile / nbx) * TY;
+  const double s = a.s, h = 0.5 * s;
+  const double Tx = (e0 - 1 + 0.5 * TX - a.nxm) * s;
+  const double Ty = (a.nxm - (f0 - 1) - 0.5 * TY) * s;
+  const double Lx = 0.5 * (TX - 1) * s, Ly = 0.5 * (TY - 1) * s;
+  const double lmax = sqrt(Lx * Lx + Ly * Ly);
+  int jlo = 0, jn = 0;
+  AdjTileView o;
+  if (lane == 0) {
+    const double cb = cos_t[v], sb = sin_t[v];
+    const double qx = Tx - a.sid * sb, qy = Ty - a.sid * cb;
+    const double U = qx * cb - qy * sb, W = -(qx * sb + qy * cb);  // W > 0: the grid is below the source
+    const double r2 = U * U + W * W, r4 = r2 * r2;
+    const double phi = atan2(U, W);
+    const double pU = W / r2, pW = -U / r2;
+    const double pUU = -2.0 * U * W / r4, pWW = 2.0 * U * W / r4, pUW = (U * U - W * W) / r4;
+    // dU/dx = cb, dU/dy = -sb, dW/dx = -sb, dW/dy = -cb
+    const double px = pU * cb - pW * sb, py = -pU * sb - pW * cb;
+    const double pxx = pUU * cb * cb - 2.0 * pUW * cb * sb + pWW * sb * sb;
+    const double pyy = pUU * sb * sb + 2.0 * pUW * sb * cb + pWW * cb * cb;
+    const double pxy = -pUU * cb * sb + pUW * (sb * sb - cb * cb) + pWW * sb * cb;
+    const double ida = a.inv_dalpha;
+    const double D = sqrt(r2), Dmin = D - lmax - h * 1.4142135623730951;
+    // third-order remainder of the expansion (its bound doubled) plus rounding
+    const double rem = 2.0 * (lmax / Dmin) * (lmax / Dmin) * (lmax / Dmin) * ida + 0.02;
+    // A ray through the tile leaves the source within delta of the direction
+    // to the tile centre, so h(|dx| + |dy|), the half-width of a cell across
+    // the ray, is at most h(|qx| + |qy|)/D + h sqrt(2) delta.
+    const double delta = asin(fmin(1.0, (lmax + h * 1.4142135623730951) / D));
+    const double hw = h * fmin(1.4142135623730951, (fabs(qx) + fabs(qy)) / D + 1.4142135623730951 * delta);
+    const double dj = asin(fmin(1.0, hw / Dmin)) * ida + rem;
+    const double jcT = a.iso - phi * ida - a.start;  // 0-based channel at the tile centre
+    const double Jx = -px * ida, Jy = -py * ida, Jxx = -0.5 * pxx * ida, Jxy = -pxy * ida, Jyy = -0.5 * pyy * ida;
+    const double span = fabs(Jx) * Lx + fabs(Jy) * Ly + fabs(Jxx) * Lx * Lx + fabs(Jxy) * Lx * Ly +
+                        fabs(Jyy) * Ly * Ly + dj + 1.0;
+    int lo = (int)floor(jcT - span), hi = (int)ceil(jcT + span);
+    lo = max(lo, 0);
+    hi = min(hi, a.C - 1);
+    jlo = lo;
+    jn = max(hi - lo + 1, 0);
+    if (jn > kAdjW) {
+      jn = kAdjW;
+      atomicOr(status, 1);
+    }
+    o.a = make_float4((float)(jcT - lo), (float)Jx, (float)Jy, (float)Jxx);
+    o.b = make_float4((float)Jxy, (float)Jyy, (float)dj, 0.0f);
+    o.c = make_int4(jn > 0 ? (int)floor(2.0 * dj) + 1 : 0, jlo, jn, 0);
+  }
+  jlo = __shfl_sync(0xffffffffu, jlo, 0);
+  jn = __shfl_sync(0xffffffffu, jn, 0);
+  int cplx = 0;
+  for (int j = lane; j < jn; j += 32) {
+    const int4 r = rec[(long long)v * a.C + jlo + j];
+    if ((r.x & 3) != kAdjRayFast) continue;
+    const int lo = (r.y & 0xffff) - 1, hi = (r.y >> 16) - 1;
+    const int c0 = (r.x >> 2) ? e0 - 1 : f0 - 1;  // the tile's first cell on the ray's major axis
+    const int c1 = c0 + ((r.x >> 2) ? TX : TY) - 1;
+    bool cx = c0 < lo || c1 > hi;
+    if (r.z >= 0) {
+      const int lc = r.z & 0xffff, lr = r.z >> 16;
+      cx = cx || (lc >= e0 - 1 && lc <= e0 + TX - 2 && lr >= f0 - 1 && lr <= f0 + TY - 2);
+    }
+    cplx |= cx;
+  }
+  cplx = __any_sync(0xffffffffu, cplx);
+  if (lane == 0) {
+    o.c.w = cplx;
+    out[item] = o;
+  }
+}
+
+// K candidate rays k0.. of one view for one cell, unrolled; candidate i
+// counts when 0 <= j0 + i < jlim.  len = min(2h/a, (h(a+c) - |b|)/(a c))
+// clipped at 0, and with cplx the walk's major-index range and lumped piece.
+template <int M, int NQ, int K, int ST>
+__device__ __forceinline__ void adj_cells(const float4* s_q, const int4* s_x, int cplx, int k0, int j0, int jlim,
+                                          float lx, float ly, int colx, int rowx, int pix, float* acc) {
+#pragma unroll
+  for (int i = 0; i < K; i++) {
+    if ((unsigned)(j0 + i) < (unsigned)jlim) {
+      const int k = k0 + i;
+      if (!VCT_INDEX_OK(k >= 0 && k < ST)) continue;
+      const float4 q0 = s_q[k];
+      const float4 q1 = s_q[ST + k];
+      const float b = fmaf(q0.x, ly, fmaf(-q0.y, lx, q0.z));
+      float len = fmaxf(fminf(q1.x, (q0.w - fabsf(b)) * q1.y), 0.0f);
+      if (cplx) {
+        const int4 x = s_x[k];
+        const int mi = x.x ? colx : rowx;
+        if (mi < (x.y & 0xffff) || mi > (x.y >> 16)) len = 0.0f;
+        if (x.z == pix) len += __int_as_float(x.w);
+      }
+      if (M > 0) acc[0] = fmaf(len, q1.z, acc[0]);
+      if (M > 1) acc[1 % M] = fmaf(len, q1.w, acc[1 % M]);
+      if (NQ > 2) {
+        const float4 q2 = s_q[2 * ST + k];
+        if (M > 2) acc[2 % M] = fmaf(len, q2.x, acc[2 % M]);
+        if (M > 3) acc[3 % M] = fmaf(len, q2.y, acc[3 % M]);
+        if (M > 4) acc[4 % M] = fmaf(len, q2.z, acc[4 % M]);
+        if (M > 5) acc[5 % M] = fmaf(len, q2.w, acc[5 % M]);
+      }
+      if (NQ > 3) {
+        const float4 q3 = s_q[3 * ST + k];
+        if (M > 6) acc[6 % M] = fmaf(len, q3.x, acc[6 % M]);
+        if (M > 7) acc[7 % M] = fmaf(len, q3.y, acc[7 % M]);
+      }
+    }
+  }
 }
 
 // The gather runs over the (N+1) x (N+1) cells with indices -1..N-1: cells
 // at index -1 lie outside the grid, but the walk's truncating cast puts their
-// pieces on index 0 (adj_fold_kernel adds them there).  One thread per cell.
-// Staged per ray (shared memory, vector loads):
-//   A = (dx, dy, offset of the ray from the tile centre, h*(|dx|+|dy|))
-//   B = (2h/max(|dx|,|dy|), 1/(|dx||dy|), lumped length, lumped pixel bits)
-//   K = (xmaj, (maj_lo+1) | (maj_hi+1) << 16), G = the ray's M factors.
-// A ray that the fast walk does not take gets h*(|dx|+|dy|) = -inf (no
-// chord) and no lumped pixel.  The chord of a line at offset b from the
-// centre of a square of half-size h, direction with components a >= c:
-// 2h/a while |b| <= h(a-c), then (h(a+c) - |b|)/(a c) down to 0.
+// pieces on index 0 (adj_fold_kernel adds them there).  One thread per cell
+// of a TX x TY tile; blocks loop over the tiles.  Per round every warp stages
+// one view's rays of the tile's channel window (from its AdjTileView): per
+// ray q0 = (dx, dy, offset from the tile centre, h(|dx|+|dy|)),
+// q1 = (2h/max(|dx|,|dy|), 1/(|dx||dy|), g0, g1), q2 = (g2..g5),
+// q3 = (g6, g7), and x = (xmaj, major-index range, lumped pixel, length).
+// A ray the fast walk does not take gets h(|dx|+|dy|) = -inf (no chord) and
+// no lumped pixel.  The chord of a line at offset b from the centre of a
+// square of half-size h, direction with components a >= c: 2h/a while
+// |b| <= h(a-c), then (h(a+c) - |b|)/(a c) down to 0.
 template <int M, int TX, int TY>
 __global__ void __launch_bounds__(TX * TY)
 adj_gather_kernel(AdjGeom a, const double* __restrict__ cos_t, const double* __restrict__ sin_t,
                   const double2* __restrict__ dir, const int4* __restrict__ rec, const float* __restrict__ gr,
-                  float* __restrict__ ext, int* __restrict__ status) {
-  constexpr int MG = (M + 3) / 4 * 4;
-  __shared__ float4 s_A[kAdjCap];
-  __shared__ float4 s_B[kAdjCap];
-  __shared__ int2 s_K[kAdjCap];
-  __shared__ float4 s_g4[(MG / 4) * kAdjCap];  // ray factors, quad q of ray k at q * kAdjCap + k
-  __shared__ int s_jlo[kAdjVB], s_jn[kAdjVB], s_base[kAdjVB + 1], s_cplx[kAdjVB], s_nvb;
-  __shared__ float s_cb[kAdjVB], s_sb[kAdjVB], s_dtx[kAdjVB], s_dty[kAdjVB];
+                  const AdjTileView* __restrict__ tv, float* __restrict__ ext) {
+  constexpr int NT = TX * TY, VB = NT / 32;  // one view per warp per round
+  constexpr int NQ = M <= 2 ? 2 : (M <= 6 ? 3 : 4);
+  __shared__ float4 s_q[NQ][VB * kAdjW];
+  __shared__ int4 s_x[VB * kAdjW];
+  __shared__ AdjTileView s_v[VB];
 
   const int N = a.N, NE1 = N + 1;
-  const int tx = threadIdx.x % TX, ty = threadIdx.x / TX;
-  const int e0 = blockIdx.x * TX, f0 = blockIdx.y * TY;  // first extended column / row
-  const int col = e0 + tx - 1, row = f0 + ty - 1;         // cell indices, -1..N-1
-  const bool live = col < N && row < N;
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  // Each warp covers a patch of PX x (32/PX) cells, as square as the tile
+  // allows: the rays its lanes read then span the fewest channels, so its
+  // shared-memory loads touch the fewest distinct lines.
+  constexpr int PX = TX >= 8 ? 8 : TX, PY = 32 / PX, WPR = TX / PX;  // warps per tile row of patches
+  static_assert(TX % PX == 0 && TY % PY == 0, "the tile must split into whole warp patches");
+  const int tx = (warp % WPR) * PX + lane % PX, ty = (warp / WPR) * PY + lane / PX;
   const double s = a.s;
   const float h = (float)(0.5 * s);
-  // Tile centre (world cm; x right, y up; row r spans y in ((n-r-1)s, (n-r)s]).
-  const double Tx = (e0 - 1 + 0.5 * TX - a.nxm) * s;
-  const double Ty = (a.nxm - (f0 - 1) - 0.5 * TY) * s;
+  // Cell-centre offsets from the tile centre, and the quadratic's terms.
   const float lx = (float)((tx + 0.5 - 0.5 * TX) * s);
   const float ly = (float)((0.5 * TY - ty - 0.5) * s);
-  const int pix = (col >= 0 && row >= 0) ? row * N + col : -2;  // -2: never a lumped pixel
-  const int colx = col + 1, rowx = row + 1;
-  const float iso = (float)a.iso, ida = (float)a.inv_dalpha;
-  const float kdj = h * ida * 1.05f;
-
-  double dacc[M];
-#pragma unroll
-  for (int m = 0; m < M; m++) dacc[m] = 0.0;
-
+  const float lxx = lx * lx, lxy = lx * ly, lyy = ly * ly;
+  const int nbx = (NE1 + TX - 1) / TX, nby = (NE1 + TY - 1) / TY;
   const int V = a.views_used;
-  for (int v0 = 0; v0 < V;) {
-    const int nvc = min(kAdjVB, V - v0);  // views considered this round
-    // Channel window of the tile for each view: the angles of the tile's
-    // corners grown by one cell, plus two channels.
-    if (threadIdx.x < nvc) {
-      const int v = v0 + threadIdx.x;
-      const double cb = cos_t[v], sb = sin_t[v];
-      const double Sx = a.sid * sb, Sy = a.sid * cb;
-      const double x0 = (e0 - 2 - a.nxm) * s, x1 = (e0 + TX - a.nxm) * s;
-      const double y0 = (a.nxm - f0 - TY) * s, y1 = (a.nxm - f0 + 2) * s;
-      float tmin = 1e30f, tmax = -1e30f;
-#pragma unroll
-      for (int k = 0; k < 4; k++) {
-        const double qx = ((k & 1) ? x1 : x0) - Sx, qy = ((k & 2) ? y1 : y0) - Sy;
-        const float u = (float)(qx * cb - qy * sb), w = (float)(qx * sb + qy * cb);
-        const float t = fan_angle(u, w);
-        tmin = fminf(tmin, t);
-        tmax = fmaxf(tmax, t);
-      }
-      int jlo = (int)floorf(iso - tmax * ida) - 2 - a.start;
-      int jhi = (int)ceilf(iso - tmin * ida) + 2 - a.start;
-      jlo = max(jlo, 0);
-      jhi = min(jhi, a.C - 1);
-      int jn = jhi - jlo + 1;
-      if (jn < 0) jn = 0;
-      if (jn > kAdjWMax) {
-        jn = kAdjWMax;
-        atomicOr(status, 1);
-      }
-      s_jlo[threadIdx.x] = jlo;
-      s_jn[threadIdx.x] = jn;
-      s_cplx[threadIdx.x] = 0;
-      s_cb[threadIdx.x] = (float)cb;
-      s_sb[threadIdx.x] = (float)sb;
-      s_dtx[threadIdx.x] = (float)(Tx - Sx);
-      s_dty[threadIdx.x] = (float)(Ty - Sy);
-    }
-    __syncthreads();
-    if (threadIdx.x == 0) {  // the views whose windows fit the staging space
-      int b = 0, k = 0;
-      for (; k < nvc && b + s_jn[k] <= kAdjCap; k++) {
-        s_base[k] = b;
-        b += s_jn[k];
-      }
-      s_base[k] = b;
-      s_nvb = k;
-    }
-    __syncthreads();
-    const int nvb = s_nvb;
-    // Stage the window's rays: direction and offset from the tile centre in
-    // FP64, then float (small for every ray that can reach the tile).
-    const int total = s_base[nvb];
-    for (int k = threadIdx.x; k < total; k += TX * TY) {
-      int vb = 0;
-      while (vb + 1 < nvb && k >= s_base[vb + 1]) vb++;
-      const int v = v0 + vb;
-      const int c = s_jlo[vb] + (k - s_base[vb]);
-      const long long ray = (long long)v * a.C + c;
-      if (!VCT_INDEX_OK(v < a.views_used && c >= 0 && c < a.C && k < kAdjCap)) continue;
-      const double cb = cos_t[v], sb = sin_t[v];
-      const double2 e = dir[c];
-      const double dx = e.x * cb + e.y * sb, dy = -e.x * sb + e.y * cb;
-      const double Sx = a.sid * sb, Sy = a.sid * cb;
-      const double bt = dx * (Ty - Sy) - dy * (Tx - Sx);
-      const float ax = fabsf((float)dx), ay = fabsf((float)dy);
-      const int4 r = rec[ray];
-      const bool fast = (r.x & 3) == kAdjRayFast;
-      s_A[k] = make_float4((float)dx, (float)dy, (float)bt, fast ? h * (ax + ay) : -INFINITY);
-      s_B[k] = make_float4(2.0f * h / fmaxf(ax, ay), 1.0f / (ax * ay), fast ? __int_as_float(r.w) : 0.0f,
-                           __int_as_float(fast ? r.z : -1));
-      s_K[k] = make_int2(r.x >> 2, r.y);
-#pragma unroll
-      for (int q = 0; q < MG / 4; q++) {
-        float4 gq;
-        gq.x = 4 * q + 0 < M ? gr[ray * M + 4 * q + 0] : 0.0f;
-        gq.y = 4 * q + 1 < M ? gr[ray * M + 4 * q + 1] : 0.0f;
-        gq.z = 4 * q + 2 < M ? gr[ray * M + 4 * q + 2] : 0.0f;
-        gq.w = 4 * q + 3 < M ? gr[ray * M + 4 * q + 3] : 0.0f;
-        s_g4[q * kAdjCap + k] = gq;
-      }
-      // Does the ray's walk end or lump inside this tile?  If no staged ray
-      // of the view does, the whole block takes the plain chord path.
-      if (fast) {
-        const int lo = (r.y & 0xffff) - 1, hi = (r.y >> 16) - 1;
-        const int c0 = (r.x >> 2) ? e0 - 1 : f0 - 1;  // the tile's first cell on the ray's major axis
-        const int c1 = c0 + ((r.x >> 2) ? TX : TY) - 1;
-        bool cplx = c0 < lo || c1 > hi;
-        if (r.z >= 0) {
-          const int lc = r.z % a.N, lr = r.z / a.N;
-          cplx = cplx || (lc >= e0 - 1 && lc <= e0 + TX - 2 && lr >= f0 - 1 && lr <= f0 + TY - 2);
-        }
-        if (cplx) atomicOr(&s_cplx[vb], 1);
-      }
-    }
-    __syncthreads();
 
-    float acc[M];
+  for (int tile = blockIdx.x; tile < nbx * nby; tile += gridDim.x) {
+    const int e0 = (tile % nbx) * TX, f0 = (tile / nbx) * TY;  // first extended column / row
+    const int col = e0 + tx - 1, row = f0 + ty - 1;              // cell indices, -1..N-1
+    // Tile centre (world cm; x right, y up; row r spans y in ((n-r-1)s, (n-r)s]).
+    const double Tx = (e0 - 1 + 0.5 * TX - a.nxm) * s;
+    const double Ty = (a.nxm - (f0 - 1) - 0.5 * TY) * s;
+    const int pix = (col >= 0 && row >= 0) ? (col | (row << 16)) : -2;  // -2: never a lumped pixel
+    const int colx = col + 1, rowx = row + 1;
+    const AdjTileView* __restrict__ tvt = tv + (size_t)tile * V;
+
+    double dacc[M];
 #pragma unroll
-    for (int m = 0; m < M; m++) acc[m] = 0.0f;
-    for (int vb = 0; vb < nvb; vb++) {
-      const float cb = s_cb[vb], sb = s_sb[vb];
-      const int jlo = s_jlo[vb], jn = s_jn[vb], base = s_base[vb];
-      // Cell centre relative to the source, its fan angle and angular
-      // half-width in channels (with a margin).
-      const float qx = s_dtx[vb] + lx, qy = s_dty[vb] + ly;
-      const float u = qx * cb - qy * sb, w = qx * sb + qy * cb;
-      const float jc = iso - fan_angle(u, w) * ida;
-      const float iq = rsqrtf(fmaf(qx, qx, qy * qy));
-      const float dj = fmaf((fabsf(qx) + fabsf(qy)) * iq * iq, kdj, 0.05f);
-      const int j0 = max((int)ceilf(jc - dj) - a.start - jlo, 0);
-      const int j1 = min((int)floorf(jc + dj) - a.start - jlo, jn - 1);
-      if (!s_cplx[vb]) {
-        // every candidate's walk covers the whole tile: chord only
-        for (int j = j0; j <= j1; j++) {
-          const int k = base + j;
-          if (!VCT_INDEX_OK(k >= 0 && k < kAdjCap)) continue;
-          const float4 A = s_A[k];
-          const float4 B = s_B[k];
-          const float b = fmaf(A.x, ly, fmaf(-A.y, lx, A.z));
-          const float num = A.w - fabsf(b);
-          const float len = num > 0.0f ? fminf(B.x, num * B.y) : 0.0f;
-#pragma unroll
-          for (int q = 0; q < MG / 4; q++) {
-            const float4 g = s_g4[q * kAdjCap + k];
-            if (4 * q + 0 < M) acc[4 * q + 0] = fmaf(len, g.x, acc[4 * q + 0]);
-            if (4 * q + 1 < M) acc[4 * q + 1] = fmaf(len, g.y, acc[4 * q + 1]);
-            if (4 * q + 2 < M) acc[4 * q + 2] = fmaf(len, g.z, acc[4 * q + 2]);
-            if (4 * q + 3 < M) acc[4 * q + 3] = fmaf(len, g.w, acc[4 * q + 3]);
-          }
+    for (int m = 0; m < M; m++) dacc[m] = 0.0;
+
+    for (int v0 = 0; v0 < V; v0 += VB) {
+      // ---- staging: warp `warp` takes view v0 + warp
+      {
+        const int v = v0 + warp;
+        int4 vc = make_int4(0, 0, 0, 0);
+        if (v < V) {
+          vc = tvt[v].c;
+          if (lane == 0) s_v[warp] = tvt[v];
+        } else if (lane == 0) {
+          s_v[warp].c = vc;
         }
-      } else {
-        for (int j = j0; j <= j1; j++) {
-          const int k = base + j;
-          if (!VCT_INDEX_OK(k >= 0 && k < kAdjCap)) continue;
-          const float4 A = s_A[k];
-          const float4 B = s_B[k];
-          const int2 K = s_K[k];
-          const float b = fmaf(A.x, ly, fmaf(-A.y, lx, A.z));
-          const float num = A.w - fabsf(b);
-          float len = num > 0.0f ? fminf(B.x, num * B.y) : 0.0f;
-          const int mi = K.x ? colx : rowx;
-          if (mi < (K.y & 0xffff) || mi > (K.y >> 16)) len = 0.0f;
-          if (__float_as_int(B.w) == pix) len += B.z;
+        const int jlo = vc.y, jn = vc.z;
+        const double cb = v < V ? cos_t[v] : 0.0, sb = v < V ? sin_t[v] : 0.0;
+        const double Sx = a.sid * sb, Sy = a.sid * cb;
+        for (int j = lane; j < jn; j += 32) {
+          const int c = jlo + j;
+          const int k = warp * kAdjW + j;
+          const long long ray = (long long)v * a.C + c;
+          if (!VCT_INDEX_OK(v < a.views_used && c >= 0 && c < a.C && j < kAdjW)) continue;
+          const double2 e = dir[c];
+          const double dx = e.x * cb + e.y * sb, dy = -e.x * sb + e.y * cb;
+          const double bt = dx * (Ty - Sy) - dy * (Tx - Sx);
+          const float ax = fabsf((float)dx), ay = fabsf((float)dy);
+          const int4 r = rec[ray];
+          const bool fast = (r.x & 3) == kAdjRayFast;
+          const float* gp = gr + ray * M;
+          float g[8];
 #pragma unroll
-          for (int q = 0; q < MG / 4; q++) {
-            const float4 g = s_g4[q * kAdjCap + k];
-            if (4 * q + 0 < M) acc[4 * q + 0] = fmaf(len, g.x, acc[4 * q + 0]);
-            if (4 * q + 1 < M) acc[4 * q + 1] = fmaf(len, g.y, acc[4 * q + 1]);
-            if (4 * q + 2 < M) acc[4 * q + 2] = fmaf(len, g.z, acc[4 * q + 2]);
-            if (4 * q + 3 < M) acc[4 * q + 3] = fmaf(len, g.w, acc[4 * q + 3]);
-          }
+          for (int m = 0; m < 8; m++) g[m] = m < M ? gp[m] : 0.0f;
+          s_q[0][k] = make_float4((float)dx, (float)dy, (float)bt, fast ? h * (ax + ay) : -INFINITY);
+          s_q[1][k] = make_float4(2.0f * h / fmaxf(ax, ay), 1.0f / (ax * ay), g[0], g[1]);
+          if (NQ > 2) s_q[2 % NQ][k] = make_float4(g[2], g[3], g[4], g[5]);
+          if (NQ > 3) s_q[3 % NQ][k] = make_float4(g[6], g[7], 0.0f, 0.0f);
+          s_x[k] = make_int4(r.x >> 2, r.y, fast ? r.z : -1, fast ? r.w : 0);
         }
       }
+      __syncthreads();
+
+      // ---- gather: every cell over the round's views
+      float acc[M];
+#pragma unroll
+      for (int m = 0; m < M; m++) acc[m] = 0.0f;
+#pragma unroll 1
+      for (int vb = 0; vb < VB; vb++) {
+        const int4 vi = s_v[vb].c;
+        if (vi.x == 0) continue;
+        const float4 fa = s_v[vb].a, fb = s_v[vb].b;
+        const float jc = fmaf(fb.y, lyy, fmaf(fb.x, lxy, fmaf(fa.w, lxx, fmaf(fa.z, ly, fmaf(fa.y, lx, fa.x)))));
+        // this cell's candidates: the integers in (jc - dj, jc + dj) that lie
+        // in the window, j0 <= j < jlim; at most kmax of them
+        const int j0 = (int)floorf(jc - fb.z) + 1;
+        const int jlim = max(min((int)ceilf(jc + fb.z), vi.z), 0);  // >= 0: the test below is unsigned
+        const int k0 = vb * kAdjW + j0;
+        switch (vi.x) {  // block-uniform
+          case 1: adj_cells<M, NQ, 1, VB * kAdjW>(&s_q[0][0], s_x, vi.w, k0, j0, jlim, lx, ly, colx, rowx, pix, acc); break;
+          case 2: adj_cells<M, NQ, 2, VB * kAdjW>(&s_q[0][0], s_x, vi.w, k0, j0, jlim, lx, ly, colx, rowx, pix, acc); break;
+          case 3: adj_cells<M, NQ, 3, VB * kAdjW>(&s_q[0][0], s_x, vi.w, k0, j0, jlim, lx, ly, colx, rowx, pix, acc); break;
+          default:
+            for (int i = 0; i < vi.x; i += 4)
+              adj_cells<M, NQ, 4, VB * kAdjW>(&s_q[0][0], s_x, vi.w, k0 + i, j0 + i, jlim, lx, ly, colx, rowx, pix, acc);
+            break;
+        }
+      }
+#pragma unroll
+      for (int m = 0; m < M; m++) dacc[m] += (double)acc[m];
+      __syncthreads();
     }
+    if (col < N && row < N) {
+      const size_t n2 = (size_t)NE1 * NE1;
+      const size_t o = (size_t)(row + 1) * NE1 + (col + 1);
 #pragma unroll
-    for (int m = 0; m < M; m++) dacc[m] += (double)acc[m];
-    __syncthreads();
-    v0 += nvb;
+      for (int m = 0; m < M; m++) ext[m * n2 + o] = (float)dacc[m];
+    }
   }
-  if (!live) return;
-  const size_t n2 = (size_t)NE1 * NE1;
-  const size_t o = (size_t)(row + 1) * NE1 + (col + 1);
-#pragma unroll
-  for (int m = 0; m < M; m++) ext[m * n2 + o] = (float)dacc[m];
 }
 
 // grad[m][r][c] = ext at (r, c), plus the folded cells at index -1 (row -1
@@ -587,46 +629,88 @@ __global__ void adj_fold_kernel(int M, int N, const float* __restrict__ ext, con
 
 // Tile shapes, largest first; the channel window of a tile grows with its
 // size and shrinks with the source distance.
-static const int kTiles[][2] = {{32, 8}, {16, 8}, {8, 8}, {8, 4}};
+static const int kTiles[][2] = {{16, 16}, {16, 8}, {8, 8}, {8, 4}};
 
 int adj_pick_tile(const AdjGeom& a, double lim) {
-  // Nearest approach of the grown tile to the source, and its half-diagonal.
+  // Nearest approach of a tile's cells to the source, and its half-diagonal.
   const double dmin = a.sid - (lim + 2.0 * a.s) * sqrt(2.0);
   if (!(dmin > 0)) return -1;
   for (int t = 0; t < 4; t++) {
     const double hd = 0.5 * sqrt((double)(kTiles[t][0] + 2) * (kTiles[t][0] + 2) +
                                  (double)(kTiles[t][1] + 2) * (kTiles[t][1] + 2)) * a.s;
     if (hd >= dmin) continue;
+    // the tile's angular extent, twice the widest cell half-width, and the
+    // window's margins (the kernel's span adds one channel each side)
     const double ang = 2.0 * asin(hd / dmin);
-    const double jn = ang * a.inv_dalpha + 6.0;
-    if (jn <= kAdjWMax) return t;
+    const double dj = asin(fmin(1.0, 0.5 * a.s * sqrt(2.0) / (dmin - hd))) * a.inv_dalpha + 0.1;
+    const double jn = ang * a.inv_dalpha + 2.0 * dj + 5.0;
+    if (jn <= kAdjW) return t;
   }
   return -1;
 }
 
-template <int M>
-static int launch_adj_gather_m(const AdjGeom& a, int tile, const double* d_cos, const double* d_sin,
-                               const double2* d_dir, const int4* d_rec, const float* d_g, float* d_ext, int* d_status,
-                               cudaStream_t st) {
-  const int TX = kTiles[tile][0], TY = kTiles[tile][1];
-  dim3 grid((a.N + 1 + TX - 1) / TX, (a.N + 1 + TY - 1) / TY);
+// Tiles of the gather for tile shape t (adj_pick_tile).
+static int tiles_of(const AdjGeom& a, int t) {
+  return ((a.N + 1 + kTiles[t][0] - 1) / kTiles[t][0]) * ((a.N + 1 + kTiles[t][1] - 1) / kTiles[t][1]);
+}
+
+size_t adj_tileview_bytes(const AdjGeom& a, int tile) {
+  if (tile < 0 || tile > 3) return 0;
+  return (size_t)tiles_of(a, tile) * a.views_used * sizeof(AdjTileView);
+}
+
+int launch_adj_tiles(const AdjGeom& a, int tile, const double* d_cos, const double* d_sin, const int4* d_rec,
+                     void* d_tv, int* d_status, cudaStream_t st) {
+  if (tile < 0 || tile > 3) return fail(VCT_E_UNSUPPORTED, "adjoint: no tile fits the channel window");
+  const long long items = (long long)tiles_of(a, tile) * a.views_used;
+  if (items == 0) return VCT_OK;
+  const unsigned blocks = (unsigned)((items * 32 + 127) / 128);
+  AdjTileView* tv = reinterpret_cast<AdjTileView*>(d_tv);
   switch (tile) {
-    case 0: adj_gather_kernel<M, 32, 8><<<grid, 256, 0, st>>>(a, d_cos, d_sin, d_dir, d_rec, d_g, d_ext, d_status); break;
-    case 1: adj_gather_kernel<M, 16, 8><<<grid, 128, 0, st>>>(a, d_cos, d_sin, d_dir, d_rec, d_g, d_ext, d_status); break;
-    case 2: adj_gather_kernel<M, 8, 8><<<grid, 64, 0, st>>>(a, d_cos, d_sin, d_dir, d_rec, d_g, d_ext, d_status); break;
-    default: adj_gather_kernel<M, 8, 4><<<grid, 32, 0, st>>>(a, d_cos, d_sin, d_dir, d_rec, d_g, d_ext, d_status); break;
+    case 0: adj_tiles_kernel<16, 16><<<blocks, 128, 0, st>>>(a, d_cos, d_sin, d_rec, tv, d_status); break;
+    case 1: adj_tiles_kernel<16, 8><<<blocks, 128, 0, st>>>(a, d_cos, d_sin, d_rec, tv, d_status); break;
+    case 2: adj_tiles_kernel<8, 8><<<blocks, 128, 0, st>>>(a, d_cos, d_sin, d_rec, tv, d_status); break;
+    default: adj_tiles_kernel<8, 4><<<blocks, 128, 0, st>>>(a, d_cos, d_sin, d_rec, tv, d_status); break;
   }
   VCT_CUDA(cudaGetLastError());
   return VCT_OK;
 }
 
+template <int M, int TX, int TY>
+static int launch_adj_gather_t(const AdjGeom& a, const double* d_cos, const double* d_sin, const double2* d_dir,
+                               const int4* d_rec, const float* d_g, const AdjTileView* d_tv, float* d_ext,
+                               cudaStream_t st) {
+  const int ntiles = ((a.N + 1 + TX - 1) / TX) * ((a.N + 1 + TY - 1) / TY);
+  int dev = 0, sms = 0, per_sm = 0;
+  VCT_CUDA(cudaGetDevice(&dev));
+  VCT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  VCT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adj_gather_kernel<M, TX, TY>, TX * TY, 0));
+  const int grid = min(ntiles, max(1, per_sm) * sms);
+  adj_gather_kernel<M, TX, TY><<<grid, TX * TY, 0, st>>>(a, d_cos, d_sin, d_dir, d_rec, d_g, d_tv, d_ext);
+  VCT_CUDA(cudaGetLastError());
+  return VCT_OK;
+}
+
+template <int M>
+static int launch_adj_gather_m(const AdjGeom& a, int tile, const double* d_cos, const double* d_sin,
+                               const double2* d_dir, const int4* d_rec, const float* d_g, const AdjTileView* d_tv,
+                               float* d_ext, cudaStream_t st) {
+  switch (tile) {
+    case 0: return launch_adj_gather_t<M, 16, 16>(a, d_cos, d_sin, d_dir, d_rec, d_g, d_tv, d_ext, st);
+    case 1: return launch_adj_gather_t<M, 16, 8>(a, d_cos, d_sin, d_dir, d_rec, d_g, d_tv, d_ext, st);
+    case 2: return launch_adj_gather_t<M, 8, 8>(a, d_cos, d_sin, d_dir, d_rec, d_g, d_tv, d_ext, st);
+    default: return launch_adj_gather_t<M, 8, 4>(a, d_cos, d_sin, d_dir, d_rec, d_g, d_tv, d_ext, st);
+  }
+}
+
 int launch_adj_gather(const AdjGeom& a, int M, int tile, const double* d_cos, const double* d_sin,
-                      const double2* d_dir, const int4* d_rec, const float* d_g, float* d_ext, int* d_status,
+                      const double2* d_dir, const int4* d_rec, const float* d_g, const void* d_tv, float* d_ext,
                       cudaStream_t st) {
   if (tile < 0 || tile > 3) return fail(VCT_E_UNSUPPORTED, "adjoint: no tile fits the channel window");
+  const AdjTileView* tv = reinterpret_cast<const AdjTileView*>(d_tv);
   switch (M) {
 #define VCT_CASE(mm) \
-  case mm: return launch_adj_gather_m<mm>(a, tile, d_cos, d_sin, d_dir, d_rec, d_g, d_ext, d_status, st);
+  case mm: return launch_adj_gather_m<mm>(a, tile, d_cos, d_sin, d_dir, d_rec, d_g, tv, d_ext, st);
     VCT_CASE(1) VCT_CASE(2) VCT_CASE(3) VCT_CASE(4) VCT_CASE(5) VCT_CASE(6) VCT_CASE(7) VCT_CASE(8)
 #undef VCT_CASE
     default: return fail(VCT_E_ARG, "adjoint: 1..8 materials");

@@ -111,6 +111,7 @@ struct vct_ctx {
   vct::DBuf<int4> adj_rec;
   vct::DBuf<int> adj_special, adj_ints;  // ints: [0] special count, [1] status
   vct::DBuf<double2> adj_dir;
+  vct::DBuf<float4> adj_tv;  // per (tile, view) records of the gather
   vct::DBuf<float> adj_g;
   vct::DBuf<double> adj_part, adj_loss;
   vct::DBuf<unsigned int> adj_gmax;

@@ -226,6 +226,7 @@ void vct_destroy(vct_ctx* c) {
   for (auto& h : c->fbp_h) h.release();
   c->fbp_g.release(); c->fbp_q.release(); c->fbp_sino.release(); c->fbp_img.release(); c->fbp_tacc.release();
   c->adj_rec.release(); c->adj_special.release(); c->adj_ints.release(); c->adj_dir.release();
+  c->adj_tv.release();
   c->adj_g.release(); c->adj_part.release(); c->adj_loss.release(); c->adj_gmax.release();
   c->adj_sacc.release(); c->adj_meas.release(); c->adj_wts.release(); c->adj_grad.release();
   c->adj_ext.release();
@@ -1086,9 +1087,17 @@ static int adj_prepare(vct_ctx* c) {
                             c->adj_special.p, c->adj_ints.p, c->stream)))
     return rc;
   c->launches++;
-  int ns = 0;
-  VCT_CUDA(cudaMemcpyAsync(&ns, c->adj_ints.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
+  // The gather's per (tile, view) records: geometry and walk plans only.
+  if ((rc = c->adj_tv.ensure((adj_tileview_bytes(a, c->adj_tile) + 15) / 16))) return rc;
+  if ((rc = launch_adj_tiles(a, c->adj_tile, c->cos_t.p, c->sin_t.p, c->adj_rec.p, c->adj_tv.p, c->adj_ints.p + 1,
+                             c->stream)))
+    return rc;
+  c->launches++;
+  int ns_status[2] = {0, 0};
+  VCT_CUDA(cudaMemcpyAsync(ns_status, c->adj_ints.p, 2 * sizeof(int), cudaMemcpyDeviceToHost, c->stream));
   VCT_CUDA(cudaStreamSynchronize(c->stream));
+  if (ns_status[1]) return fail(VCT_E_UNSUPPORTED, "adjoint: a tile's channel window overflowed");
+  const int ns = ns_status[0];
   c->adj_nspecial = ns;
   // Terms per pixel of the scatter: at most a few segments per ray and pixel.
   a.log2_terms = (int)ceil(log2(4.0 * ns + 2.0));
@@ -1145,7 +1154,7 @@ static int adj_run(vct_ctx* c, int mode, const float* d_meas, const float* d_wts
   }
   if ((rc = c->adj_ext.ensure((size_t)M * (dg.N + 1) * (dg.N + 1)))) return rc;
   if ((rc = launch_adj_gather(c->ag, M, c->adj_tile, c->cos_t.p, c->sin_t.p, c->adj_dir.p, c->adj_rec.p, d_g,
-                              c->adj_ext.p, c->adj_ints.p + 1, c->stream)))
+                              c->adj_tv.p, c->adj_ext.p, c->stream)))
     return rc;
   c->timer.mark("adj_gather_kernel", c->stream);
   if ((rc = launch_adj_fold(c->ag, M, sacc, c->adj_gmax.p, c->adj_ext.p, d_grad, c->stream))) return rc;

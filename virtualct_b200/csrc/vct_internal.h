@@ -215,8 +215,14 @@ int adj_pick_tile(const AdjGeom& a, double lim);
 // Gather into d_ext [M][N+1][N+1] (cells -1..N-1), then fold into d_grad
 // [M][N][N] together with the exact-walk rays' fixed-point sums (d_sacc may
 // be NULL).  Two launches.
+// Per (tile, view) records of the gather (geometry only, once per context):
+// their size in bytes, and the kernel that fills them (window overflow sets
+// bit 0 of *d_status).
+size_t adj_tileview_bytes(const AdjGeom& a, int tile);
+int launch_adj_tiles(const AdjGeom& a, int tile, const double* d_cos, const double* d_sin, const int4* d_rec,
+                     void* d_tv, int* d_status, cudaStream_t st);
 int launch_adj_gather(const AdjGeom& a, int M, int tile, const double* d_cos, const double* d_sin,
-                      const double2* d_dir, const int4* d_rec, const float* d_g, float* d_ext, int* d_status,
+                      const double2* d_dir, const int4* d_rec, const float* d_g, const void* d_tv, float* d_ext,
                       cudaStream_t st);
 // Cells at index -1 onto index 0 and the exact-walk rays' fixed-point sums
 // added: d_ext [M][N+1][N+1] -> d_grad [M][N][N].

@@ -338,7 +338,8 @@ constexpr int kAdjW = 64;
 
 // Per (tile, view), computed once per context from the geometry and the walk
 // plans (adj_tiles_kernel):
-//   a = (J0, Jx, Jy, Jxx), b = (Jxy, Jyy, dj, 0), c = (kmax, jlo, jn, cplx).
+//   a = (J0, Jx, Jy, Jxx), b = (Jxy, Jyy, dj, bits of kmax | jn << 8 |
+//   cplx << 16), c = (kmax, jlo, jn, cplx).
 // The channel coordinate of a cell centre at offset (lx, ly) from the tile
 // centre is modelled as jc = J0 + Jx lx + Jy ly + Jxx lx^2 + Jxy lx ly +
 // Jyy ly^2 (second-order Taylor expansion of the fan angle at the tile
@@ -411,7 +412,7 @@ __global__ void adj_tiles_kernel(AdjGeom a, const double* __restrict__ cos_t, co
     }
     o.a = make_float4((float)(jcT - lo), (float)Jx, (float)Jy, (float)Jxx);
     o.b = make_float4((float)Jxy, (float)Jyy, (float)dj, 0.0f);
-    o.c = make_int4(jn > 0 ? (int)floor(2.0 * dj) + 1 : 0, jlo, jn, 0);
+    o.c = make_int4(jn > 0 ? min((int)floor(2.0 * dj) + 1, 255) : 0, jlo, jn, 0);
   }
   jlo = __shfl_sync(0xffffffffu, jlo, 0);
   jn = __shfl_sync(0xffffffffu, jn, 0);
@@ -432,6 +433,8 @@ __global__ void adj_tiles_kernel(AdjGeom a, const double* __restrict__ cos_t, co
   cplx = __any_sync(0xffffffffu, cplx);
   if (lane == 0) {
     o.c.w = cplx;
+    // what the gather's cell loop reads, in b.w: kmax | jn << 8 | cplx << 16
+    o.b.w = __int_as_float(o.c.x | (o.c.z << 8) | (cplx << 16));
     out[item] = o;
   }
 }
@@ -487,16 +490,26 @@ __device__ __forceinline__ void adj_cells(const float4* s_q, const int4* s_x, in
 // no lumped pixel.  The chord of a line at offset b from the centre of a
 // square of half-size h, direction with components a >= c: 2h/a while
 // |b| <= h(a-c), then (h(a+c) - |b|)/(a c) down to 0.
+#ifndef VCT_ADJ_VPW
+#define VCT_ADJ_VPW 1  // views each warp stages per round
+#endif
+#ifndef VCT_ADJ_MINBLOCKS
+#define VCT_ADJ_MINBLOCKS 0
+#endif
+#ifndef VCT_ADJ_VUNROLL
+#define VCT_ADJ_VUNROLL 1
+#endif
 template <int M, int TX, int TY>
-__global__ void __launch_bounds__(TX * TY)
+__global__ void __launch_bounds__(TX * TY, VCT_ADJ_MINBLOCKS)
 adj_gather_kernel(AdjGeom a, const double* __restrict__ cos_t, const double* __restrict__ sin_t,
                   const double2* __restrict__ dir, const int4* __restrict__ rec, const float* __restrict__ gr,
                   const AdjTileView* __restrict__ tv, float* __restrict__ ext) {
-  constexpr int NT = TX * TY, VB = NT / 32;  // one view per warp per round
+  constexpr int NW = TX * TY / 32, VB = NW * VCT_ADJ_VPW;  // views per round
+  constexpr int kVUnroll = VCT_ADJ_VUNROLL;
   constexpr int NQ = M <= 2 ? 2 : (M <= 6 ? 3 : 4);
   __shared__ float4 s_q[NQ][VB * kAdjW];
   __shared__ int4 s_x[VB * kAdjW];
-  __shared__ AdjTileView s_v[VB];
+  __shared__ float4 s_v[VB][2];  // a, b of each staged view's AdjTileView
 
   const int N = a.N, NE1 = N + 1;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
@@ -530,22 +543,24 @@ adj_gather_kernel(AdjGeom a, const double* __restrict__ cos_t, const double* __r
     for (int m = 0; m < M; m++) dacc[m] = 0.0;
 
     for (int v0 = 0; v0 < V; v0 += VB) {
-      // ---- staging: warp `warp` takes view v0 + warp
-      {
-        const int v = v0 + warp;
+      // ---- staging: warp `warp` takes views v0 + warp + NW * u
+#pragma unroll 1
+      for (int u = 0; u < VCT_ADJ_VPW; u++) {
+        const int vs = warp + NW * u;  // slot
+        const int v = v0 + vs;
         int4 vc = make_int4(0, 0, 0, 0);
         if (v < V) {
           vc = tvt[v].c;
-          if (lane == 0) s_v[warp] = tvt[v];
-        } else if (lane == 0) {
-          s_v[warp].c = vc;
+          if (lane < 2) s_v[vs][lane] = lane ? tvt[v].b : tvt[v].a;
+        } else if (lane == 1) {
+          s_v[vs][1] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);  // kmax 0: nothing to gather
         }
         const int jlo = vc.y, jn = vc.z;
         const double cb = v < V ? cos_t[v] : 0.0, sb = v < V ? sin_t[v] : 0.0;
         const double Sx = a.sid * sb, Sy = a.sid * cb;
         for (int j = lane; j < jn; j += 32) {
           const int c = jlo + j;
-          const int k = warp * kAdjW + j;
+          const int k = vs * kAdjW + j;
           const long long ray = (long long)v * a.C + c;
           if (!VCT_INDEX_OK(v < a.views_used && c >= 0 && c < a.C && j < kAdjW)) continue;
           const double2 e = dir[c];
@@ -571,11 +586,13 @@ adj_gather_kernel(AdjGeom a, const double* __restrict__ cos_t, const double* __r
       float acc[M];
 #pragma unroll
       for (int m = 0; m < M; m++) acc[m] = 0.0f;
-#pragma unroll 1
+#pragma unroll kVUnroll
       for (int vb = 0; vb < VB; vb++) {
-        const int4 vi = s_v[vb].c;
+        const float4 fb = s_v[vb][1];
+        const int bits = __float_as_int(fb.w);
+        const int4 vi = make_int4(bits & 0xff, 0, (bits >> 8) & 0xff, bits >> 16);  // kmax, -, jn, cplx
         if (vi.x == 0) continue;
-        const float4 fa = s_v[vb].a, fb = s_v[vb].b;
+        const float4 fa = s_v[vb][0];
         const float jc = fmaf(fb.y, lyy, fmaf(fb.x, lxy, fmaf(fa.w, lxx, fmaf(fa.z, ly, fmaf(fa.y, lx, fa.x)))));
         // this cell's candidates: the integers in (jc - dj, jc + dj) that lie
         // in the window, j0 <= j < jlim; at most kmax of them

@@ -490,9 +490,10 @@ __device__ __forceinline__ void adj_cells(const float4* s_q, const int4* s_x, in
 // no lumped pixel.  The chord of a line at offset b from the centre of a
 // square of half-size h, direction with components a >= c: 2h/a while
 // |b| <= h(a-c), then (h(a+c) - |b|)/(a c) down to 0.
-#ifndef VCT_ADJ_VPW
-#define VCT_ADJ_VPW 1  // views each warp stages per round
-#endif
+// Resident blocks per SM the registers are held to, and how far the loop over
+// a round's views is unrolled (measured on the 512^2, 800 x 609 gradient:
+// 3 blocks per SM 1.27 ms and unrolling by 2 1.15 ms, against 1.14 ms for
+// the defaults).
 #ifndef VCT_ADJ_MINBLOCKS
 #define VCT_ADJ_MINBLOCKS 0
 #endif
@@ -504,7 +505,7 @@ __global__ void __launch_bounds__(TX * TY, VCT_ADJ_MINBLOCKS)
 adj_gather_kernel(AdjGeom a, const double* __restrict__ cos_t, const double* __restrict__ sin_t,
                   const double2* __restrict__ dir, const int4* __restrict__ rec, const float* __restrict__ gr,
                   const AdjTileView* __restrict__ tv, float* __restrict__ ext) {
-  constexpr int NW = TX * TY / 32, VB = NW * VCT_ADJ_VPW;  // views per round
+  constexpr int NW = TX * TY / 32, VB = NW;  // views per round: one per warp
   constexpr int kVUnroll = VCT_ADJ_VUNROLL;
   constexpr int NQ = M <= 2 ? 2 : (M <= 6 ? 3 : 4);
   __shared__ float4 s_q[NQ][VB * kAdjW];
@@ -543,10 +544,9 @@ adj_gather_kernel(AdjGeom a, const double* __restrict__ cos_t, const double* __r
     for (int m = 0; m < M; m++) dacc[m] = 0.0;
 
     for (int v0 = 0; v0 < V; v0 += VB) {
-      // ---- staging: warp `warp` takes views v0 + warp + NW * u
-#pragma unroll 1
-      for (int u = 0; u < VCT_ADJ_VPW; u++) {
-        const int vs = warp + NW * u;  // slot
+      // ---- staging: warp `warp` takes view v0 + warp
+      {
+        const int vs = warp;  // slot
         const int v = v0 + vs;
         int4 vc = make_int4(0, 0, 0, 0);
         if (v < V) {

@@ -725,6 +725,21 @@ def bench_batched(stream, warmup, n=256):
     t_batch = _event_ms(stream, lambda: b.run(stream.cuda_stream), max(warmup, 3))
     cfg = b.config()
     b.close()
+
+    # The same slices without the FBP: MBFPA alone, the work the plain
+    # single-slice rays*bins/s figure measures.
+    mjobs = [vct.Job(j.geometry, j.maps, j.mu, j.pdf, sino=j.sino, sigma=j.sigma, seed=j.seed) for j in jobs]
+
+    def plain_mb():
+        for c, j in zip(ctxs, mjobs):
+            c.set_maps(j.maps)
+            c.mbfpa_dev(j.sigma, j.seed, j.sino)
+
+    t_plain_mb = _event_ms(stream, plain_mb, max(warmup, 3))
+    bm = vct.Batch(mjobs, tune=True)
+    t_batch_mb = _event_ms(stream, lambda: bm.run(stream.cuda_stream), max(warmup, 3))
+    cfg_mb = bm.config()
+    bm.close()
     for c in ctxs:
         c.close()
     return {"workload": f"{n} uneven slices: grids 256/384/512, kVp 80-140, 360-900 views, 512-800 channels, "
@@ -732,7 +747,11 @@ def bench_batched(stream, warmup, n=256):
             "value": units / t_batch * 1e3, "unit": "rays*bins/s", "slices_per_s": n / t_batch * 1e3,
             "ms_per_batch": t_batch, "plain_value": units / t_plain * 1e3, "plain_ms_per_batch": t_plain,
             "speedup_vs_plain": t_plain / t_batch, "rays_bins_per_batch": units, "create_and_tune_s": t_create,
-            "tuned": cfg, "l2": "inputs and outputs of one batch exceed L2"}
+            "tuned": cfg, "l2": "inputs and outputs of one batch exceed L2",
+            "mbfpa_only": {"value": units / t_batch_mb * 1e3, "unit": "rays*bins/s", "ms_per_batch": t_batch_mb,
+                           "plain_value": units / t_plain_mb * 1e3, "plain_ms_per_batch": t_plain_mb,
+                           "speedup_vs_plain": t_plain_mb / t_batch_mb, "tuned": cfg_mb,
+                           "what": "the same slices without the FBP (MBFPA: forward, normalisation, noise)"}}
 
 
 def bench_batched_adjoint(stream, warmup, n=64):

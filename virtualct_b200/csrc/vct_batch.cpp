@@ -1,15 +1,18 @@
 // Batch engine: many slices of uneven size in one captured CUDA graph (no
 // counterpart in the reference, which runs one slice per process).
 //
-// Per run, the graph holds
+// Per run of an MBFPA batch the graph holds one launch per stage, each over
+// the blocks of every job:
 //   - the packing of every job's maps into its padded layout;
 //   - ONE persistent forward launch over the ray tiles of all jobs
 //     (forward_batch_kernel), which writes every job's un-normalised sinogram
 //     and statistics;
-//   - then, on `branches` parallel streams, per job: the max-normalisation and
-//     noise of vct_mbfpa, and the FBP when the job asks for an image;
-//   or, for jobs that ask for a gradient, the adjoint (loss and dl/drho) of
-//   each job on the parallel streams.
+//   - the max-normalisation and noise of vct_mbfpa;
+//   - the FBP's weight, filter and backprojection (quarter-turn and general
+//     backprojector jobs in one launch each), for the jobs that ask for an
+//     image.
+// A batch of jobs that ask for a gradient runs the adjoint (loss and dl/drho)
+// of each job on `branches` parallel streams.
 // The ray-tile size of the persistent launch and the view split of the
 // backprojector are chosen by timing candidates on (a sample of) the batch
 // itself when it is created.
@@ -38,6 +41,12 @@ struct vct_batch {
   // persistent forward
   DBuf<FwdJob> d_jobs;
   DBuf<unsigned int> d_counter;
+  // the batched stages around it: map packing, normalisation + noise, FBP
+  DBuf<PackJob> d_pack;
+  DBuf<PostJob> d_post;
+  DBuf<unsigned int> d_first;  // [pack n+1][post kPostStages][n+1]
+  unsigned int pack_blocks = 0, post_blocks[kPostStages] = {};
+  int cmax = 0, winmax = 0;
   unsigned int ntiles = 0;
   int tile_rays = 64, blocks_per_sm = 0, grid = 0, view_groups = 4;
   double tuned_ms = 0.0;
@@ -89,7 +98,8 @@ int enqueue_forward(vct_batch* b, cudaStream_t st) {
                               b->d_counter.p, st);
 }
 
-// Everything after the forward, per job, spread over the branch streams.
+// The adjoint of every job (loss and gradient), spread over the branch
+// streams.
 int enqueue_jobs(vct_batch* b) {
   VCT_CUDA(cudaEventRecord(b->ev[0], b->stream));
   const int K = (int)b->branch.size();
@@ -101,12 +111,7 @@ int enqueue_jobs(vct_batch* b) {
     cudaStream_t st = b->branch[i % K];
     cudaStream_t saved = c->stream;
     c->stream = st;
-    if (b->adjoint) {
-      rc = ctx_adj_run(c, 0, j.d_meas, j.d_weights, nullptr, j.d_grad, j.d_loss);
-    } else {
-      rc = launch_normalize_noise(c->dg, j.d_sino, j.d_sino, c->stats.p, ctx_pad_zero(c), j.sigma, j.seed, st);
-      if (!rc && j.d_img) rc = ctx_fbp(c, j.d_sino, j.filter, j.d_img, b->view_groups);
-    }
+    rc = ctx_adj_run(c, 0, j.d_meas, j.d_weights, nullptr, j.d_grad, j.d_loss);
     c->stream = saved;
   }
   if (rc) return rc;
@@ -117,14 +122,74 @@ int enqueue_jobs(vct_batch* b) {
   return VCT_OK;
 }
 
+// The job tables of the batched stages (after every context exists and its
+// filter is built): per job its arguments and, per stage, its first block.
+int upload_stage_tables(vct_batch* b) {
+  const int n = b->n;
+  std::vector<PackJob> pk(n);
+  std::vector<PostJob> post(n);
+  std::vector<unsigned int> first((size_t)(1 + kPostStages) * (n + 1), 0u);
+  unsigned int* fp = first.data();
+  unsigned int* fs = first.data() + (n + 1);
+  unsigned int acc_pack = 0, acc[kPostStages] = {};
+  b->cmax = b->winmax = 0;
+  for (int i = 0; i < n; i++) {
+    vct_ctx* c = b->ctx[i];
+    const vct_job& j = b->jobs[i];
+    pk[i] = PackJob{j.d_maps, c->maps.p, c->dg.N};
+    fp[i] = acc_pack;
+    acc_pack += pack_maps_blocks(c->dg.N);
+    PostJob& p = post[i];
+    p = PostJob{};
+    const vct_geometry& g = c->geo;
+    fbp_bp_params(g.views, g.width, g.start_channel, c->dg.C, c->dg.N, g.pixel_cm, g.sid_cm, g.max_beta, g.xfactor,
+                  &p);
+    p.sino = j.d_sino;
+    p.stats = c->stats.p;
+    p.pad_zero = ctx_pad_zero(c);
+    p.sigma = j.sigma;
+    p.key0 = (unsigned int)j.seed;
+    p.key1 = (unsigned int)(j.seed >> 32);
+    if (j.d_img) {
+      p.img = j.d_img;
+      p.coeff = c->fbp_coeff.p;
+      p.h0 = c->fbp_h[j.filter].p;
+      p.cs = reinterpret_cast<const float2*>(c->cs_f.p);
+      p.g = c->fbp_g.p;
+      p.q = c->fbp_q.p;
+      b->cmax = std::max(b->cmax, p.C);
+      if (!p.sym) b->winmax = std::max(b->winmax, p.win);
+    }
+    unsigned int blk[kPostStages];
+    post_job_blocks(p, blk);
+    for (int k = 0; k < kPostStages; k++) {
+      fs[k * (n + 1) + i] = acc[k];
+      acc[k] += blk[k];
+    }
+  }
+  fp[n] = acc_pack;
+  for (int k = 0; k < kPostStages; k++) fs[k * (n + 1) + n] = acc[k];
+  b->pack_blocks = acc_pack;
+  for (int k = 0; k < kPostStages; k++) b->post_blocks[k] = acc[k];
+  int rc;
+  if ((rc = b->d_pack.ensure(n)) || (rc = b->d_post.ensure(n)) || (rc = b->d_first.ensure(first.size()))) return rc;
+  VCT_CUDA(cudaMemcpy(b->d_pack.p, pk.data(), n * sizeof(PackJob), cudaMemcpyHostToDevice));
+  VCT_CUDA(cudaMemcpy(b->d_post.p, post.data(), n * sizeof(PostJob), cudaMemcpyHostToDevice));
+  VCT_CUDA(cudaMemcpy(b->d_first.p, first.data(), first.size() * sizeof(unsigned int), cudaMemcpyHostToDevice));
+  return VCT_OK;
+}
+
 int enqueue_all(vct_batch* b) {
   int rc;
-  for (int i = 0; i < b->n; i++) {
-    vct_ctx* c = b->ctx[i];
-    if ((rc = launch_pack_maps(b->jobs[i].d_maps, b->M, c->dg.N, c->maps.p, b->stream))) return rc;
-  }
-  if (!b->adjoint && (rc = enqueue_forward(b, b->stream))) return rc;
-  return enqueue_jobs(b);
+  const int n = b->n;
+  if ((rc = launch_pack_maps_batch(b->d_pack.p, b->d_first.p, n, b->M, b->pack_blocks, b->stream))) return rc;
+  if (b->adjoint) return enqueue_jobs(b);
+  if ((rc = enqueue_forward(b, b->stream))) return rc;
+  const unsigned int* fs = b->d_first.p + (n + 1);
+  if ((rc = launch_normalize_noise_batch(b->d_post.p, fs + kPostNorm * (n + 1), n, b->post_blocks[kPostNorm],
+                                         b->stream)))
+    return rc;
+  return launch_fbp_batch(b->d_post.p, fs, n, b->post_blocks, b->cmax, b->winmax, b->view_groups, b->stream);
 }
 
 // Milliseconds of fn() on the batch stream: best of `reps` after one warm-up.
@@ -215,6 +280,9 @@ void release(vct_batch* b) {
   for (auto c : b->ctx) vct_destroy(c);
   b->d_jobs.release();
   b->d_counter.release();
+  b->d_pack.release();
+  b->d_post.release();
+  b->d_first.release();
 }
 
 }  // namespace
@@ -287,6 +355,7 @@ int vct_batch_create(const vct_job* jobs, int n, int M, int device, int tune, vc
     b->grid = b->blocks_per_sm * sm_count(device);
     if ((rc = upload_jobs(b, b->tile_rays))) return bail(rc);
   }
+  if ((rc = upload_stage_tables(b))) return bail(rc);
   if (tune && (rc = autotune(b))) return bail(rc);
   // Capture one run.
   cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);

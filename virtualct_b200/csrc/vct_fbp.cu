@@ -24,12 +24,9 @@ namespace vct {
 // line integral y = -ln p becomes |y| + alpha |y|^beta (the reference program
 // takes the logarithm in single precision, logf, and stores exp(-y') as float
 // for the FBP to take -ln again; here y' goes straight into the weight).
-__global__ void fbp_weight_kernel(const float* __restrict__ sino, int V, int W, int start, int C,
-                                  const double* __restrict__ coeff, double bh_alpha, double bh_beta,
-                                  float* __restrict__ g) {
-  const long long n = (long long)V * C;
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= n) return;
+__device__ __forceinline__ void fbp_weight_elem(const float* __restrict__ sino, long long i, int W, int start, int C,
+                                                const double* __restrict__ coeff, double bh_alpha, double bh_beta,
+                                                float* __restrict__ g) {
   const int v = (int)(i / C);
   const int k = (int)(i - (long long)v * C);
   const float pf = sino[(size_t)v * W + start + k];
@@ -41,6 +38,15 @@ __global__ void fbp_weight_kernel(const float* __restrict__ sino, int V, int W, 
     y = -log((double)pf);
   }
   g[i] = (float)(y * coeff[k]);
+}
+
+__global__ void fbp_weight_kernel(const float* __restrict__ sino, int V, int W, int start, int C,
+                                  const double* __restrict__ coeff, double bh_alpha, double bh_beta,
+                                  float* __restrict__ g) {
+  const long long n = (long long)V * C;
+  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  fbp_weight_elem(sino, i, W, start, C, coeff, bh_alpha, bh_beta, g);
 }
 
 int launch_fbp_weight(const float* d_sino, int V, int W, int start, int C, const double* d_coeff,
@@ -84,13 +90,11 @@ int launch_beam_hardening(float* d_p, long long n, double alpha, double beta, cu
 constexpr int FC_T = 128, FC_R = 5;
 
 template <bool TRANSPOSE>
-__global__ void __launch_bounds__(FC_T)
-fbp_filter_kernel(const float* __restrict__ G, const float* __restrict__ h0, const float* __restrict__ cm,
-                  int V, int C, int in_mode, float* __restrict__ Q) {
-  extern __shared__ float sm[];
+__device__ __forceinline__ void fbp_filter_view(const float* __restrict__ G, const float* __restrict__ h0,
+                                                const float* __restrict__ cm, int v, int C, int in_mode,
+                                                float* __restrict__ Q, float* sm) {
   float* sg = sm;                 // [C + FC_R]  (zero tail)
   float* sh = sm + C + FC_R;      // [2C + FC_R] h0(d) at index d + C, zero outside
-  const int v = blockIdx.x;
   for (int k = threadIdx.x; k < C + FC_R; k += FC_T)
     sg[k] = k < C ? (TRANSPOSE ? G[(size_t)v * C + k] * cm[k] : G[(size_t)v * C + k]) : 0.0f;
   for (int d = threadIdx.x; d < 2 * C + FC_R; d += FC_T) sh[d] = (d >= 1 && d < 2 * C) ? h0[d - 1] : 0.0f;
@@ -126,6 +130,14 @@ fbp_filter_kernel(const float* __restrict__ G, const float* __restrict__ h0, con
       }
     }
   }
+}
+
+template <bool TRANSPOSE>
+__global__ void __launch_bounds__(FC_T)
+fbp_filter_kernel(const float* __restrict__ G, const float* __restrict__ h0, const float* __restrict__ cm,
+                  int V, int C, int in_mode, float* __restrict__ Q) {
+  extern __shared__ float sm[];
+  fbp_filter_view<TRANSPOSE>(G, h0, cm, blockIdx.x, C, in_mode, Q, sm);
 }
 
 int launch_fbp_filter(const float* d_g, const float* d_h0, const float* d_cm, int V, int C, int in_mode,
@@ -187,16 +199,15 @@ __device__ __forceinline__ float bp_channel(float xx, float yy, float c, float s
 // interpolation is one 8-byte load.
 constexpr int BP_TX = 32, BP_TY = 8, BP_PIX = 2, BP_VC = 32;
 
-__global__ void __launch_bounds__(BP_TX * BP_TY, 4)
-fbp_bp_kernel(const float* __restrict__ Q, int V, int C, int N, int win, float scale, float sid,
-              float inv_dbeta, float center, float out_scale, const float2* __restrict__ cs,
-              float* __restrict__ img, int row0, int row1) {
-  extern __shared__ float2 sm2[];
+__device__ __forceinline__ void fbp_bp_block(int bx, int by, const float* __restrict__ Q, int V, int C, int N,
+                                             int win, float scale, float sid, float inv_dbeta, float center,
+                                             float out_scale, const float2* __restrict__ cs, float* __restrict__ img,
+                                             int row0, int row1, float2* sm2) {
   float2* sQ = sm2;                                        // [BP_VC][win] pairs
   float2* sCS = sQ + BP_VC * win;                          // [BP_VC]
   int* sOff = reinterpret_cast<int*>(sCS + BP_VC);         // [BP_VC]
   const int tid = threadIdx.y * BP_TX + threadIdx.x;
-  const int x0 = blockIdx.x * BP_TX, y0 = row0 + blockIdx.y * (BP_TY * BP_PIX);
+  const int x0 = bx * BP_TX, y0 = row0 + by * (BP_TY * BP_PIX);
   const int x = x0 + threadIdx.x;
   const float cp = (float)N / 2.0f - 0.5f;
   // Inscribed-circle mask (FBP/misc.cpp:20-36): (y-r)^2 + (x-r)^2 <= r^2.
@@ -275,6 +286,15 @@ fbp_bp_kernel(const float* __restrict__ Q, int V, int C, int N, int win, float s
   }
 }
 
+__global__ void __launch_bounds__(BP_TX * BP_TY, 4)
+fbp_bp_kernel(const float* __restrict__ Q, int V, int C, int N, int win, float scale, float sid,
+              float inv_dbeta, float center, float out_scale, const float2* __restrict__ cs,
+              float* __restrict__ img, int row0, int row1) {
+  extern __shared__ float2 sm2[];
+  fbp_bp_block(blockIdx.x, blockIdx.y, Q, V, C, N, win, scale, sid, inv_dbeta, center, out_scale, cs, img, row0,
+               row1, sm2);
+}
+
 // Backprojection with the square grid's quarter-turn symmetry, for V
 // divisible by 4 and even N.  Pixel (x, y) in view j and pixel
 // (N-1-y, x) in view j + V/4 have the same rotated coordinates (X, Y): with
@@ -324,14 +344,14 @@ __device__ __forceinline__ void bp_orbit_view(const float* __restrict__ Q, int V
 }
 
 template <int VS>
-__global__ void __launch_bounds__(BS_TX * BS_TY * VS)
-fbp_bp_sym_kernel(const float* __restrict__ Q, int V, int C, int N, float scale, float sid, float inv_dbeta,
-                  float center, float out_scale, const float2* __restrict__ cs, float* __restrict__ img, int y_lo,
-                  int y_hi) {
-  __shared__ float part[VS - 1][4][BS_TX * BS_TY];
+__device__ __forceinline__ void fbp_bp_sym_block(int bx, int by, const float* __restrict__ Q, int V, int C, int N,
+                                                 float scale, float sid, float inv_dbeta, float center,
+                                                 float out_scale, const float2* __restrict__ cs,
+                                                 float* __restrict__ img, int y_lo, int y_hi,
+                                                 float (*part)[4][BS_TX * BS_TY]) {
   const int H = N / 2, V4 = V / 4;
-  const int x = blockIdx.x * BS_TX + threadIdx.x;
-  const int y = y_lo + blockIdx.y * BS_TY + threadIdx.y;  // orbit rows [y_lo, y_hi) of [0, N/2)
+  const int x = bx * BS_TX + threadIdx.x;
+  const int y = y_lo + by * BS_TY + threadIdx.y;  // orbit rows [y_lo, y_hi) of [0, N/2)
   const int lt = threadIdx.y * BS_TX + threadIdx.x;
   const int z = threadIdx.z;
   const double r = (double)(N - 1) / 2.0;
@@ -368,6 +388,16 @@ fbp_bp_sym_kernel(const float* __restrict__ Q, int V, int C, int N, float scale,
       img[(size_t)py[q] * N + px[q]] = in ? a * out_scale : 0.0f;
     }
   }
+}
+
+template <int VS>
+__global__ void __launch_bounds__(BS_TX * BS_TY * VS)
+fbp_bp_sym_kernel(const float* __restrict__ Q, int V, int C, int N, float scale, float sid, float inv_dbeta,
+                  float center, float out_scale, const float2* __restrict__ cs, float* __restrict__ img, int y_lo,
+                  int y_hi) {
+  __shared__ float part[VS - 1][4][BS_TX * BS_TY];
+  fbp_bp_sym_block<VS>(blockIdx.x, blockIdx.y, Q, V, C, N, scale, sid, inv_dbeta, center, out_scale, cs, img, y_lo,
+                       y_hi, part);
 }
 
 // ------------------------------------------------- backprojection transpose
@@ -627,13 +657,8 @@ int launch_fbp_backproject_t(const float* d_u, int V, int C, int N, double pixel
 
 int fbp_band_count(int V, int N) { return (V % 4 == 0 && N % 2 == 0) ? N / 2 : N; }
 
-int launch_fbp_backproject(const float* d_q, int V, int C, int N, double pixel_cm, double sid,
-                           double max_beta, int xfactor, const float* d_cs, float* d_img,
-                           cudaStream_t st, int view_groups, int band0, int band1) {
-  if (band1 < 0) band1 = fbp_band_count(V, N);
-  if (band0 < 0 || band0 > band1 || band1 > fbp_band_count(V, N))
-    return fail(VCT_E_ARG, "fbp: band outside the image");
-  if (band0 == band1) return VCT_OK;
+void fbp_bp_params(int V, int W, int start, int C, int N, double pixel_cm, double sid, double max_beta, int xfactor,
+                   PostJob* j) {
   const int half = (C - 1) / 2;
   const double dbeta_det = max_beta / half;
   const double dbeta = 2.0 * 3.141592653589793 / V;
@@ -645,29 +670,150 @@ int launch_fbp_backproject(const float* d_q, int V, int C, int N, double pixel_c
   if (near_cm > tile_cm) win = (int)(tile_cm / near_cm / dbeta_det) + 8;
   win = ((win + 31) / 32) * 32;
   if (win > C + 4) win = C + 4;
-  if (V % 4 == 0 && N % 2 == 0) {
+  j->V = V;
+  j->W = W;
+  j->C = C;
+  j->start = start;
+  j->N = N;
+  j->sym = V % 4 == 0 && N % 2 == 0;
+  j->win = win;
+  j->scale = (float)pixel_cm;
+  j->sid = (float)sid;
+  j->inv_dbeta = (float)(1.0 / dbeta_det);
+  j->center = (float)(C / 2);
+  j->out_scale = (float)(dbeta * xfactor);
+}
+
+static size_t bp_gen_smem(int win) {
+  return (size_t)BP_VC * win * sizeof(float2) + BP_VC * (sizeof(float2) + sizeof(int));
+}
+
+int launch_fbp_backproject(const float* d_q, int V, int C, int N, double pixel_cm, double sid,
+                           double max_beta, int xfactor, const float* d_cs, float* d_img,
+                           cudaStream_t st, int view_groups, int band0, int band1) {
+  if (band1 < 0) band1 = fbp_band_count(V, N);
+  if (band0 < 0 || band0 > band1 || band1 > fbp_band_count(V, N))
+    return fail(VCT_E_ARG, "fbp: band outside the image");
+  if (band0 == band1) return VCT_OK;
+  PostJob p{};
+  fbp_bp_params(V, C, 0, C, N, pixel_cm, sid, max_beta, xfactor, &p);
+  const float2* cs2 = reinterpret_cast<const float2*>(d_cs);
+  if (p.sym) {
     const int H = N / 2;
     dim3 grid((H + BS_TX - 1) / BS_TX, (band1 - band0 + BS_TY - 1) / BS_TY);
-    const float a_sc = (float)pixel_cm, a_sid = (float)sid, a_ib = (float)(1.0 / dbeta_det), a_c = (float)(C / 2),
-                a_os = (float)(dbeta * xfactor);
-    const float2* cs2 = reinterpret_cast<const float2*>(d_cs);
     switch (view_groups) {
-      case 2: fbp_bp_sym_kernel<2><<<grid, dim3(BS_TX, BS_TY, 2), 0, st>>>(d_q, V, C, N, a_sc, a_sid, a_ib, a_c, a_os, cs2, d_img, band0, band1); break;
-      case 8: fbp_bp_sym_kernel<8><<<grid, dim3(BS_TX, BS_TY, 8), 0, st>>>(d_q, V, C, N, a_sc, a_sid, a_ib, a_c, a_os, cs2, d_img, band0, band1); break;
-      default: fbp_bp_sym_kernel<BS_VS><<<grid, dim3(BS_TX, BS_TY, BS_VS), 0, st>>>(d_q, V, C, N, a_sc, a_sid, a_ib, a_c, a_os, cs2, d_img, band0, band1); break;
+      case 2: fbp_bp_sym_kernel<2><<<grid, dim3(BS_TX, BS_TY, 2), 0, st>>>(d_q, V, C, N, p.scale, p.sid, p.inv_dbeta, p.center, p.out_scale, cs2, d_img, band0, band1); break;
+      case 8: fbp_bp_sym_kernel<8><<<grid, dim3(BS_TX, BS_TY, 8), 0, st>>>(d_q, V, C, N, p.scale, p.sid, p.inv_dbeta, p.center, p.out_scale, cs2, d_img, band0, band1); break;
+      default: fbp_bp_sym_kernel<BS_VS><<<grid, dim3(BS_TX, BS_TY, BS_VS), 0, st>>>(d_q, V, C, N, p.scale, p.sid, p.inv_dbeta, p.center, p.out_scale, cs2, d_img, band0, band1); break;
     }
     VCT_CUDA(cudaGetLastError());
     return VCT_OK;
   }
   dim3 grid((N + BP_TX - 1) / BP_TX, (band1 - band0 + BP_TY * BP_PIX - 1) / (BP_TY * BP_PIX));
   dim3 block(BP_TX, BP_TY);
-  const size_t smem = (size_t)BP_VC * win * sizeof(float2) + BP_VC * (sizeof(float2) + sizeof(int));
+  const size_t smem = bp_gen_smem(p.win);
   VCT_CUDA(cudaFuncSetAttribute(fbp_bp_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  fbp_bp_kernel<<<grid, block, smem, st>>>(d_q, V, C, N, win, (float)pixel_cm, (float)sid,
-                                           (float)(1.0 / dbeta_det), (float)(C / 2),
-                                           (float)(dbeta * xfactor),
-                                           reinterpret_cast<const float2*>(d_cs), d_img, band0, band1);
+  fbp_bp_kernel<<<grid, block, smem, st>>>(d_q, V, C, N, p.win, p.scale, p.sid, p.inv_dbeta, p.center, p.out_scale,
+                                           cs2, d_img, band0, band1);
   VCT_CUDA(cudaGetLastError());
+  return VCT_OK;
+}
+
+// ------------------------------------------------------------------ batch
+// Job of block b in a batched stage: the last j with first[j] <= b.
+__device__ __forceinline__ int post_job_of(const unsigned int* __restrict__ first, int n, unsigned int b) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (first[mid] <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+void post_job_blocks(const PostJob& j, unsigned int blocks[kPostStages]) {
+  blocks[kPostNorm] = (unsigned int)(((long long)j.V * j.W + 255) / 256);
+  blocks[kPostWeight] = blocks[kPostFilter] = blocks[kPostBpSym] = blocks[kPostBpGen] = 0;
+  if (!j.img) return;
+  blocks[kPostWeight] = (unsigned int)(((long long)j.V * j.C + 255) / 256);
+  blocks[kPostFilter] = (unsigned int)j.V;
+  if (j.sym) {
+    const int H = j.N / 2;
+    blocks[kPostBpSym] = (unsigned int)(((H + BS_TX - 1) / BS_TX) * ((H + BS_TY - 1) / BS_TY));
+  } else {
+    blocks[kPostBpGen] = (unsigned int)(((j.N + BP_TX - 1) / BP_TX) * ((j.N + BP_TY * BP_PIX - 1) / (BP_TY * BP_PIX)));
+  }
+}
+
+__global__ void fbp_weight_batch_kernel(const PostJob* __restrict__ jobs, const unsigned int* __restrict__ first,
+                                        int n) {
+  const int jx = post_job_of(first, n, blockIdx.x);
+  const PostJob& J = jobs[jx];
+  const long long i = (long long)(blockIdx.x - first[jx]) * blockDim.x + threadIdx.x;
+  if (i >= (long long)J.V * J.C) return;
+  fbp_weight_elem(J.sino, i, J.W, J.start, J.C, J.coeff, 0.0, 0.0, J.g);
+}
+
+__global__ void __launch_bounds__(FC_T) fbp_filter_batch_kernel(const PostJob* __restrict__ jobs,
+                                                                const unsigned int* __restrict__ first, int n) {
+  extern __shared__ float sm[];
+  const int jx = post_job_of(first, n, blockIdx.x);
+  const PostJob& J = jobs[jx];
+  fbp_filter_view<false>(J.g, J.h0, J.h0 + 2 * J.C - 1, (int)(blockIdx.x - first[jx]), J.C, 0, J.q, sm);
+}
+
+template <int VS>
+__global__ void __launch_bounds__(BS_TX * BS_TY * VS)
+fbp_bp_sym_batch_kernel(const PostJob* __restrict__ jobs, const unsigned int* __restrict__ first, int n) {
+  __shared__ float part[VS - 1][4][BS_TX * BS_TY];
+  const int jx = post_job_of(first, n, blockIdx.x);
+  const PostJob& J = jobs[jx];
+  const int H = J.N / 2, nbx = (H + BS_TX - 1) / BS_TX;
+  const int b = (int)(blockIdx.x - first[jx]);
+  fbp_bp_sym_block<VS>(b % nbx, b / nbx, J.q, J.V, J.C, J.N, J.scale, J.sid, J.inv_dbeta, J.center, J.out_scale,
+                       J.cs, J.img, 0, H, part);
+}
+
+__global__ void __launch_bounds__(BP_TX * BP_TY, 4)
+fbp_bp_batch_kernel(const PostJob* __restrict__ jobs, const unsigned int* __restrict__ first, int n) {
+  extern __shared__ float2 sm2[];
+  const int jx = post_job_of(first, n, blockIdx.x);
+  const PostJob& J = jobs[jx];
+  const int nbx = (J.N + BP_TX - 1) / BP_TX;
+  const int b = (int)(blockIdx.x - first[jx]);
+  fbp_bp_block(b % nbx, b / nbx, J.q, J.V, J.C, J.N, J.win, J.scale, J.sid, J.inv_dbeta, J.center, J.out_scale, J.cs,
+               J.img, 0, J.N, sm2);
+}
+
+int launch_fbp_batch(const PostJob* d_jobs, const unsigned int* d_first, int n, const unsigned int nblocks[kPostStages],
+                     int cmax, int winmax, int view_groups, cudaStream_t st) {
+  const unsigned int* f = d_first;
+  if (nblocks[kPostWeight]) {
+    fbp_weight_batch_kernel<<<nblocks[kPostWeight], 256, 0, st>>>(d_jobs, f + kPostWeight * (n + 1), n);
+    VCT_CUDA(cudaGetLastError());
+  }
+  if (nblocks[kPostFilter]) {
+    const size_t smem = (size_t)(3 * cmax + 2 * FC_R) * sizeof(float);
+    if (smem > 220 * 1024) return fail(VCT_E_UNSUPPORTED, "filter: channel count above the shared-memory limit");
+    VCT_CUDA(cudaFuncSetAttribute(fbp_filter_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    fbp_filter_batch_kernel<<<nblocks[kPostFilter], FC_T, smem, st>>>(d_jobs, f + kPostFilter * (n + 1), n);
+    VCT_CUDA(cudaGetLastError());
+  }
+  if (nblocks[kPostBpSym]) {
+    const unsigned int* fs = f + kPostBpSym * (n + 1);
+    switch (view_groups) {
+      case 2: fbp_bp_sym_batch_kernel<2><<<nblocks[kPostBpSym], dim3(BS_TX, BS_TY, 2), 0, st>>>(d_jobs, fs, n); break;
+      case 8: fbp_bp_sym_batch_kernel<8><<<nblocks[kPostBpSym], dim3(BS_TX, BS_TY, 8), 0, st>>>(d_jobs, fs, n); break;
+      default: fbp_bp_sym_batch_kernel<BS_VS><<<nblocks[kPostBpSym], dim3(BS_TX, BS_TY, BS_VS), 0, st>>>(d_jobs, fs, n); break;
+    }
+    VCT_CUDA(cudaGetLastError());
+  }
+  if (nblocks[kPostBpGen]) {
+    const size_t smem = bp_gen_smem(winmax);
+    VCT_CUDA(cudaFuncSetAttribute(fbp_bp_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    fbp_bp_batch_kernel<<<nblocks[kPostBpGen], dim3(BP_TX, BP_TY), smem, st>>>(d_jobs, f + kPostBpGen * (n + 1), n);
+    VCT_CUDA(cudaGetLastError());
+  }
   return VCT_OK;
 }
 

@@ -33,11 +33,9 @@
 namespace vct {
 
 // ---------------------------------------------------------------- map packing
-__global__ void pack_maps_kernel(const int16_t* __restrict__ maps, int M, int N,
-                                 PixelRec* __restrict__ out, PixelRec* __restrict__ out_t) {
+__device__ __forceinline__ void pack_maps_elem(int p, const int16_t* __restrict__ maps, int M, int N,
+                                               PixelRec* __restrict__ out, PixelRec* __restrict__ out_t) {
   const int P = N + 2 * kPad;
-  const int p = blockIdx.x * blockDim.x + threadIdx.x;
-  if (p >= P * P) return;
   const int r = p / P - kPad, c = p % P - kPad;  // padded row/column in [-kPad, N+kPad)
   PixelRec rec;
   const bool inside = r >= -1 && c >= -1 && r < N && c < N;
@@ -52,6 +50,48 @@ __global__ void pack_maps_kernel(const int16_t* __restrict__ maps, int M, int N,
   // Transposed copy (column-major): walks whose major axis is x step along
   // a column of it, so a warp's rays read neighbouring records.
   if (out_t) out_t[(c + kPad) * P + (r + kPad)] = rec;
+}
+
+__global__ void pack_maps_kernel(const int16_t* __restrict__ maps, int M, int N,
+                                 PixelRec* __restrict__ out, PixelRec* __restrict__ out_t) {
+  const int P = N + 2 * kPad;
+  const int p = blockIdx.x * blockDim.x + threadIdx.x;
+  if (p >= P * P) return;
+  pack_maps_elem(p, maps, M, N, out, out_t);
+}
+
+unsigned int pack_maps_blocks(int N) {
+  const int P = N + 2 * kPad;
+  return (unsigned int)((P * P + 255) / 256);
+}
+
+// Job of block b in a batched launch: the last j with first[j] <= b.
+__device__ __forceinline__ int batch_job_of(const unsigned int* __restrict__ first, int n, unsigned int b) {
+  int lo = 0, hi = n - 1;
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (first[mid] <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+__global__ void pack_maps_batch_kernel(const PackJob* __restrict__ jobs, const unsigned int* __restrict__ first,
+                                       int n, int M) {
+  const int jx = batch_job_of(first, n, blockIdx.x);
+  const PackJob J = jobs[jx];
+  const int P = J.N + 2 * kPad;
+  const int p = (int)(blockIdx.x - first[jx]) * blockDim.x + threadIdx.x;
+  if (p >= P * P) return;
+  pack_maps_elem(p, J.maps, M, J.N, J.out, VCT_FWD_DUAL_LAYOUT ? J.out + (size_t)P * P : nullptr);
+}
+
+int launch_pack_maps_batch(const PackJob* d_jobs, const unsigned int* d_first, int n, int M, unsigned int nblocks,
+                           cudaStream_t st) {
+  if (nblocks == 0) return VCT_OK;
+  pack_maps_batch_kernel<<<nblocks, 256, 0, st>>>(d_jobs, d_first, n, M);
+  VCT_CUDA(cudaGetLastError());
+  return VCT_OK;
 }
 
 int launch_pack_maps(const int16_t* d_maps, int M, int N, PixelRec* d_packed, cudaStream_t st) {
@@ -375,11 +415,9 @@ int forward_batch_occupancy(int M, int ne_max, int* blocks_per_sm) {
 // (:51-76): p += sigma*z, p < 0 -> projection_min/10, p > 1 -> 1, with
 // z = sqrt(-2 ln u1) sin(2 pi u2) (:46-49).  u1, u2 come from Philox4x32-10
 // keyed by the 64-bit seed, counter (channel, view, 0, 0).
-__global__ void normalize_noise_kernel(const float* __restrict__ in, float* __restrict__ out, int V,
-                                       int W, const FwdStats* __restrict__ stats, int pad_zero,
-                                       double sigma, uint32_t k0, uint32_t k1, long long i0, long long i1) {
-  const long long i = i0 + (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  if (i >= i1) return;
+__device__ __forceinline__ void normalize_noise_elem(const float* __restrict__ in, float* __restrict__ out,
+                                                     long long i, int W, const FwdStats* __restrict__ stats,
+                                                     int pad_zero, double sigma, uint32_t k0, uint32_t k1) {
   const float pmax = __uint_as_float(stats->max_bits);
   float pmin_raw = __uint_as_float(stats->min_bits);
   if (pad_zero) pmin_raw = fminf(pmin_raw, 0.0f);
@@ -405,6 +443,31 @@ __global__ void normalize_noise_kernel(const float* __restrict__ in, float* __re
   if (nstar < 0) o = (float)(pmin / 10);
   if (nstar > 1.0) o = 1.0f;
   out[i] = o;
+}
+
+__global__ void normalize_noise_kernel(const float* __restrict__ in, float* __restrict__ out, int V,
+                                       int W, const FwdStats* __restrict__ stats, int pad_zero,
+                                       double sigma, uint32_t k0, uint32_t k1, long long i0, long long i1) {
+  const long long i = i0 + (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= i1) return;
+  normalize_noise_elem(in, out, i, W, stats, pad_zero, sigma, k0, k1);
+}
+
+__global__ void normalize_noise_batch_kernel(const PostJob* __restrict__ jobs, const unsigned int* __restrict__ first,
+                                             int n) {
+  const int jx = batch_job_of(first, n, blockIdx.x);
+  const PostJob& J = jobs[jx];
+  const long long i = (long long)(blockIdx.x - first[jx]) * blockDim.x + threadIdx.x;
+  if (i >= (long long)J.V * J.W) return;
+  normalize_noise_elem(J.sino, J.sino, i, J.W, J.stats, J.pad_zero, J.sigma, J.key0, J.key1);
+}
+
+int launch_normalize_noise_batch(const PostJob* d_jobs, const unsigned int* d_first, int n, unsigned int nblocks,
+                                 cudaStream_t st) {
+  if (nblocks == 0) return VCT_OK;
+  normalize_noise_batch_kernel<<<nblocks, 256, 0, st>>>(d_jobs, d_first, n);
+  VCT_CUDA(cudaGetLastError());
+  return VCT_OK;
 }
 
 int launch_normalize_noise(const DevGeom& g, const float* d_in, float* d_out, const FwdStats* d_stats,

@@ -141,6 +141,51 @@ int launch_forward_batch(const FwdJob* d_jobs, int njobs, int M, int tile_rays, 
 int forward_batch_occupancy(int M, int ne_max, int* blocks_per_sm);
 int launch_normalize_noise(const DevGeom& g, const float* d_in, float* d_out, const FwdStats* d_stats,
                            int pad_zero, double sigma, uint64_t seed, cudaStream_t st, int r0 = 0, int r1 = -1);
+// The batch engine's launches after the forward (vct_batch.cpp): one launch
+// per stage runs the blocks of every job.  A PostJob holds one job's
+// arguments of the single-slice normalisation/noise and FBP kernels; per
+// stage, first[stage * (n + 1) + j] is the index of job j's first block
+// (prefix sums; first[.. + n] is the stage's block count).  The blocks do
+// exactly what the single-slice launches do, so results are bit-identical.
+struct PostJob {
+  float* sino;            // [V][W]: un-normalised in, normalised (+ noise) out
+  const FwdStats* stats;
+  int V, W, pad_zero;
+  double sigma;
+  unsigned int key0, key1;
+  float* img;             // [N][N], or NULL (no FBP)
+  const double* coeff;    // weight factors [C]
+  const float* h0;        // filter kernel [2C-1], then the row factors [C]
+  const float2* cs;       // (cos, sin) per view
+  float* g;               // weighted sinogram [V][C]
+  float* q;               // filtered sinogram [V][C]
+  int C, start, N, sym, win;
+  float scale, sid, inv_dbeta, center, out_scale;
+};
+enum { kPostNorm = 0, kPostWeight, kPostFilter, kPostBpSym, kPostBpGen, kPostStages };
+// Block counts of one job per stage (0 where the stage does not apply).
+void post_job_blocks(const PostJob& j, unsigned int blocks[kPostStages]);
+// The backprojector's launch parameters of one slice (as launch_fbp_backproject
+// derives them): fills C, start, N, sym, win, scale, sid, inv_dbeta, center,
+// out_scale.
+void fbp_bp_params(int V, int W, int start, int C, int N, double pixel_cm, double sid, double max_beta, int xfactor,
+                   PostJob* j);
+int launch_normalize_noise_batch(const PostJob* d_jobs, const unsigned int* d_first, int n, unsigned int nblocks,
+                                 cudaStream_t st);
+// weight, filter and the two backprojectors; cmax: largest channel count,
+// winmax: largest staged window of a general-backprojector job.
+int launch_fbp_batch(const PostJob* d_jobs, const unsigned int* d_first, int n, const unsigned int nblocks[kPostStages],
+                     int cmax, int winmax, int view_groups, cudaStream_t st);
+// Map packing of many slices in one launch: job j packs maps[j] (N[j]) into
+// out[j]; first[j] is its first block.
+struct PackJob {
+  const int16_t* maps;
+  PixelRec* out;
+  int N;
+};
+int launch_pack_maps_batch(const PackJob* d_jobs, const unsigned int* d_first, int n, int M, unsigned int nblocks,
+                           cudaStream_t st);
+unsigned int pack_maps_blocks(int N);
 // bh_alpha != 0: beam-hardening correction of the line integrals on the way.
 int launch_fbp_weight(const float* d_sino, int V, int W, int start, int C, const double* d_coeff,
                       float* d_g, cudaStream_t st, double bh_alpha = 0.0, double bh_beta = 0.0);

@@ -99,6 +99,7 @@ struct vct_ctx {
   vct::DBuf<double> fbp_coeff;  // SID*cos((k-cw)*dbeta)*dbeta
   vct::DBuf<float> fbp_h[3];    // per filter (1 Ram-Lak, 2 Shepp-Logan): h0[2C-1] + row factors[C]
   vct::DBuf<float> fbp_g, fbp_q, fbp_sino, fbp_img;
+  vct::DBuf<float2> fbp_q2;  // filtered rows as interpolation pairs (quarter-turn backprojector)
   vct::DBuf<unsigned long long> fbp_tacc;  // FBP transpose: fixed-point row sums + max|u|
   double bh_alpha = 0.0, bh_beta = 0.0;
   vct::DBuf<double> sq_part;  // calc_squdiff_quad block partials

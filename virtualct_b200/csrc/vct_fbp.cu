@@ -92,7 +92,7 @@ constexpr int FC_T = 128, FC_R = 5;
 template <bool TRANSPOSE>
 __device__ __forceinline__ void fbp_filter_view(const float* __restrict__ G, const float* __restrict__ h0,
                                                 const float* __restrict__ cm, int v, int C, int in_mode,
-                                                float* __restrict__ Q, float* sm) {
+                                                float* __restrict__ Q, float2* __restrict__ Q2, float* sm) {
   float* sg = sm;                 // [C + FC_R]  (zero tail)
   float* sh = sm + C + FC_R;      // [2C + FC_R] h0(d) at index d + C, zero outside
   for (int k = threadIdx.x; k < C + FC_R; k += FC_T)
@@ -130,22 +130,31 @@ __device__ __forceinline__ void fbp_filter_view(const float* __restrict__ G, con
       }
     }
   }
+  if (Q2) {
+    // The row again as interpolation pairs (q[m], q[m+1]), for the
+    // quarter-turn backprojector's 8-byte loads; the block's writes above
+    // are visible after the barrier.
+    __syncthreads();
+    const float* qr = Q + (size_t)v * C;
+    for (int m = threadIdx.x; m < C; m += FC_T)
+      Q2[(size_t)v * C + m] = make_float2(qr[m], m + 1 < C ? qr[m + 1] : 0.0f);
+  }
 }
 
 template <bool TRANSPOSE>
 __global__ void __launch_bounds__(FC_T)
 fbp_filter_kernel(const float* __restrict__ G, const float* __restrict__ h0, const float* __restrict__ cm,
-                  int V, int C, int in_mode, float* __restrict__ Q) {
+                  int V, int C, int in_mode, float* __restrict__ Q, float2* __restrict__ Q2) {
   extern __shared__ float sm[];
-  fbp_filter_view<TRANSPOSE>(G, h0, cm, blockIdx.x, C, in_mode, Q, sm);
+  fbp_filter_view<TRANSPOSE>(G, h0, cm, blockIdx.x, C, in_mode, Q, Q2, sm);
 }
 
 int launch_fbp_filter(const float* d_g, const float* d_h0, const float* d_cm, int V, int C, int in_mode,
-                      float* d_q, cudaStream_t st) {
+                      float* d_q, cudaStream_t st, float2* d_q2) {
   const size_t smem = (size_t)(3 * C + 2 * FC_R) * sizeof(float);
   if (smem > 220 * 1024) return fail(VCT_E_UNSUPPORTED, "filter: channel count above the shared-memory limit");
   VCT_CUDA(cudaFuncSetAttribute(fbp_filter_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  fbp_filter_kernel<false><<<V, FC_T, smem, st>>>(d_g, d_h0, d_cm, V, C, in_mode, d_q);
+  fbp_filter_kernel<false><<<V, FC_T, smem, st>>>(d_g, d_h0, d_cm, V, C, in_mode, d_q, d_q2);
   VCT_CUDA(cudaGetLastError());
   return VCT_OK;
 }
@@ -155,7 +164,7 @@ int launch_fbp_filter_t(const float* d_q, const float* d_h0, const float* d_cm, 
   const size_t smem = (size_t)(3 * C + 2 * FC_R) * sizeof(float);
   if (smem > 220 * 1024) return fail(VCT_E_UNSUPPORTED, "filter: channel count above the shared-memory limit");
   VCT_CUDA(cudaFuncSetAttribute(fbp_filter_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  fbp_filter_kernel<true><<<V, FC_T, smem, st>>>(d_q, d_h0, d_cm, V, C, 0, d_g);
+  fbp_filter_kernel<true><<<V, FC_T, smem, st>>>(d_q, d_h0, d_cm, V, C, 0, d_g, nullptr);
   VCT_CUDA(cudaGetLastError());
   return VCT_OK;
 }
@@ -315,10 +324,14 @@ fbp_bp_kernel(const float* __restrict__ Q, int V, int C, int N, int win, float s
 // warp read neighbouring channels).
 constexpr int BS_TX = 32, BS_TY = 4, BS_VS = 4;  // BS_VS: the default view split
 
-__device__ __forceinline__ void bp_orbit_view(const float* __restrict__ Q, int V, int V4, int C, float xx, float yy,
-                                              float2 t, int j, float sid, float inv_dbeta, float center,
-                                              float acc[4]) {
-  // FBP/reconstructImageTOMO.cpp:67-73, shared by the orbit.
+// One base view j of an orbit: the geometry (FBP/reconstructImageTOMO.cpp:
+// 67-73) once, then the four rotated rows, row q at qbase + off[q] (views
+// mod V, the offsets set by the caller for j's quarter).  PAIRS: Q2 holds
+// (q[c], q[c+1]) pairs, one 8-byte load per row; else two loads from Q.
+template <bool PAIRS>
+__device__ __forceinline__ void bp_orbit_view(const float* __restrict__ Q, const float2* __restrict__ Q2, int C,
+                                              float xx, float yy, float2 t, long long jrow, const long long off[4],
+                                              float sid, float inv_dbeta, float center, float acc[4]) {
   const float X = xx * t.x + yy * t.y;
   const float Y = -xx * t.y + yy * t.x;
   const float d = sid - Y;
@@ -331,24 +344,30 @@ __device__ __forceinline__ void bp_orbit_view(const float* __restrict__ Q, int V
   const int gi = fg > -1.0f ? (__float_as_int(big) - 0x4B000000) : -1;
   const float w = fg - (big - 8388608.0f);
   if ((unsigned)gi < (unsigned)(C - 1)) {
+    const long long base = jrow + gi;
 #pragma unroll
     for (int q = 0; q < 4; q++) {
-      int row = j + q * V4;
-      row = row >= V ? row - V : row;
-      if (!VCT_INDEX_OK(row >= 0 && row < V)) continue;
-      const float* qr = Q + (size_t)row * C + gi;
-      const float q0 = __ldg(qr), q1 = __ldg(qr + 1);
+      float q0, q1;
+      if (PAIRS) {
+        const float2 p = __ldg(Q2 + base + off[q]);
+        q0 = p.x;
+        q1 = p.y;
+      } else {
+        const float* qr = Q + base + off[q];
+        q0 = __ldg(qr);
+        q1 = __ldg(qr + 1);
+      }
       acc[q] = fmaf(fmaf(w, q1 - q0, q0), iL2, acc[q]);
     }
   }
 }
 
-template <int VS>
-__device__ __forceinline__ void fbp_bp_sym_block(int bx, int by, const float* __restrict__ Q, int V, int C, int N,
-                                                 float scale, float sid, float inv_dbeta, float center,
-                                                 float out_scale, const float2* __restrict__ cs,
-                                                 float* __restrict__ img, int y_lo, int y_hi,
-                                                 float (*part)[4][BS_TX * BS_TY]) {
+template <int VS, bool PAIRS>
+__device__ __forceinline__ void fbp_bp_sym_block(int bx, int by, const float* __restrict__ Q,
+                                                 const float2* __restrict__ Q2, int V, int C, int N, float scale,
+                                                 float sid, float inv_dbeta, float center, float out_scale,
+                                                 const float2* __restrict__ cs, float* __restrict__ img, int y_lo,
+                                                 int y_hi, float (*part)[4][BS_TX * BS_TY]) {
   const int H = N / 2, V4 = V / 4;
   const int x = bx * BS_TX + threadIdx.x;
   const int y = y_lo + by * BS_TY + threadIdx.y;  // orbit rows [y_lo, y_hi) of [0, N/2)
@@ -364,13 +383,22 @@ __device__ __forceinline__ void fbp_bp_sym_block(int bx, int by, const float* __
     const float xx = -((float)x - cp) * scale;
     const float yy = -((float)y - cp) * scale;
     const int jb = (int)((long long)V * z / VS), je = (int)((long long)V * (z + 1) / VS);
-    int j = jb;
-    for (; j + 1 < je; j += 2) {
-      const float2 t0 = __ldg(cs + j), t1 = __ldg(cs + j + 1);
-      bp_orbit_view(Q, V, V4, C, xx, yy, t0, j, sid, inv_dbeta, center, acc);
-      bp_orbit_view(Q, V, V4, C, xx, yy, t1, j + 1, sid, inv_dbeta, center, acc);
+    // Base views in quarter `seg` (j in [seg V/4, (seg+1) V/4)): row q is
+    // j + q V/4, less V where that passes V, i.e. where q + seg >= 4.
+    for (int seg = 0; seg < 4; seg++) {
+      const int s0 = max(jb, seg * V4), s1 = min(je, (seg + 1) * V4);
+      if (s0 >= s1) continue;
+      long long off[4];
+#pragma unroll
+      for (int q = 0; q < 4; q++) off[q] = (long long)(q * V4 - (q + seg >= 4 ? V : 0)) * C;
+      int j = s0;
+      for (; j + 1 < s1; j += 2) {
+        const float2 t0 = __ldg(cs + j), t1 = __ldg(cs + j + 1);
+        bp_orbit_view<PAIRS>(Q, Q2, C, xx, yy, t0, (long long)j * C, off, sid, inv_dbeta, center, acc);
+        bp_orbit_view<PAIRS>(Q, Q2, C, xx, yy, t1, (long long)(j + 1) * C, off, sid, inv_dbeta, center, acc);
+      }
+      if (j < s1) bp_orbit_view<PAIRS>(Q, Q2, C, xx, yy, __ldg(cs + j), (long long)j * C, off, sid, inv_dbeta, center, acc);
     }
-    if (j < je) bp_orbit_view(Q, V, V4, C, xx, yy, __ldg(cs + j), j, sid, inv_dbeta, center, acc);
   }
   if (z > 0) {
 #pragma unroll
@@ -390,14 +418,14 @@ __device__ __forceinline__ void fbp_bp_sym_block(int bx, int by, const float* __
   }
 }
 
-template <int VS>
+template <int VS, bool PAIRS>
 __global__ void __launch_bounds__(BS_TX * BS_TY * VS)
-fbp_bp_sym_kernel(const float* __restrict__ Q, int V, int C, int N, float scale, float sid, float inv_dbeta,
-                  float center, float out_scale, const float2* __restrict__ cs, float* __restrict__ img, int y_lo,
-                  int y_hi) {
+fbp_bp_sym_kernel(const float* __restrict__ Q, const float2* __restrict__ Q2, int V, int C, int N, float scale,
+                  float sid, float inv_dbeta, float center, float out_scale, const float2* __restrict__ cs,
+                  float* __restrict__ img, int y_lo, int y_hi) {
   __shared__ float part[VS - 1][4][BS_TX * BS_TY];
-  fbp_bp_sym_block<VS>(blockIdx.x, blockIdx.y, Q, V, C, N, scale, sid, inv_dbeta, center, out_scale, cs, img, y_lo,
-                       y_hi, part);
+  fbp_bp_sym_block<VS, PAIRS>(blockIdx.x, blockIdx.y, Q, Q2, V, C, N, scale, sid, inv_dbeta, center, out_scale, cs,
+                              img, y_lo, y_hi, part);
 }
 
 // ------------------------------------------------- backprojection transpose
@@ -690,7 +718,7 @@ static size_t bp_gen_smem(int win) {
 
 int launch_fbp_backproject(const float* d_q, int V, int C, int N, double pixel_cm, double sid,
                            double max_beta, int xfactor, const float* d_cs, float* d_img,
-                           cudaStream_t st, int view_groups, int band0, int band1) {
+                           cudaStream_t st, int view_groups, int band0, int band1, const float2* d_q2) {
   if (band1 < 0) band1 = fbp_band_count(V, N);
   if (band0 < 0 || band0 > band1 || band1 > fbp_band_count(V, N))
     return fail(VCT_E_ARG, "fbp: band outside the image");
@@ -701,11 +729,24 @@ int launch_fbp_backproject(const float* d_q, int V, int C, int N, double pixel_c
   if (p.sym) {
     const int H = N / 2;
     dim3 grid((H + BS_TX - 1) / BS_TX, (band1 - band0 + BS_TY - 1) / BS_TY);
-    switch (view_groups) {
-      case 2: fbp_bp_sym_kernel<2><<<grid, dim3(BS_TX, BS_TY, 2), 0, st>>>(d_q, V, C, N, p.scale, p.sid, p.inv_dbeta, p.center, p.out_scale, cs2, d_img, band0, band1); break;
-      case 8: fbp_bp_sym_kernel<8><<<grid, dim3(BS_TX, BS_TY, 8), 0, st>>>(d_q, V, C, N, p.scale, p.sid, p.inv_dbeta, p.center, p.out_scale, cs2, d_img, band0, band1); break;
-      default: fbp_bp_sym_kernel<BS_VS><<<grid, dim3(BS_TX, BS_TY, BS_VS), 0, st>>>(d_q, V, C, N, p.scale, p.sid, p.inv_dbeta, p.center, p.out_scale, cs2, d_img, band0, band1); break;
+#define VCT_SYM(vs, pairs)                                                                                \
+  fbp_bp_sym_kernel<vs, pairs><<<grid, dim3(BS_TX, BS_TY, vs), 0, st>>>(d_q, d_q2, V, C, N, p.scale, p.sid, \
+                                                                        p.inv_dbeta, p.center, p.out_scale, cs2, \
+                                                                        d_img, band0, band1)
+    if (d_q2) {
+      switch (view_groups) {
+        case 2: VCT_SYM(2, true); break;
+        case 8: VCT_SYM(8, true); break;
+        default: VCT_SYM(BS_VS, true); break;
+      }
+    } else {
+      switch (view_groups) {
+        case 2: VCT_SYM(2, false); break;
+        case 8: VCT_SYM(8, false); break;
+        default: VCT_SYM(BS_VS, false); break;
+      }
     }
+#undef VCT_SYM
     VCT_CUDA(cudaGetLastError());
     return VCT_OK;
   }
@@ -759,7 +800,7 @@ __global__ void __launch_bounds__(FC_T) fbp_filter_batch_kernel(const PostJob* _
   extern __shared__ float sm[];
   const int jx = post_job_of(first, n, blockIdx.x);
   const PostJob& J = jobs[jx];
-  fbp_filter_view<false>(J.g, J.h0, J.h0 + 2 * J.C - 1, (int)(blockIdx.x - first[jx]), J.C, 0, J.q, sm);
+  fbp_filter_view<false>(J.g, J.h0, J.h0 + 2 * J.C - 1, (int)(blockIdx.x - first[jx]), J.C, 0, J.q, J.q2, sm);
 }
 
 template <int VS>
@@ -770,8 +811,8 @@ fbp_bp_sym_batch_kernel(const PostJob* __restrict__ jobs, const unsigned int* __
   const PostJob& J = jobs[jx];
   const int H = J.N / 2, nbx = (H + BS_TX - 1) / BS_TX;
   const int b = (int)(blockIdx.x - first[jx]);
-  fbp_bp_sym_block<VS>(b % nbx, b / nbx, J.q, J.V, J.C, J.N, J.scale, J.sid, J.inv_dbeta, J.center, J.out_scale,
-                       J.cs, J.img, 0, H, part);
+  fbp_bp_sym_block<VS, true>(b % nbx, b / nbx, J.q, J.q2, J.V, J.C, J.N, J.scale, J.sid, J.inv_dbeta, J.center,
+                             J.out_scale, J.cs, J.img, 0, H, part);
 }
 
 __global__ void __launch_bounds__(BP_TX * BP_TY, 4)

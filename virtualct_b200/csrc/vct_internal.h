@@ -159,6 +159,7 @@ struct PostJob {
   const float2* cs;       // (cos, sin) per view
   float* g;               // weighted sinogram [V][C]
   float* q;               // filtered sinogram [V][C]
+  float2* q2;             // its interpolation pairs [V][C] (quarter-turn jobs), or NULL
   int C, start, N, sym, win;
   float scale, sid, inv_dbeta, center, out_scale;
 };
@@ -190,17 +191,22 @@ unsigned int pack_maps_blocks(int N);
 int launch_fbp_weight(const float* d_sino, int V, int W, int start, int C, const double* d_coeff,
                       float* d_g, cudaStream_t st, double bh_alpha = 0.0, double bh_beta = 0.0);
 int launch_beam_hardening(float* d_p, long long n, double alpha, double beta, cudaStream_t st);
+// d_q2 (optional): the filtered rows also as interpolation pairs
+// (q[c], q[c+1]) [V][C], for the quarter-turn backprojector.
 int launch_fbp_filter(const float* d_g, const float* d_h0, const float* d_cm, int V, int C, int in_mode,
-                      float* d_q, cudaStream_t st);
+                      float* d_q, cudaStream_t st, float2* d_q2 = nullptr);
 // view_groups: how many warp groups split the views of the quarter-turn
 // backprojector (2, 4 or 8; other values mean 4).
 // band0..band1: the image rows [band0, band1) of the general backprojector,
 // or the orbit rows [band0, band1) of [0, N/2) of the quarter-turn one
 // (fbp_band_count); pixels outside the band are not written.
 int fbp_band_count(int V, int N);
+// d_q2 (optional): the pairs of launch_fbp_filter, read by the quarter-turn
+// backprojector instead of two loads from d_q.
 int launch_fbp_backproject(const float* d_q, int V, int C, int N, double pixel_cm, double sid,
                            double max_beta, int xfactor, const float* d_cs, float* d_img,
-                           cudaStream_t st, int view_groups = 4, int band0 = 0, int band1 = -1);
+                           cudaStream_t st, int view_groups = 4, int band0 = 0, int band1 = -1,
+                           const float2* d_q2 = nullptr);
 // Transposes of the three FBP steps (vct_fbp.cu).
 size_t fbp_backproject_t_scratch(int V, int C, int N);  // 64-bit words of d_acc
 int launch_fbp_backproject_t(const float* d_u, int V, int C, int N, double pixel_cm, double sid, double max_beta,

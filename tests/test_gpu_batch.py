@@ -99,6 +99,9 @@ def test_adjoint_batch_matches_plain(cuda_device):
                             grad=torch.zeros((6, g.recon_size, g.recon_size), dtype=torch.float32, device="cuda"),
                             loss=torch.zeros(1, dtype=torch.float64, device="cuda")))
     with vct.Batch(jobs) as b:
+        # packing, reset, persistent forward, loss sums, exact-walk scatter,
+        # gather (one launch per tile shape present) and fold, for every job
+        assert 1 <= b.config()["kernels_per_run"] <= 10, b.config()
         b.run()
         b.synchronize()
         for j, (loss, grad) in zip(jobs, ref):

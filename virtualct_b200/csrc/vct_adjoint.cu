@@ -108,6 +108,75 @@ constexpr int kAdjFwdThreads = 128;
 // g_m.  MODE 0: loss (meas, optional weights); MODE 1: VJP (upstream
 // dl/d(y/ynorm) in `meas`).  Per-block loss partials are summed in a fixed
 // order.
+// The ray's walk, y, D_m and ray factors g_m; returns its loss term (MODE 0).
+template <int M, int MODE>
+__device__ __forceinline__ double adj_forward_ray(const DevGeom& g, const PixelRec* __restrict__ maps,
+                                                  const double* __restrict__ s_mu, const float* __restrict__ s_pdf,
+                                                  int NE, double ynorm, const double* __restrict__ cos_t,
+                                                  const double* __restrict__ sin_t,
+                                                  const double* __restrict__ det_px0,
+                                                  const double* __restrict__ det_py0, const int4* __restrict__ rec,
+                                                  const float* __restrict__ meas, const float* __restrict__ wts,
+                                                  float* __restrict__ gout, unsigned int* __restrict__ gmax_special,
+                                                  long long ray) {
+  double loss = 0.0;
+  const int v = (int)(ray / g.C);
+  const int c = (int)(ray - (long long)v * g.C);
+  const int kind = rec[ray].x & 3;
+  RayAcc a;
+  acc_init(a);
+  if (kind != kAdjRayNone) {
+    Ray r;
+    ray_setup(g, cos_t[v], sin_t[v], det_px0[c], det_py0[c], r);
+    if (kind == kAdjRayFast)
+      walk_fast<M>(g, maps, r, a);
+    else
+      walk_exact<M>(g, maps, r, a);
+  }
+  double L[8];
+  finish_lines<M>(a, L, g.dens_div);
+  double y = 0.0, D[M];
+#pragma unroll
+  for (int m = 0; m < M; m++) D[m] = 0.0;
+  for (int e = 0; e < NE; e++) {
+    double x = 0.0;
+#pragma unroll
+    for (int m = 0; m < M; m++) x = __fma_rn(s_mu[e * M + m], L[m], x);
+    const int nI = __double2int_rd(x);
+    if (nI <= 125) {
+      const float fr = (float)(x - (double)nI);
+      const float scale = __int_as_float((127 - nI) << 23);
+      const double t = (double)(s_pdf[e] * ex2_approx_f(-fr) * scale);
+      y += t;
+#pragma unroll
+      for (int m = 0; m < M; m++) D[m] = __fma_rn(t, s_mu[e * M + m], D[m]);
+    }
+  }
+  const double kLn2 = 0.6931471805599453;
+  const size_t si = (size_t)v * g.width + g.start + c;
+  double f = 0.0;  // g_m = f * D_m (D_m still in log2 units)
+  if (MODE == 0) {
+    const double p = (double)meas[si];
+    if (p > 0.0 && y > 0.0) {
+      const double wgt = wts ? (double)wts[si] : p;
+      const double rres = log(y / ynorm) - log(p);
+      loss = 0.5 * wgt * rres * rres;
+      f = -wgt * rres / y * kLn2;
+    }
+  } else {
+    f = -(double)meas[si] / ynorm * kLn2;
+  }
+  float gm = 0.0f;
+#pragma unroll
+  for (int m = 0; m < M; m++) {
+    const float gv = (float)(f * D[m]);
+    gout[ray * M + m] = gv;
+    gm = fmaxf(gm, fabsf(gv));
+  }
+  if (kind == kAdjRayExact) atomicMax(gmax_special, __float_as_uint(gm));
+  return loss;
+}
+
 template <int M, int MODE>
 __global__ void __launch_bounds__(kAdjFwdThreads)
 adj_forward_kernel(DevGeom g, const PixelRec* __restrict__ maps, const double* __restrict__ mu_l2,
@@ -127,62 +196,9 @@ adj_forward_kernel(DevGeom g, const PixelRec* __restrict__ maps, const double* _
   const long long nrays = (long long)g.views_used * g.C;
   const long long ray = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   double loss = 0.0;
-  if (ray < nrays) {
-    const int v = (int)(ray / g.C);
-    const int c = (int)(ray - (long long)v * g.C);
-    const int kind = rec[ray].x & 3;
-    RayAcc a;
-    acc_init(a);
-    if (kind != kAdjRayNone) {
-      Ray r;
-      ray_setup(g, cos_t[v], sin_t[v], det_px0[c], det_py0[c], r);
-      if (kind == kAdjRayFast)
-        walk_fast<M>(g, maps, r, a);
-      else
-        walk_exact<M>(g, maps, r, a);
-    }
-    double L[8];
-    finish_lines<M>(a, L, g.dens_div);
-    double y = 0.0, D[M];
-#pragma unroll
-    for (int m = 0; m < M; m++) D[m] = 0.0;
-    for (int e = 0; e < NE; e++) {
-      double x = 0.0;
-#pragma unroll
-      for (int m = 0; m < M; m++) x = __fma_rn(s_mu[e * M + m], L[m], x);
-      const int nI = __double2int_rd(x);
-      if (nI <= 125) {
-        const float fr = (float)(x - (double)nI);
-        const float scale = __int_as_float((127 - nI) << 23);
-        const double t = (double)(s_pdf[e] * ex2_approx_f(-fr) * scale);
-        y += t;
-#pragma unroll
-        for (int m = 0; m < M; m++) D[m] = __fma_rn(t, s_mu[e * M + m], D[m]);
-      }
-    }
-    const double kLn2 = 0.6931471805599453;
-    const size_t si = (size_t)v * g.width + g.start + c;
-    double f = 0.0;  // g_m = f * D_m (D_m still in log2 units)
-    if (MODE == 0) {
-      const double p = (double)meas[si];
-      if (p > 0.0 && y > 0.0) {
-        const double wgt = wts ? (double)wts[si] : p;
-        const double rres = log(y / ynorm) - log(p);
-        loss = 0.5 * wgt * rres * rres;
-        f = -wgt * rres / y * kLn2;
-      }
-    } else {
-      f = -(double)meas[si] / ynorm * kLn2;
-    }
-    float gm = 0.0f;
-#pragma unroll
-    for (int m = 0; m < M; m++) {
-      const float gv = (float)(f * D[m]);
-      gout[ray * M + m] = gv;
-      gm = fmaxf(gm, fabsf(gv));
-    }
-    if (kind == kAdjRayExact) atomicMax(gmax_special, __float_as_uint(gm));
-  }
+  if (ray < nrays)
+    loss = adj_forward_ray<M, MODE>(g, maps, s_mu, s_pdf, NE, ynorm, cos_t, sin_t, det_px0, det_py0, rec, meas, wts,
+                                    gout, gmax_special, ray);
   if (MODE == 0) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) loss += __shfl_xor_sync(0xffffffffu, loss, o);
@@ -500,18 +516,18 @@ __device__ __forceinline__ void adj_cells(const float4* s_q, const int4* s_x, in
 #ifndef VCT_ADJ_VUNROLL
 #define VCT_ADJ_VUNROLL 1
 #endif
+// One tile of the gather (all views), by a block of TX * TY threads; shared
+// staging space from the caller.
 template <int M, int TX, int TY>
-__global__ void __launch_bounds__(TX * TY, VCT_ADJ_MINBLOCKS)
-adj_gather_kernel(AdjGeom a, const double* __restrict__ cos_t, const double* __restrict__ sin_t,
-                  const double2* __restrict__ dir, const int4* __restrict__ rec, const float* __restrict__ gr,
-                  const AdjTileView* __restrict__ tv, float* __restrict__ ext) {
+__device__ __forceinline__ void adj_gather_tile(const AdjGeom& a, int tile, const double* __restrict__ cos_t,
+                                                const double* __restrict__ sin_t, const double2* __restrict__ dir,
+                                                const int4* __restrict__ rec, const float* __restrict__ gr,
+                                                const AdjTileView* __restrict__ tv, float* __restrict__ ext,
+                                                float4* s_qf, int4* s_x, float4 (*s_v)[2]) {
   constexpr int NW = TX * TY / 32, VB = NW;  // views per round: one per warp
-  constexpr int kVUnroll = VCT_ADJ_VUNROLL;
   constexpr int NQ = M <= 2 ? 2 : (M <= 6 ? 3 : 4);
-  __shared__ float4 s_q[NQ][VB * kAdjW];
-  __shared__ int4 s_x[VB * kAdjW];
-  __shared__ float4 s_v[VB][2];  // a, b of each staged view's AdjTileView
-
+  constexpr int kVUnroll = VCT_ADJ_VUNROLL;
+  float4 (*s_q)[VB * kAdjW] = reinterpret_cast<float4 (*)[VB * kAdjW]>(s_qf);
   const int N = a.N, NE1 = N + 1;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   // Each warp covers a patch of PX x (32/PX) cells, as square as the tile
@@ -526,109 +542,122 @@ adj_gather_kernel(AdjGeom a, const double* __restrict__ cos_t, const double* __r
   const float lx = (float)((tx + 0.5 - 0.5 * TX) * s);
   const float ly = (float)((0.5 * TY - ty - 0.5) * s);
   const float lxx = lx * lx, lxy = lx * ly, lyy = ly * ly;
-  const int nbx = (NE1 + TX - 1) / TX, nby = (NE1 + TY - 1) / TY;
+  const int nbx = (NE1 + TX - 1) / TX;
   const int V = a.views_used;
+  const int e0 = (tile % nbx) * TX, f0 = (tile / nbx) * TY;  // first extended column / row
+  const int col = e0 + tx - 1, row = f0 + ty - 1;              // cell indices, -1..N-1
+  // Tile centre (world cm; x right, y up; row r spans y in ((n-r-1)s, (n-r)s]).
+  const double Tx = (e0 - 1 + 0.5 * TX - a.nxm) * s;
+  const double Ty = (a.nxm - (f0 - 1) - 0.5 * TY) * s;
+  const int pix = (col >= 0 && row >= 0) ? (col | (row << 16)) : -2;  // -2: never a lumped pixel
+  const int colx = col + 1, rowx = row + 1;
+  const AdjTileView* __restrict__ tvt = tv + (size_t)tile * V;
 
-  for (int tile = blockIdx.x; tile < nbx * nby; tile += gridDim.x) {
-    const int e0 = (tile % nbx) * TX, f0 = (tile / nbx) * TY;  // first extended column / row
-    const int col = e0 + tx - 1, row = f0 + ty - 1;              // cell indices, -1..N-1
-    // Tile centre (world cm; x right, y up; row r spans y in ((n-r-1)s, (n-r)s]).
-    const double Tx = (e0 - 1 + 0.5 * TX - a.nxm) * s;
-    const double Ty = (a.nxm - (f0 - 1) - 0.5 * TY) * s;
-    const int pix = (col >= 0 && row >= 0) ? (col | (row << 16)) : -2;  // -2: never a lumped pixel
-    const int colx = col + 1, rowx = row + 1;
-    const AdjTileView* __restrict__ tvt = tv + (size_t)tile * V;
-
-    double dacc[M];
+  double dacc[M];
 #pragma unroll
-    for (int m = 0; m < M; m++) dacc[m] = 0.0;
+  for (int m = 0; m < M; m++) dacc[m] = 0.0;
 
-    for (int v0 = 0; v0 < V; v0 += VB) {
-      // ---- staging: warp `warp` takes view v0 + warp
-      {
-        const int vs = warp;  // slot
-        const int v = v0 + vs;
-        int4 vc = make_int4(0, 0, 0, 0);
-        if (v < V) {
-          vc = tvt[v].c;
-          if (lane < 2) s_v[vs][lane] = lane ? tvt[v].b : tvt[v].a;
-        } else if (lane == 1) {
-          s_v[vs][1] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);  // kmax 0: nothing to gather
-        }
-        const int jlo = vc.y, jn = vc.z;
-        const double cb = v < V ? cos_t[v] : 0.0, sb = v < V ? sin_t[v] : 0.0;
-        const double Sx = a.sid * sb, Sy = a.sid * cb;
-        for (int j = lane; j < jn; j += 32) {
-          const int c = jlo + j;
-          const int k = vs * kAdjW + j;
-          const long long ray = (long long)v * a.C + c;
-          if (!VCT_INDEX_OK(v < a.views_used && c >= 0 && c < a.C && j < kAdjW)) continue;
-          const double2 e = dir[c];
-          const double dx = e.x * cb + e.y * sb, dy = -e.x * sb + e.y * cb;
-          const double bt = dx * (Ty - Sy) - dy * (Tx - Sx);
-          const float ax = fabsf((float)dx), ay = fabsf((float)dy);
-          const int4 r = rec[ray];
-          const bool fast = (r.x & 3) == kAdjRayFast;
-          const float* gp = gr + ray * M;
-          float g[8];
-#pragma unroll
-          for (int m = 0; m < 8; m++) g[m] = m < M ? gp[m] : 0.0f;
-          s_q[0][k] = make_float4((float)dx, (float)dy, (float)bt, fast ? h * (ax + ay) : -INFINITY);
-          s_q[1][k] = make_float4(2.0f * h / fmaxf(ax, ay), 1.0f / (ax * ay), g[0], g[1]);
-          if (NQ > 2) s_q[2 % NQ][k] = make_float4(g[2], g[3], g[4], g[5]);
-          if (NQ > 3) s_q[3 % NQ][k] = make_float4(g[6], g[7], 0.0f, 0.0f);
-          s_x[k] = make_int4(r.x >> 2, r.y, fast ? r.z : -1, fast ? r.w : 0);
-        }
+  for (int v0 = 0; v0 < V; v0 += VB) {
+    // ---- staging: warp `warp` takes view v0 + warp
+    {
+      const int vs = warp;  // slot
+      const int v = v0 + vs;
+      int4 vc = make_int4(0, 0, 0, 0);
+      if (v < V) {
+        vc = tvt[v].c;
+        if (lane < 2) s_v[vs][lane] = lane ? tvt[v].b : tvt[v].a;
+      } else if (lane == 1) {
+        s_v[vs][1] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);  // kmax 0: nothing to gather
       }
-      __syncthreads();
-
-      // ---- gather: every cell over the round's views
-      float acc[M];
+      const int jlo = vc.y, jn = vc.z;
+      const double cb = v < V ? cos_t[v] : 0.0, sb = v < V ? sin_t[v] : 0.0;
+      const double Sx = a.sid * sb, Sy = a.sid * cb;
+      for (int j = lane; j < jn; j += 32) {
+        const int c = jlo + j;
+        const int k = vs * kAdjW + j;
+        const long long ray = (long long)v * a.C + c;
+        if (!VCT_INDEX_OK(v < a.views_used && c >= 0 && c < a.C && j < kAdjW)) continue;
+        const double2 e = dir[c];
+        const double dx = e.x * cb + e.y * sb, dy = -e.x * sb + e.y * cb;
+        const double bt = dx * (Ty - Sy) - dy * (Tx - Sx);
+        const float ax = fabsf((float)dx), ay = fabsf((float)dy);
+        const int4 r = rec[ray];
+        const bool fast = (r.x & 3) == kAdjRayFast;
+        const float* gp = gr + ray * M;
+        float g[8];
 #pragma unroll
-      for (int m = 0; m < M; m++) acc[m] = 0.0f;
+        for (int m = 0; m < 8; m++) g[m] = m < M ? gp[m] : 0.0f;
+        s_q[0][k] = make_float4((float)dx, (float)dy, (float)bt, fast ? h * (ax + ay) : -INFINITY);
+        s_q[1][k] = make_float4(2.0f * h / fmaxf(ax, ay), 1.0f / (ax * ay), g[0], g[1]);
+        if (NQ > 2) s_q[2 % NQ][k] = make_float4(g[2], g[3], g[4], g[5]);
+        if (NQ > 3) s_q[3 % NQ][k] = make_float4(g[6], g[7], 0.0f, 0.0f);
+        s_x[k] = make_int4(r.x >> 2, r.y, fast ? r.z : -1, fast ? r.w : 0);
+      }
+    }
+    __syncthreads();
+
+    // ---- gather: every cell over the round's views
+    float acc[M];
+#pragma unroll
+    for (int m = 0; m < M; m++) acc[m] = 0.0f;
 #pragma unroll kVUnroll
-      for (int vb = 0; vb < VB; vb++) {
-        const float4 fb = s_v[vb][1];
-        const int bits = __float_as_int(fb.w);
-        const int4 vi = make_int4(bits & 0xff, 0, (bits >> 8) & 0xff, bits >> 16);  // kmax, -, jn, cplx
-        if (vi.x == 0) continue;
-        const float4 fa = s_v[vb][0];
-        const float jc = fmaf(fb.y, lyy, fmaf(fb.x, lxy, fmaf(fa.w, lxx, fmaf(fa.z, ly, fmaf(fa.y, lx, fa.x)))));
-        // this cell's candidates: the integers in (jc - dj, jc + dj) that lie
-        // in the window, j0 <= j < jlim; at most kmax of them
-        const int j0 = (int)floorf(jc - fb.z) + 1;
-        const int jlim = max(min((int)ceilf(jc + fb.z), vi.z), 0);  // >= 0: the test below is unsigned
-        const int k0 = vb * kAdjW + j0;
-        switch (vi.x) {  // block-uniform
-          case 1: adj_cells<M, NQ, 1, VB * kAdjW>(&s_q[0][0], s_x, vi.w, k0, j0, jlim, lx, ly, colx, rowx, pix, acc); break;
-          case 2: adj_cells<M, NQ, 2, VB * kAdjW>(&s_q[0][0], s_x, vi.w, k0, j0, jlim, lx, ly, colx, rowx, pix, acc); break;
-          case 3: adj_cells<M, NQ, 3, VB * kAdjW>(&s_q[0][0], s_x, vi.w, k0, j0, jlim, lx, ly, colx, rowx, pix, acc); break;
-          default:
-            for (int i = 0; i < vi.x; i += 4)
-              adj_cells<M, NQ, 4, VB * kAdjW>(&s_q[0][0], s_x, vi.w, k0 + i, j0 + i, jlim, lx, ly, colx, rowx, pix, acc);
-            break;
-        }
+    for (int vb = 0; vb < VB; vb++) {
+      const float4 fb = s_v[vb][1];
+      const int bits = __float_as_int(fb.w);
+      const int4 vi = make_int4(bits & 0xff, 0, (bits >> 8) & 0xff, bits >> 16);  // kmax, -, jn, cplx
+      if (vi.x == 0) continue;
+      const float4 fa = s_v[vb][0];
+      const float jc = fmaf(fb.y, lyy, fmaf(fb.x, lxy, fmaf(fa.w, lxx, fmaf(fa.z, ly, fmaf(fa.y, lx, fa.x)))));
+      // this cell's candidates: the integers in (jc - dj, jc + dj) that lie
+      // in the window, j0 <= j < jlim; at most kmax of them
+      const int j0 = (int)floorf(jc - fb.z) + 1;
+      const int jlim = max(min((int)ceilf(jc + fb.z), vi.z), 0);  // >= 0: the test below is unsigned
+      const int k0 = vb * kAdjW + j0;
+      switch (vi.x) {  // block-uniform
+        case 1: adj_cells<M, NQ, 1, VB * kAdjW>(&s_q[0][0], s_x, vi.w, k0, j0, jlim, lx, ly, colx, rowx, pix, acc); break;
+        case 2: adj_cells<M, NQ, 2, VB * kAdjW>(&s_q[0][0], s_x, vi.w, k0, j0, jlim, lx, ly, colx, rowx, pix, acc); break;
+        case 3: adj_cells<M, NQ, 3, VB * kAdjW>(&s_q[0][0], s_x, vi.w, k0, j0, jlim, lx, ly, colx, rowx, pix, acc); break;
+        default:
+          for (int i = 0; i < vi.x; i += 4)
+            adj_cells<M, NQ, 4, VB * kAdjW>(&s_q[0][0], s_x, vi.w, k0 + i, j0 + i, jlim, lx, ly, colx, rowx, pix, acc);
+          break;
       }
-#pragma unroll
-      for (int m = 0; m < M; m++) dacc[m] += (double)acc[m];
-      __syncthreads();
     }
-    if (col < N && row < N) {
-      const size_t n2 = (size_t)NE1 * NE1;
-      const size_t o = (size_t)(row + 1) * NE1 + (col + 1);
 #pragma unroll
-      for (int m = 0; m < M; m++) ext[m * n2 + o] = (float)dacc[m];
-    }
+    for (int m = 0; m < M; m++) dacc[m] += (double)acc[m];
+    __syncthreads();
   }
+  if (col < N && row < N) {
+    const size_t n2 = (size_t)NE1 * NE1;
+    const size_t o = (size_t)(row + 1) * NE1 + (col + 1);
+#pragma unroll
+    for (int m = 0; m < M; m++) ext[m * n2 + o] = (float)dacc[m];
+  }
+}
+
+template <int M, int TX, int TY>
+__global__ void __launch_bounds__(TX * TY, VCT_ADJ_MINBLOCKS)
+adj_gather_kernel(AdjGeom a, const double* __restrict__ cos_t, const double* __restrict__ sin_t,
+                  const double2* __restrict__ dir, const int4* __restrict__ rec, const float* __restrict__ gr,
+                  const AdjTileView* __restrict__ tv, float* __restrict__ ext) {
+  constexpr int VB = TX * TY / 32;
+  constexpr int NQ = M <= 2 ? 2 : (M <= 6 ? 3 : 4);
+  __shared__ float4 s_q[NQ][VB * kAdjW];
+  __shared__ int4 s_x[VB * kAdjW];
+  __shared__ float4 s_v[VB][2];  // a, b of each staged view's AdjTileView
+  const int NE1 = a.N + 1;
+  const int ntiles = ((NE1 + TX - 1) / TX) * ((NE1 + TY - 1) / TY);
+  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
+    adj_gather_tile<M, TX, TY>(a, tile, cos_t, sin_t, dir, rec, gr, tv, ext, &s_q[0][0], s_x, s_v);
 }
 
 // grad[m][r][c] = ext at (r, c), plus the folded cells at index -1 (row -1
 // onto row 0, column -1 onto column 0), plus the exact-walk rays'
 // fixed-point sums; fixed order, so the result is deterministic.
-__global__ void adj_fold_kernel(int M, int N, const float* __restrict__ ext, const unsigned long long* __restrict__ sacc,
-                                const unsigned int* __restrict__ gmax, double lmax, int log2_terms,
-                                float* __restrict__ grad) {
-  const long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+__device__ __forceinline__ void adj_fold_elem(long long i, int M, int N, const float* __restrict__ ext,
+                                              const unsigned long long* __restrict__ sacc,
+                                              const unsigned int* __restrict__ gmax, double lmax, int log2_terms,
+                                              float* __restrict__ grad) {
   const size_t n2 = (size_t)N * N, e2 = (size_t)(N + 1) * (N + 1);
   if (i >= (long long)M * n2) return;
   const int m = (int)(i / n2);
@@ -642,6 +671,12 @@ __global__ void adj_fold_kernel(int M, int N, const float* __restrict__ ext, con
   if (r == 0 && c == 0) v += e[0];
   if (sacc) v += (double)(long long)sacc[i] / special_scale(*gmax, lmax, log2_terms);
   grad[i] = (float)v;
+}
+
+__global__ void adj_fold_kernel(int M, int N, const float* __restrict__ ext, const unsigned long long* __restrict__ sacc,
+                                const unsigned int* __restrict__ gmax, double lmax, int log2_terms,
+                                float* __restrict__ grad) {
+  adj_fold_elem((long long)blockIdx.x * blockDim.x + threadIdx.x, M, N, ext, sacc, gmax, lmax, log2_terms, grad);
 }
 
 // Tile shapes, largest first; the channel window of a tile grows with its
@@ -741,6 +776,240 @@ int launch_adj_fold(const AdjGeom& a, int M, const unsigned long long* d_sacc, c
                                                                 d_grad);
   VCT_CUDA(cudaGetLastError());
   return VCT_OK;
+}
+
+// ------------------------------------------------------------------ batch
+// The batched stages of many slices' loss and gradient (vct_batch.cpp).
+__device__ __forceinline__ int adj_job_of(const unsigned int* __restrict__ first, int n, unsigned int b) {
+  int lo = 0, hi = n - 1;  // the last job whose first block is <= b
+  while (lo < hi) {
+    const int mid = (lo + hi + 1) >> 1;
+    if (first[mid] <= b) lo = mid;
+    else hi = mid - 1;
+  }
+  return lo;
+}
+
+__host__ __device__ unsigned int adj_job_ray_tiles(const DevGeom& g) {
+  const long long nrays = (long long)g.views_used * g.C;
+  return (unsigned int)((nrays + kAdjFwdThreads - 1) / kAdjFwdThreads);
+}
+
+void adj_job_blocks(const AdjJob& j, int M, int tile, unsigned int blocks[kAdjStages]) {
+  const long long n2 = (long long)j.a.N * j.a.N;
+  blocks[kAdjStReset] = j.sacc ? (unsigned int)((M * n2 + 255) / 256) : 1u;
+  blocks[kAdjStLoss] = 1u;
+  blocks[kAdjStSpecial] = (unsigned int)((j.nspecial + 127) / 128);
+  for (int t = 0; t < 4; t++) blocks[kAdjStGather + t] = t == tile ? (unsigned int)tiles_of(j.a, tile) : 0u;
+  blocks[kAdjStFold] = (unsigned int)((M * n2 + 255) / 256);
+}
+
+// gmax and the exact-walk accumulators of every job back to zero.
+__global__ void adj_reset_batch_kernel(const AdjJob* __restrict__ jobs, const unsigned int* __restrict__ first, int n,
+                                       int M) {
+  const int jx = adj_job_of(first, n, blockIdx.x);
+  const AdjJob& J = jobs[jx];
+  const unsigned int b = blockIdx.x - first[jx];
+  if (b == 0 && threadIdx.x == 0) *J.gmax = 0u;
+  if (!J.sacc) return;
+  const long long i = (long long)b * blockDim.x + threadIdx.x;
+  if (i < (long long)M * J.a.N * J.a.N) J.sacc[i] = 0ull;
+}
+
+// The persistent adjoint forward: every warp takes 128-ray tiles (the plain
+// kernel's blocks) in job order from a counter and walks them in four
+// chunks of 32 rays (the plain kernel's warps), reducing each chunk's loss
+// as the plain kernel does and summing the chunks in warp order: the tile's
+// loss partial equals the plain block's.
+constexpr int kAdjBatchWarps = kAdjFwdThreads / 32;
+
+template <int M>
+__global__ void __launch_bounds__(kAdjFwdThreads)
+adj_forward_batch_kernel(const AdjJob* __restrict__ jobs, int njobs, unsigned int ntiles, int ne_max,
+                         unsigned int* __restrict__ counter) {
+  extern __shared__ double smem[];
+  const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+  const size_t slot = (size_t)ne_max * M + (size_t)(ne_max + 1) / 2;
+  double* s_mu = smem + (size_t)warp * slot;                           // [ne_max][M]
+  float* s_pdf = reinterpret_cast<float*>(s_mu + (size_t)ne_max * M);  // [ne_max]
+  int cur = -1;
+  for (;;) {
+    unsigned int t = 0;
+    int j = 0;
+    if (lane == 0) {
+      t = atomicAdd(counter, 1u);
+      if (t < ntiles) {
+        int lo = 0, hi = njobs - 1;  // last job whose first tile is <= t
+        while (lo < hi) {
+          const int mid = (lo + hi + 1) >> 1;
+          if (jobs[mid].tile0 <= t) lo = mid;
+          else hi = mid - 1;
+        }
+        j = lo;
+      }
+    }
+    t = __shfl_sync(0xffffffffu, t, 0);
+    j = __shfl_sync(0xffffffffu, j, 0);
+    if (t >= ntiles) break;
+    const AdjJob& J = jobs[j];
+    if (j != cur) {
+      __syncwarp();  // every lane is done with the previous job's slot
+      for (int i = lane; i < J.NE * M; i += 32) s_mu[i] = J.mu[i];
+      for (int i = lane; i < J.NE; i += 32) s_pdf[i] = J.pdf[i];
+      __syncwarp();
+      cur = j;
+    }
+    const long long nrays = (long long)J.g.views_used * J.g.C;
+    const long long base = (long long)(t - J.tile0) * kAdjFwdThreads;
+    double part = 0.0;
+    for (int k = 0; k < kAdjFwdThreads / 32; k++) {
+      const long long ray = base + k * 32 + lane;
+      double loss = 0.0;
+      if (ray < nrays)
+        loss = adj_forward_ray<M, 0>(J.g, J.maps, s_mu, s_pdf, J.NE, J.ynorm, J.cos_t, J.sin_t, J.px0, J.py0, J.rec,
+                                     J.meas, J.wts, J.gr, J.gmax, ray);
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) loss += __shfl_xor_sync(0xffffffffu, loss, o);
+      part += loss;
+    }
+    if (lane == 0) J.part[t - J.tile0] = part;
+  }
+}
+
+// Fixed-order sum of one job's loss partials (adj_loss_kernel's order).
+__global__ void adj_loss_batch_kernel(const AdjJob* __restrict__ jobs) {
+  __shared__ double s[256];
+  const AdjJob& J = jobs[blockIdx.x];
+  const int n = (int)adj_job_ray_tiles(J.g);
+  double t = 0.0;
+  for (int i = threadIdx.x; i < n; i += 256) t += J.part[i];
+  s[threadIdx.x] = t;
+  __syncthreads();
+  for (int w = 128; w > 0; w >>= 1) {
+    if ((int)threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *J.loss = s[0];
+}
+
+template <int M>
+__global__ void adj_special_batch_kernel(const AdjJob* __restrict__ jobs, const unsigned int* __restrict__ first,
+                                         int n) {
+  const int jx = adj_job_of(first, n, blockIdx.x);
+  const AdjJob& J = jobs[jx];
+  const int i = (int)(blockIdx.x - first[jx]) * blockDim.x + threadIdx.x;
+  if (i >= J.nspecial) return;
+  const double scale = special_scale(*J.gmax, J.lmax, J.log2_terms);
+  const DevGeom& g = J.g;
+  const int ray = J.special[i];
+  const int v = ray / g.C, c = ray - (ray / g.C) * g.C;
+  Ray r;
+  if (!ray_setup(g, J.cos_t[v], J.sin_t[v], J.px0[c], J.py0[c], r)) return;
+  walk_exact_to(g, r, ScatterSink<M>{J.gr + (size_t)ray * M, scale, J.sacc, g.N});
+}
+
+template <int M, int TX, int TY>
+__global__ void __launch_bounds__(TX * TY, VCT_ADJ_MINBLOCKS)
+adj_gather_batch_kernel(const AdjJob* __restrict__ jobs, const unsigned int* __restrict__ first, int n) {
+  constexpr int VB = TX * TY / 32;
+  constexpr int NQ = M <= 2 ? 2 : (M <= 6 ? 3 : 4);
+  __shared__ float4 s_q[NQ][VB * kAdjW];
+  __shared__ int4 s_x[VB * kAdjW];
+  __shared__ float4 s_v[VB][2];
+  const unsigned int total = first[n];
+  for (unsigned int b = blockIdx.x; b < total; b += gridDim.x) {
+    const int jx = adj_job_of(first, n, b);
+    const AdjJob& J = jobs[jx];
+    adj_gather_tile<M, TX, TY>(J.a, (int)(b - first[jx]), J.cos_t, J.sin_t, J.dir, J.rec, J.gr,
+                               reinterpret_cast<const AdjTileView*>(J.tv), J.ext, &s_q[0][0], s_x, s_v);
+  }
+}
+
+__global__ void adj_fold_batch_kernel(const AdjJob* __restrict__ jobs, const unsigned int* __restrict__ first, int n,
+                                      int M) {
+  const int jx = adj_job_of(first, n, blockIdx.x);
+  const AdjJob& J = jobs[jx];
+  const long long i = (long long)(blockIdx.x - first[jx]) * blockDim.x + threadIdx.x;
+  adj_fold_elem(i, M, J.a.N, J.ext, J.sacc, J.gmax, J.lmax, J.log2_terms, J.grad);
+}
+
+template <int M, int TX, int TY>
+static int launch_adj_gather_batch_t(const AdjJob* d_jobs, const unsigned int* d_first, int n, unsigned int blocks,
+                                     cudaStream_t st) {
+  int dev = 0, sms = 0, per_sm = 0;
+  VCT_CUDA(cudaGetDevice(&dev));
+  VCT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  VCT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, adj_gather_batch_kernel<M, TX, TY>, TX * TY, 0));
+  const unsigned int grid = min(blocks, (unsigned int)(max(1, per_sm) * sms));
+  adj_gather_batch_kernel<M, TX, TY><<<grid, TX * TY, 0, st>>>(d_jobs, d_first, n);
+  VCT_CUDA(cudaGetLastError());
+  return VCT_OK;
+}
+
+template <int M>
+static int launch_adj_batch_m(const AdjJob* d_jobs, const unsigned int* d_first, int n, int ne_max,
+                              unsigned int ntiles_ray, const unsigned int nb[kAdjStages], unsigned int* d_counter,
+                              cudaStream_t st, cudaStream_t side, cudaEvent_t ev_fork, cudaEvent_t ev_join) {
+  const unsigned int* f = d_first;
+  adj_reset_batch_kernel<<<nb[kAdjStReset], 256, 0, st>>>(d_jobs, f + kAdjStReset * (n + 1), n, M);
+  VCT_CUDA(cudaGetLastError());
+  VCT_CUDA(cudaMemsetAsync(d_counter, 0, sizeof(unsigned int), st));
+  {
+    const size_t smem = kAdjBatchWarps * ((size_t)ne_max * M + (size_t)(ne_max + 1) / 2) * sizeof(double);
+    int dev = 0, sms = 0, per_sm = 0;
+    VCT_CUDA(cudaGetDevice(&dev));
+    VCT_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+    auto k = adj_forward_batch_kernel<M>;
+    VCT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    VCT_CUDA(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, kAdjFwdThreads, smem));
+    const unsigned int grid = min(ntiles_ray, (unsigned int)(max(1, per_sm) * sms));
+    if (grid) k<<<grid, kAdjFwdThreads, smem, st>>>(d_jobs, n, ntiles_ray, ne_max, d_counter);
+    VCT_CUDA(cudaGetLastError());
+  }
+  adj_loss_batch_kernel<<<n, 256, 0, st>>>(d_jobs);
+  VCT_CUDA(cudaGetLastError());
+  const bool fork = nb[kAdjStSpecial] && side && side != st && ev_fork && ev_join;
+  if (nb[kAdjStSpecial]) {
+    if (fork) {
+      VCT_CUDA(cudaEventRecord(ev_fork, st));
+      VCT_CUDA(cudaStreamWaitEvent(side, ev_fork, 0));
+    }
+    adj_special_batch_kernel<M><<<nb[kAdjStSpecial], 128, 0, fork ? side : st>>>(d_jobs, f + kAdjStSpecial * (n + 1), n);
+    VCT_CUDA(cudaGetLastError());
+    if (fork) VCT_CUDA(cudaEventRecord(ev_join, side));
+  }
+  // one gather launch per tile shape present (each job in its own shape)
+  for (int t = 0; t < 4; t++) {
+    const unsigned int blocks = nb[kAdjStGather + t];
+    if (!blocks) continue;
+    const unsigned int* fg = f + (kAdjStGather + t) * (n + 1);
+    int rc;
+    switch (t) {
+      case 0: rc = launch_adj_gather_batch_t<M, 16, 16>(d_jobs, fg, n, blocks, st); break;
+      case 1: rc = launch_adj_gather_batch_t<M, 16, 8>(d_jobs, fg, n, blocks, st); break;
+      case 2: rc = launch_adj_gather_batch_t<M, 8, 8>(d_jobs, fg, n, blocks, st); break;
+      default: rc = launch_adj_gather_batch_t<M, 8, 4>(d_jobs, fg, n, blocks, st); break;
+    }
+    if (rc) return rc;
+  }
+  if (fork) VCT_CUDA(cudaStreamWaitEvent(st, ev_join, 0));
+  adj_fold_batch_kernel<<<nb[kAdjStFold], 256, 0, st>>>(d_jobs, f + kAdjStFold * (n + 1), n, M);
+  VCT_CUDA(cudaGetLastError());
+  return VCT_OK;
+}
+
+int launch_adj_batch(const AdjJob* d_jobs, const unsigned int* d_first, int n, int M, int ne_max,
+                     unsigned int ntiles_ray, const unsigned int nblocks[kAdjStages], unsigned int* d_counter,
+                     cudaStream_t st, cudaStream_t side, cudaEvent_t ev_fork, cudaEvent_t ev_join) {
+  switch (M) {
+#define VCT_CASE(mm)                                                                                          \
+  case mm:                                                                                                    \
+    return launch_adj_batch_m<mm>(d_jobs, d_first, n, ne_max, ntiles_ray, nblocks, d_counter, st, side, ev_fork, \
+                                  ev_join);
+    VCT_CASE(1) VCT_CASE(2) VCT_CASE(3) VCT_CASE(4) VCT_CASE(5) VCT_CASE(6) VCT_CASE(7) VCT_CASE(8)
+#undef VCT_CASE
+    default: return fail(VCT_E_ARG, "adjoint: 1..8 materials");
+  }
 }
 
 VCT_BOUNDS_READER(bounds_adjoint)

@@ -12,7 +12,10 @@
 //     backprojector jobs in one launch each), for the jobs that ask for an
 //     image.
 // A batch of jobs that ask for a gradient runs the adjoint (loss and dl/drho)
-// of each job on `branches` parallel streams.
+// the same way: map packing, a reset of the exact-walk accumulators, ONE
+// persistent adjoint forward over the 128-ray tiles of all jobs, the loss
+// sums, the exact-walk scatter, the pixel-driven gather over the tiles of
+// all jobs and the fold, one launch each.
 // The ray-tile size of the persistent launch and the view split of the
 // backprojector are chosen by timing candidates on (a sample of) the batch
 // itself when it is created.
@@ -36,8 +39,8 @@ struct vct_batch {
   std::vector<vct_job> jobs;
   std::vector<vct_ctx*> ctx;
   cudaStream_t stream = nullptr;
-  std::vector<cudaStream_t> branch;
-  std::vector<cudaEvent_t> ev;  // [0] fork, [1..] joins
+  cudaStream_t side = nullptr;                           // the adjoint's exact-walk scatter
+  cudaEvent_t ev_fork = nullptr, ev_join = nullptr;
   // persistent forward
   DBuf<FwdJob> d_jobs;
   DBuf<unsigned int> d_counter;
@@ -45,6 +48,10 @@ struct vct_batch {
   DBuf<PackJob> d_pack;
   DBuf<PostJob> d_post;
   DBuf<unsigned int> d_first;  // [pack n+1][post kPostStages][n+1]
+  // the adjoint's batched stages
+  DBuf<AdjJob> d_adj;
+  DBuf<unsigned int> d_adj_first;  // [kAdjStages][n+1]
+  unsigned int adj_blocks[kAdjStages] = {}, adj_ray_tiles = 0;
   unsigned int pack_blocks = 0, post_blocks[kPostStages] = {};
   int cmax = 0, winmax = 0;
   unsigned int ntiles = 0;
@@ -55,8 +62,6 @@ struct vct_batch {
 };
 
 namespace {
-
-constexpr int kBranches = 8;
 
 int sm_count(int device) {
   int n = 0;
@@ -96,30 +101,6 @@ int upload_jobs(vct_batch* b, int tile_rays) {
 int enqueue_forward(vct_batch* b, cudaStream_t st) {
   return launch_forward_batch(b->d_jobs.p, b->n, b->M, b->tile_rays, b->ntiles, b->ne_max, b->grid,
                               b->d_counter.p, st);
-}
-
-// The adjoint of every job (loss and gradient), spread over the branch
-// streams.
-int enqueue_jobs(vct_batch* b) {
-  VCT_CUDA(cudaEventRecord(b->ev[0], b->stream));
-  const int K = (int)b->branch.size();
-  for (int k = 0; k < K; k++) VCT_CUDA(cudaStreamWaitEvent(b->branch[k], b->ev[0], 0));
-  int rc = VCT_OK;
-  for (int i = 0; i < b->n && !rc; i++) {
-    vct_ctx* c = b->ctx[i];
-    const vct_job& j = b->jobs[i];
-    cudaStream_t st = b->branch[i % K];
-    cudaStream_t saved = c->stream;
-    c->stream = st;
-    rc = ctx_adj_run(c, 0, j.d_meas, j.d_weights, nullptr, j.d_grad, j.d_loss);
-    c->stream = saved;
-  }
-  if (rc) return rc;
-  for (int k = 0; k < K; k++) {
-    VCT_CUDA(cudaEventRecord(b->ev[1 + k], b->branch[k]));
-    VCT_CUDA(cudaStreamWaitEvent(b->stream, b->ev[1 + k], 0));
-  }
-  return VCT_OK;
 }
 
 // The job tables of the batched stages (after every context exists and its
@@ -180,11 +161,74 @@ int upload_stage_tables(vct_batch* b) {
   return VCT_OK;
 }
 
+// The adjoint job table: every job's loss-and-gradient arguments (each job
+// gathers in its own tile shape), 128-ray tiles for the persistent forward,
+// and per stage each job's first block.
+int upload_adjoint_tables(vct_batch* b) {
+  const int n = b->n;
+  int rc;
+  std::vector<AdjJob> h(n);
+  std::vector<unsigned int> first((size_t)kAdjStages * (n + 1), 0u);
+  unsigned int acc[kAdjStages] = {}, tiles = 0;
+  for (int i = 0; i < n; i++) {
+    vct_ctx* c = b->ctx[i];
+    const vct_job& j = b->jobs[i];
+    AdjJob& J = h[i];
+    J = AdjJob{};
+    J.g = c->dg;
+    J.a = c->ag;
+    J.maps = c->maps.p;
+    J.mu = c->mu_log2.p;
+    J.pdf = c->pdf.p;
+    J.NE = c->NE;
+    J.ynorm = c->ynorm;
+    J.cos_t = c->cos_t.p;
+    J.sin_t = c->sin_t.p;
+    J.px0 = c->det_px0.p;
+    J.py0 = c->det_py0.p;
+    J.dir = c->adj_dir.p;
+    J.rec = c->adj_rec.p;
+    J.tv = c->adj_tv.p;
+    J.meas = j.d_meas;
+    J.wts = j.d_weights;
+    J.gr = c->adj_g.p;
+    J.part = c->adj_part.p;
+    J.loss = j.d_loss ? j.d_loss : c->adj_loss.p;
+    J.gmax = c->adj_gmax.p;
+    J.special = c->adj_special.p;
+    J.nspecial = c->adj_nspecial;
+    J.sacc = c->adj_nspecial > 0 ? c->adj_sacc.p : nullptr;
+    J.lmax = c->ag.lmax;
+    J.log2_terms = c->ag.log2_terms;
+    J.ext = c->adj_ext.p;
+    J.grad = j.d_grad;
+    J.tile0 = tiles;
+    tiles += adj_job_ray_tiles(c->dg);
+    unsigned int blk[kAdjStages];
+    adj_job_blocks(J, b->M, c->adj_tile, blk);
+    for (int k = 0; k < kAdjStages; k++) {
+      first[(size_t)k * (n + 1) + i] = acc[k];
+      acc[k] += blk[k];
+    }
+  }
+  for (int k = 0; k < kAdjStages; k++) {
+    first[(size_t)k * (n + 1) + n] = acc[k];
+    b->adj_blocks[k] = acc[k];
+  }
+  b->adj_ray_tiles = tiles;
+  if ((rc = b->d_adj.ensure(n)) || (rc = b->d_adj_first.ensure(first.size()))) return rc;
+  VCT_CUDA(cudaMemcpy(b->d_adj.p, h.data(), n * sizeof(AdjJob), cudaMemcpyHostToDevice));
+  VCT_CUDA(cudaMemcpy(b->d_adj_first.p, first.data(), first.size() * sizeof(unsigned int), cudaMemcpyHostToDevice));
+  return VCT_OK;
+}
+
 int enqueue_all(vct_batch* b) {
   int rc;
   const int n = b->n;
   if ((rc = launch_pack_maps_batch(b->d_pack.p, b->d_first.p, n, b->M, b->pack_blocks, b->stream))) return rc;
-  if (b->adjoint) return enqueue_jobs(b);
+  if (b->adjoint)
+    return launch_adj_batch(b->d_adj.p, b->d_adj_first.p, n, b->M, b->ne_max, b->adj_ray_tiles, b->adj_blocks,
+                            b->d_counter.p, b->stream, b->side, b->ev_fork, b->ev_join);
   if ((rc = enqueue_forward(b, b->stream))) return rc;
   const unsigned int* fs = b->d_first.p + (n + 1);
   if ((rc = launch_normalize_noise_batch(b->d_post.p, fs + kPostNorm * (n + 1), n, b->post_blocks[kPostNorm],
@@ -275,8 +319,9 @@ int autotune(vct_batch* b) {
 void release(vct_batch* b) {
   if (b->exec) cudaGraphExecDestroy(b->exec);
   if (b->graph) cudaGraphDestroy(b->graph);
-  for (auto e : b->ev) cudaEventDestroy(e);
-  for (auto s : b->branch) cudaStreamDestroy(s);
+  if (b->ev_fork) cudaEventDestroy(b->ev_fork);
+  if (b->ev_join) cudaEventDestroy(b->ev_join);
+  if (b->side) cudaStreamDestroy(b->side);
   if (b->stream) cudaStreamDestroy(b->stream);
   for (auto c : b->ctx) vct_destroy(c);
   b->d_jobs.release();
@@ -284,6 +329,8 @@ void release(vct_batch* b) {
   b->d_pack.release();
   b->d_post.release();
   b->d_first.release();
+  b->d_adj.release();
+  b->d_adj_first.release();
 }
 
 }  // namespace
@@ -314,20 +361,11 @@ int vct_batch_create(const vct_job* jobs, int n, int M, int device, int tune, vc
     delete b;
     return code;
   };
-  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess)
+  if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaStreamCreateWithFlags(&b->side, cudaStreamNonBlocking) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->ev_fork, cudaEventDisableTiming) != cudaSuccess ||
+      cudaEventCreateWithFlags(&b->ev_join, cudaEventDisableTiming) != cudaSuccess)
     return bail(fail(VCT_E_CUDA, "vct_batch_create: stream"));
-  for (int k = 0; k < kBranches; k++) {
-    cudaStream_t s;
-    if (cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking) != cudaSuccess)
-      return bail(fail(VCT_E_CUDA, "vct_batch_create: stream"));
-    b->branch.push_back(s);
-  }
-  for (int k = 0; k <= kBranches; k++) {
-    cudaEvent_t e;
-    if (cudaEventCreateWithFlags(&e, cudaEventDisableTiming) != cudaSuccess)
-      return bail(fail(VCT_E_CUDA, "vct_batch_create: event"));
-    b->ev.push_back(e);
-  }
   // One context per job: geometry tables, packed maps, spectrum, scratch.
   for (int i = 0; i < n; i++) {
     const vct_job& j = jobs[i];
@@ -357,6 +395,7 @@ int vct_batch_create(const vct_job* jobs, int n, int M, int device, int tune, vc
     if ((rc = upload_jobs(b, b->tile_rays))) return bail(rc);
   }
   if ((rc = upload_stage_tables(b))) return bail(rc);
+  if (adj && (rc = upload_adjoint_tables(b))) return bail(rc);
   if (tune && (rc = autotune(b))) return bail(rc);
   // Capture one run.
   cudaError_t e = cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal);
@@ -395,7 +434,7 @@ int vct_batch_synchronize(vct_batch* b) {
 
 int vct_batch_config(const vct_batch* b, int* tile_rays, int* blocks_per_sm, int* view_groups, int* kernels) {
   if (!b) return fail(VCT_E_ARG, "vct_batch_config: null batch");
-  if (tile_rays) *tile_rays = b->adjoint ? 0 : b->tile_rays;
+  if (tile_rays) *tile_rays = b->adjoint ? 128 : b->tile_rays;
   if (blocks_per_sm) *blocks_per_sm = b->blocks_per_sm;
   if (view_groups) *view_groups = b->view_groups;
   if (kernels) {

@@ -280,4 +280,58 @@ int launch_adj_gather(const AdjGeom& a, int M, int tile, const double* d_cos, co
 int launch_adj_fold(const AdjGeom& a, int M, const unsigned long long* d_sacc, const unsigned int* d_gmax,
                     const float* d_ext, float* d_grad, cudaStream_t st);
 
+// Loss and gradient of many slices, one launch per stage (vct_batch.cpp):
+// the arguments of one job's vct_forward_adjoint_dev.  Per stage,
+// first[stage * (n + 1) + j] is job j's first block (prefix sums); the
+// persistent forward takes 128-ray tiles from a counter (tile0: the job's
+// first tile).  Each block does what the single-slice launch does, in the
+// same order, so losses and gradients are bit-identical.
+struct AdjJob {
+  DevGeom g;
+  AdjGeom a;
+  const PixelRec* maps;
+  const double* mu;  // [NE][M] mu*log2(e)/xfactor
+  const float* pdf;
+  int NE;
+  double ynorm;
+  const double* cos_t;
+  const double* sin_t;
+  const double* px0;
+  const double* py0;
+  const double2* dir;
+  const int4* rec;
+  const void* tv;    // the gather's per (tile, view) records (the batch's tile shape)
+  const float* meas;
+  const float* wts;
+  float* gr;         // ray factors [rays][M]
+  double* part;      // loss partials, one per 128-ray tile
+  double* loss;
+  unsigned int* gmax;
+  const int* special;
+  int nspecial;
+  unsigned long long* sacc;  // exact-walk sums [M][N][N], NULL without exact-walk rays
+  double lmax;
+  int log2_terms;
+  float* ext;        // [M][N+1][N+1]
+  float* grad;       // [M][N][N]
+  unsigned int tile0;
+};
+// Stages; the gather has one stage per tile shape (a job's own shape,
+// adj_pick_tile), kAdjStGather + shape.
+enum { kAdjStReset = 0, kAdjStLoss, kAdjStSpecial, kAdjStGather, kAdjStFold = kAdjStGather + 4, kAdjStages };
+// Block counts of one job per stage for its gather tile shape and M elements.
+void adj_job_blocks(const AdjJob& j, int M, int tile, unsigned int blocks[kAdjStages]);
+// 128-ray tiles of one job's persistent forward.
+#if defined(__CUDACC__)
+__host__ __device__
+#endif
+unsigned int adj_job_ray_tiles(const DevGeom& g);
+// The exact-walk scatter runs on `side` (forked after the loss sums with
+// ev_fork, joined before the fold with ev_join) so that it overlaps the
+// gather; side == st runs everything in order on st.
+int launch_adj_batch(const AdjJob* d_jobs, const unsigned int* d_first, int n, int M, int ne_max,
+                     unsigned int ntiles_ray, const unsigned int nblocks[kAdjStages], unsigned int* d_counter,
+                     cudaStream_t st, cudaStream_t side = nullptr, cudaEvent_t ev_fork = nullptr,
+                     cudaEvent_t ev_join = nullptr);
+
 }  // namespace vct

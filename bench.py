@@ -202,11 +202,12 @@ def fbp_roofline(stages, views, channels, mask_px, peaks):
     peak at BP_FLOP_PER_UPDATE per (mask pixel, view) update."""
     used = views // 2 * 2
     out = {"stages_ms": stages}
-    t_f = stages.get("fbp_filter_kernel")
+    t_f = stages.get("fbp_weight_filter_kernel")
     t_b = stages.get("fbp_backproject")
     if t_f:
         fl = 2.0 * views * channels * channels
-        out["filter"] = {"bound": "fp32", "achieved": fl / t_f / 1e9, "peak": peaks["fp32_tflops"], "unit": "TFLOP/s",
+        out["filter"] = {"kernel": "fbp_weight_filter_kernel (the weight -ln p * coeff fused into the row load)",
+                         "bound": "fp32", "achieved": fl / t_f / 1e9, "peak": peaks["fp32_tflops"], "unit": "TFLOP/s",
                          "frac": fl / t_f / 1e9 / peaks["fp32_tflops"], "flop_per_launch": fl, "launch_ms": t_f}
     if t_b:
         upd = float(mask_px) * used

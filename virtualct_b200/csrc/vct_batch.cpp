@@ -136,7 +136,6 @@ int upload_stage_tables(vct_batch* b) {
       p.coeff = c->fbp_coeff.p;
       p.h0 = c->fbp_h[j.filter].p;
       p.cs = reinterpret_cast<const float2*>(c->cs_f.p);
-      p.g = c->fbp_g.p;
       p.q = c->fbp_q.p;
       p.q2 = p.sym ? c->fbp_q2.p : nullptr;
       b->cmax = std::max(b->cmax, p.C);
@@ -382,7 +381,7 @@ int vct_batch_create(const vct_job* jobs, int n, int M, int device, int tune, vc
     } else if (j.d_img) {
       if ((rc = ctx_build_filter(c, j.filter))) return bail(rc);
       const size_t vc = (size_t)j.geo.views * (j.geo.end_channel - j.geo.start_channel);
-      if ((rc = c->fbp_g.ensure(vc)) || (rc = c->fbp_q.ensure(vc)) || (rc = c->fbp_q2.ensure(vc))) return bail(rc);
+      if ((rc = c->fbp_q.ensure(vc)) || (rc = c->fbp_q2.ensure(vc))) return bail(rc);
     }
     if (cudaStreamSynchronize(c->stream) != cudaSuccess) return bail(fail(VCT_E_CUDA, "vct_batch_create: job set-up"));
   }

@@ -82,40 +82,77 @@ int launch_beam_hardening(float* d_p, long long n, double alpha, double beta, cu
 // constant factors folded into g).  prepareConstMap's rows are one kernel
 // shifted, h[m][k] = c_m h0(m-k), with c_m = 1 except the renormalised edge
 // rows (:114-123), so each view is a 1-D convolution: one block per view, g
-// and h0 in shared memory, each thread FC consecutive outputs with a sliding
-// register window over h0; k runs in ascending order as in the reference.
+// and h0 in shared memory.  Register tiling: each thread owns FC_R = 4
+// consecutive outputs and takes k in chunks of 4; per chunk one 128-bit
+// load of g (the same for every thread) and two aligned 128-bit loads of
+// the 8 kernel values h0(m0 - k0 - 3 .. m0 - k0 + 4) feed 16 FMAs.  For each
+// output k runs in ascending order, as in the reference.
+// WEIGHT: the row is loaded straight from the sinogram and weighted on the
+// way (the weight kernel's g = -ln p * coeff, optionally with the
+// beam-hardening correction), so the weighted sinogram is never stored.
 // TRANSPOSE: the transposed filter, g[v][k] = sum_m h0(m-k) c_m q[v][m]; h0
 // is even (both kernels depend on |m-k| only), so it is the same convolution
 // with the row factor applied to the input instead of the output.
-constexpr int FC_T = 128, FC_R = 5;
+constexpr int FC_R = 4, FC_TMAX = 256;
 
-template <bool TRANSPOSE>
+// Shared memory of one view: g padded to a multiple of 4 (+4 zeros), then
+// h0(d) at index OFF + d for |d| <= C-1 (zero around it), OFF = 3 mod 4 so
+// the window loads are 16-byte aligned.
+__host__ __device__ inline int fc_cpad(int C) { return (C + 3) / 4 * 4; }
+__host__ __device__ inline int fc_off(int C) { return fc_cpad(C) + 3; }
+__host__ __device__ inline int fc_smem_floats(int C) { return (fc_cpad(C) + 4) + (fc_off(C) + fc_cpad(C) + 8); }
+// Threads per block for C channels: one pass of 4 outputs each, up to 256.
+inline int fc_threads(int C) {
+  int t = ((C + FC_R - 1) / FC_R + 31) / 32 * 32;
+  return t > FC_TMAX ? FC_TMAX : t;
+}
+
+template <bool TRANSPOSE, bool WEIGHT>
 __device__ __forceinline__ void fbp_filter_view(const float* __restrict__ G, const float* __restrict__ h0,
                                                 const float* __restrict__ cm, int v, int C, int in_mode,
-                                                float* __restrict__ Q, float2* __restrict__ Q2, float* sm) {
-  float* sg = sm;                 // [C + FC_R]  (zero tail)
-  float* sh = sm + C + FC_R;      // [2C + FC_R] h0(d) at index d + C, zero outside
-  for (int k = threadIdx.x; k < C + FC_R; k += FC_T)
-    sg[k] = k < C ? (TRANSPOSE ? G[(size_t)v * C + k] * cm[k] : G[(size_t)v * C + k]) : 0.0f;
-  for (int d = threadIdx.x; d < 2 * C + FC_R; d += FC_T) sh[d] = (d >= 1 && d < 2 * C) ? h0[d - 1] : 0.0f;
-  __syncthreads();
-  // Each pass covers FC_T * FC_R outputs (one pass up to 640 channels).
-  for (int m0 = threadIdx.x * FC_R; m0 < C; m0 += FC_T * FC_R) {
-    float acc[FC_R];
-    float win[FC_R];  // win[j] = h0(m0 + j - k)
-#pragma unroll
-    for (int j = 0; j < FC_R; j++) {
-      acc[j] = 0.0f;
-      win[j] = sh[m0 + j + C];  // k = 0
+                                                float* __restrict__ Q, float2* __restrict__ Q2, float* sm,
+                                                int W = 0, int start = 0, const double* __restrict__ coeff = nullptr,
+                                                double bh_alpha = 0.0, double bh_beta = 0.0) {
+  const int cpad = fc_cpad(C), off = fc_off(C);
+  float* sg = sm;              // [cpad + 4]
+  float* sh = sm + cpad + 4;   // [off + cpad + 8]
+  const int nt = blockDim.x;
+  for (int k = threadIdx.x; k < cpad + 4; k += nt) {
+    float gk = 0.0f;
+    if (k < C) {
+      if (WEIGHT) {
+        const float pf = G[(size_t)v * W + start + k];
+        double y;
+        if (bh_alpha != 0.0) {
+          y = -(double)logf(pf);
+          y = fabs(y) + bh_alpha * pow(fabs(y), bh_beta);
+        } else {
+          y = -log((double)pf);
+        }
+        gk = (float)(y * coeff[k]);
+      } else {
+        gk = TRANSPOSE ? G[(size_t)v * C + k] * cm[k] : G[(size_t)v * C + k];
+      }
     }
-    for (int k = 0; k < C; k++) {
-      const float gk = sg[k];
+    sg[k] = gk;
+  }
+  for (int x = threadIdx.x; x < off + cpad + 8; x += nt) {
+    const int d = x - off;
+    sh[x] = (d > -C && d < C) ? h0[d + C - 1] : 0.0f;
+  }
+  __syncthreads();
+  for (int m0 = threadIdx.x * FC_R; m0 < C; m0 += nt * FC_R) {
+    float acc[FC_R] = {0.0f, 0.0f, 0.0f, 0.0f};
+    for (int k0 = 0; k0 < cpad; k0 += 4) {
+      const float4 g4 = *reinterpret_cast<const float4*>(sg + k0);
+      const float4 wa = *reinterpret_cast<const float4*>(sh + off + m0 - k0 - 3);
+      const float4 wb = *reinterpret_cast<const float4*>(sh + off + m0 - k0 + 1);
+      const float w[8] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};  // h0(m0 - k0 - 3 + i)
+      const float g[4] = {g4.x, g4.y, g4.z, g4.w};
 #pragma unroll
-      for (int j = 0; j < FC_R; j++) acc[j] = fmaf(win[j], gk, acc[j]);
-      // k -> k+1: h0(m0 + j - k - 1) = win[j-1]; win[0] needs a new value.
+      for (int i = 0; i < 4; i++)
 #pragma unroll
-      for (int j = FC_R - 1; j > 0; j--) win[j] = win[j - 1];
-      win[0] = sh[m0 - k - 1 + C];
+        for (int j = 0; j < FC_R; j++) acc[j] = fmaf(w[j - i + 3], g[i], acc[j]);  // h0(m0 + j - (k0 + i))
     }
 #pragma unroll
     for (int j = 0; j < FC_R; j++) {
@@ -136,35 +173,62 @@ __device__ __forceinline__ void fbp_filter_view(const float* __restrict__ G, con
     // are visible after the barrier.
     __syncthreads();
     const float* qr = Q + (size_t)v * C;
-    for (int m = threadIdx.x; m < C; m += FC_T)
+    for (int m = threadIdx.x; m < C; m += nt)
       Q2[(size_t)v * C + m] = make_float2(qr[m], m + 1 < C ? qr[m + 1] : 0.0f);
   }
 }
 
 template <bool TRANSPOSE>
-__global__ void __launch_bounds__(FC_T)
+__global__ void __launch_bounds__(FC_TMAX)
 fbp_filter_kernel(const float* __restrict__ G, const float* __restrict__ h0, const float* __restrict__ cm,
                   int V, int C, int in_mode, float* __restrict__ Q, float2* __restrict__ Q2) {
-  extern __shared__ float sm[];
-  fbp_filter_view<TRANSPOSE>(G, h0, cm, blockIdx.x, C, in_mode, Q, Q2, sm);
+  extern __shared__ __align__(16) float sm[];
+  fbp_filter_view<TRANSPOSE, false>(G, h0, cm, blockIdx.x, C, in_mode, Q, Q2, sm);
+}
+
+// Weight and filter in one pass, from the sinogram [V][W].
+__global__ void __launch_bounds__(FC_TMAX)
+fbp_weight_filter_kernel(const float* __restrict__ sino, int W, int start, const double* __restrict__ coeff,
+                         double bh_alpha, double bh_beta, const float* __restrict__ h0, const float* __restrict__ cm,
+                         int V, int C, int in_mode, float* __restrict__ Q, float2* __restrict__ Q2) {
+  extern __shared__ __align__(16) float sm[];
+  fbp_filter_view<false, true>(sino, h0, cm, blockIdx.x, C, in_mode, Q, Q2, sm, W, start, coeff, bh_alpha, bh_beta);
+}
+
+static int filter_smem(int C, size_t* bytes) {
+  *bytes = (size_t)fc_smem_floats(C) * sizeof(float);
+  if (*bytes > 220 * 1024) return fail(VCT_E_UNSUPPORTED, "filter: channel count above the shared-memory limit");
+  return VCT_OK;
 }
 
 int launch_fbp_filter(const float* d_g, const float* d_h0, const float* d_cm, int V, int C, int in_mode,
                       float* d_q, cudaStream_t st, float2* d_q2) {
-  const size_t smem = (size_t)(3 * C + 2 * FC_R) * sizeof(float);
-  if (smem > 220 * 1024) return fail(VCT_E_UNSUPPORTED, "filter: channel count above the shared-memory limit");
+  size_t smem;
+  if (int rc = filter_smem(C, &smem)) return rc;
   VCT_CUDA(cudaFuncSetAttribute(fbp_filter_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  fbp_filter_kernel<false><<<V, FC_T, smem, st>>>(d_g, d_h0, d_cm, V, C, in_mode, d_q, d_q2);
+  fbp_filter_kernel<false><<<V, fc_threads(C), smem, st>>>(d_g, d_h0, d_cm, V, C, in_mode, d_q, d_q2);
+  VCT_CUDA(cudaGetLastError());
+  return VCT_OK;
+}
+
+int launch_fbp_weight_filter(const float* d_sino, int W, int start, const double* d_coeff, double bh_alpha,
+                             double bh_beta, const float* d_h0, const float* d_cm, int V, int C, int in_mode,
+                             float* d_q, float2* d_q2, cudaStream_t st) {
+  size_t smem;
+  if (int rc = filter_smem(C, &smem)) return rc;
+  VCT_CUDA(cudaFuncSetAttribute(fbp_weight_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  fbp_weight_filter_kernel<<<V, fc_threads(C), smem, st>>>(d_sino, W, start, d_coeff, bh_alpha, bh_beta, d_h0, d_cm,
+                                                          V, C, in_mode, d_q, d_q2);
   VCT_CUDA(cudaGetLastError());
   return VCT_OK;
 }
 
 int launch_fbp_filter_t(const float* d_q, const float* d_h0, const float* d_cm, int V, int C, float* d_g,
                         cudaStream_t st) {
-  const size_t smem = (size_t)(3 * C + 2 * FC_R) * sizeof(float);
-  if (smem > 220 * 1024) return fail(VCT_E_UNSUPPORTED, "filter: channel count above the shared-memory limit");
+  size_t smem;
+  if (int rc = filter_smem(C, &smem)) return rc;
   VCT_CUDA(cudaFuncSetAttribute(fbp_filter_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-  fbp_filter_kernel<true><<<V, FC_T, smem, st>>>(d_q, d_h0, d_cm, V, C, 0, d_g, nullptr);
+  fbp_filter_kernel<true><<<V, fc_threads(C), smem, st>>>(d_q, d_h0, d_cm, V, C, 0, d_g, nullptr);
   VCT_CUDA(cudaGetLastError());
   return VCT_OK;
 }
@@ -323,6 +387,9 @@ fbp_bp_kernel(const float* __restrict__ Q, int V, int C, int N, int win, float s
 // rows of each base view are read through the L1 cache (the 32 pixels of a
 // warp read neighbouring channels).
 constexpr int BS_TX = 32, BS_TY = 4, BS_VS = 4;  // BS_VS: the default view split
+#ifndef VCT_BP_UNROLL
+#define VCT_BP_UNROLL 8
+#endif
 
 // One base view j of an orbit: the geometry (FBP/reconstructImageTOMO.cpp:
 // 67-73) once, then the four rotated rows, row q at qbase + off[q] (views
@@ -392,12 +459,15 @@ __device__ __forceinline__ void fbp_bp_sym_block(int bx, int by, const float* __
 #pragma unroll
       for (int q = 0; q < 4; q++) off[q] = (long long)(q * V4 - (q + seg >= 4 ? V : 0)) * C;
       int j = s0;
-      for (; j + 1 < s1; j += 2) {
-        const float2 t0 = __ldg(cs + j), t1 = __ldg(cs + j + 1);
-        bp_orbit_view<PAIRS>(Q, Q2, C, xx, yy, t0, (long long)j * C, off, sid, inv_dbeta, center, acc);
-        bp_orbit_view<PAIRS>(Q, Q2, C, xx, yy, t1, (long long)(j + 1) * C, off, sid, inv_dbeta, center, acc);
+      // VCT_BP_UNROLL base views per iteration: their row loads are in flight together
+      for (; j + VCT_BP_UNROLL - 1 < s1; j += VCT_BP_UNROLL) {
+#pragma unroll
+        for (int u = 0; u < VCT_BP_UNROLL; u++)
+          bp_orbit_view<PAIRS>(Q, Q2, C, xx, yy, __ldg(cs + j + u), (long long)(j + u) * C, off, sid, inv_dbeta,
+                               center, acc);
       }
-      if (j < s1) bp_orbit_view<PAIRS>(Q, Q2, C, xx, yy, __ldg(cs + j), (long long)j * C, off, sid, inv_dbeta, center, acc);
+      for (; j < s1; j++)
+        bp_orbit_view<PAIRS>(Q, Q2, C, xx, yy, __ldg(cs + j), (long long)j * C, off, sid, inv_dbeta, center, acc);
     }
   }
   if (z > 0) {
@@ -776,8 +846,7 @@ void post_job_blocks(const PostJob& j, unsigned int blocks[kPostStages]) {
   blocks[kPostNorm] = (unsigned int)(((long long)j.V * j.W + 255) / 256);
   blocks[kPostWeight] = blocks[kPostFilter] = blocks[kPostBpSym] = blocks[kPostBpGen] = 0;
   if (!j.img) return;
-  blocks[kPostWeight] = (unsigned int)(((long long)j.V * j.C + 255) / 256);
-  blocks[kPostFilter] = (unsigned int)j.V;
+  blocks[kPostFilter] = (unsigned int)j.V;  // weight applied on the filter's row load
   if (j.sym) {
     const int H = j.N / 2;
     blocks[kPostBpSym] = (unsigned int)(((H + BS_TX - 1) / BS_TX) * ((H + BS_TY - 1) / BS_TY));
@@ -786,21 +855,13 @@ void post_job_blocks(const PostJob& j, unsigned int blocks[kPostStages]) {
   }
 }
 
-__global__ void fbp_weight_batch_kernel(const PostJob* __restrict__ jobs, const unsigned int* __restrict__ first,
-                                        int n) {
+__global__ void __launch_bounds__(FC_TMAX) fbp_filter_batch_kernel(const PostJob* __restrict__ jobs,
+                                                                   const unsigned int* __restrict__ first, int n) {
+  extern __shared__ __align__(16) float sm[];
   const int jx = post_job_of(first, n, blockIdx.x);
   const PostJob& J = jobs[jx];
-  const long long i = (long long)(blockIdx.x - first[jx]) * blockDim.x + threadIdx.x;
-  if (i >= (long long)J.V * J.C) return;
-  fbp_weight_elem(J.sino, i, J.W, J.start, J.C, J.coeff, 0.0, 0.0, J.g);
-}
-
-__global__ void __launch_bounds__(FC_T) fbp_filter_batch_kernel(const PostJob* __restrict__ jobs,
-                                                                const unsigned int* __restrict__ first, int n) {
-  extern __shared__ float sm[];
-  const int jx = post_job_of(first, n, blockIdx.x);
-  const PostJob& J = jobs[jx];
-  fbp_filter_view<false>(J.g, J.h0, J.h0 + 2 * J.C - 1, (int)(blockIdx.x - first[jx]), J.C, 0, J.q, J.q2, sm);
+  fbp_filter_view<false, true>(J.sino, J.h0, J.h0 + 2 * J.C - 1, (int)(blockIdx.x - first[jx]), J.C, 0, J.q, J.q2,
+                               sm, J.W, J.start, J.coeff, 0.0, 0.0);
 }
 
 template <int VS>
@@ -829,15 +890,12 @@ fbp_bp_batch_kernel(const PostJob* __restrict__ jobs, const unsigned int* __rest
 int launch_fbp_batch(const PostJob* d_jobs, const unsigned int* d_first, int n, const unsigned int nblocks[kPostStages],
                      int cmax, int winmax, int view_groups, cudaStream_t st) {
   const unsigned int* f = d_first;
-  if (nblocks[kPostWeight]) {
-    fbp_weight_batch_kernel<<<nblocks[kPostWeight], 256, 0, st>>>(d_jobs, f + kPostWeight * (n + 1), n);
-    VCT_CUDA(cudaGetLastError());
-  }
-  if (nblocks[kPostFilter]) {
-    const size_t smem = (size_t)(3 * cmax + 2 * FC_R) * sizeof(float);
-    if (smem > 220 * 1024) return fail(VCT_E_UNSUPPORTED, "filter: channel count above the shared-memory limit");
+  if (nblocks[kPostFilter]) {  // the weight is applied on the filter's row load
+    size_t smem;
+    if (int rc = filter_smem(cmax, &smem)) return rc;
     VCT_CUDA(cudaFuncSetAttribute(fbp_filter_batch_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    fbp_filter_batch_kernel<<<nblocks[kPostFilter], FC_T, smem, st>>>(d_jobs, f + kPostFilter * (n + 1), n);
+    fbp_filter_batch_kernel<<<nblocks[kPostFilter], fc_threads(cmax), smem, st>>>(d_jobs, f + kPostFilter * (n + 1),
+                                                                                  n);
     VCT_CUDA(cudaGetLastError());
   }
   if (nblocks[kPostBpSym]) {

@@ -664,25 +664,22 @@ static int fbp_into(vct_ctx* c, const float* d_sino, int filter, int in_mode, fl
   if (filter != 1 && filter != 2) return fail(VCT_E_ARG, "filter must be 1 (Ram-Lak) or 2 (Shepp-Logan)");
   const int V = c->geo.views, C = c->dg.C;
   if ((rc = build_filter(c, filter))) return rc;
-  if ((rc = c->fbp_g.ensure((size_t)V * C)) || (rc = c->fbp_q.ensure((size_t)V * C))) return rc;
+  if ((rc = c->fbp_q.ensure((size_t)V * C))) return rc;
   // the quarter-turn backprojector reads the filtered rows as pairs
   const bool sym = V % 4 == 0 && c->dg.N % 2 == 0;
   if (sym && (rc = c->fbp_q2.ensure((size_t)V * C))) return rc;
   float2* q2 = sym ? c->fbp_q2.p : nullptr;
   c->timer.begin(c->stream);
-  if ((rc = launch_fbp_weight(d_sino, V, c->geo.width, c->geo.start_channel, C, c->fbp_coeff.p, c->fbp_g.p,
-                              c->stream, c->bh_alpha, c->bh_beta)))
+  if ((rc = launch_fbp_weight_filter(d_sino, c->geo.width, c->geo.start_channel, c->fbp_coeff.p, c->bh_alpha,
+                                     c->bh_beta, c->fbp_h[filter].p, c->fbp_h[filter].p + 2 * C - 1, V, C, in_mode,
+                                     c->fbp_q.p, q2, c->stream)))
     return rc;
-  c->timer.mark("fbp_weight_kernel", c->stream);
-  if ((rc = launch_fbp_filter(c->fbp_g.p, c->fbp_h[filter].p, c->fbp_h[filter].p + 2 * C - 1, V, C, in_mode,
-                              c->fbp_q.p, c->stream, q2)))
-    return rc;
-  c->timer.mark("fbp_filter_kernel", c->stream);
+  c->timer.mark("fbp_weight_filter_kernel", c->stream);
   if ((rc = launch_fbp_backproject(c->fbp_q.p, V, C, c->dg.N, c->geo.pixel_cm, c->geo.sid_cm, c->geo.max_beta,
                                    c->geo.xfactor, c->cs_f.p, d_img, c->stream, view_groups, band0, band1, q2)))
     return rc;
   c->timer.mark("fbp_backproject", c->stream);
-  c->launches += 3;
+  c->launches += 2;
   return VCT_OK;
 }
 

@@ -157,13 +157,12 @@ struct PostJob {
   const double* coeff;    // weight factors [C]
   const float* h0;        // filter kernel [2C-1], then the row factors [C]
   const float2* cs;       // (cos, sin) per view
-  float* g;               // weighted sinogram [V][C]
   float* q;               // filtered sinogram [V][C]
   float2* q2;             // its interpolation pairs [V][C] (quarter-turn jobs), or NULL
   int C, start, N, sym, win;
   float scale, sid, inv_dbeta, center, out_scale;
 };
-enum { kPostNorm = 0, kPostWeight, kPostFilter, kPostBpSym, kPostBpGen, kPostStages };
+enum { kPostNorm = 0, kPostWeight, kPostFilter, kPostBpSym, kPostBpGen, kPostStages };  // kPostWeight: no blocks (fused into the filter)
 // Block counts of one job per stage (0 where the stage does not apply).
 void post_job_blocks(const PostJob& j, unsigned int blocks[kPostStages]);
 // The backprojector's launch parameters of one slice (as launch_fbp_backproject
@@ -191,6 +190,11 @@ unsigned int pack_maps_blocks(int N);
 int launch_fbp_weight(const float* d_sino, int V, int W, int start, int C, const double* d_coeff,
                       float* d_g, cudaStream_t st, double bh_alpha = 0.0, double bh_beta = 0.0);
 int launch_beam_hardening(float* d_p, long long n, double alpha, double beta, cudaStream_t st);
+// launch_fbp_weight + launch_fbp_filter in one pass (the weighted sinogram is
+// not stored).
+int launch_fbp_weight_filter(const float* d_sino, int W, int start, const double* d_coeff, double bh_alpha,
+                             double bh_beta, const float* d_h0, const float* d_cm, int V, int C, int in_mode,
+                             float* d_q, float2* d_q2, cudaStream_t st);
 // d_q2 (optional): the filtered rows also as interpolation pairs
 // (q[c], q[c+1]) [V][C], for the quarter-turn backprojector.
 int launch_fbp_filter(const float* d_g, const float* d_h0, const float* d_cm, int V, int C, int in_mode,

@@ -26,21 +26,11 @@ int main(int argc, char** argv) {
   FILE* f = fopen(argv[1], "rb");
   if (!f || fread(maps.data(), 2, maps.size(), f) != maps.size()) return 3;
   fclose(f);
-  // Padded layout of pack_maps_kernel: row/column -1 repeats 0, the rest of
-  // the border is 0.
+  // The device layout, packed by the product's own per-pixel routine: both
+  // 16-byte layouts and the split copy.
   std::vector<PixelRec> packed(map_records(N));
   const int P = N + 2 * kMapPad;
-  for (int r = -kMapPad; r < N + kMapPad; r++)
-    for (int c = -kMapPad; c < N + kMapPad; c++) {
-      const bool inside = r >= -1 && c >= -1 && r < N && c < N;
-      const size_t src = (size_t)(r < 0 ? 0 : r) * N + (c < 0 ? 0 : c);
-      PixelRec& rec = packed[pad_index(c, r, N)];
-      for (int m = 0; m < 8; m++) {
-        int16_t v = (inside && m < M) ? maps[m * (size_t)N * N + src] : 0;
-        rec.m[m] = v < 0 ? 0 : v;
-      }
-      packed[(size_t)P * P + (size_t)(c + kMapPad) * P + (r + kMapPad)] = rec;  // transposed copy
-    }
+  for (int p = 0; p < P * P; p++) pack_maps_elem(p, maps.data(), M, N, packed.data(), packed.data() + (size_t)P * P);
   // Geometry exactly as vct_create derives it (defaults of physParamsTOMO.h).
   DevGeom dg;
   dg.N = N;

@@ -33,8 +33,9 @@
 namespace vct {
 
 // ---------------------------------------------------------------- map packing
-__device__ __forceinline__ void pack_maps_elem(int p, const int16_t* __restrict__ maps, int M, int N,
-                                               PixelRec* __restrict__ out, PixelRec* __restrict__ out_t) {
+// out_t, when given, receives the transposed copy.
+VCT_HD void pack_maps_elem(int p, const int16_t* __restrict__ maps, int M, int N, PixelRec* __restrict__ out,
+                           PixelRec* __restrict__ out_t) {
   const int P = N + 2 * kPad;
   const int r = p / P - kPad, c = p % P - kPad;  // padded row/column in [-kPad, N+kPad)
   PixelRec rec;

@@ -451,6 +451,171 @@ VCT_HD void acc_words(const int4& w, unsigned int q, unsigned long long* P, unsi
   }
 }
 
+// State of one ray's fast walk from fast_begin to fast_end.  Event times are
+// in fixed point, so the loop runs on the integer pipes:
+//   kh  = k << 12, k the next major event (an integer step, 1..K);
+//   T   = the next minor event in units of 2^-44 steps, 64 bits (its high
+//         word is in units of 2^-12 steps, so k is due first iff kh <= T.hi);
+//   t31 = the current time in units of 2^-31 steps, modulo 2^32.
+// A segment's weight is the difference of its end and start times in 2^-31
+// steps (0..2^31), so the weights of a ray add up to exactly K steps.  Minor
+// events advance by DT = dt * 2^44 rounded (2^-45 steps per event at most;
+// the reference's own crossing points are found afresh per step).
+template <int M>
+struct FastWalk {
+  static constexpr int kWords = (M + 1) / 2;
+  const int4* m4;         // the layout walked (row-major, or transposed for x-major rays)
+  int P2;                 // P * P: padded indices are below it
+  int pix, dpix_maj, dpix_min, pix_first;
+  unsigned long long T, DT;
+  unsigned int kh, kend, t31;
+  int it, it_max, nseg;
+  int pix_lumped;         // the lumped first segment (entry to the first major gridline)
+  double rr_first;
+  unsigned long long accP[kWords], accH[kWords];
+};
+
+// Every iteration closes kFastUnroll segments.  The event logic does not
+// depend on the map, so the segments are laid out first and their gathers
+// issued together before any is consumed.
+constexpr int kFastUnroll = VCT_FWD_UNROLL;
+
+// Sets up the event loop of a ray whose plan is kPlanWalk.
+template <int M>
+VCT_HD void fast_begin(const DevGeom& g, const PixelRec* __restrict__ maps, const FastPlan& pl, FastWalk<M>& w) {
+  const int N = g.N;
+  const int xmaj = pl.xmaj, maj0 = pl.maj0, min0 = pl.min0, dirw = pl.dirw;
+  const int P = N + 2 * kPad;
+  const PixelRec* __restrict__ mp = maps;
+  if (xmaj && VCT_FWD_DUAL_LAYOUT) {
+    // transposed copy: (col, row) at (col + kPad) * P + (row + kPad)
+    mp = maps + (size_t)P * P;
+    w.pix = (maj0 + kPad) * P + (min0 + kPad);
+    w.dpix_maj = (pl.pha_pos ? 1 : -1) * P;
+    w.dpix_min = -dirw;
+  } else if (xmaj) {
+    w.pix = pad_index(maj0, min0, N);
+    w.dpix_maj = pl.pha_pos ? 1 : -1;
+    w.dpix_min = -dirw * P;
+  } else {
+    w.pix = pad_index(min0, maj0, N);
+    w.dpix_maj = (pl.pha_pos ? -1 : 1) * P;
+    w.dpix_min = dirw;
+  }
+  w.pix_first = w.pix;
+  w.P2 = P * P;
+  w.m4 = reinterpret_cast<const int4*>(mp);
+  // Times beyond 2^18 steps (past every walk's end) are clamped there.
+  const double kTcap = 262144.0;  // 2^18 steps
+  w.T = (unsigned long long)dmul_rn(fmin(pl.tmin0, kTcap), 17592186044416.0);  // 2^44
+  w.DT = (unsigned long long)dmul_rn(fmin(pl.dt, kTcap), 17592186044416.0);
+  w.kh = 1u << 12;                          // next major event: step 1
+  w.kend = (unsigned int)pl.K << 12;        // the last major event, step K
+  w.t31 = 0u;
+  w.it = 0;
+  w.it_max = (8 * N + 128) / kFastUnroll;
+  w.nseg = 0;
+  w.pix_lumped = pl.pix_lumped;
+  w.rr_first = pl.rr_first;
+#pragma unroll
+  for (int i = 0; i < FastWalk<M>::kWords; i++) w.accP[i] = w.accH[i] = 0ull;
+}
+
+// Bulk iterations carry no per-slot end test.  A segment ends at the next
+// major event at the latest, so the next major event advances by at most one
+// step per segment: while k + kFastUnroll - 1 <= K every slot of the
+// iteration starts before step K.  The integer sums do not depend on how the
+// segments are grouped, so the result is the same as the checked loop's.
+template <int M>
+VCT_HD bool fast_bulk_ok(const FastWalk<M>& w) {
+  constexpr unsigned int kSpan = (unsigned int)(kFastUnroll - 1) << 12;
+  return w.it < w.it_max && w.kend >= kSpan && w.kh <= w.kend - kSpan;
+}
+
+template <int M>
+VCT_HD void fast_layout_bulk(FastWalk<M>& w, int px[kFastUnroll], unsigned int wq[kFastUnroll]) {
+#pragma unroll
+  for (int u = 0; u < kFastUnroll; u++) {
+    const bool mj = w.kh <= (unsigned int)(w.T >> 32);
+    const unsigned int e31 = mj ? w.kh << 19 : (unsigned int)(w.T >> 13);
+    wq[u] = e31 - w.t31;
+    px[u] = w.pix;
+    w.t31 = e31;
+    if (mj) w.kh += 1u << 12;
+    else w.T += w.DT;
+    w.pix += mj ? w.dpix_maj : w.dpix_min;
+  }
+  w.nseg += kFastUnroll;
+  w.it++;
+}
+
+// The last iterations, each slot tested against the end: a slot is live
+// while major event K has not been passed.  Past the end, slots repeat the
+// first segment's pixel with weight 0; the indices stay inside the padded
+// border because the walk ends within one step of the square.
+template <int M>
+VCT_HD void fast_layout_checked(FastWalk<M>& w, int px[kFastUnroll], unsigned int wq[kFastUnroll]) {
+#pragma unroll
+  for (int u = 0; u < kFastUnroll; u++) {
+    const bool live = w.kh <= w.kend;
+    const bool mj = w.kh <= (unsigned int)(w.T >> 32);
+    const unsigned int e31 = mj ? w.kh << 19 : (unsigned int)(w.T >> 13);
+    wq[u] = live ? e31 - w.t31 : 0u;
+    px[u] = live ? w.pix : w.pix_first;
+    w.nseg += live;
+    if (live) {
+      w.t31 = e31;
+      if (mj) w.kh += 1u << 12;
+      else w.T += w.DT;
+      w.pix += mj ? w.dpix_maj : w.dpix_min;
+    }
+  }
+  w.it++;
+}
+
+// The records of the laid-out segments, all loads issued before any is used.
+template <int M>
+VCT_HD void fast_load(const FastWalk<M>& w, const int px[kFastUnroll], int4 wv[kFastUnroll]) {
+#pragma unroll
+  for (int u = 0; u < kFastUnroll; u++)
+    wv[u] = VCT_INDEX_OK(px[u] >= 0 && px[u] < w.P2) ? ldg4(w.m4 + px[u]) : make_int4(0, 0, 0, 0);
+}
+
+template <int M>
+VCT_HD void fast_acc(FastWalk<M>& w, const int4 wv[kFastUnroll], const unsigned int wq[kFastUnroll]) {
+#pragma unroll
+  for (int u = 0; u < kFastUnroll; u++) acc_words<M>(wv[u], wq[u], w.accP, w.accH);
+}
+
+// Walks what is left of the ray and adds its sums and the lumped first
+// segment to the ray's accumulator.
+template <int M>
+VCT_HD void fast_end(const PixelRec* __restrict__ maps, FastWalk<M>& w, RayAcc& a) {
+  while (fast_bulk_ok(w)) {
+    int px[kFastUnroll];
+    unsigned int wq[kFastUnroll];
+    int4 wv[kFastUnroll];
+    fast_layout_bulk(w, px, wq);
+    fast_load(w, px, wv);
+    fast_acc(w, wv, wq);
+  }
+  while (w.it < w.it_max && w.kh <= w.kend) {
+    int px[kFastUnroll];
+    unsigned int wq[kFastUnroll];
+    int4 wv[kFastUnroll];
+    fast_layout_checked(w, px, wq);
+    fast_load(w, px, wv);
+    fast_acc(w, wv, wq);
+  }
+#pragma unroll
+  for (int i = 0; i < FastWalk<M>::kWords; i++) {
+    a.Lq[2 * i] += w.accP[i] - (w.accH[i] << 16);
+    if (2 * i + 1 < M) a.Lq[2 * i + 1] += w.accH[i];
+  }
+  a.nseg += w.nseg;
+  if (w.pix_lumped >= 0 && VCT_INDEX_OK(w.pix_lumped < w.P2)) gather_add_exact<M>(maps, w.pix_lumped, w.rr_first, a);
+}
+
 // Returns false when the ray needs the exact walk.
 template <int M>
 VCT_HD bool walk_fast(const DevGeom& g, const PixelRec* __restrict__ maps, const Ray& r, RayAcc& a) {
@@ -458,123 +623,10 @@ VCT_HD bool walk_fast(const DevGeom& g, const PixelRec* __restrict__ maps, const
   fast_plan(g, r, pl);
   if (pl.status == kPlanExact) return false;
   if (pl.status == kPlanEmpty) return true;
-  const int N = g.N;
-  const int xmaj = pl.xmaj, maj0 = pl.maj0, min0 = pl.min0, dirw = pl.dirw;
-  const int pix_lumped = pl.pix_lumped;
-  const double rr_first = pl.rr_first;
   a.sec = pl.sec;
-  const int P = N + 2 * kPad;
-  int pix, dpix_maj, dpix_min;
-  const PixelRec* __restrict__ mp = maps;
-  if (xmaj && VCT_FWD_DUAL_LAYOUT) {
-    // transposed copy: (col, row) at (col + kPad) * P + (row + kPad)
-    mp = maps + (size_t)P * P;
-    pix = (maj0 + kPad) * P + (min0 + kPad);
-    dpix_maj = (pl.pha_pos ? 1 : -1) * P;
-    dpix_min = -dirw;
-  } else if (xmaj) {
-    pix = pad_index(maj0, min0, N);
-    dpix_maj = pl.pha_pos ? 1 : -1;
-    dpix_min = -dirw * P;
-  } else {
-    pix = pad_index(min0, maj0, N);
-    dpix_maj = (pl.pha_pos ? -1 : 1) * P;
-    dpix_min = dirw;
-  }
-  const int pix_first = pix;
-  // Event times in fixed point, so the loop runs on the integer pipes:
-  //   kh  = k << 12, k the next major event (an integer step, 1..K);
-  //   T   = the next minor event in units of 2^-44 steps, 64 bits (its high
-  //         word is in units of 2^-12 steps, so k is due first iff kh <= T.hi);
-  //   t31 = the current time in units of 2^-31 steps, modulo 2^32.
-  // A segment's weight is the difference of its end and start times in
-  // 2^-31 steps (0..2^31), so the weights of a ray add up to exactly K steps.
-  // Minor events advance by DT = dt * 2^44 rounded (2^-45 steps per event at
-  // most; the reference's own crossing points are found afresh per step).
-  // Times beyond 2^18 steps (past every walk's end) are clamped there.
-  const double kTcap = 262144.0;                         // 2^18 steps
-  unsigned long long T = (unsigned long long)dmul_rn(fmin(pl.tmin0, kTcap), 17592186044416.0);  // 2^44
-  const unsigned long long DT = (unsigned long long)dmul_rn(fmin(pl.dt, kTcap), 17592186044416.0);
-  unsigned int kh = 1u << 12;                            // next major event: step 1
-  const unsigned int kend = (unsigned int)pl.K << 12;    // the last major event, step K
-  unsigned int t31 = 0u;
-  const int4* __restrict__ m4 = reinterpret_cast<const int4*>(mp);
-  constexpr int kWords = (M + 1) / 2;
-  unsigned long long accP[kWords], accH[kWords];
-#pragma unroll
-  for (int i = 0; i < kWords; i++) accP[i] = accH[i] = 0ull;
-  int nseg = 0;
-  // Every iteration closes one segment.  The event logic does not depend on
-  // the map, so kUnroll segments are laid out first and their gathers issued
-  // together before any is consumed.  Past the end, slots repeat the first
-  // segment's pixel with weight 0; the indices stay inside the padded border
-  // because the walk ends within one step of the square.
-  constexpr int kUnroll = VCT_FWD_UNROLL;
-  const int it_max = (8 * N + 128) / kUnroll;
-  int it = 0;
-  // Bulk iterations, with no per-slot end test.  A segment ends at the next
-  // major event at the latest, so the next major event advances by at most
-  // one step per segment: while k + kUnroll - 1 <= K every slot of the
-  // iteration starts before step K.  The integer sums do not depend on how
-  // the segments are grouped, so the result is the same as the checked
-  // loop's alone.
-  const unsigned int kbulk = kend - ((unsigned int)(kUnroll - 1) << 12);
-  for (; it < it_max && kend >= ((unsigned int)(kUnroll - 1) << 12) && kh <= kbulk; it++) {
-    int px[kUnroll];
-    unsigned int wq[kUnroll];
-#pragma unroll
-    for (int u = 0; u < kUnroll; u++) {
-      const bool mj = kh <= (unsigned int)(T >> 32);
-      const unsigned int e31 = mj ? kh << 19 : (unsigned int)(T >> 13);
-      wq[u] = e31 - t31;
-      px[u] = pix;
-      t31 = e31;
-      if (mj) kh += 1u << 12;
-      else T += DT;
-      pix += mj ? dpix_maj : dpix_min;
-    }
-    nseg += kUnroll;
-    int4 wv[kUnroll];
-#pragma unroll
-    for (int u = 0; u < kUnroll; u++)
-      wv[u] = VCT_INDEX_OK(px[u] >= 0 && px[u] < P * P) ? ldg4(m4 + px[u]) : make_int4(0, 0, 0, 0);
-#pragma unroll
-    for (int u = 0; u < kUnroll; u++) acc_words<M>(wv[u], wq[u], accP, accH);
-  }
-  // The last iterations, each slot tested against the end: a slot is live
-  // while major event K has not been passed.
-  for (; it < it_max && kh <= kend; it++) {
-    int px[kUnroll];
-    unsigned int wq[kUnroll];
-#pragma unroll
-    for (int u = 0; u < kUnroll; u++) {
-      const bool live = kh <= kend;
-      const bool mj = kh <= (unsigned int)(T >> 32);
-      const unsigned int e31 = mj ? kh << 19 : (unsigned int)(T >> 13);
-      wq[u] = live ? e31 - t31 : 0u;
-      px[u] = live ? pix : pix_first;
-      nseg += live;
-      if (live) {
-        t31 = e31;
-        if (mj) kh += 1u << 12;
-        else T += DT;
-        pix += mj ? dpix_maj : dpix_min;
-      }
-    }
-    int4 wv[kUnroll];
-#pragma unroll
-    for (int u = 0; u < kUnroll; u++)
-      wv[u] = VCT_INDEX_OK(px[u] >= 0 && px[u] < P * P) ? ldg4(m4 + px[u]) : make_int4(0, 0, 0, 0);
-#pragma unroll
-    for (int u = 0; u < kUnroll; u++) acc_words<M>(wv[u], wq[u], accP, accH);
-  }
-#pragma unroll
-  for (int i = 0; i < kWords; i++) {
-    a.Lq[2 * i] += accP[i] - (accH[i] << 16);
-    if (2 * i + 1 < M) a.Lq[2 * i + 1] += accH[i];
-  }
-  a.nseg += nseg;
-  if (pix_lumped >= 0 && VCT_INDEX_OK(pix_lumped < P * P)) gather_add_exact<M>(maps, pix_lumped, rr_first, a);
+  FastWalk<M> w;
+  fast_begin(g, maps, pl, w);
+  fast_end(maps, w, a);
   return true;
 }
 

@@ -455,41 +455,77 @@ __global__ void adj_tiles_kernel(AdjGeom a, const double* __restrict__ cos_t, co
   }
 }
 
+// Staged rays of one round in shared memory, ST slots.  Per slot, for a ray
+// of direction (dx, dy) and offset bt of its line from the tile centre, with
+// a = max(|dx|, |dy|), c = min(...) (each at least 1e-12) and h half a pixel:
+//   q[0]  = (sign(dx)/|dy|, sign(dy)/|dx|, bt/(h |dx| |dy|), g0)
+//   q[1]  = (g1, g2, g3, g4)                     (5 to 8 elements)
+//   t     = the remaining 1-3 factors (float, float2 or float4)
+//   x     = (xmaj, major-index range, lumped pixel, lumped length / h)
+// A cell at offset (lx, ly) = h (lx', ly') from the tile centre then has
+// b = q0.x ly' - q0.y lx' + q0.z = (offset of the line from the cell centre)
+// / (h a c), and its chord in units of h is min(2/a, (a+c)/(a c) - |b|)
+// clipped at 0, with 1/a = min(|q0.x|, |q0.y|) and (a+c)/(a c) = |q0.x| +
+// |q0.y|: three floats of geometry per ray.  A ray the fast walk does not
+// take has q0.z = +inf (no chord) and no lumped pixel.
+template <int M, int ST>
+struct AdjStage {
+  static constexpr int NQ4 = 1 + (M - 1) / 4;
+  static constexpr int R = (M - 1) % 4;
+  static constexpr int TW = R == 0 ? 0 : (R == 1 ? 1 : (R == 2 ? 2 : 4));  // tail floats per slot
+  static constexpr int MT = 1 + 4 * (NQ4 - 1);                           // first factor in the tail
+  float4 q[NQ4][ST];
+  alignas(16) float t[TW > 0 ? TW * ST : 4];
+  int4 x[ST];
+  float4 v[ST / kAdjW][2];  // a, b of each staged view's AdjTileView
+};
+
 // K candidate rays k0.. of one view for one cell, unrolled; candidate i
-// counts when 0 <= j0 + i < jlim.  len = min(2h/a, (h(a+c) - |b|)/(a c))
-// clipped at 0, and with cplx the walk's major-index range and lumped piece.
-template <int M, int NQ, int K, int ST>
-__device__ __forceinline__ void adj_cells(const float4* s_q, const int4* s_x, int cplx, int k0, int j0, int jlim,
-                                          float lx, float ly, int colx, int rowx, int pix, float* acc) {
+// counts when 0 <= j0 + i < jlim.  Chords in units of h (above), and with
+// cplx the walk's major-index range and lumped piece.
+template <int M, int K, int ST>
+__device__ __forceinline__ void adj_cells(const AdjStage<M, ST>& S, int cplx, int k0, int j0, int jlim, float lxh,
+                                          float lyh, int colx, int rowx, int pix, float* acc) {
+  using St = AdjStage<M, ST>;
 #pragma unroll
   for (int i = 0; i < K; i++) {
     if ((unsigned)(j0 + i) < (unsigned)jlim) {
       const int k = k0 + i;
       if (!VCT_INDEX_OK(k >= 0 && k < ST)) continue;
-      const float4 q0 = s_q[k];
-      const float4 q1 = s_q[ST + k];
-      const float b = fmaf(q0.x, ly, fmaf(-q0.y, lx, q0.z));
-      float len = fmaxf(fminf(q1.x, (q0.w - fabsf(b)) * q1.y), 0.0f);
+      const float4 q0 = S.q[0][k];
+      const float b = fmaf(q0.x, lyh, fmaf(-q0.y, lxh, q0.z));
+      const float ax = fabsf(q0.x), ay = fabsf(q0.y);
+      const float mn = fminf(ax, ay);
+      float len = fmaxf(fminf(mn + mn, (ax + ay) - fabsf(b)), 0.0f);
       if (cplx) {
-        const int4 x = s_x[k];
+        const int4 x = S.x[k];
         const int mi = x.x ? colx : rowx;
         if (mi < (x.y & 0xffff) || mi > (x.y >> 16)) len = 0.0f;
         if (x.z == pix) len += __int_as_float(x.w);
       }
-      if (M > 0) acc[0] = fmaf(len, q1.z, acc[0]);
-      if (M > 1) acc[1 % M] = fmaf(len, q1.w, acc[1 % M]);
-      if (NQ > 2) {
-        const float4 q2 = s_q[2 * ST + k];
-        if (M > 2) acc[2 % M] = fmaf(len, q2.x, acc[2 % M]);
-        if (M > 3) acc[3 % M] = fmaf(len, q2.y, acc[3 % M]);
-        if (M > 4) acc[4 % M] = fmaf(len, q2.z, acc[4 % M]);
-        if (M > 5) acc[5 % M] = fmaf(len, q2.w, acc[5 % M]);
+#define VCT_ACC(m, val) \
+  if ((m) < M) acc[(m) % M] = fmaf(len, (val), acc[(m) % M])
+      VCT_ACC(0, q0.w);
+      if (St::NQ4 > 1) {
+        const float4 q1 = S.q[St::NQ4 - 1][k];
+        VCT_ACC(1, q1.x);
+        VCT_ACC(2, q1.y);
+        VCT_ACC(3, q1.z);
+        VCT_ACC(4, q1.w);
       }
-      if (NQ > 3) {
-        const float4 q3 = s_q[3 * ST + k];
-        if (M > 6) acc[6 % M] = fmaf(len, q3.x, acc[6 % M]);
-        if (M > 7) acc[7 % M] = fmaf(len, q3.y, acc[7 % M]);
+      if (St::TW == 1) {
+        VCT_ACC(St::MT, S.t[k]);
+      } else if (St::TW == 2) {
+        const float2 t = reinterpret_cast<const float2*>(S.t)[k];
+        VCT_ACC(St::MT, t.x);
+        VCT_ACC(St::MT + 1, t.y);
+      } else if (St::TW == 4) {
+        const float4 t = reinterpret_cast<const float4*>(S.t)[k];
+        VCT_ACC(St::MT, t.x);
+        VCT_ACC(St::MT + 1, t.y);
+        VCT_ACC(St::MT + 2, t.z);
       }
+#undef VCT_ACC
     }
   }
 }
@@ -498,12 +534,8 @@ __device__ __forceinline__ void adj_cells(const float4* s_q, const int4* s_x, in
 // at index -1 lie outside the grid, but the walk's truncating cast puts their
 // pieces on index 0 (adj_fold_kernel adds them there).  One thread per cell
 // of a TX x TY tile; blocks loop over the tiles.  Per round every warp stages
-// one view's rays of the tile's channel window (from its AdjTileView): per
-// ray q0 = (dx, dy, offset from the tile centre, h(|dx|+|dy|)),
-// q1 = (2h/max(|dx|,|dy|), 1/(|dx||dy|), g0, g1), q2 = (g2..g5),
-// q3 = (g6, g7), and x = (xmaj, major-index range, lumped pixel, length).
-// A ray the fast walk does not take gets h(|dx|+|dy|) = -inf (no chord) and
-// no lumped pixel.  The chord of a line at offset b from the centre of a
+// one view's rays of the tile's channel window (from its AdjTileView) into an
+// AdjStage slot row.  The chord of a line at offset b from the centre of a
 // square of half-size h, direction with components a >= c: 2h/a while
 // |b| <= h(a-c), then (h(a+c) - |b|)/(a c) down to 0.
 // Resident blocks per SM the registers are held to, and how far the loop over
@@ -516,6 +548,9 @@ __device__ __forceinline__ void adj_cells(const float4* s_q, const int4* s_x, in
 #ifndef VCT_ADJ_VUNROLL
 #define VCT_ADJ_VUNROLL 1
 #endif
+#ifndef VCT_ADJ_LANEMAP
+#define VCT_ADJ_LANEMAP 1
+#endif
 // One tile of the gather (all views), by a block of TX * TY threads; shared
 // staging space from the caller.
 template <int M, int TX, int TY>
@@ -523,11 +558,11 @@ __device__ __forceinline__ void adj_gather_tile(const AdjGeom& a, int tile, cons
                                                 const double* __restrict__ sin_t, const double2* __restrict__ dir,
                                                 const int4* __restrict__ rec, const float* __restrict__ gr,
                                                 const AdjTileView* __restrict__ tv, float* __restrict__ ext,
-                                                float4* s_qf, int4* s_x, float4 (*s_v)[2]) {
+                                                AdjStage<M, TX * TY / 32 * kAdjW>& S) {
   constexpr int NW = TX * TY / 32, VB = NW;  // views per round: one per warp
-  constexpr int NQ = M <= 2 ? 2 : (M <= 6 ? 3 : 4);
+  constexpr int ST = VB * kAdjW;
+  using St = AdjStage<M, ST>;
   constexpr int kVUnroll = VCT_ADJ_VUNROLL;
-  float4 (*s_q)[VB * kAdjW] = reinterpret_cast<float4 (*)[VB * kAdjW]>(s_qf);
   const int N = a.N, NE1 = N + 1;
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   // Each warp covers a patch of PX x (32/PX) cells, as square as the tile
@@ -535,13 +570,23 @@ __device__ __forceinline__ void adj_gather_tile(const AdjGeom& a, int tile, cons
   // shared-memory loads touch the fewest distinct lines.
   constexpr int PX = TX >= 8 ? 8 : TX, PY = 32 / PX, WPR = TX / PX;  // warps per tile row of patches
   static_assert(TX % PX == 0 && TY % PY == 0, "the tile must split into whole warp patches");
+#if VCT_ADJ_LANEMAP
+  // Within the 8 x 4 patch, each quarter of the warp (8 lanes, one phase of
+  // a 16-byte shared load) covers a 4 x 2 block of cells rather than a row
+  // of 8, so its candidate rays span fewer channels.
+  static_assert(PX == 8, "the quarter-warp blocks assume 8 x 4 patches");
+  const int px_ = (lane & 3) | (((lane >> 3) & 1) << 2), py_ = ((lane >> 2) & 1) | ((lane >> 4) << 1);
+  const int tx = (warp % WPR) * PX + px_, ty = (warp / WPR) * PY + py_;
+#else
   const int tx = (warp % WPR) * PX + lane % PX, ty = (warp / WPR) * PY + lane / PX;
-  const double s = a.s;
-  const float h = (float)(0.5 * s);
+#endif
+  const double s = a.s, hd = 0.5 * s;
+  const float ihf = (float)(1.0 / hd);
   // Cell-centre offsets from the tile centre, and the quadratic's terms.
   const float lx = (float)((tx + 0.5 - 0.5 * TX) * s);
   const float ly = (float)((0.5 * TY - ty - 0.5) * s);
   const float lxx = lx * lx, lxy = lx * ly, lyy = ly * ly;
+  const float lxh = (float)(2 * tx + 1 - TX), lyh = (float)(TY - 2 * ty - 1);  // (lx, ly) / h
   const int nbx = (NE1 + TX - 1) / TX;
   const int V = a.views_used;
   const int e0 = (tile % nbx) * TX, f0 = (tile / nbx) * TY;  // first extended column / row
@@ -565,9 +610,9 @@ __device__ __forceinline__ void adj_gather_tile(const AdjGeom& a, int tile, cons
       int4 vc = make_int4(0, 0, 0, 0);
       if (v < V) {
         vc = tvt[v].c;
-        if (lane < 2) s_v[vs][lane] = lane ? tvt[v].b : tvt[v].a;
+        if (lane < 2) S.v[vs][lane] = lane ? tvt[v].b : tvt[v].a;
       } else if (lane == 1) {
-        s_v[vs][1] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);  // kmax 0: nothing to gather
+        S.v[vs][1] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);  // kmax 0: nothing to gather
       }
       const int jlo = vc.y, jn = vc.z;
       const double cb = v < V ? cos_t[v] : 0.0, sb = v < V ? sin_t[v] : 0.0;
@@ -580,18 +625,22 @@ __device__ __forceinline__ void adj_gather_tile(const AdjGeom& a, int tile, cons
         const double2 e = dir[c];
         const double dx = e.x * cb + e.y * sb, dy = -e.x * sb + e.y * cb;
         const double bt = dx * (Ty - Sy) - dy * (Tx - Sx);
-        const float ax = fabsf((float)dx), ay = fabsf((float)dy);
+        const float rx = __frcp_rn(fmaxf(fabsf((float)dx), 1e-12f)), ry = __frcp_rn(fmaxf(fabsf((float)dy), 1e-12f));
         const int4 r = rec[ray];
         const bool fast = (r.x & 3) == kAdjRayFast;
         const float* gp = gr + ray * M;
         float g[8];
 #pragma unroll
         for (int m = 0; m < 8; m++) g[m] = m < M ? gp[m] : 0.0f;
-        s_q[0][k] = make_float4((float)dx, (float)dy, (float)bt, fast ? h * (ax + ay) : -INFINITY);
-        s_q[1][k] = make_float4(2.0f * h / fmaxf(ax, ay), 1.0f / (ax * ay), g[0], g[1]);
-        if (NQ > 2) s_q[2 % NQ][k] = make_float4(g[2], g[3], g[4], g[5]);
-        if (NQ > 3) s_q[3 % NQ][k] = make_float4(g[6], g[7], 0.0f, 0.0f);
-        s_x[k] = make_int4(r.x >> 2, r.y, fast ? r.z : -1, fast ? r.w : 0);
+        S.q[0][k] = make_float4(copysignf(ry, (float)dx), copysignf(rx, (float)dy),
+                                fast ? (float)bt * ihf * rx * ry : INFINITY, g[0]);
+        if (St::NQ4 > 1) S.q[St::NQ4 - 1][k] = make_float4(g[1], g[2], g[3], g[4]);
+        if (St::TW == 1) S.t[k] = g[St::MT];
+        if (St::TW == 2) reinterpret_cast<float2*>(S.t)[k] = make_float2(g[St::MT], g[(St::MT + 1) & 7]);
+        if (St::TW == 4)
+          reinterpret_cast<float4*>(S.t)[k] = make_float4(g[St::MT], g[(St::MT + 1) & 7], g[(St::MT + 2) & 7], 0.0f);
+        S.x[k] = make_int4(r.x >> 2, r.y, fast ? r.z : -1,
+                           fast ? __float_as_int(__int_as_float(r.w) * ihf) : 0);
       }
     }
     __syncthreads();
@@ -602,11 +651,11 @@ __device__ __forceinline__ void adj_gather_tile(const AdjGeom& a, int tile, cons
     for (int m = 0; m < M; m++) acc[m] = 0.0f;
 #pragma unroll kVUnroll
     for (int vb = 0; vb < VB; vb++) {
-      const float4 fb = s_v[vb][1];
+      const float4 fb = S.v[vb][1];
       const int bits = __float_as_int(fb.w);
       const int4 vi = make_int4(bits & 0xff, 0, (bits >> 8) & 0xff, bits >> 16);  // kmax, -, jn, cplx
       if (vi.x == 0) continue;
-      const float4 fa = s_v[vb][0];
+      const float4 fa = S.v[vb][0];
       const float jc = fmaf(fb.y, lyy, fmaf(fb.x, lxy, fmaf(fa.w, lxx, fmaf(fa.z, ly, fmaf(fa.y, lx, fa.x)))));
       // this cell's candidates: the integers in (jc - dj, jc + dj) that lie
       // in the window, j0 <= j < jlim; at most kmax of them
@@ -614,12 +663,12 @@ __device__ __forceinline__ void adj_gather_tile(const AdjGeom& a, int tile, cons
       const int jlim = max(min((int)ceilf(jc + fb.z), vi.z), 0);  // >= 0: the test below is unsigned
       const int k0 = vb * kAdjW + j0;
       switch (vi.x) {  // block-uniform
-        case 1: adj_cells<M, NQ, 1, VB * kAdjW>(&s_q[0][0], s_x, vi.w, k0, j0, jlim, lx, ly, colx, rowx, pix, acc); break;
-        case 2: adj_cells<M, NQ, 2, VB * kAdjW>(&s_q[0][0], s_x, vi.w, k0, j0, jlim, lx, ly, colx, rowx, pix, acc); break;
-        case 3: adj_cells<M, NQ, 3, VB * kAdjW>(&s_q[0][0], s_x, vi.w, k0, j0, jlim, lx, ly, colx, rowx, pix, acc); break;
+        case 1: adj_cells<M, 1, ST>(S, vi.w, k0, j0, jlim, lxh, lyh, colx, rowx, pix, acc); break;
+        case 2: adj_cells<M, 2, ST>(S, vi.w, k0, j0, jlim, lxh, lyh, colx, rowx, pix, acc); break;
+        case 3: adj_cells<M, 3, ST>(S, vi.w, k0, j0, jlim, lxh, lyh, colx, rowx, pix, acc); break;
         default:
           for (int i = 0; i < vi.x; i += 4)
-            adj_cells<M, NQ, 4, VB * kAdjW>(&s_q[0][0], s_x, vi.w, k0 + i, j0 + i, jlim, lx, ly, colx, rowx, pix, acc);
+            adj_cells<M, 4, ST>(S, vi.w, k0 + i, j0 + i, jlim, lxh, lyh, colx, rowx, pix, acc);
           break;
       }
     }
@@ -631,7 +680,7 @@ __device__ __forceinline__ void adj_gather_tile(const AdjGeom& a, int tile, cons
     const size_t n2 = (size_t)NE1 * NE1;
     const size_t o = (size_t)(row + 1) * NE1 + (col + 1);
 #pragma unroll
-    for (int m = 0; m < M; m++) ext[m * n2 + o] = (float)dacc[m];
+    for (int m = 0; m < M; m++) ext[m * n2 + o] = (float)(dacc[m] * hd);  // chords were in units of h
   }
 }
 
@@ -640,15 +689,11 @@ __global__ void __launch_bounds__(TX * TY, VCT_ADJ_MINBLOCKS)
 adj_gather_kernel(AdjGeom a, const double* __restrict__ cos_t, const double* __restrict__ sin_t,
                   const double2* __restrict__ dir, const int4* __restrict__ rec, const float* __restrict__ gr,
                   const AdjTileView* __restrict__ tv, float* __restrict__ ext) {
-  constexpr int VB = TX * TY / 32;
-  constexpr int NQ = M <= 2 ? 2 : (M <= 6 ? 3 : 4);
-  __shared__ float4 s_q[NQ][VB * kAdjW];
-  __shared__ int4 s_x[VB * kAdjW];
-  __shared__ float4 s_v[VB][2];  // a, b of each staged view's AdjTileView
+  __shared__ AdjStage<M, TX * TY / 32 * kAdjW> S;
   const int NE1 = a.N + 1;
   const int ntiles = ((NE1 + TX - 1) / TX) * ((NE1 + TY - 1) / TY);
   for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
-    adj_gather_tile<M, TX, TY>(a, tile, cos_t, sin_t, dir, rec, gr, tv, ext, &s_q[0][0], s_x, s_v);
+    adj_gather_tile<M, TX, TY>(a, tile, cos_t, sin_t, dir, rec, gr, tv, ext, S);
 }
 
 // grad[m][r][c] = ext at (r, c), plus the folded cells at index -1 (row -1
@@ -911,17 +956,13 @@ __global__ void adj_special_batch_kernel(const AdjJob* __restrict__ jobs, const 
 template <int M, int TX, int TY>
 __global__ void __launch_bounds__(TX * TY, VCT_ADJ_MINBLOCKS)
 adj_gather_batch_kernel(const AdjJob* __restrict__ jobs, const unsigned int* __restrict__ first, int n) {
-  constexpr int VB = TX * TY / 32;
-  constexpr int NQ = M <= 2 ? 2 : (M <= 6 ? 3 : 4);
-  __shared__ float4 s_q[NQ][VB * kAdjW];
-  __shared__ int4 s_x[VB * kAdjW];
-  __shared__ float4 s_v[VB][2];
+  __shared__ AdjStage<M, TX * TY / 32 * kAdjW> S;
   const unsigned int total = first[n];
   for (unsigned int b = blockIdx.x; b < total; b += gridDim.x) {
     const int jx = adj_job_of(first, n, b);
     const AdjJob& J = jobs[jx];
     adj_gather_tile<M, TX, TY>(J.a, (int)(b - first[jx]), J.cos_t, J.sin_t, J.dir, J.rec, J.gr,
-                               reinterpret_cast<const AdjTileView*>(J.tv), J.ext, &s_q[0][0], s_x, s_v);
+                               reinterpret_cast<const AdjTileView*>(J.tv), J.ext, S);
   }
 }
 

@@ -298,14 +298,17 @@ __global__ void adj_special_kernel(DevGeom g, const double* __restrict__ cos_t, 
                                    const int* __restrict__ special, const int* __restrict__ nspecial,
                                    const float* __restrict__ gr, const unsigned int* __restrict__ gmax,
                                    double lmax, int log2_terms, unsigned long long* __restrict__ acc) {
+  // one warp per ray (the walk's steps across the lanes)
   const int n = *nspecial;
   const double scale = special_scale(*gmax, lmax, log2_terms);
-  for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+  const int lane = threadIdx.x & 31;
+  const int nw = gridDim.x * (blockDim.x >> 5);
+  for (int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5); i < n; i += nw) {
     const int ray = special[i];
     const int v = ray / g.C, c = ray - (ray / g.C) * g.C;
     Ray r;
     if (!ray_setup(g, cos_t[v], sin_t[v], det_px0[c], det_py0[c], r)) continue;
-    walk_exact_to(g, r, ScatterSink<M>{gr + (size_t)ray * M, scale, acc, g.N});
+    walk_exact_warp(g, r, ScatterSink<M>{gr + (size_t)ray * M, scale, acc, g.N}, lane);
   }
 }
 
@@ -314,7 +317,7 @@ int launch_adj_special(const DevGeom& g, int M, const double* d_cos, const doubl
                        const float* d_g, const unsigned int* d_gmax, double lmax, int log2_terms,
                        unsigned long long* d_acc, cudaStream_t st) {
   if (nspecial_host <= 0) return VCT_OK;
-  const int blocks = (nspecial_host + 127) / 128;
+  const int blocks = (nspecial_host + 3) / 4;  // 4 warps of 32, one ray each
   switch (M) {
 #define VCT_CASE(mm)                                                                                        \
   case mm:                                                                                                  \
@@ -844,7 +847,7 @@ void adj_job_blocks(const AdjJob& j, int M, int tile, unsigned int blocks[kAdjSt
   const long long n2 = (long long)j.a.N * j.a.N;
   blocks[kAdjStReset] = j.sacc ? (unsigned int)((M * n2 + 255) / 256) : 1u;
   blocks[kAdjStLoss] = 1u;
-  blocks[kAdjStSpecial] = (unsigned int)((j.nspecial + 127) / 128);
+  blocks[kAdjStSpecial] = (unsigned int)((j.nspecial + 3) / 4);  // 128 threads, a warp per ray
   for (int t = 0; t < 4; t++) blocks[kAdjStGather + t] = t == tile ? (unsigned int)tiles_of(j.a, tile) : 0u;
   blocks[kAdjStFold] = (unsigned int)((M * n2 + 255) / 256);
 }
@@ -942,7 +945,7 @@ __global__ void adj_special_batch_kernel(const AdjJob* __restrict__ jobs, const 
                                          int n) {
   const int jx = adj_job_of(first, n, blockIdx.x);
   const AdjJob& J = jobs[jx];
-  const int i = (int)(blockIdx.x - first[jx]) * blockDim.x + threadIdx.x;
+  const int i = (int)(blockIdx.x - first[jx]) * (blockDim.x >> 5) + (threadIdx.x >> 5);  // one warp per ray
   if (i >= J.nspecial) return;
   const double scale = special_scale(*J.gmax, J.lmax, J.log2_terms);
   const DevGeom& g = J.g;
@@ -950,7 +953,7 @@ __global__ void adj_special_batch_kernel(const AdjJob* __restrict__ jobs, const 
   const int v = ray / g.C, c = ray - (ray / g.C) * g.C;
   Ray r;
   if (!ray_setup(g, J.cos_t[v], J.sin_t[v], J.px0[c], J.py0[c], r)) return;
-  walk_exact_to(g, r, ScatterSink<M>{J.gr + (size_t)ray * M, scale, J.sacc, g.N});
+  walk_exact_warp(g, r, ScatterSink<M>{J.gr + (size_t)ray * M, scale, J.sacc, g.N}, threadIdx.x & 31);
 }
 
 template <int M, int TX, int TY>

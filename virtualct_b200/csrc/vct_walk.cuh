@@ -293,6 +293,83 @@ VCT_HD void walk_exact_to(const DevGeom& g, const Ray& r, const Sink& sink) {
   }
 }
 
+#if defined(__CUDACC__)
+// walk_exact_to by a whole warp, for sinks whose result does not depend on
+// the order of the segments (the adjoint's fixed-point scatter).  Step ik of
+// the walk depends only on ik and on step ik - 1's point, so lane l takes the
+// steps ik = 32 c + l of chunk c, gets step ik - 1's point from lane l - 1
+// (or from the previous chunk), and emits the segments of its step exactly as
+// the sequential loop does, with the same expressions.  A step runs while
+// the points of all earlier steps are inside the square (a ballot per
+// chunk), which is the sequential loop's test.  The major / minor roles of
+// x and y are swapped for y-major rays; every expression keeps the
+// reference's order of operations (:113-283).
+template <class Sink>
+__device__ void walk_exact_warp(const DevGeom& g, const Ray& r, const Sink& sink, int lane) {
+  const double lim = g.lim, s = g.s;
+  const bool xmaj = fabs(r.xi - r.xf) > fabs(r.yi - r.yf);
+  const double su = xmaj ? r.sx : r.sy, sw = xmaj ? r.sy : r.sx;
+  const double pu = xmaj ? r.px : r.py, pw = xmaj ? r.py : r.px;
+  const double ui = xmaj ? r.xi : r.yi, uf = xmaj ? r.xf : r.yf;
+  const double wi = xmaj ? r.yi : r.xi, wf = xmaj ? r.yf : r.xf;
+  const double pha = (uf - ui) / fabs(ui - uf);
+  int uin;
+  if ((ui < 0 && (uf - ui) < 0) || (ui > 0 && (uf - ui) > 0))
+    uin = trunc_i32((double)trunc_i32(ui) + (uf - ui) / fabs(uf - ui));
+  else
+    uin = trunc_i32(ui);
+  const double wdir = (wf - wi) / fabs(wf - wi);
+  const int max_steps = 4 * g.N + 64;
+  auto emit_uw = [&](double u0, double w0, double u1, double w1) {
+    if (xmaj) emit(g, u0, w0, u1, w1, sink);
+    else emit(g, w0, u0, w1, u1, sink);
+  };
+  double cu = 0.0, cw = 0.0;  // step ik - 1's point for lane 0 (previous chunk's lane 31)
+  int cwm = 0;
+  for (int base = 0; base < max_steps; base += 32) {
+    const int ik = base + lane;
+    const double u = uin + pha * ik * s;
+    const double w = (u - su) / (pu - su) * (pw - sw) + sw;
+    const int wm = trunc_i32(w / s);
+    double up = __shfl_up_sync(0xffffffffu, u, 1), wp = __shfl_up_sync(0xffffffffu, w, 1);
+    int wmp = __shfl_up_sync(0xffffffffu, wm, 1);
+    if (lane == 0) {
+      up = cu;
+      wp = cw;
+      wmp = cwm;
+    }
+    // the state the loop tests before step ik: step ik - 1's point, or for
+    // ik = 0 the first point, which equals step 0's
+    const bool in = ik == 0 ? (u <= lim && u >= -lim && w <= lim && w >= -lim)
+                            : (up <= lim && up >= -lim && wp <= lim && wp >= -lim);
+    const unsigned int stop = __ballot_sync(0xffffffffu, !(in && ik < max_steps));
+    const int nrun = stop ? __ffs(stop) - 1 : 32;
+    if (lane < nrun) {
+      double ub = ik == 0 ? ui : up, wb = ik == 0 ? wi : wp;  // segment start
+      if (ik != 0 && (wm != wmp || (w / fabs(w) != wp / fabs(wp)))) {
+        double wiii;
+        if ((w < 0 && (wf - wi) < 0) || (w > 0 && (wf - wi) > 0))
+          wiii = (double)(wm * s);
+        else
+          wiii = (double)(wm * s) - wdir * s;
+        const double uiii = (wiii - sw) / (pw - sw) * (pu - su) + su;
+        const double chy = (u - uiii) * (u - uiii) + (w - wiii) * (w - wiii);
+        if (chy != 0) {
+          emit_uw(ub, wb, uiii, wiii);
+          ub = uiii;
+          wb = wiii;
+        }
+      }
+      emit_uw(ub, wb, u, w);
+    }
+    if (nrun < 32) break;
+    cu = __shfl_sync(0xffffffffu, u, 31);
+    cw = __shfl_sync(0xffffffffu, w, 31);
+    cwm = __shfl_sync(0xffffffffu, wm, 31);
+  }
+}
+#endif
+
 template <int M>
 VCT_HD void walk_exact(const DevGeom& g, const PixelRec* __restrict__ maps, const Ray& r, RayAcc& a) {
   walk_exact_to(g, r, GatherSink<M>{maps, &a});

@@ -497,9 +497,9 @@ __device__ __forceinline__ void adj_cells(const AdjStage<M, ST>& S, int cplx, in
       if (!VCT_INDEX_OK(k >= 0 && k < ST)) continue;
       const float4 q0 = S.q[0][k];
       const float b = fmaf(q0.x, lyh, fmaf(-q0.y, lxh, q0.z));
+      // min(2/a, 1/a + 1/c - |b|) = 1/a + 1/c - max(1/c - 1/a, |b|)
       const float ax = fabsf(q0.x), ay = fabsf(q0.y);
-      const float mn = fminf(ax, ay);
-      float len = fmaxf(fminf(mn + mn, (ax + ay) - fabsf(b)), 0.0f);
+      float len = fmaxf((ax + ay) - fmaxf(fabsf(ax - ay), fabsf(b)), 0.0f);
       if (cplx) {
         const int4 x = S.x[k];
         const int mi = x.x ? colx : rowx;
@@ -544,7 +544,8 @@ __device__ __forceinline__ void adj_cells(const AdjStage<M, ST>& S, int cplx, in
 // Resident blocks per SM the registers are held to, and how far the loop over
 // a round's views is unrolled (measured on the 512^2, 800 x 609 gradient:
 // 3 blocks per SM 1.27 ms and unrolling by 2 1.15 ms, against 1.14 ms for
-// the defaults).
+// the defaults; later, 5 blocks per SM (48 registers, small spills) 1.16 ms
+// against 1.02 ms).
 #ifndef VCT_ADJ_MINBLOCKS
 #define VCT_ADJ_MINBLOCKS 0
 #endif

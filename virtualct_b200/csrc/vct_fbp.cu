@@ -666,8 +666,13 @@ fbp_bp_t_scatter_kernel(const float* __restrict__ U, const float* __restrict__ U
   const int o0 = (int)((long long)np * part / BT_PARTS), o1 = (int)((long long)np * (part + 1) / BT_PARTS);
   for (int i = 0; i < 4; i++) {
     const float2 t = __ldg(cs + b + i * V4);
+    // Neighbouring lanes take neighbouring pixels across the rays (along x
+    // when the view's rays run closer to y, else along y), so their bins
+    // differ and their shared-memory adds do not collide.
+    const bool alongy = fabsf(t.y) > fabsf(t.x);
     for (int o = o0 + threadIdx.x; o < o1; o += blockDim.x) {
-      const int x = o % H, y = o / H;
+      const int f = o % H, sl = o / H;
+      const int x = alongy ? sl : f, y = alongy ? f : sl;
       if (((double)y - r) * ((double)y - r) + ((double)x - r) * ((double)x - r) > r * r) continue;
       const float xx = -((float)x - cp) * scale;
       const float yy = -((float)y - cp) * scale;
@@ -682,10 +687,20 @@ fbp_bp_t_scatter_kernel(const float* __restrict__ U, const float* __restrict__ U
       const int gi = fg > -1.0f ? (__float_as_int(big) - 0x4B000000) : -1;
       const float w = fg - (big - 8388608.0f);
       if ((unsigned)gi >= (unsigned)(C - 1)) continue;
-      // u at the orbit's pixels (x, y), (n1-y, x), (n1-x, n1-y), (y, n1-x);
-      // the second and fourth through the transposed copy.
-      const float uq[4] = {__ldg(U + (size_t)y * N + x), __ldg(UT + (size_t)(n1 - y) * N + x),
-                           __ldg(U + (size_t)(n1 - y) * N + (n1 - x)), __ldg(UT + (size_t)y * N + (n1 - x))};
+      // u at the orbit's pixels (x, y), (n1-y, x), (n1-x, n1-y), (y, n1-x),
+      // each read along a row of u or of its transposed copy ut.
+      float uq[4];
+      if (!alongy) {
+        uq[0] = __ldg(U + (size_t)y * N + x);
+        uq[1] = __ldg(UT + (size_t)(n1 - y) * N + x);
+        uq[2] = __ldg(U + (size_t)(n1 - y) * N + (n1 - x));
+        uq[3] = __ldg(UT + (size_t)y * N + (n1 - x));
+      } else {
+        uq[0] = __ldg(UT + (size_t)x * N + y);
+        uq[1] = __ldg(U + (size_t)x * N + (n1 - y));
+        uq[2] = __ldg(UT + (size_t)(n1 - x) * N + (n1 - y));
+        uq[3] = __ldg(U + (size_t)(n1 - x) * N + y);
+      }
 #pragma unroll
       for (int q = 0; q < 4; q++) {
         const float val = uq[q] * iL2;

@@ -541,13 +541,19 @@ __device__ __forceinline__ void adj_cells(const AdjStage<M, ST>& S, int cplx, in
 // AdjStage slot row.  The chord of a line at offset b from the centre of a
 // square of half-size h, direction with components a >= c: 2h/a while
 // |b| <= h(a-c), then (h(a+c) - |b|)/(a c) down to 0.
-// Resident blocks per SM the registers are held to, and how far the loop over
-// a round's views is unrolled (measured on the 512^2, 800 x 609 gradient:
-// 3 blocks per SM 1.27 ms and unrolling by 2 1.15 ms, against 1.14 ms for
-// the defaults; later, 5 blocks per SM (48 registers, small spills) 1.16 ms
-// against 1.02 ms).
+// Resident blocks per SM the registers are held to for up to 6 elements (4
+// for the 256-thread tiles, in proportion for smaller ones: 64 registers;
+// 7-8 elements are left to the compiler), and how far the loop over a round's views is unrolled
+// (measured on the 512^2, 800 x 609 gradient: 3 blocks per SM 1.27 ms and
+// unrolling by 2 1.15 ms, against 1.14 ms at 4; later, 5 blocks per SM (48
+// registers, small spills) 1.16 ms against 1.02 ms).
 #ifndef VCT_ADJ_MINBLOCKS
-#define VCT_ADJ_MINBLOCKS 0
+#define VCT_ADJ_MINBLOCKS 4
+#endif
+constexpr int adj_min_blocks(int M, int threads) { return M <= 6 ? VCT_ADJ_MINBLOCKS * 256 / threads : 0; }
+// The batch's gather (its job lookup costs registers) is left to the compiler.
+#ifndef VCT_ADJ_BATCH_MINBLOCKS
+#define VCT_ADJ_BATCH_MINBLOCKS 0
 #endif
 #ifndef VCT_ADJ_VUNROLL
 #define VCT_ADJ_VUNROLL 1
@@ -557,8 +563,10 @@ __device__ __forceinline__ void adj_cells(const AdjStage<M, ST>& S, int cplx, in
 #endif
 // One tile of the gather (all views), by a block of TX * TY threads; shared
 // staging space from the caller.
-template <int M, int TX, int TY>
-__device__ __forceinline__ void adj_gather_tile(const AdjGeom& a, int tile, const double* __restrict__ cos_t,
+// NCH: the number of view ranges the tile's views are split into (chunk is
+// this item's); partial sums go to slot `chunk` of ext.
+template <int M, int TX, int TY, int NCH>
+__device__ __forceinline__ void adj_gather_tile(const AdjGeom& a, int tile, int chunk, const double* __restrict__ cos_t,
                                                 const double* __restrict__ sin_t, const double2* __restrict__ dir,
                                                 const int4* __restrict__ rec, const float* __restrict__ gr,
                                                 const AdjTileView* __restrict__ tv, float* __restrict__ ext,
@@ -601,25 +609,28 @@ __device__ __forceinline__ void adj_gather_tile(const AdjGeom& a, int tile, cons
   const int pix = (col >= 0 && row >= 0) ? (col | (row << 16)) : -2;  // -2: never a lumped pixel
   const int colx = col + 1, rowx = row + 1;
   const AdjTileView* __restrict__ tvt = tv + (size_t)tile * V;
+  // this item's views [vb, ve)
+  const int vb = NCH == 1 ? 0 : (int)((long long)V * chunk / NCH);
+  const int ve = NCH == 1 ? V : (int)((long long)V * (chunk + 1) / NCH);
 
   double dacc[M];
 #pragma unroll
   for (int m = 0; m < M; m++) dacc[m] = 0.0;
 
-  for (int v0 = 0; v0 < V; v0 += VB) {
+  for (int v0 = vb; v0 < ve; v0 += VB) {
     // ---- staging: warp `warp` takes view v0 + warp
     {
       const int vs = warp;  // slot
       const int v = v0 + vs;
       int4 vc = make_int4(0, 0, 0, 0);
-      if (v < V) {
+      if (v < ve) {
         vc = tvt[v].c;
         if (lane < 2) S.v[vs][lane] = lane ? tvt[v].b : tvt[v].a;
       } else if (lane == 1) {
         S.v[vs][1] = make_float4(0.0f, 0.0f, 0.0f, 0.0f);  // kmax 0: nothing to gather
       }
       const int jlo = vc.y, jn = vc.z;
-      const double cb = v < V ? cos_t[v] : 0.0, sb = v < V ? sin_t[v] : 0.0;
+      const double cb = v < ve ? cos_t[v] : 0.0, sb = v < ve ? sin_t[v] : 0.0;
       const double Sx = a.sid * sb, Sy = a.sid * cb;
       for (int j = lane; j < jn; j += 32) {
         const int c = jlo + j;
@@ -682,27 +693,29 @@ __device__ __forceinline__ void adj_gather_tile(const AdjGeom& a, int tile, cons
   }
   if (col < N && row < N) {
     const size_t n2 = (size_t)NE1 * NE1;
-    const size_t o = (size_t)(row + 1) * NE1 + (col + 1);
+    const size_t o = (NCH == 1 ? 0 : (size_t)chunk * M * n2) + (size_t)(row + 1) * NE1 + (col + 1);
 #pragma unroll
     for (int m = 0; m < M; m++) ext[m * n2 + o] = (float)(dacc[m] * hd);  // chords were in units of h
   }
 }
 
 template <int M, int TX, int TY>
-__global__ void __launch_bounds__(TX * TY, VCT_ADJ_MINBLOCKS)
+__global__ void __launch_bounds__(TX * TY, adj_min_blocks(M, TX * TY))
 adj_gather_kernel(AdjGeom a, const double* __restrict__ cos_t, const double* __restrict__ sin_t,
                   const double2* __restrict__ dir, const int4* __restrict__ rec, const float* __restrict__ gr,
                   const AdjTileView* __restrict__ tv, float* __restrict__ ext) {
   __shared__ AdjStage<M, TX * TY / 32 * kAdjW> S;
   const int NE1 = a.N + 1;
   const int ntiles = ((NE1 + TX - 1) / TX) * ((NE1 + TY - 1) / TY);
-  for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x)
-    adj_gather_tile<M, TX, TY>(a, tile, cos_t, sin_t, dir, rec, gr, tv, ext, S);
+  for (int item = blockIdx.x; item < ntiles * kAdjChunks; item += gridDim.x)
+    adj_gather_tile<M, TX, TY, kAdjChunks>(a, item % ntiles, item / ntiles, cos_t, sin_t, dir, rec, gr, tv, ext, S);
 }
 
 // grad[m][r][c] = ext at (r, c), plus the folded cells at index -1 (row -1
-// onto row 0, column -1 onto column 0), plus the exact-walk rays'
-// fixed-point sums; fixed order, so the result is deterministic.
+// onto row 0, column -1 onto column 0), summed over the view chunks, plus
+// the exact-walk rays' fixed-point sums; fixed order, so the result is
+// deterministic.
+template <int NCH>
 __device__ __forceinline__ void adj_fold_elem(long long i, int M, int N, const float* __restrict__ ext,
                                               const unsigned long long* __restrict__ sacc,
                                               const unsigned int* __restrict__ gmax, double lmax, int log2_terms,
@@ -712,12 +725,16 @@ __device__ __forceinline__ void adj_fold_elem(long long i, int M, int N, const f
   const int m = (int)(i / n2);
   const int p = (int)(i - (long long)m * n2);
   const int r = p / N, c = p - (p / N) * N;
-  const float* e = ext + m * e2;
   const int N1 = N + 1;
-  double v = e[(r + 1) * N1 + (c + 1)];
-  if (c == 0) v += e[(r + 1) * N1];
-  if (r == 0) v += e[c + 1];
-  if (r == 0 && c == 0) v += e[0];
+  double v = 0.0;
+#pragma unroll
+  for (int k = 0; k < NCH; k++) {
+    const float* e = ext + ((size_t)k * M + m) * e2;
+    v += e[(r + 1) * N1 + (c + 1)];
+    if (c == 0) v += e[(r + 1) * N1];
+    if (r == 0) v += e[c + 1];
+    if (r == 0 && c == 0) v += e[0];
+  }
   if (sacc) v += (double)(long long)sacc[i] / special_scale(*gmax, lmax, log2_terms);
   grad[i] = (float)v;
 }
@@ -725,7 +742,8 @@ __device__ __forceinline__ void adj_fold_elem(long long i, int M, int N, const f
 __global__ void adj_fold_kernel(int M, int N, const float* __restrict__ ext, const unsigned long long* __restrict__ sacc,
                                 const unsigned int* __restrict__ gmax, double lmax, int log2_terms,
                                 float* __restrict__ grad) {
-  adj_fold_elem((long long)blockIdx.x * blockDim.x + threadIdx.x, M, N, ext, sacc, gmax, lmax, log2_terms, grad);
+  adj_fold_elem<kAdjChunks>((long long)blockIdx.x * blockDim.x + threadIdx.x, M, N, ext, sacc, gmax, lmax, log2_terms,
+                            grad);
 }
 
 // Tile shapes, largest first; the channel window of a tile grows with its
@@ -849,7 +867,8 @@ void adj_job_blocks(const AdjJob& j, int M, int tile, unsigned int blocks[kAdjSt
   blocks[kAdjStReset] = j.sacc ? (unsigned int)((M * n2 + 255) / 256) : 1u;
   blocks[kAdjStLoss] = 1u;
   blocks[kAdjStSpecial] = (unsigned int)((j.nspecial + 3) / 4);  // 128 threads, a warp per ray
-  for (int t = 0; t < 4; t++) blocks[kAdjStGather + t] = t == tile ? (unsigned int)tiles_of(j.a, tile) : 0u;
+  for (int t = 0; t < 4; t++)
+    blocks[kAdjStGather + t] = t == tile ? (unsigned int)(tiles_of(j.a, tile) * kAdjChunks) : 0u;
   blocks[kAdjStFold] = (unsigned int)((M * n2 + 255) / 256);
 }
 
@@ -958,15 +977,19 @@ __global__ void adj_special_batch_kernel(const AdjJob* __restrict__ jobs, const 
 }
 
 template <int M, int TX, int TY>
-__global__ void __launch_bounds__(TX * TY, VCT_ADJ_MINBLOCKS)
+__global__ void __launch_bounds__(TX * TY, VCT_ADJ_BATCH_MINBLOCKS)
 adj_gather_batch_kernel(const AdjJob* __restrict__ jobs, const unsigned int* __restrict__ first, int n) {
   __shared__ AdjStage<M, TX * TY / 32 * kAdjW> S;
   const unsigned int total = first[n];
   for (unsigned int b = blockIdx.x; b < total; b += gridDim.x) {
+    // the same view ranges as the single-slice gather, so the sums (and the
+    // gradient) are bit-identical to it
     const int jx = adj_job_of(first, n, b);
     const AdjJob& J = jobs[jx];
-    adj_gather_tile<M, TX, TY>(J.a, (int)(b - first[jx]), J.cos_t, J.sin_t, J.dir, J.rec, J.gr,
-                               reinterpret_cast<const AdjTileView*>(J.tv), J.ext, S);
+    const int ntiles = ((J.a.N + TX) / TX) * ((J.a.N + TY) / TY);  // tiles of the (N+1)^2 cells
+    const int item = (int)(b - first[jx]);
+    adj_gather_tile<M, TX, TY, kAdjChunks>(J.a, item % ntiles, item / ntiles, J.cos_t, J.sin_t, J.dir, J.rec, J.gr,
+                                           reinterpret_cast<const AdjTileView*>(J.tv), J.ext, S);
   }
 }
 
@@ -975,7 +998,7 @@ __global__ void adj_fold_batch_kernel(const AdjJob* __restrict__ jobs, const uns
   const int jx = adj_job_of(first, n, blockIdx.x);
   const AdjJob& J = jobs[jx];
   const long long i = (long long)(blockIdx.x - first[jx]) * blockDim.x + threadIdx.x;
-  adj_fold_elem(i, M, J.a.N, J.ext, J.sacc, J.gmax, J.lmax, J.log2_terms, J.grad);
+  adj_fold_elem<kAdjChunks>(i, M, J.a.N, J.ext, J.sacc, J.gmax, J.lmax, J.log2_terms, J.grad);
 }
 
 template <int M, int TX, int TY>

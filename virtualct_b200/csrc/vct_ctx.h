@@ -118,7 +118,7 @@ struct vct_ctx {
   vct::DBuf<unsigned int> adj_gmax;
   vct::DBuf<unsigned long long> adj_sacc;
   vct::DBuf<float> adj_meas, adj_wts, adj_grad;
-  vct::DBuf<float> adj_ext;  // [M][N+1][N+1] gather output before the fold
+  vct::DBuf<float> adj_ext;  // [kAdjChunks][M][N+1][N+1] gather partial sums before the fold
   vct::Pipe* pipe = nullptr;  // vct_mbfpa_many
   vct::StageTimer timer;      // vct_set_stage_timing
 };

@@ -1154,7 +1154,7 @@ static int adj_run(vct_ctx* c, int mode, const float* d_meas, const float* d_wts
     c->launches++;
     sacc = c->adj_sacc.p;
   }
-  if ((rc = c->adj_ext.ensure((size_t)M * (dg.N + 1) * (dg.N + 1)))) return rc;
+  if ((rc = c->adj_ext.ensure((size_t)kAdjChunks * M * (dg.N + 1) * (dg.N + 1)))) return rc;
   if ((rc = launch_adj_gather(c->ag, M, c->adj_tile, c->cos_t.p, c->sin_t.p, c->adj_dir.p, c->adj_rec.p, d_g,
                               c->adj_tv.p, c->adj_ext.p, c->stream)))
     return rc;

@@ -245,6 +245,14 @@ constexpr int kAdjRayNone = 0;   // no segment
 constexpr int kAdjRayFast = 1;   // fast walk: lumped segment + chords in a major-index range
 constexpr int kAdjRayExact = 2;  // exact walk (scattered in fixed point)
 
+// The gather splits each tile's views into kAdjChunks consecutive ranges,
+// each a separate work item with its own partial sums (summed in order by
+// the fold), so the items spread evenly over the resident blocks.
+#ifndef VCT_ADJ_CHUNKS
+#define VCT_ADJ_CHUNKS 2
+#endif
+constexpr int kAdjChunks = VCT_ADJ_CHUNKS;
+
 struct AdjGeom {
   int N, nxm, C, start, views_used;
   int log2_terms;     // bound on log2(terms per pixel) of the exact-walk scatter
@@ -316,7 +324,7 @@ struct AdjJob {
   unsigned long long* sacc;  // exact-walk sums [M][N][N], NULL without exact-walk rays
   double lmax;
   int log2_terms;
-  float* ext;        // [M][N+1][N+1]
+  float* ext;        // [kAdjChunks][M][N+1][N+1]
   float* grad;       // [M][N][N]
   unsigned int tile0;
 };

@@ -55,8 +55,10 @@ __global__ void adj_plan_kernel(DevGeom g, const double* __restrict__ cos_t, con
     else
       fast_plan(g, r, p);
     if (p.status == kPlanExact) {
+      const int idx = atomicAdd(nspecial, 1);
       o.x = kAdjRayExact;
-      special[atomicAdd(nspecial, 1)] = (int)ray;
+      o.y = idx;  // its place in the list (and in the line-integral buffer)
+      special[idx] = (int)ray;
     } else if (p.status == kPlanWalk) {
       const int lo = min(p.maj0, p.majK), hi = max(p.maj0, p.majK);
       o.x = kAdjRayFast | (p.xmaj << 2);
@@ -116,25 +118,30 @@ __device__ __forceinline__ double adj_forward_ray(const DevGeom& g, const PixelR
                                                   const double* __restrict__ sin_t,
                                                   const double* __restrict__ det_px0,
                                                   const double* __restrict__ det_py0, const int4* __restrict__ rec,
-                                                  const float* __restrict__ meas, const float* __restrict__ wts,
+                                                  const double* __restrict__ lsp, const float* __restrict__ meas,
+                                                  const float* __restrict__ wts,
                                                   float* __restrict__ gout, unsigned int* __restrict__ gmax_special,
                                                   long long ray) {
   double loss = 0.0;
   const int v = (int)(ray / g.C);
   const int c = (int)(ray - (long long)v * g.C);
-  const int kind = rec[ray].x & 3;
-  RayAcc a;
-  acc_init(a);
-  if (kind != kAdjRayNone) {
-    Ray r;
-    ray_setup(g, cos_t[v], sin_t[v], det_px0[c], det_py0[c], r);
-    if (kind == kAdjRayFast)
-      walk_fast<M>(g, maps, r, a);
-    else
-      walk_exact<M>(g, maps, r, a);
-  }
+  const int4 rc = rec[ray];
+  const int kind = rc.x & 3;
   double L[8];
-  finish_lines<M>(a, L, g.dens_div);
+  if (kind == kAdjRayExact) {
+    // walked beforehand by a whole warp (adj_lines_kernel)
+#pragma unroll
+    for (int m = 0; m < M; m++) L[m] = lsp[(size_t)rc.y * M + m];
+  } else {
+    RayAcc a;
+    acc_init(a);
+    if (kind == kAdjRayFast) {
+      Ray r;
+      ray_setup(g, cos_t[v], sin_t[v], det_px0[c], det_py0[c], r);
+      walk_fast<M>(g, maps, r, a);
+    }
+    finish_lines<M>(a, L, g.dens_div);
+  }
   double y = 0.0, D[M];
 #pragma unroll
   for (int m = 0; m < M; m++) D[m] = 0.0;
@@ -182,7 +189,7 @@ __global__ void __launch_bounds__(kAdjFwdThreads)
 adj_forward_kernel(DevGeom g, const PixelRec* __restrict__ maps, const double* __restrict__ mu_l2,
                    const float* __restrict__ pdf, int NE, double ynorm, const double* __restrict__ cos_t,
                    const double* __restrict__ sin_t, const double* __restrict__ det_px0,
-                   const double* __restrict__ det_py0, const int4* __restrict__ rec,
+                   const double* __restrict__ det_py0, const int4* __restrict__ rec, const double* __restrict__ lsp,
                    const float* __restrict__ meas, const float* __restrict__ wts, float* __restrict__ gout,
                    double* __restrict__ loss_part, unsigned int* __restrict__ gmax_special) {
   extern __shared__ double smem[];
@@ -197,8 +204,8 @@ adj_forward_kernel(DevGeom g, const PixelRec* __restrict__ maps, const double* _
   const long long ray = (long long)blockIdx.x * blockDim.x + threadIdx.x;
   double loss = 0.0;
   if (ray < nrays)
-    loss = adj_forward_ray<M, MODE>(g, maps, s_mu, s_pdf, NE, ynorm, cos_t, sin_t, det_px0, det_py0, rec, meas, wts,
-                                    gout, gmax_special, ray);
+    loss = adj_forward_ray<M, MODE>(g, maps, s_mu, s_pdf, NE, ynorm, cos_t, sin_t, det_px0, det_py0, rec, lsp, meas,
+                                    wts, gout, gmax_special, ray);
   if (MODE == 0) {
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) loss += __shfl_xor_sync(0xffffffffu, loss, o);
@@ -215,9 +222,9 @@ adj_forward_kernel(DevGeom g, const PixelRec* __restrict__ maps, const double* _
 template <int M>
 static int launch_adj_forward_m(const DevGeom& g, const PixelRec* d_maps, const double* d_mu_l2, const float* d_pdf,
                                 int NE, double ynorm, const double* d_cos, const double* d_sin, const double* d_px0,
-                                const double* d_py0, const int4* d_rec, int mode, const float* d_meas,
-                                const float* d_wts, float* d_g, double* d_loss_part, unsigned int* d_gmax,
-                                cudaStream_t st) {
+                                const double* d_py0, const int4* d_rec, const double* d_lsp, int mode,
+                                const float* d_meas, const float* d_wts, float* d_g, double* d_loss_part,
+                                unsigned int* d_gmax, cudaStream_t st) {
   const long long nrays = (long long)g.views_used * g.C;
   const int blocks = (int)((nrays + kAdjFwdThreads - 1) / kAdjFwdThreads);
   const size_t smem = (size_t)NE * M * sizeof(double) + (size_t)NE * sizeof(float);
@@ -225,7 +232,7 @@ static int launch_adj_forward_m(const DevGeom& g, const PixelRec* d_maps, const 
   auto k = mode == 0 ? adj_forward_kernel<M, 0> : adj_forward_kernel<M, 1>;
   VCT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   k<<<blocks, kAdjFwdThreads, smem, st>>>(g, d_maps, d_mu_l2, d_pdf, NE, ynorm, d_cos, d_sin, d_px0, d_py0, d_rec,
-                                          d_meas, d_wts, d_g, d_loss_part, d_gmax);
+                                          d_lsp, d_meas, d_wts, d_g, d_loss_part, d_gmax);
   VCT_CUDA(cudaGetLastError());
   return VCT_OK;
 }
@@ -237,17 +244,74 @@ int adj_forward_blocks(const DevGeom& g) {
 
 int launch_adj_forward(const DevGeom& g, const PixelRec* d_maps, int M, const double* d_mu_l2, const float* d_pdf,
                        int NE, double ynorm, const double* d_cos, const double* d_sin, const double* d_px0,
-                       const double* d_py0, const int4* d_rec, int mode, const float* d_meas, const float* d_wts,
-                       float* d_g, double* d_loss_part, unsigned int* d_gmax, cudaStream_t st) {
+                       const double* d_py0, const int4* d_rec, const double* d_lsp, int mode, const float* d_meas,
+                       const float* d_wts, float* d_g, double* d_loss_part, unsigned int* d_gmax, cudaStream_t st) {
   switch (M) {
-#define VCT_CASE(mm)                                                                                             \
-  case mm:                                                                                                       \
-    return launch_adj_forward_m<mm>(g, d_maps, d_mu_l2, d_pdf, NE, ynorm, d_cos, d_sin, d_px0, d_py0, d_rec, mode, \
-                                    d_meas, d_wts, d_g, d_loss_part, d_gmax, st);
+#define VCT_CASE(mm)                                                                                              \
+  case mm:                                                                                                        \
+    return launch_adj_forward_m<mm>(g, d_maps, d_mu_l2, d_pdf, NE, ynorm, d_cos, d_sin, d_px0, d_py0, d_rec, d_lsp, \
+                                    mode, d_meas, d_wts, d_g, d_loss_part, d_gmax, st);
     VCT_CASE(1) VCT_CASE(2) VCT_CASE(3) VCT_CASE(4) VCT_CASE(5) VCT_CASE(6) VCT_CASE(7) VCT_CASE(8)
 #undef VCT_CASE
     default: return fail(VCT_E_ARG, "adjoint: 1..8 materials");
   }
+}
+
+// ------------------------------------------- exact-walk rays: line integrals
+// One warp per listed ray: walk_exact_warp with the gather sink, each lane's
+// segment sums then added over the warp in a fixed order.  Same segments as
+// walk_exact in one thread, the FP64 sum in another order; deterministic.
+template <int M>
+__device__ __forceinline__ void adj_lines_ray(const DevGeom& g, const PixelRec* __restrict__ maps,
+                                              const double* __restrict__ cos_t, const double* __restrict__ sin_t,
+                                              const double* __restrict__ det_px0, const double* __restrict__ det_py0,
+                                              int ray, double* __restrict__ out, int lane) {
+  const int v = ray / g.C, c = ray - (ray / g.C) * g.C;
+  RayAcc t;
+  acc_init(t);
+  Ray r;
+  if (ray_setup(g, cos_t[v], sin_t[v], det_px0[c], det_py0[c], r))  // the same for every lane
+    walk_exact_warp(g, r, GatherSink<M>{maps, &t}, lane);
+#pragma unroll
+  for (int m = 0; m < M; m++) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t.Ld[m] += __shfl_xor_sync(0xffffffffu, t.Ld[m], o);
+  }
+  double L[8];
+  finish_lines<M>(t, L, g.dens_div);
+  if (lane == 0) {
+#pragma unroll
+    for (int m = 0; m < M; m++) out[m] = L[m];
+  }
+}
+
+template <int M>
+__global__ void adj_lines_kernel(DevGeom g, const PixelRec* __restrict__ maps, const double* __restrict__ cos_t,
+                                 const double* __restrict__ sin_t, const double* __restrict__ det_px0,
+                                 const double* __restrict__ det_py0, const int* __restrict__ special, int n,
+                                 double* __restrict__ lsp) {
+  const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (i >= n) return;  // warp-uniform
+  adj_lines_ray<M>(g, maps, cos_t, sin_t, det_px0, det_py0, special[i], lsp + (size_t)i * M, threadIdx.x & 31);
+}
+
+int launch_adj_lines(const DevGeom& g, int M, const PixelRec* d_maps, const double* d_cos, const double* d_sin,
+                     const double* d_px0, const double* d_py0, const int* d_special, int nspecial_host, double* d_lsp,
+                     cudaStream_t st) {
+  if (nspecial_host <= 0) return VCT_OK;
+  const int blocks = (nspecial_host + 3) / 4;  // 4 warps of 32, one ray each
+  switch (M) {
+#define VCT_CASE(mm)                                                                                         \
+  case mm:                                                                                                   \
+    adj_lines_kernel<mm><<<blocks, 128, 0, st>>>(g, d_maps, d_cos, d_sin, d_px0, d_py0, d_special, nspecial_host, \
+                                                 d_lsp);                                                     \
+    break;
+    VCT_CASE(1) VCT_CASE(2) VCT_CASE(3) VCT_CASE(4) VCT_CASE(5) VCT_CASE(6) VCT_CASE(7) VCT_CASE(8)
+#undef VCT_CASE
+    default: return fail(VCT_E_ARG, "adjoint: 1..8 materials");
+  }
+  VCT_CUDA(cudaGetLastError());
+  return VCT_OK;
 }
 
 // Fixed-order sum of the per-block loss partials.
@@ -865,6 +929,7 @@ __host__ __device__ unsigned int adj_job_ray_tiles(const DevGeom& g) {
 void adj_job_blocks(const AdjJob& j, int M, int tile, unsigned int blocks[kAdjStages]) {
   const long long n2 = (long long)j.a.N * j.a.N;
   blocks[kAdjStReset] = j.sacc ? (unsigned int)((M * n2 + 255) / 256) : 1u;
+  blocks[kAdjStLines] = (unsigned int)((j.nspecial + 3) / 4);  // 128 threads, a warp per ray
   blocks[kAdjStLoss] = 1u;
   blocks[kAdjStSpecial] = (unsigned int)((j.nspecial + 3) / 4);  // 128 threads, a warp per ray
   for (int t = 0; t < 4; t++)
@@ -935,7 +1000,7 @@ adj_forward_batch_kernel(const AdjJob* __restrict__ jobs, int njobs, unsigned in
       double loss = 0.0;
       if (ray < nrays)
         loss = adj_forward_ray<M, 0>(J.g, J.maps, s_mu, s_pdf, J.NE, J.ynorm, J.cos_t, J.sin_t, J.px0, J.py0, J.rec,
-                                     J.meas, J.wts, J.gr, J.gmax, ray);
+                                     J.lsp, J.meas, J.wts, J.gr, J.gmax, ray);
 #pragma unroll
       for (int o = 16; o > 0; o >>= 1) loss += __shfl_xor_sync(0xffffffffu, loss, o);
       part += loss;
@@ -958,6 +1023,17 @@ __global__ void adj_loss_batch_kernel(const AdjJob* __restrict__ jobs) {
     __syncthreads();
   }
   if (threadIdx.x == 0) *J.loss = s[0];
+}
+
+template <int M>
+__global__ void adj_lines_batch_kernel(const AdjJob* __restrict__ jobs, const unsigned int* __restrict__ first,
+                                       int n) {
+  const int jx = adj_job_of(first, n, blockIdx.x);
+  const AdjJob& J = jobs[jx];
+  const int i = (int)(blockIdx.x - first[jx]) * (blockDim.x >> 5) + (threadIdx.x >> 5);  // one warp per ray
+  if (i >= J.nspecial) return;
+  adj_lines_ray<M>(J.g, J.maps, J.cos_t, J.sin_t, J.px0, J.py0, J.special[i], J.lsp + (size_t)i * M,
+                   threadIdx.x & 31);
 }
 
 template <int M>
@@ -1022,6 +1098,10 @@ static int launch_adj_batch_m(const AdjJob* d_jobs, const unsigned int* d_first,
   adj_reset_batch_kernel<<<nb[kAdjStReset], 256, 0, st>>>(d_jobs, f + kAdjStReset * (n + 1), n, M);
   VCT_CUDA(cudaGetLastError());
   VCT_CUDA(cudaMemsetAsync(d_counter, 0, sizeof(unsigned int), st));
+  if (nb[kAdjStLines]) {
+    adj_lines_batch_kernel<M><<<nb[kAdjStLines], 128, 0, st>>>(d_jobs, f + kAdjStLines * (n + 1), n);
+    VCT_CUDA(cudaGetLastError());
+  }
   {
     const size_t smem = kAdjBatchWarps * ((size_t)ne_max * M + (size_t)(ne_max + 1) / 2) * sizeof(double);
     int dev = 0, sms = 0, per_sm = 0;

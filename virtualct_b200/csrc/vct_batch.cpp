@@ -196,6 +196,7 @@ int upload_adjoint_tables(vct_batch* b) {
     J.gmax = c->adj_gmax.p;
     J.special = c->adj_special.p;
     J.nspecial = c->adj_nspecial;
+    J.lsp = c->adj_lsp.p;
     J.sacc = c->adj_nspecial > 0 ? c->adj_sacc.p : nullptr;
     J.lmax = c->ag.lmax;
     J.log2_terms = c->ag.log2_terms;

@@ -117,6 +117,7 @@ struct vct_ctx {
   vct::DBuf<double> adj_part, adj_loss;
   vct::DBuf<unsigned int> adj_gmax;
   vct::DBuf<unsigned long long> adj_sacc;
+  vct::DBuf<double> adj_lsp;  // exact-walk rays' line integrals [nspecial][M]
   vct::DBuf<float> adj_meas, adj_wts, adj_grad;
   vct::DBuf<float> adj_ext;  // [kAdjChunks][M][N+1][N+1] gather partial sums before the fold
   vct::Pipe* pipe = nullptr;  // vct_mbfpa_many

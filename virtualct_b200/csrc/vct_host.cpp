@@ -229,7 +229,7 @@ void vct_destroy(vct_ctx* c) {
   c->adj_rec.release(); c->adj_special.release(); c->adj_ints.release(); c->adj_dir.release();
   c->adj_tv.release();
   c->adj_g.release(); c->adj_part.release(); c->adj_loss.release(); c->adj_gmax.release();
-  c->adj_sacc.release(); c->adj_meas.release(); c->adj_wts.release(); c->adj_grad.release();
+  c->adj_sacc.release(); c->adj_lsp.release(); c->adj_meas.release(); c->adj_wts.release(); c->adj_grad.release();
   c->adj_ext.release();
   c->sq_part.release();
   c->ir_proj.release(); c->ir_reproj.release(); c->ir_img.release(); c->ir_out.release();
@@ -1121,9 +1121,17 @@ static int adj_run(vct_ctx* c, int mode, const float* d_meas, const float* d_wts
   if (!d_g) {
     if (!c->maps_ready || !c->spectrum_ready) return fail(VCT_E_STATE, "adjoint: maps or spectrum not set");
     if ((rc = c->adj_g.ensure((size_t)nrays * M))) return rc;
+    if (c->adj_nspecial > 0) {
+      if ((rc = c->adj_lsp.ensure((size_t)c->adj_nspecial * M))) return rc;
+      if ((rc = launch_adj_lines(dg, M, c->maps.p, c->cos_t.p, c->sin_t.p, c->det_px0.p, c->det_py0.p,
+                                 c->adj_special.p, c->adj_nspecial, c->adj_lsp.p, c->stream)))
+        return rc;
+      c->timer.mark("adj_lines_kernel", c->stream);
+      c->launches++;
+    }
     if ((rc = launch_adj_forward(dg, c->maps.p, M, c->mu_log2.p, c->pdf.p, c->NE, c->ynorm, c->cos_t.p, c->sin_t.p,
-                                 c->det_px0.p, c->det_py0.p, c->adj_rec.p, mode, d_meas, d_wts, c->adj_g.p,
-                                 c->adj_part.p, c->adj_gmax.p, c->stream)))
+                                 c->det_px0.p, c->det_py0.p, c->adj_rec.p, c->adj_lsp.p, mode, d_meas, d_wts,
+                                 c->adj_g.p, c->adj_part.p, c->adj_gmax.p, c->stream)))
       return rc;
     c->timer.mark("adj_forward_kernel", c->stream);
     c->launches++;

@@ -265,8 +265,13 @@ int launch_adj_plan(const DevGeom& g, const double* d_cos, const double* d_sin, 
 int adj_forward_blocks(const DevGeom& g);
 int launch_adj_forward(const DevGeom& g, const PixelRec* d_maps, int M, const double* d_mu_l2, const float* d_pdf,
                        int NE, double ynorm, const double* d_cos, const double* d_sin, const double* d_px0,
-                       const double* d_py0, const int4* d_rec, int mode, const float* d_meas, const float* d_wts,
-                       float* d_g, double* d_loss_part, unsigned int* d_gmax, cudaStream_t st);
+                       const double* d_py0, const int4* d_rec, const double* d_lsp, int mode, const float* d_meas,
+                       const float* d_wts, float* d_g, double* d_loss_part, unsigned int* d_gmax, cudaStream_t st);
+// Line integrals [nspecial][M] of the rays the fast walk hands back (the
+// exact walk, one warp per ray); adj_forward reads them for those rays.
+int launch_adj_lines(const DevGeom& g, int M, const PixelRec* d_maps, const double* d_cos, const double* d_sin,
+                     const double* d_px0, const double* d_py0, const int* d_special, int nspecial_host, double* d_lsp,
+                     cudaStream_t st);
 int launch_adj_loss(const double* d_part, int n, double* d_out, cudaStream_t st);
 int launch_adj_special(const DevGeom& g, int M, const double* d_cos, const double* d_sin, const double* d_px0,
                        const double* d_py0, const int* d_special, const int* d_nspecial, int nspecial_host,
@@ -321,6 +326,7 @@ struct AdjJob {
   unsigned int* gmax;
   const int* special;
   int nspecial;
+  double* lsp;       // exact-walk rays' line integrals [nspecial][M]
   unsigned long long* sacc;  // exact-walk sums [M][N][N], NULL without exact-walk rays
   double lmax;
   int log2_terms;
@@ -330,7 +336,7 @@ struct AdjJob {
 };
 // Stages; the gather has one stage per tile shape (a job's own shape,
 // adj_pick_tile), kAdjStGather + shape.
-enum { kAdjStReset = 0, kAdjStLoss, kAdjStSpecial, kAdjStGather, kAdjStFold = kAdjStGather + 4, kAdjStages };
+enum { kAdjStReset = 0, kAdjStLines, kAdjStLoss, kAdjStSpecial, kAdjStGather, kAdjStFold = kAdjStGather + 4, kAdjStages };
 // Block counts of one job per stage for its gather tile shape and M elements.
 void adj_job_blocks(const AdjJob& j, int M, int tile, unsigned int blocks[kAdjStages]);
 // 128-ray tiles of one job's persistent forward.

@@ -258,27 +258,15 @@ int launch_adj_forward(const DevGeom& g, const PixelRec* d_maps, int M, const do
 }
 
 // ------------------------------------------- exact-walk rays: line integrals
-// One warp per listed ray: walk_exact_warp with the gather sink, each lane's
-// segment sums then added over the warp in a fixed order.  Same segments as
-// walk_exact in one thread, the FP64 sum in another order; deterministic.
+// One warp per listed ray (exact_lines_warp).
 template <int M>
 __device__ __forceinline__ void adj_lines_ray(const DevGeom& g, const PixelRec* __restrict__ maps,
                                               const double* __restrict__ cos_t, const double* __restrict__ sin_t,
                                               const double* __restrict__ det_px0, const double* __restrict__ det_py0,
                                               int ray, double* __restrict__ out, int lane) {
-  const int v = ray / g.C, c = ray - (ray / g.C) * g.C;
-  RayAcc t;
-  acc_init(t);
-  Ray r;
-  if (ray_setup(g, cos_t[v], sin_t[v], det_px0[c], det_py0[c], r))  // the same for every lane
-    walk_exact_warp(g, r, GatherSink<M>{maps, &t}, lane);
-#pragma unroll
-  for (int m = 0; m < M; m++) {
-#pragma unroll
-    for (int o = 16; o > 0; o >>= 1) t.Ld[m] += __shfl_xor_sync(0xffffffffu, t.Ld[m], o);
-  }
   double L[8];
-  finish_lines<M>(t, L, g.dens_div);
+  int nseg;
+  exact_lines_warp<M>(g, maps, cos_t, sin_t, det_px0, det_py0, ray, L, &nseg, lane);
   if (lane == 0) {
 #pragma unroll
     for (int m = 0; m < M; m++) out[m] = L[m];

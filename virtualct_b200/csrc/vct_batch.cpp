@@ -44,6 +44,8 @@ struct vct_batch {
   // persistent forward
   DBuf<FwdJob> d_jobs;
   DBuf<unsigned int> d_counter;
+  DBuf<unsigned int> d_xfirst;  // prefix sums of the jobs' exact-walk ray counts
+  unsigned int nexact_total = 0;
   // the batched stages around it: map packing, normalisation + noise, FBP
   DBuf<PackJob> d_pack;
   DBuf<PostJob> d_post;
@@ -72,6 +74,7 @@ int sm_count(int device) {
 // The job table for a tile size: tile0 of every job, total tiles.
 int upload_jobs(vct_batch* b, int tile_rays) {
   std::vector<FwdJob> h(b->n);
+  std::vector<unsigned int> xfirst((size_t)b->n + 1, 0u);
   unsigned long long tiles = 0;
   for (int i = 0; i < b->n; i++) {
     const vct_ctx* c = b->ctx[i];
@@ -88,6 +91,9 @@ int upload_jobs(vct_batch* b, int tile_rays) {
     J.stats = c->stats.p;
     J.NE = c->NE;
     J.fast = !c->dg.rmax_active;
+    J.exact = J.fast && c->fwd_nexact > 0 ? c->fwd_exact.p + 1 : nullptr;
+    J.nexact = J.exact ? c->fwd_nexact : 0;
+    xfirst[i + 1] = xfirst[i] + (unsigned int)J.nexact;
     J.tile0 = (unsigned int)tiles;
     const long long nrays = (long long)c->dg.views_used * c->dg.C;
     tiles += (unsigned long long)((nrays + tile_rays - 1) / tile_rays);
@@ -95,12 +101,16 @@ int upload_jobs(vct_batch* b, int tile_rays) {
   if (tiles >= 0xffffffffull) return fail(VCT_E_ARG, "batch: too many ray tiles");
   b->ntiles = (unsigned int)tiles;
   VCT_CUDA(cudaMemcpy(b->d_jobs.p, h.data(), h.size() * sizeof(FwdJob), cudaMemcpyHostToDevice));
+  int rc;
+  if ((rc = b->d_xfirst.ensure(xfirst.size()))) return rc;
+  VCT_CUDA(cudaMemcpy(b->d_xfirst.p, xfirst.data(), xfirst.size() * sizeof(unsigned int), cudaMemcpyHostToDevice));
+  b->nexact_total = xfirst[b->n];
   return VCT_OK;
 }
 
 int enqueue_forward(vct_batch* b, cudaStream_t st) {
   return launch_forward_batch(b->d_jobs.p, b->n, b->M, b->tile_rays, b->ntiles, b->ne_max, b->grid,
-                              b->d_counter.p, st);
+                              b->d_counter.p, b->d_xfirst.p, b->nexact_total, st);
 }
 
 // The job tables of the batched stages (after every context exists and its
@@ -326,6 +336,7 @@ void release(vct_batch* b) {
   for (auto c : b->ctx) vct_destroy(c);
   b->d_jobs.release();
   b->d_counter.release();
+  b->d_xfirst.release();
   b->d_pack.release();
   b->d_post.release();
   b->d_first.release();

@@ -111,6 +111,10 @@ struct vct_ctx {
   vct::AdjGeom ag{};
   vct::DBuf<int4> adj_rec;
   vct::DBuf<int> adj_special, adj_ints;  // ints: [0] special count, [1] status
+  // The rays the fast walk hands back (geometry only, listed by vct_create):
+  // [0] their count, then the rays; the forward walks them a warp per ray.
+  vct::DBuf<int> fwd_exact;
+  int fwd_nexact = 0;
   vct::DBuf<double2> adj_dir;
   vct::DBuf<float4> adj_tv;  // per (tile, view) records of the gather
   vct::DBuf<float> adj_g;

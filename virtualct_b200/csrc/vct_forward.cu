@@ -151,6 +151,25 @@ __device__ __forceinline__ float spectral_compensated(const double L[8], const d
   return (float)accd;
 }
 
+// The polyenergetic value of a ray from its line integrals: the reference's
+// float sum in bin order (MB/reprojection_TOMO.cpp:196-197, MB/main.cpp:504)
+// or the compensated FP64 sum.
+template <int M, int SUM_MODE>
+__device__ __forceinline__ float ray_value(const double L[8], const double* __restrict__ mu,
+                                           const float* __restrict__ pdf, int NE) {
+  if (SUM_MODE == VCT_SUM_REFERENCE) {
+    float accf = 0.0f;
+    for (int e = 0; e < NE; e++) {
+      double t = 0.0;
+#pragma unroll
+      for (int m = 0; m < M; m++) t = __fma_rn(mu[e * M + m], L[m], t);
+      accf = __fadd_rn(accf, (float)((double)pdf[e] * exp(-t)));
+    }
+    return accf;
+  }
+  return spectral_compensated<M>(L, mu, pdf, NE);
+}
+
 // One thread per ray (view v, channel c), rays numbered view-major so a warp
 // holds 32 neighbouring channels of one view (similar paths and lengths).
 // mu: [NE][M] in shared memory -- mu/xfactor for the reference summation,
@@ -161,7 +180,7 @@ __global__ void __launch_bounds__(kFwdThreads, VCT_FWD_MINBLOCKS)
 forward_kernel(DevGeom g, const PixelRec* __restrict__ maps, const double* __restrict__ mu_tab,
                const float* __restrict__ pdf, int NE, const double* __restrict__ cos_t,
                const double* __restrict__ sin_t, const double* __restrict__ det_px0,
-               const double* __restrict__ det_py0, int fast, float* __restrict__ out,
+               const double* __restrict__ det_py0, int fast, int defer, float* __restrict__ out,
                double* __restrict__ lint, FwdStats* __restrict__ stats, long long ray0, long long ray1) {
   extern __shared__ double smem[];
   double* s_mu = smem;                                             // [NE][M]
@@ -172,7 +191,7 @@ forward_kernel(DevGeom g, const PixelRec* __restrict__ maps, const double* __res
 
   // rays [ray0, ray1) of the views_used * C
   const long long ray = ray0 + (long long)blockIdx.x * blockDim.x + threadIdx.x;
-  const bool active = ray < ray1;
+  bool active = ray < ray1;
   float val = 0.0f;
   int nseg = 0;
   if (active) {
@@ -184,31 +203,25 @@ forward_kernel(DevGeom g, const PixelRec* __restrict__ maps, const double* __res
     if (ray_setup(g, cos_t[v], sin_t[v], det_px0[c], det_py0[c], r)) {
       bool done = false;
       if (fast) done = walk_fast<M>(g, maps, r, a);
-      if (!done) walk_exact<M>(g, maps, r, a);
-    }
-    nseg = a.nseg;
-    double L[8];
-    finish_lines<M>(a, L, g.dens_div);
-    if (lint) {
-#pragma unroll
-      for (int m = 0; m < M; m++) lint[ray * M + m] = L[m];
-    }
-    if (out) {
-      if (SUM_MODE == VCT_SUM_REFERENCE) {
-        // (float)(pdf*exp(-transp/xfactor)) summed in float in bin order,
-        // MB/reprojection_TOMO.cpp:196-197 and MB/main.cpp:504.
-        float accf = 0.0f;
-        for (int e = 0; e < NE; e++) {
-          double t = 0.0;
-#pragma unroll
-          for (int m = 0; m < M; m++) t = __fma_rn(s_mu[e * M + m], L[m], t);
-          accf = __fadd_rn(accf, (float)((double)s_pdf[e] * exp(-t)));
-        }
-        val = accf;
-      } else {
-        val = spectral_compensated<M>(L, s_mu, s_pdf, NE);
+      // with defer, a ray the fast walk hands back is left to
+      // forward_lines_kernel (a warp per ray) and counts nowhere here
+      if (!done) {
+        if (defer) active = false;
+        else walk_exact<M>(g, maps, r, a);
       }
-      out[(size_t)v * g.width + g.start + c] = val;
+    }
+    if (active) {
+      nseg = a.nseg;
+      double L[8];
+      finish_lines<M>(a, L, g.dens_div);
+      if (lint) {
+#pragma unroll
+        for (int m = 0; m < M; m++) lint[ray * M + m] = L[m];
+      }
+      if (out) {
+        val = ray_value<M, SUM_MODE>(L, s_mu, s_pdf, NE);
+        out[(size_t)v * g.width + g.start + c] = val;
+      }
     }
   }
   float vmax = warp_max(active ? val : 0.0f);
@@ -222,25 +235,102 @@ forward_kernel(DevGeom g, const PixelRec* __restrict__ maps, const double* __res
   }
 }
 
+// The rays the fast walk hands back (rays through the grid origin at even
+// channel counts: the central channel of every view), listed once per
+// context, walked by a whole warp each (exact_lines_warp) after the main
+// kernel has skipped them: walked there in one thread each they held their
+// blocks several times longer than the rest (512^2, 800 x 608 rays: 1.33
+// against 0.53 ms for 609 channels).  Lane 0 does the ray's epilogue and its
+// share of the statistics.
+template <int M, int SUM_MODE>
+__global__ void forward_lines_kernel(DevGeom g, const PixelRec* __restrict__ maps, const double* __restrict__ mu_tab,
+                                     const float* __restrict__ pdf, int NE, const double* __restrict__ cos_t,
+                                     const double* __restrict__ sin_t, const double* __restrict__ det_px0,
+                                     const double* __restrict__ det_py0, const int* __restrict__ exact, int nexact,
+                                     float* __restrict__ out, double* __restrict__ lint,
+                                     FwdStats* __restrict__ stats, long long ray0, long long ray1) {
+  const int i = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (i >= nexact) return;  // warp-uniform
+  const int ray = exact[i];
+  if (ray < ray0 || ray >= ray1) return;
+  const int lane = threadIdx.x & 31;
+  double L[8];
+  int nseg;
+  exact_lines_warp<M>(g, maps, cos_t, sin_t, det_px0, det_py0, ray, L, &nseg, lane);
+  if (lane != 0) return;
+  if (lint) {
+#pragma unroll
+    for (int m = 0; m < M; m++) lint[(size_t)ray * M + m] = L[m];
+  }
+  float val = 0.0f;
+  if (out) {
+    const int v = ray / g.C, c = ray - (ray / g.C) * g.C;
+    val = ray_value<M, SUM_MODE>(L, mu_tab, pdf, NE);
+    out[(size_t)v * g.width + g.start + c] = val;
+  }
+  atomicMax(&stats->max_bits, __float_as_uint(val));
+  atomicMin(&stats->min_bits, __float_as_uint(val));
+  atomicAdd(&stats->segments, (unsigned long long)nseg);
+}
+
+// Lists the rays of [0, views_used * C) whose fast-walk plan is the exact
+// walk: count first (list == nullptr), then fill (any order).
+__global__ void exact_list_kernel(DevGeom g, const double* __restrict__ cos_t, const double* __restrict__ sin_t,
+                                  const double* __restrict__ det_px0, const double* __restrict__ det_py0,
+                                  int* __restrict__ list, int cap, int* __restrict__ count) {
+  const long long nrays = (long long)g.views_used * g.C;
+  const long long ray = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+  if (ray >= nrays) return;
+  const int v = (int)(ray / g.C), c = (int)(ray - (long long)v * g.C);
+  Ray r;
+  if (!ray_setup(g, cos_t[v], sin_t[v], det_px0[c], det_py0[c], r)) return;
+  FastPlan p;
+  fast_plan(g, r, p);
+  if (p.status != kPlanExact) return;
+  const int k = atomicAdd(count, 1);
+  if (list && k < cap) list[k] = (int)ray;
+}
+
+int launch_exact_list(const DevGeom& g, const double* d_cos, const double* d_sin, const double* d_px0,
+                      const double* d_py0, int* d_list, int cap, int* d_count, cudaStream_t st) {
+  const long long nrays = (long long)g.views_used * g.C;
+  VCT_CUDA(cudaMemsetAsync(d_count, 0, sizeof(int), st));
+  if (nrays == 0) return VCT_OK;
+  exact_list_kernel<<<(unsigned)((nrays + 255) / 256), 256, 0, st>>>(g, d_cos, d_sin, d_px0, d_py0, d_list, cap,
+                                                                     d_count);
+  VCT_CUDA(cudaGetLastError());
+  return VCT_OK;
+}
+
 template <int M>
 static int launch_forward_m(const DevGeom& g, const PixelRec* d_maps, const double* d_mu,
                             const float* d_pdf, int NE, const double* d_cos, const double* d_sin,
                             const double* d_px0, const double* d_py0, int sum_mode, int fast,
-                            float* d_out, double* d_lint, FwdStats* d_stats, cudaStream_t st, int v0, int v1) {
+                            float* d_out, double* d_lint, FwdStats* d_stats, cudaStream_t st, int v0, int v1,
+                            const int* d_exact, int nexact) {
   const long long ray0 = (long long)v0 * g.C, ray1 = (long long)v1 * g.C;
   const int blocks = (int)((ray1 - ray0 + kFwdThreads - 1) / kFwdThreads);
   const size_t smem = (size_t)NE * M * sizeof(double) + (size_t)NE * sizeof(float);
   if (blocks == 0) return VCT_OK;
+  const int defer = fast && d_exact && nexact > 0;
   if (sum_mode == VCT_SUM_REFERENCE) {
     auto k = forward_kernel<M, VCT_SUM_REFERENCE>;
     VCT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k<<<blocks, kFwdThreads, smem, st>>>(g, d_maps, d_mu, d_pdf, NE, d_cos, d_sin, d_px0, d_py0, fast,
+    k<<<blocks, kFwdThreads, smem, st>>>(g, d_maps, d_mu, d_pdf, NE, d_cos, d_sin, d_px0, d_py0, fast, defer,
                                           d_out, d_lint, d_stats, ray0, ray1);
+    VCT_CUDA(cudaGetLastError());
+    if (defer)
+      forward_lines_kernel<M, VCT_SUM_REFERENCE><<<(nexact + 3) / 4, 128, 0, st>>>(
+          g, d_maps, d_mu, d_pdf, NE, d_cos, d_sin, d_px0, d_py0, d_exact, nexact, d_out, d_lint, d_stats, ray0, ray1);
   } else {
     auto k = forward_kernel<M, VCT_SUM_COMPENSATED>;
     VCT_CUDA(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    k<<<blocks, kFwdThreads, smem, st>>>(g, d_maps, d_mu, d_pdf, NE, d_cos, d_sin, d_px0, d_py0, fast,
+    k<<<blocks, kFwdThreads, smem, st>>>(g, d_maps, d_mu, d_pdf, NE, d_cos, d_sin, d_px0, d_py0, fast, defer,
                                           d_out, d_lint, d_stats, ray0, ray1);
+    VCT_CUDA(cudaGetLastError());
+    if (defer)
+      forward_lines_kernel<M, VCT_SUM_COMPENSATED><<<(nexact + 3) / 4, 128, 0, st>>>(
+          g, d_maps, d_mu, d_pdf, NE, d_cos, d_sin, d_px0, d_py0, d_exact, nexact, d_out, d_lint, d_stats, ray0, ray1);
   }
   VCT_CUDA(cudaGetLastError());
   return VCT_OK;
@@ -249,14 +339,16 @@ static int launch_forward_m(const DevGeom& g, const PixelRec* d_maps, const doub
 int launch_forward(const DevGeom& g, const PixelRec* d_maps, int M, const double* d_mu_tab,
                    const float* d_pdf, int NE, const double* d_cos, const double* d_sin,
                    const double* d_det_ox, const double* d_det_oy, int sum_mode, int fast, float* d_out,
-                   double* d_lint, FwdStats* d_stats, cudaStream_t st, int v0, int v1) {
+                   double* d_lint, FwdStats* d_stats, cudaStream_t st, int v0, int v1, const int* d_exact,
+                   int nexact) {
   fast = fast && !g.rmax_active;
   if (v1 < 0) v1 = g.views_used;
   if (v0 < 0 || v0 > v1 || v1 > g.views_used) return fail(VCT_E_ARG, "forward: view range outside the views used");
   switch (M) {
-#define VCT_CASE(mm) \
-  case mm:           \
-    return launch_forward_m<mm>(g, d_maps, d_mu_tab, d_pdf, NE, d_cos, d_sin, d_det_ox, d_det_oy, sum_mode, fast, d_out, d_lint, d_stats, st, v0, v1);
+#define VCT_CASE(mm)                                                                                               \
+  case mm:                                                                                                         \
+    return launch_forward_m<mm>(g, d_maps, d_mu_tab, d_pdf, NE, d_cos, d_sin, d_det_ox, d_det_oy, sum_mode, fast, \
+                                d_out, d_lint, d_stats, st, v0, v1, d_exact, nexact);
     VCT_CASE(1) VCT_CASE(2) VCT_CASE(3) VCT_CASE(4) VCT_CASE(5) VCT_CASE(6) VCT_CASE(7) VCT_CASE(8)
 #undef VCT_CASE
     default:
@@ -325,7 +417,7 @@ forward_batch_kernel(const FwdJob* __restrict__ jobs, int njobs, int tile_rays, 
     const long long base = (long long)(t - J.tile0) * tile_rays;
     for (int r = lane; r < tile_rays; r += 32) {
       const long long ray = base + r;
-      const bool active = ray < nrays;
+      bool active = ray < nrays;
       float val = 0.0f;
       int nseg = 0;
       if (active) {
@@ -337,13 +429,18 @@ forward_batch_kernel(const FwdJob* __restrict__ jobs, int njobs, int tile_rays, 
         if (ray_setup(g, J.cos_t[v], J.sin_t[v], J.px0[c], J.py0[c], rr)) {
           bool done = false;
           if (J.fast) done = walk_fast<M>(g, J.maps, rr, a);
-          if (!done) walk_exact<M>(g, J.maps, rr, a);
+          if (!done) {
+            if (J.nexact > 0) active = false;  // listed: forward_lines_batch_kernel walks it
+            else walk_exact<M>(g, J.maps, rr, a);
+          }
         }
-        nseg = a.nseg;
-        double L[8];
-        finish_lines<M>(a, L, g.dens_div);
-        val = spectral_compensated<M>(L, s_mu, s_pdf, J.NE);
-        J.out[(size_t)v * g.width + g.start + c] = val;
+        if (active) {
+          nseg = a.nseg;
+          double L[8];
+          finish_lines<M>(a, L, g.dens_div);
+          val = spectral_compensated<M>(L, s_mu, s_pdf, J.NE);
+          J.out[(size_t)v * g.width + g.start + c] = val;
+        }
       }
       float vmax = warp_max(active ? val : 0.0f);
       float vmin = warp_min(active ? val : 3.0e38f);
@@ -378,15 +475,47 @@ static int launch_forward_batch_m(const FwdJob* d_jobs, int njobs, int tile_rays
   return VCT_OK;
 }
 
+// The jobs' listed exact-walk rays (xfirst: prefix sums of their counts),
+// a warp per ray, as forward_lines_kernel does for one slice.
+template <int M>
+__global__ void forward_lines_batch_kernel(const FwdJob* __restrict__ jobs, const unsigned int* __restrict__ xfirst,
+                                           int n) {
+  const unsigned int w = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+  if (w >= xfirst[n]) return;  // warp-uniform
+  const int jx = batch_job_of(xfirst, n, w);
+  const FwdJob& J = jobs[jx];
+  const int lane = threadIdx.x & 31;
+  const int ray = J.exact[w - xfirst[jx]];
+  double L[8];
+  int nseg;
+  exact_lines_warp<M>(J.g, J.maps, J.cos_t, J.sin_t, J.px0, J.py0, ray, L, &nseg, lane);
+  if (lane != 0) return;
+  const int v = ray / J.g.C, c = ray - (ray / J.g.C) * J.g.C;
+  const float val = spectral_compensated<M>(L, J.mu, J.pdf, J.NE);
+  J.out[(size_t)v * J.g.width + J.g.start + c] = val;
+  atomicMax(&J.stats->max_bits, __float_as_uint(val));
+  atomicMin(&J.stats->min_bits, __float_as_uint(val));
+  atomicAdd(&J.stats->segments, (unsigned long long)nseg);
+}
+
 int launch_forward_batch(const FwdJob* d_jobs, int njobs, int M, int tile_rays, unsigned int ntiles, int ne_max,
-                         int grid, unsigned int* d_counter, cudaStream_t st) {
+                         int grid, unsigned int* d_counter, const unsigned int* d_xfirst, unsigned int nexact_total,
+                         cudaStream_t st) {
   if (tile_rays < 32 || tile_rays % 32) return fail(VCT_E_ARG, "batch: tile size must be a multiple of 32 rays");
   reset_stats_kernel<<<(njobs + 127) / 128, 128, 0, st>>>(d_jobs, njobs);
   VCT_CUDA(cudaGetLastError());
   VCT_CUDA(cudaMemsetAsync(d_counter, 0, sizeof(unsigned int), st));
+  int rc;
   switch (M) {
-#define VCT_CASE(mm) \
-  case mm: return launch_forward_batch_m<mm>(d_jobs, njobs, tile_rays, ntiles, ne_max, grid, d_counter, st);
+#define VCT_CASE(mm)                                                                                      \
+  case mm:                                                                                                \
+    if ((rc = launch_forward_batch_m<mm>(d_jobs, njobs, tile_rays, ntiles, ne_max, grid, d_counter, st))) \
+      return rc;                                                                                          \
+    if (nexact_total > 0) {                                                                               \
+      forward_lines_batch_kernel<mm><<<(nexact_total + 3) / 4, 128, 0, st>>>(d_jobs, d_xfirst, njobs);    \
+      VCT_CUDA(cudaGetLastError());                                                                       \
+    }                                                                                                     \
+    return VCT_OK;
     VCT_CASE(1) VCT_CASE(2) VCT_CASE(3) VCT_CASE(4) VCT_CASE(5) VCT_CASE(6) VCT_CASE(7) VCT_CASE(8)
 #undef VCT_CASE
     default: return fail(VCT_E_ARG, "number of materials must be 1..8");

@@ -211,6 +211,26 @@ int vct_create(const vct_geometry* g, int device, vct_ctx** out) {
       (e = cudaMemcpy(c->det_py0.p, py0.data(), C * sizeof(double), cudaMemcpyHostToDevice)) ||
       (e = cudaMemcpy(c->fbp_coeff.p, coeff.data(), C * sizeof(double), cudaMemcpyHostToDevice)))
     return bail(cuda_fail(e, "vct_create: table upload"));
+  // The rays the fast walk hands back to the exact walk (rays through the
+  // grid origin at even channel counts): counted, then listed.
+  if (!c->dg.rmax_active) {
+    int n = 0;
+    if ((rc = c->fwd_exact.ensure(1)) ||
+        (rc = launch_exact_list(c->dg, c->cos_t.p, c->sin_t.p, c->det_px0.p, c->det_py0.p, nullptr, 0, c->fwd_exact.p,
+                                c->stream)))
+      return bail(rc);
+    if ((e = cudaMemcpyAsync(&n, c->fwd_exact.p, sizeof(int), cudaMemcpyDeviceToHost, c->stream)) ||
+        (e = cudaStreamSynchronize(c->stream)))
+      return bail(cuda_fail(e, "vct_create: exact-walk rays"));
+    if (n > 0) {
+      if ((rc = c->fwd_exact.ensure((size_t)n + 1)) ||
+          (rc = launch_exact_list(c->dg, c->cos_t.p, c->sin_t.p, c->det_px0.p, c->det_py0.p, c->fwd_exact.p + 1, n,
+                                  c->fwd_exact.p, c->stream)))
+        return bail(rc);
+      if ((e = cudaStreamSynchronize(c->stream))) return bail(cuda_fail(e, "vct_create: exact-walk rays"));
+    }
+    c->fwd_nexact = n;
+  }
   *out = c;
   return VCT_OK;
 }
@@ -221,7 +241,7 @@ void vct_destroy(vct_ctx* c) {
   if (c->own_stream) cudaStreamSynchronize(c->own_stream);
   c->cos_t.release(); c->sin_t.release(); c->cs_f.release(); c->det_px0.release(); c->det_py0.release();
   c->maps_raw.release(); c->maps.release(); c->mu_scaled.release(); c->mu_log2.release(); c->pdf.release();
-  c->full.release(); c->out.release(); c->stats.release();
+  c->full.release(); c->out.release(); c->stats.release(); c->fwd_exact.release();
   c->fbp_coeff.release();
   for (auto& h : c->fbp_h) h.release();
   c->fbp_g.release(); c->fbp_q.release(); c->fbp_sino.release(); c->fbp_img.release(); c->fbp_tacc.release();
@@ -421,6 +441,13 @@ int vct_set_walk_mode(vct_ctx* c, int mode) {
   return VCT_OK;
 }
 
+// The exact-walk ray list the forward defers (with the fast walk), and the
+// launches one forward takes.
+static const int* exact_list(const vct_ctx* c) { return c->fwd_nexact > 0 ? c->fwd_exact.p + 1 : nullptr; }
+static int forward_launches(const vct_ctx* c) {
+  return 1 + (c->fwd_nexact > 0 && c->walk_mode == VCT_WALK_FAST && !c->dg.rmax_active);
+}
+
 static int forward_into(vct_ctx* c, float* d_out, double* d_lint) {
   if (!c->maps_ready || !c->spectrum_ready) return fail(VCT_E_STATE, "forward: maps or spectrum not set");
   const size_t nsino = (size_t)c->geo.views * c->geo.width;
@@ -430,10 +457,10 @@ static int forward_into(vct_ctx* c, float* d_out, double* d_lint) {
   c->timer.begin(c->stream);
   int rc = launch_forward(c->dg, c->maps.p, c->M, mu_tab, c->pdf.p, c->NE, c->cos_t.p, c->sin_t.p,
                           c->det_px0.p, c->det_py0.p, c->sum_mode, c->walk_mode == VCT_WALK_FAST, d_out,
-                          d_lint, c->stats.p, c->stream);
+                          d_lint, c->stats.p, c->stream, 0, -1, exact_list(c), c->fwd_nexact);
   if (rc) return rc;
   c->timer.mark("forward_kernel", c->stream);
-  c->launches++;
+  c->launches += forward_launches(c);
   return VCT_OK;
 }
 
@@ -698,9 +725,9 @@ int vct_forward_views_dev(vct_ctx* c, int v0, int v1, float* d_out, float* d_max
   if (v1 > v0) {
     rc = launch_forward(c->dg, c->maps.p, c->M, mu_tab, c->pdf.p, c->NE, c->cos_t.p, c->sin_t.p, c->det_px0.p,
                         c->det_py0.p, c->sum_mode, c->walk_mode == VCT_WALK_FAST, d_out, nullptr, c->stats.p,
-                        c->stream, v0, v1);
+                        c->stream, v0, v1, exact_list(c), c->fwd_nexact);
     if (rc) return rc;
-    c->launches++;
+    c->launches += forward_launches(c);
   }
   // (max, min) of the rows as two floats: FwdStats begins with their bits
   VCT_CUDA(cudaMemcpyAsync(d_maxmin, c->stats.p, 2 * sizeof(float), cudaMemcpyDeviceToDevice, c->stream));
@@ -832,9 +859,10 @@ int vct_ir_step(vct_ctx* c, const float* proj, const float* npf, const float* be
   VCT_CUDA(cudaMemcpyAsync(c->stats.p, c->stats.p + 1, sizeof(FwdStats), cudaMemcpyDeviceToDevice, c->stream));
   if ((rc = launch_forward(c->dg, c->maps.p, c->M, c->mu_scaled.p + (size_t)(c->NE - 1) * c->M, c->pdf.p + c->NE - 1,
                            1, c->cos_t.p, c->sin_t.p, c->det_px0.p, c->det_py0.p, VCT_SUM_REFERENCE,
-                           c->walk_mode == VCT_WALK_FAST, c->ir_reproj.p, nullptr, c->stats.p, c->stream)))
+                           c->walk_mode == VCT_WALK_FAST, c->ir_reproj.p, nullptr, c->stats.p, c->stream, 0, -1,
+                           exact_list(c), c->fwd_nexact)))
     return rc;
-  c->launches++;
+  c->launches += forward_launches(c);
   // calc_squdiff_quad over the measured rows used (the measured sinogram
   // holds the views used, row k = view k).
   if ((rc = vct_squdiff_dev(c, c->ir_proj.p, c->ir_reproj.p, ite, thinout, num_ite, c->ir_out.p))) return rc;

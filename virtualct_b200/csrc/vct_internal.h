@@ -119,7 +119,13 @@ int launch_pack_maps(const int16_t* d_maps, int M, int N, PixelRec* d_packed, cu
 int launch_forward(const DevGeom& g, const PixelRec* d_maps, int M, const double* d_mu_tab,
                    const float* d_pdf, int NE, const double* d_cos, const double* d_sin,
                    const double* d_det_ox, const double* d_det_oy, int sum_mode, int fast, float* d_out,
-                   double* d_lint, FwdStats* d_stats, cudaStream_t st, int v0 = 0, int v1 = -1);
+                   double* d_lint, FwdStats* d_stats, cudaStream_t st, int v0 = 0, int v1 = -1,
+                   const int* d_exact = nullptr, int nexact = 0);
+// The rays whose fast-walk plan is the exact walk (geometry only): with
+// d_list == nullptr only their count (*d_count); else up to cap of them.
+// launch_forward given that list walks them a warp per ray after the rest.
+int launch_exact_list(const DevGeom& g, const double* d_cos, const double* d_sin, const double* d_px0,
+                      const double* d_py0, int* d_list, int cap, int* d_count, cudaStream_t st);
 // One slice of a batched forward (vct_batch.cpp): its geometry, device
 // tables and outputs.  tile0 is the index of its first ray tile.
 struct FwdJob {
@@ -133,11 +139,15 @@ struct FwdJob {
   const double* py0;
   float* out;        // [views][width]
   FwdStats* stats;
+  const int* exact;  // the rays the fast walk hands back (walked a warp per ray after the rest), or NULL
+  int nexact;
   unsigned int tile0;
   int NE, fast;
 };
+// d_xfirst: prefix sums [njobs + 1] of the jobs' nexact (total nexact_total).
 int launch_forward_batch(const FwdJob* d_jobs, int njobs, int M, int tile_rays, unsigned int ntiles, int ne_max,
-                         int grid, unsigned int* d_counter, cudaStream_t st);
+                         int grid, unsigned int* d_counter, const unsigned int* d_xfirst, unsigned int nexact_total,
+                         cudaStream_t st);
 int forward_batch_occupancy(int M, int ne_max, int* blocks_per_sm);
 int launch_normalize_noise(const DevGeom& g, const float* d_in, float* d_out, const FwdStats* d_stats,
                            int pad_zero, double sigma, uint64_t seed, cudaStream_t st, int r0 = 0, int r1 = -1);

@@ -370,6 +370,34 @@ __device__ void walk_exact_warp(const DevGeom& g, const Ray& r, const Sink& sink
 }
 #endif
 
+#if defined(__CUDACC__)
+// The line integrals L[0..M) (g/cm^2) and segment count of one ray of the
+// exact walk, by a whole warp: walk_exact_warp with the gather sink, each
+// lane's segment sums then added over the warp in a fixed order.  The same
+// segments as walk_exact in one thread, the FP64 sum in another order;
+// deterministic.  Every lane gets the result; every lane must call this.
+template <int M>
+__device__ void exact_lines_warp(const DevGeom& g, const PixelRec* __restrict__ maps, const double* __restrict__ cos_t,
+                                 const double* __restrict__ sin_t, const double* __restrict__ det_px0,
+                                 const double* __restrict__ det_py0, int ray, double L[8], int* nseg, int lane) {
+  const int v = ray / g.C, c = ray - (ray / g.C) * g.C;
+  RayAcc t;
+  acc_init(t);
+  Ray r;
+  if (ray_setup(g, cos_t[v], sin_t[v], det_px0[c], det_py0[c], r))  // the same for every lane
+    walk_exact_warp(g, r, GatherSink<M>{maps, &t}, lane);
+#pragma unroll
+  for (int m = 0; m < M; m++) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) t.Ld[m] += __shfl_xor_sync(0xffffffffu, t.Ld[m], o);
+  }
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) t.nseg += __shfl_xor_sync(0xffffffffu, t.nseg, o);
+  finish_lines<M>(t, L, g.dens_div);
+  *nseg = t.nseg;
+}
+#endif
+
 template <int M>
 VCT_HD void walk_exact(const DevGeom& g, const PixelRec* __restrict__ maps, const Ray& r, RayAcc& a) {
   walk_exact_to(g, r, GatherSink<M>{maps, &a});

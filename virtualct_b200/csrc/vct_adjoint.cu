@@ -759,15 +759,14 @@ adj_gather_kernel(AdjGeom a, const double* __restrict__ cos_t, const double* __r
   __shared__ AdjStage<M, TX * TY / 32 * kAdjW> S;
   const int NE1 = a.N + 1;
   const int ntiles = ((NE1 + TX - 1) / TX) * ((NE1 + TY - 1) / TY);
-  for (int item = blockIdx.x; item < ntiles * kAdjChunks; item += gridDim.x)
-    adj_gather_tile<M, TX, TY, kAdjChunks>(a, item % ntiles, item / ntiles, cos_t, sin_t, dir, rec, gr, tv, ext, S);
+  for (int item = blockIdx.x; item < ntiles * adj_chunks(M); item += gridDim.x)
+    adj_gather_tile<M, TX, TY, adj_chunks(M)>(a, item % ntiles, item / ntiles, cos_t, sin_t, dir, rec, gr, tv, ext, S);
 }
 
 // grad[m][r][c] = ext at (r, c), plus the folded cells at index -1 (row -1
 // onto row 0, column -1 onto column 0), summed over the view chunks, plus
 // the exact-walk rays' fixed-point sums; fixed order, so the result is
 // deterministic.
-template <int NCH>
 __device__ __forceinline__ void adj_fold_elem(long long i, int M, int N, const float* __restrict__ ext,
                                               const unsigned long long* __restrict__ sacc,
                                               const unsigned int* __restrict__ gmax, double lmax, int log2_terms,
@@ -779,8 +778,7 @@ __device__ __forceinline__ void adj_fold_elem(long long i, int M, int N, const f
   const int r = p / N, c = p - (p / N) * N;
   const int N1 = N + 1;
   double v = 0.0;
-#pragma unroll
-  for (int k = 0; k < NCH; k++) {
+  for (int k = 0; k < adj_chunks(M); k++) {
     const float* e = ext + ((size_t)k * M + m) * e2;
     v += e[(r + 1) * N1 + (c + 1)];
     if (c == 0) v += e[(r + 1) * N1];
@@ -794,8 +792,7 @@ __device__ __forceinline__ void adj_fold_elem(long long i, int M, int N, const f
 __global__ void adj_fold_kernel(int M, int N, const float* __restrict__ ext, const unsigned long long* __restrict__ sacc,
                                 const unsigned int* __restrict__ gmax, double lmax, int log2_terms,
                                 float* __restrict__ grad) {
-  adj_fold_elem<kAdjChunks>((long long)blockIdx.x * blockDim.x + threadIdx.x, M, N, ext, sacc, gmax, lmax, log2_terms,
-                            grad);
+  adj_fold_elem((long long)blockIdx.x * blockDim.x + threadIdx.x, M, N, ext, sacc, gmax, lmax, log2_terms, grad);
 }
 
 // Tile shapes, largest first; the channel window of a tile grows with its
@@ -921,7 +918,7 @@ void adj_job_blocks(const AdjJob& j, int M, int tile, unsigned int blocks[kAdjSt
   blocks[kAdjStLoss] = 1u;
   blocks[kAdjStSpecial] = (unsigned int)((j.nspecial + 3) / 4);  // 128 threads, a warp per ray
   for (int t = 0; t < 4; t++)
-    blocks[kAdjStGather + t] = t == tile ? (unsigned int)(tiles_of(j.a, tile) * kAdjChunks) : 0u;
+    blocks[kAdjStGather + t] = t == tile ? (unsigned int)(tiles_of(j.a, tile) * adj_chunks(M)) : 0u;
   blocks[kAdjStFold] = (unsigned int)((M * n2 + 255) / 256);
 }
 
@@ -1052,7 +1049,7 @@ adj_gather_batch_kernel(const AdjJob* __restrict__ jobs, const unsigned int* __r
     const AdjJob& J = jobs[jx];
     const int ntiles = ((J.a.N + TX) / TX) * ((J.a.N + TY) / TY);  // tiles of the (N+1)^2 cells
     const int item = (int)(b - first[jx]);
-    adj_gather_tile<M, TX, TY, kAdjChunks>(J.a, item % ntiles, item / ntiles, J.cos_t, J.sin_t, J.dir, J.rec, J.gr,
+    adj_gather_tile<M, TX, TY, adj_chunks(M)>(J.a, item % ntiles, item / ntiles, J.cos_t, J.sin_t, J.dir, J.rec, J.gr,
                                            reinterpret_cast<const AdjTileView*>(J.tv), J.ext, S);
   }
 }
@@ -1062,7 +1059,7 @@ __global__ void adj_fold_batch_kernel(const AdjJob* __restrict__ jobs, const uns
   const int jx = adj_job_of(first, n, blockIdx.x);
   const AdjJob& J = jobs[jx];
   const long long i = (long long)(blockIdx.x - first[jx]) * blockDim.x + threadIdx.x;
-  adj_fold_elem<kAdjChunks>(i, M, J.a.N, J.ext, J.sacc, J.gmax, J.lmax, J.log2_terms, J.grad);
+  adj_fold_elem(i, M, J.a.N, J.ext, J.sacc, J.gmax, J.lmax, J.log2_terms, J.grad);
 }
 
 template <int M, int TX, int TY>

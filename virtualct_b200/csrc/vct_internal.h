@@ -262,6 +262,13 @@ constexpr int kAdjRayExact = 2;  // exact walk (scattered in fixed point)
 #define VCT_ADJ_CHUNKS 2
 #endif
 constexpr int kAdjChunks = VCT_ADJ_CHUNKS;
+// The ranges used for M elements: kAdjChunks up to 6 elements, one above (at
+// 8 elements the batch's gather lost more to the split, in registers, than
+// the single slice gained).
+#if defined(__CUDACC__)
+__host__ __device__
+#endif
+constexpr int adj_chunks(int M) { return M <= 6 ? kAdjChunks : 1; }
 
 struct AdjGeom {
   int N, nxm, C, start, views_used;

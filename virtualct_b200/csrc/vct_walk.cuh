@@ -23,10 +23,12 @@ VCT_HD int pad_index(int col, int row, int N) { return (col + kPad) + (row + kPa
 // on the 512^2 slice with 800 x 609 rays: 2 / 4 / 5 / 6 / 8 / 12 segments gave
 // 0.85 / 0.77 / 0.75 / 0.73 / 0.76 / 0.75 ms, with no spills).  Capping
 // registers for 6 / 7 / 8 blocks per SM (small spills) gave 0.734 / 0.738 /
-// 0.800 ms against 0.738 ms uncapped: the walk is issue-bound, so no cap is
-// set.
+// 0.800 ms against 0.738 ms at 5: more resident warps do not help.  The cap
+// of 5 blocks matters for 8 elements, where the compiler would otherwise take
+// 102 registers, which the 256-register allocation unit rounds to 4 blocks
+// (the 8-element 6 MV slice: 0.601 ms against 0.575 ms at 5).
 #ifndef VCT_FWD_MINBLOCKS
-#define VCT_FWD_MINBLOCKS 0
+#define VCT_FWD_MINBLOCKS 5
 #endif
 #ifndef VCT_FWD_UNROLL
 #define VCT_FWD_UNROLL 6

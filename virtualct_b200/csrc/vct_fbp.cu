@@ -387,6 +387,12 @@ fbp_bp_kernel(const float* __restrict__ Q, int V, int C, int N, int win, float s
 // rows of each base view are read through the L1 cache (the 32 pixels of a
 // warp read neighbouring channels).
 constexpr int BS_TX = 32, BS_TY = 4, BS_VS = 4;  // BS_VS: the default view split
+// (Also measured: the register cap for 4 blocks of 512 threads per SM, 32
+// registers, 0.213 ms against 0.127 ms; each batch of U base views computing
+// its geometry first and then issuing all 4U row loads unconditionally
+// (clamped channels), U = 2 / 4 / 8 at 60 / 82 / 127 registers: 0.135 /
+// 0.145 / 0.123 ms -- the last too close to pay for its register footprint
+// in the batch's kernel.)
 #ifndef VCT_BP_UNROLL
 #define VCT_BP_UNROLL 8
 #endif

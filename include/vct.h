@@ -73,7 +73,9 @@ typedef struct vct_ctx vct_ctx;
 
 /* Creates a context on CUDA device `device` for geometry g.  Precomputes the
  * view trig tables (MB/projectionDataTOMO.cpp:362-368, MB/misc_TOMO.cpp:82-100)
- * and detector tables on the host and uploads them. */
+ * and detector tables on the host and uploads them, and lists (one kernel on
+ * the context's stream, then a wait for it) the rays the fast walk hands to
+ * the exact walk, which the forward walks a warp per ray. */
 int vct_create(const vct_geometry* g, int device, vct_ctx** out);
 void vct_destroy(vct_ctx* ctx);
 /* cudaStream_t passed as an opaque pointer; NULL = the context's own stream

@@ -43,9 +43,9 @@ METRIC = "MBFPA rays*bins/s (FBP slices/s alongside)"
 # --no-cpu-baseline --no-extras`): DRAM bytes read + written per launch (the two
 # map copies once; the gathers hit L1/L2) and warp instructions executed per
 # launch.  Not measured by the run that prints them.
-FWD_CAPTURE = {"dram_bytes": 8581632, "warp_instructions": 2.935e8,
-               "source": "ncu capture of forward_kernel<6,0> (integer fixed-point event loop, 6 gathers in flight), "
-                         "commit 730a6a4"}
+FWD_CAPTURE = {"dram_bytes": 8582400, "warp_instructions": 2.932e8,
+               "source": "ncu capture of forward_kernel<6,0> (integer fixed-point event loop, 6 gathers in flight, "
+                         "5 blocks per SM), commit 48c9d28"}
 CONFIG_NAME = "plain MBFPA+FBP single slice: 512^2, 6 elements, 800 views x 609 channels, 120 kVp Kramers 110 bins"
 # mask pixels of the 512^2 reconstruction circle (FBP/misc.cpp:9-37)
 MASK_PX = 205012

@@ -93,7 +93,13 @@ int launch_beam_hardening(float* d_p, long long n, double alpha, double beta, cu
 // TRANSPOSE: the transposed filter, g[v][k] = sum_m h0(m-k) c_m q[v][m]; h0
 // is even (both kernels depend on |m-k| only), so it is the same convolution
 // with the row factor applied to the input instead of the output.
-constexpr int FC_R = 4, FC_TMAX = 256;
+// Outputs per thread (4 / 8 / 12 measured 31 / 37 / 34 us at 800 x 609:
+// fewer threads per view's block hide less of the shared-load latency).
+#ifndef VCT_FC_R
+#define VCT_FC_R 4
+#endif
+constexpr int FC_R = VCT_FC_R, FC_TMAX = 256;
+static_assert(FC_R % 4 == 0, "outputs per thread: a multiple of 4");
 
 // Shared memory of one view: g padded to a multiple of 4 (+4 zeros), then
 // h0(d) at index OFF + d for |d| <= C-1 (zero around it), OFF = 3 mod 4 so
@@ -142,12 +148,20 @@ __device__ __forceinline__ void fbp_filter_view(const float* __restrict__ G, con
   }
   __syncthreads();
   for (int m0 = threadIdx.x * FC_R; m0 < C; m0 += nt * FC_R) {
-    float acc[FC_R] = {0.0f, 0.0f, 0.0f, 0.0f};
+    float acc[FC_R];
+#pragma unroll
+    for (int j = 0; j < FC_R; j++) acc[j] = 0.0f;
     for (int k0 = 0; k0 < cpad; k0 += 4) {
       const float4 g4 = *reinterpret_cast<const float4*>(sg + k0);
-      const float4 wa = *reinterpret_cast<const float4*>(sh + off + m0 - k0 - 3);
-      const float4 wb = *reinterpret_cast<const float4*>(sh + off + m0 - k0 + 1);
-      const float w[8] = {wa.x, wa.y, wa.z, wa.w, wb.x, wb.y, wb.z, wb.w};  // h0(m0 - k0 - 3 + i)
+      float w[FC_R + 4];  // h0(m0 - k0 - 3 + i)
+#pragma unroll
+      for (int b = 0; b < FC_R / 4 + 1; b++) {
+        const float4 wb = *reinterpret_cast<const float4*>(sh + off + m0 - k0 - 3 + 4 * b);
+        w[4 * b] = wb.x;
+        w[4 * b + 1] = wb.y;
+        w[4 * b + 2] = wb.z;
+        w[4 * b + 3] = wb.w;
+      }
       const float g[4] = {g4.x, g4.y, g4.z, g4.w};
 #pragma unroll
       for (int i = 0; i < 4; i++)

@@ -41,6 +41,45 @@ def test_small_forward_matches_reference(cuda_device, views, mode, walk):
     assert not out[used:].any()  # rows past views/2*2 stay 0, as in the reference
 
 
+@pytest.mark.parametrize("mode", [vct.SUM_COMPENSATED, vct.SUM_REFERENCE])
+def test_even_channels_exact_rays_by_warp(cuda_device, mode):
+    """At an even channel count the central channel of every view passes
+    through the grid origin and takes the exact walk; with the fast walk those
+    rays are listed once and each is walked by a whole warp after the rest.
+    The sinogram and line integrals against the FP64 oracle, and those rays'
+    line integrals against the exact walk in one thread per ray (the same
+    segments, summed in another order)."""
+    import torch
+
+    N, pix, views, C = 128, 0.1, 120, 512
+    t = golden("mu_tables.npz")
+    maps = phantoms.ellipse_phantom(13, N, border_px=2)
+    g = O.geom(views=views, channels=C, recon_size=N, pixel_cm=pix)
+    c, s = O.trig_tables(views)
+    f64, lint = O.forward_fp64_maps(g, c, s, maps, t["kv120_mu"], t["kv120_pdf"], want_lint=True)
+    geo = vct.Geometry.with_channels(C, views=views, recon_size=N, pixel_cm=pix)
+    res = {}
+    for walk in (vct.WALK_FAST, vct.WALK_EXACT):
+        with vct.Context(geo) as ctx:
+            ctx.set_sum_mode(mode)
+            ctx.set_walk_mode(walk)
+            ctx.set_maps(maps)
+            ctx.set_spectrum(t["kv120_mu"], t["kv120_pdf"])
+            out = ctx.forward()
+            L = torch.zeros((views, C, 6), dtype=torch.float64, device="cuda")
+            ctx.line_integrals_dev(L)
+            ctx.synchronize()
+            res[walk] = (out, L.cpu().numpy())
+    out_f, L_f = res[vct.WALK_FAST]
+    _, L_e = res[vct.WALK_EXACT]
+    scale = max(1.0, np.abs(lint).max())
+    central = C // 2
+    assert np.abs(L_e[:, central]).max() > 0
+    assert np.max(np.abs(L_f[:, central] - L_e[:, central])) <= 1e-12 * scale
+    assert np.max(np.abs(L_f - lint)) <= 1e-8 * scale
+    assert max_rel(out_f, f64) < (FP64_RTOL if mode == vct.SUM_COMPENSATED else SINO_RTOL)
+
+
 @pytest.mark.parametrize("walk", [vct.WALK_FAST, vct.WALK_EXACT])
 @pytest.mark.parametrize("N,pix,views", [(64, 0.4, 40), (128, 0.1, 120)])
 def test_line_integrals_vs_fp64_oracle(cuda_device, walk, N, pix, views):

@@ -607,8 +607,11 @@ constexpr int adj_min_blocks(int M, int threads) { return M <= 6 ? VCT_ADJ_MINBL
 #ifndef VCT_ADJ_BATCH_MINBLOCKS
 #define VCT_ADJ_BATCH_MINBLOCKS 0
 #endif
+// The loop over a round's views unrolled by 2: 0.989 -> 0.969 ms at 512^2 /
+// 800 x 609 (gradient bit-identical; 1024^2, 8 elements and the 64-slice
+// batch unchanged within 0.6%).
 #ifndef VCT_ADJ_VUNROLL
-#define VCT_ADJ_VUNROLL 1
+#define VCT_ADJ_VUNROLL 2
 #endif
 #ifndef VCT_ADJ_LANEMAP
 #define VCT_ADJ_LANEMAP 1

@@ -618,13 +618,19 @@ fbp_bp_t_kernel(const float* __restrict__ U, int V, int C, int N, float scale, f
 // geometry, evaluated once (bp_orbit_view's formula), adds (1-w)/L^2 u and
 // w/L^2 u to bins gi and gi+1 of the four rows of the orbit.  Block
 // (b, part) owns rows b, b+V/4, b+V/2, b+3V/4 -- the rows base views
-// b + i V/4 reach through the quarter turn -- and one eighth of the orbit
+// b + i V/4 reach through the quarter turn -- and one BT_PARTS-th of the orbit
 // pixels; it sums in shared memory and flushes to a global accumulator.
 // Sums are 64-bit fixed point (scale 2^62 / (N^2 max|u| max 1/L^2), so no sum
 // can overflow): integer sums do not depend on order, so the result is the
 // same from run to run whatever the atomics' order.  The rotated pixels are
 // read from a transposed copy of u, so every read is along a row.
-constexpr int BT_PARTS = 8;
+// Parts of the orbit pixels per base view (blocks V/4 x parts): 2 / 4 / 8 /
+// 16 / 32 / 64 measured 0.569 / 0.526 / 0.432 / 0.411 / 0.413 / 0.438 ms at
+// 512^2 from 800 x 609 (output bit-identical).
+#ifndef VCT_BT_PARTS
+#define VCT_BT_PARTS 16
+#endif
+constexpr int BT_PARTS = VCT_BT_PARTS;
 
 // s += v (64-bit, two's complement) as two 32-bit shared-memory atomics: the
 // low word's carry is read from the value it held before the add, and the

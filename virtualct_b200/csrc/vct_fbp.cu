@@ -13,6 +13,8 @@
 //                in shared memory.
 #include <cuda_runtime.h>
 
+#include <algorithm>
+
 #include "vct_internal.h"
 #include "vct_fastmath.cuh"
 
@@ -618,12 +620,12 @@ fbp_bp_t_kernel(const float* __restrict__ U, int V, int C, int N, float scale, f
 // geometry, evaluated once (bp_orbit_view's formula), adds (1-w)/L^2 u and
 // w/L^2 u to bins gi and gi+1 of the four rows of the orbit.  Block
 // (b, part) owns rows b, b+V/4, b+V/2, b+3V/4 -- the rows base views
-// b + i V/4 reach through the quarter turn -- and one BT_PARTS-th of the orbit
-// pixels; it sums in shared memory and flushes to a global accumulator.
-// Sums are 64-bit fixed point (scale 2^62 / (N^2 max|u| max 1/L^2), so no sum
-// can overflow): integer sums do not depend on order, so the result is the
-// same from run to run whatever the atomics' order.  The rotated pixels are
-// read from a transposed copy of u, so every read is along a row.
+// b + i V/4 reach through the quarter turn -- and one part of the orbit
+// pixels (at most BT_PART_PIXELS of them); it sums in shared memory and
+// flushes to a global 64-bit accumulator.  Every sum is in integers (fixed
+// point), so it does not depend on the order of the atomics and the result
+// is the same from run to run.  The rotated pixels are read from a
+// transposed copy of u, so every read is along a row.
 // Parts of the orbit pixels per base view (blocks V/4 x parts): 2 / 4 / 8 /
 // 16 / 32 / 64 measured 0.569 / 0.526 / 0.432 / 0.411 / 0.413 / 0.438 ms at
 // 512^2 from 800 x 609 (output bit-identical).
@@ -631,18 +633,30 @@ fbp_bp_t_kernel(const float* __restrict__ U, int V, int C, int N, float scale, f
 #define VCT_BT_PARTS 16
 #endif
 constexpr int BT_PARTS = VCT_BT_PARTS;
+// Largest part: a shared slot (row, bin) then takes at most 4 x 4096 = 2^14
+// adds (one per pixel of the part for each of the four base views).
+constexpr int BT_PART_PIXELS = 4096;
+// Fixed point: a contribution c becomes rint(c fx) with fx = 2^33 / (max|u|
+// max 1/L^2), so |rint(c fx)| <= 2^33, split as h 2^17 + l with |h|, |l| <=
+// 2^16: the slot sums of h and of l stay within 2^14 x 2^16 = 2^30 (32-bit,
+// no carries), and a part's total h 2^17 + l within 2^47.
+constexpr float BT_FIX_BITS = 8589934592.0f;  // 2^33
 
-// s += v (64-bit, two's complement) as two 32-bit shared-memory atomics: the
-// low word's carry is read from the value it held before the add, and the
-// high word is touched only when it changes.  Low and high words live in
-// separate arrays, so neighbouring bins are neighbouring banks.  (Measured:
-// 0.85 ms for the 512^2, 800 x 609 transpose against 1.86 ms with 64-bit atomics and
-// 1.50 ms with float ones.)
-__device__ __forceinline__ void add64_split(unsigned int* lo, unsigned int* hi, unsigned long long v) {
-  const unsigned int vlo = (unsigned int)v, vhi = (unsigned int)(v >> 32);
-  const unsigned int old = atomicAdd(lo, vlo);
-  const unsigned int carry = (unsigned int)(old + vlo < old);
-  if (vhi + carry) atomicAdd(hi, vhi + carry);
+// lo += l, hi += h for rint(v) = h 2^17 + l: h = rint(v 2^-17), l = rint(v -
+// h 2^17), both by the 1.5 * 2^23 rounding constant (|v 2^-17|, |l| < 2^22).
+// v - h 2^17 is exact in the FMA (a multiple of v's ulp below 2^17), and h 2^17
+// is even, so h 2^17 + l equals __float2ll_rn(v), ties included.  Both adds are
+// fire-and-forget shared-memory atomics.  (Measured: 0.85 ms for the 512^2,
+// 800 x 609 transpose with two-word 64-bit adds that carried through the
+// returned low word, against 1.86 ms with 64-bit atomics and 1.50 ms with
+// float ones.)
+__device__ __forceinline__ void bt_add(int* lo, int* hi, float v) {
+  const float th = fmaf(v, 7.62939453125e-06f, 12582912.0f);  // v 2^-17 + 1.5 2^23
+  const int h = __float_as_int(th) - 0x4B400000;
+  const float r = fmaf(th - 12582912.0f, -131072.0f, v);
+  const int l = __float_as_int(r + 12582912.0f) - 0x4B400000;
+  atomicAdd(lo, l);
+  atomicAdd(hi, h);
 }
 
 // ut[c][r] = u[r][c], N x N, 32 x 32 tiles through shared memory.
@@ -669,37 +683,42 @@ __global__ void absmax_kernel(const float* __restrict__ u, long long n, unsigned
   if ((threadIdx.x & 31) == 0 && m > 0.0f) atomicMax(out, __float_as_uint(m));
 }
 
-__device__ __forceinline__ float bt_fixed_scale(const unsigned long long* umax_slot, int N, float il2max) {
+__device__ __forceinline__ float bt_fixed_scale(const unsigned long long* umax_slot, float il2max) {
   const float um = __uint_as_float((unsigned int)*umax_slot);
   if (!(um > 0.0f)) return 1.0f;
-  return (float)(4.611686018427387904e18 / ((double)N * N * (double)um * (double)il2max));  // 2^62 / bound
+  return (float)((double)BT_FIX_BITS / ((double)um * (double)il2max));  // 2^33 / max |c|
 }
 
 __global__ void __launch_bounds__(256)
 fbp_bp_t_scatter_kernel(const float* __restrict__ U, const float* __restrict__ UT, int V, int C, int N, float scale,
                         float sid, float inv_dbeta, float center, float il2max, const float2* __restrict__ cs,
                         unsigned long long* __restrict__ acc) {
-  extern __shared__ unsigned int s_lo[];  // [4][C] low words, then [4][C] high words
-  unsigned int* s_hi = s_lo + 4 * C;
-  const int b = blockIdx.x, part = blockIdx.y;
+  extern __shared__ int s_lo[];  // [4][C] sums of l, then [4][C] sums of h
+  int* s_hi = s_lo + 4 * C;
+  const int b = blockIdx.x, part = blockIdx.y, parts = gridDim.y;
   const int V4 = V / 4, H = N / 2, n1 = N - 1;
-  for (int i = threadIdx.x; i < 8 * C; i += blockDim.x) s_lo[i] = 0u;
-  const float fx = bt_fixed_scale(acc + (size_t)V * C, N, il2max);
+  for (int i = threadIdx.x; i < 8 * C; i += blockDim.x) s_lo[i] = 0;
+  const float fx = bt_fixed_scale(acc + (size_t)V * C, il2max);
   __syncthreads();
-  const double r = (double)n1 / 2.0;
   const float cp = (float)N / 2.0f - 0.5f;
   const int np = H * H;
-  const int o0 = (int)((long long)np * part / BT_PARTS), o1 = (int)((long long)np * (part + 1) / BT_PARTS);
+  const int o0 = (int)((long long)np * part / parts), o1 = (int)((long long)np * (part + 1) / parts);
+  const int o_first = o0 + threadIdx.x;
   for (int i = 0; i < 4; i++) {
     const float2 t = __ldg(cs + b + i * V4);
     // Neighbouring lanes take neighbouring pixels across the rays (along x
     // when the view's rays run closer to y, else along y), so their bins
     // differ and their shared-memory adds do not collide.
     const bool alongy = fabsf(t.y) > fabsf(t.x);
-    for (int o = o0 + threadIdx.x; o < o1; o += blockDim.x) {
-      const int f = o % H, sl = o / H;
+    // Orbit pixel o = sl H + f, stepped by the block size without a division.
+    int f = o_first % H, sl = o_first / H;
+    for (int o = o_first; o < o1; o += blockDim.x) {
       const int x = alongy ? sl : f, y = alongy ? f : sl;
-      if (((double)y - r) * ((double)y - r) + ((double)x - r) * ((double)x - r) > r * r) continue;
+      f += blockDim.x;
+      while (f >= H) f -= H, sl++;
+      // Inscribed-circle mask, exactly: (2y-N+1)^2 + (2x-N+1)^2 <= (N-1)^2.
+      const int dy2 = 2 * y - n1, dx2 = 2 * x - n1;
+      if (dy2 * dy2 + dx2 * dx2 > n1 * n1) continue;
       const float xx = -((float)x - cp) * scale;
       const float yy = -((float)y - cp) * scale;
       // FBP/reconstructImageTOMO.cpp:67-73, as bp_orbit_view.
@@ -708,7 +727,7 @@ fbp_bp_t_scatter_kernel(const float* __restrict__ U, const float* __restrict__ U
       const float d = sid - Y;
       const float rd = rcp_approx(d);
       const float fg = atan_small(X * rd) * inv_dbeta + center;
-      const float iL2 = rcp_approx(fmaf(d, d, X * X));
+      const float iL2f = rcp_approx(fmaf(d, d, X * X)) * fx;
       const float big = __fadd_rz(fmaxf(fg, 0.0f), 8388608.0f);
       const int gi = fg > -1.0f ? (__float_as_int(big) - 0x4B000000) : -1;
       const float w = fg - (big - 8388608.0f);
@@ -729,24 +748,24 @@ fbp_bp_t_scatter_kernel(const float* __restrict__ U, const float* __restrict__ U
       }
 #pragma unroll
       for (int q = 0; q < 4; q++) {
-        const float val = uq[q] * iL2;
+        const float val = uq[q] * iL2f;                 // u / L^2 in fixed-point units
         const float c1 = w * val, c0 = val - c1;  // (1 - w) val and w val
         const int at = ((i + q) & 3) * C + gi;
-        add64_split(s_lo + at, s_hi + at, (unsigned long long)__float2ll_rn(c0 * fx));
-        add64_split(s_lo + at + 1, s_hi + at + 1, (unsigned long long)__float2ll_rn(c1 * fx));
+        bt_add(s_lo + at, s_hi + at, c0);
+        bt_add(s_lo + at + 1, s_hi + at + 1, c1);
       }
     }
   }
   __syncthreads();
   for (int i = threadIdx.x; i < 4 * C; i += blockDim.x) {
-    const unsigned long long v = ((unsigned long long)s_hi[i] << 32) | s_lo[i];
-    if (v) atomicAdd(acc + (size_t)(b + (i / C) * V4) * C + (i % C), v);
+    const long long v = (long long)s_hi[i] * 131072 + s_lo[i];
+    if (v) atomicAdd(acc + (size_t)(b + (i / C) * V4) * C + (i % C), (unsigned long long)v);
   }
 }
 
 __global__ void fbp_bp_t_finish_kernel(const unsigned long long* __restrict__ acc, int V, int C, int N, float il2max,
                                        float out_scale, float* __restrict__ qb) {
-  const float fx = bt_fixed_scale(acc + (size_t)V * C, N, il2max);
+  const float fx = bt_fixed_scale(acc + (size_t)V * C, il2max);
   const long long n = (long long)V * C;
   for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
     qb[i] = (float)((double)(long long)acc[i] / (double)fx) * out_scale;
@@ -776,13 +795,14 @@ int launch_fbp_backproject_t(const float* d_u, int V, int C, int N, double pixel
     const double reach = 0.5 * (N - 1) * pixel_cm * 1.4142135623730951;
     if (!(sid > reach)) return fail(VCT_E_UNSUPPORTED, "fbp transpose: the grid reaches the source");
     const float il2max = (float)(2.0 / ((sid - reach) * (sid - reach)));
-    const size_t smem = (size_t)4 * C * sizeof(unsigned long long);
+    const size_t smem = (size_t)8 * C * sizeof(int);
     float* d_ut = reinterpret_cast<float*>(d_acc + (size_t)V * C + 1);
     VCT_CUDA(cudaMemsetAsync(d_acc, 0, ((size_t)V * C + 1) * sizeof(unsigned long long), st));
     absmax_kernel<<<148 * 4, 256, 0, st>>>(d_u, (long long)N * N, reinterpret_cast<unsigned int*>(d_acc + (size_t)V * C));
     transpose_kernel<<<dim3((N + 31) / 32, (N + 31) / 32), dim3(32, 8), 0, st>>>(d_u, N, d_ut);
     VCT_CUDA(cudaFuncSetAttribute(fbp_bp_t_scatter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    fbp_bp_t_scatter_kernel<<<dim3(V / 4, BT_PARTS), 256, smem, st>>>(
+    const int parts = std::max(BT_PARTS, (int)(((long long)(N / 2) * (N / 2) + BT_PART_PIXELS - 1) / BT_PART_PIXELS));
+    fbp_bp_t_scatter_kernel<<<dim3(V / 4, parts), 256, smem, st>>>(
         d_u, d_ut, V, C, N, (float)pixel_cm, (float)sid, (float)(1.0 / dbeta_det), (float)(C / 2), il2max,
         reinterpret_cast<const float2*>(d_cs), d_acc);
     fbp_bp_t_finish_kernel<<<148 * 4, 256, 0, st>>>(d_acc, V, C, N, il2max, (float)(dbeta * xfactor), d_qb);

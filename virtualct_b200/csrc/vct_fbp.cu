@@ -86,17 +86,19 @@ int launch_beam_hardening(float* d_p, long long n, double alpha, double beta, cu
 // rows (:114-123), so each view is a 1-D convolution: one block per view, g
 // and h0 in shared memory.  Register tiling: each thread owns FC_R = 4
 // consecutive outputs and takes k in chunks of 4; per chunk one 128-bit
-// load of g (the same for every thread) and two aligned 128-bit loads of
-// the 8 kernel values h0(m0 - k0 - 3 .. m0 - k0 + 4) feed 16 FMAs.  For each
-// output k runs in ascending order, as in the reference.
+// load of g (the same for every thread) and one aligned 128-bit load of
+// the 4 new kernel values of a sliding window of 8, h0(m0 - k0 - 3 .. m0 -
+// k0 + 4), feed 16 FMAs.  For each output k runs in ascending order, as in
+// the reference.
 // WEIGHT: the row is loaded straight from the sinogram and weighted on the
 // way (the weight kernel's g = -ln p * coeff, optionally with the
 // beam-hardening correction), so the weighted sinogram is never stored.
 // TRANSPOSE: the transposed filter, g[v][k] = sum_m h0(m-k) c_m q[v][m]; h0
 // is even (both kernels depend on |m-k| only), so it is the same convolution
 // with the row factor applied to the input instead of the output.
-// Outputs per thread (4 / 8 / 12 measured 31 / 37 / 34 us at 800 x 609:
-// fewer threads per view's block hide less of the shared-load latency).
+// Outputs per thread (4 / 8 / 12 measured 28.6 / 31.4 / 34.0 us at 800 x 609
+// with the sliding window, 30.4 us before it with 4: fewer threads per
+// view's block hide less of the shared-load latency).
 #ifndef VCT_FC_R
 #define VCT_FC_R 4
 #endif
@@ -153,22 +155,38 @@ __device__ __forceinline__ void fbp_filter_view(const float* __restrict__ G, con
     float acc[FC_R];
 #pragma unroll
     for (int j = 0; j < FC_R; j++) acc[j] = 0.0f;
-    for (int k0 = 0; k0 < cpad; k0 += 4) {
-      const float4 g4 = *reinterpret_cast<const float4*>(sg + k0);
-      float w[FC_R + 4];  // h0(m0 - k0 - 3 + i)
+    // The window h0(m0 - k0 - 3 + i), i < FC_R + 4, slides down by 4 per
+    // chunk: the upper FC_R values are the previous chunk's lower ones, so
+    // each chunk loads only 4 new kernel values (one 128-bit load).
+    float w[FC_R + 4];
 #pragma unroll
-      for (int b = 0; b < FC_R / 4 + 1; b++) {
-        const float4 wb = *reinterpret_cast<const float4*>(sh + off + m0 - k0 - 3 + 4 * b);
-        w[4 * b] = wb.x;
-        w[4 * b + 1] = wb.y;
-        w[4 * b + 2] = wb.z;
-        w[4 * b + 3] = wb.w;
-      }
+    for (int b = 1; b < FC_R / 4 + 1; b++) {
+      const float4 wb = *reinterpret_cast<const float4*>(sh + off + m0 - 3 + 4 * b);
+      w[4 * b] = wb.x;
+      w[4 * b + 1] = wb.y;
+      w[4 * b + 2] = wb.z;
+      w[4 * b + 3] = wb.w;
+    }
+    // Loads one chunk ahead (sg has 4 zeros past cpad, and sh + off + m0 -
+    // cpad - 3 = sh + m0), so the FMAs do not wait on shared memory.
+    float4 g4n = *reinterpret_cast<const float4*>(sg);
+    float4 wbn = *reinterpret_cast<const float4*>(sh + off + m0 - 3);
+#pragma unroll 4
+    for (int k0 = 0; k0 < cpad; k0 += 4) {
+      const float4 g4 = g4n, wb = wbn;
+      g4n = *reinterpret_cast<const float4*>(sg + k0 + 4);
+      wbn = *reinterpret_cast<const float4*>(sh + off + m0 - k0 - 7);
+      w[0] = wb.x;
+      w[1] = wb.y;
+      w[2] = wb.z;
+      w[3] = wb.w;
       const float g[4] = {g4.x, g4.y, g4.z, g4.w};
 #pragma unroll
       for (int i = 0; i < 4; i++)
 #pragma unroll
         for (int j = 0; j < FC_R; j++) acc[j] = fmaf(w[j - i + 3], g[i], acc[j]);  // h0(m0 + j - (k0 + i))
+#pragma unroll
+      for (int i = FC_R + 3; i >= 4; i--) w[i] = w[i - 4];
     }
 #pragma unroll
     for (int j = 0; j < FC_R; j++) {

@@ -593,16 +593,23 @@ __device__ __forceinline__ void adj_cells(const AdjStage<M, ST>& S, int cplx, in
 // AdjStage slot row.  The chord of a line at offset b from the centre of a
 // square of half-size h, direction with components a >= c: 2h/a while
 // |b| <= h(a-c), then (h(a+c) - |b|)/(a c) down to 0.
-// Resident blocks per SM the registers are held to for up to 6 elements (4
-// for the 256-thread tiles, in proportion for smaller ones: 64 registers;
-// 7-8 elements are left to the compiler), and how far the loop over a round's views is unrolled
+// Resident blocks per SM the registers are held to (4 for the 256-thread
+// tiles, in proportion for smaller ones: 64 registers; for 8 elements at
+// 1024^2, 1440 x 1600 the gather 10.80 -> 10.61 ms against the compiler's 80
+// registers, 3 blocks 11.41 ms; 7 elements then also lose the spills the
+// compiler's own choice had), and how far the loop over a round's views is unrolled
 // (measured on the 512^2, 800 x 609 gradient: 3 blocks per SM 1.27 ms and
 // unrolling by 2 1.15 ms, against 1.14 ms at 4; later, 5 blocks per SM (48
 // registers, small spills) 1.16 ms against 1.02 ms).
 #ifndef VCT_ADJ_MINBLOCKS
 #define VCT_ADJ_MINBLOCKS 4
 #endif
-constexpr int adj_min_blocks(int M, int threads) { return M <= 6 ? VCT_ADJ_MINBLOCKS * 256 / threads : 0; }
+#ifndef VCT_ADJ_CAP_MAXM
+#define VCT_ADJ_CAP_MAXM 8
+#endif
+constexpr int adj_min_blocks(int M, int threads) {
+  return M <= VCT_ADJ_CAP_MAXM ? VCT_ADJ_MINBLOCKS * 256 / threads : 0;
+}
 // The batch's gather (its job lookup costs registers) is left to the compiler.
 #ifndef VCT_ADJ_BATCH_MINBLOCKS
 #define VCT_ADJ_BATCH_MINBLOCKS 0

@@ -610,10 +610,18 @@ __device__ __forceinline__ void adj_cells(const AdjStage<M, ST>& S, int cplx, in
 constexpr int adj_min_blocks(int M, int threads) {
   return M <= VCT_ADJ_CAP_MAXM ? VCT_ADJ_MINBLOCKS * 256 / threads : 0;
 }
-// The batch's gather (its job lookup costs registers) is left to the compiler.
+// The batch's gather (its job lookup costs registers) is left to the compiler
+// (held to 64 registers at 7-8 elements it spills 72-88 bytes: the 8-slice
+// 1024^2 dual-energy descent 285 -> 307 ms per iteration).
 #ifndef VCT_ADJ_BATCH_MINBLOCKS
 #define VCT_ADJ_BATCH_MINBLOCKS 0
 #endif
+#ifndef VCT_ADJ_BATCH_CAP_MINM
+#define VCT_ADJ_BATCH_CAP_MINM 9
+#endif
+constexpr int adj_batch_min_blocks(int M, int threads) {
+  return M >= VCT_ADJ_BATCH_CAP_MINM ? VCT_ADJ_MINBLOCKS * 256 / threads : VCT_ADJ_BATCH_MINBLOCKS;
+}
 // The loop over a round's views unrolled by 2: 0.989 -> 0.969 ms at 512^2 /
 // 800 x 609 (gradient bit-identical; 1024^2, 8 elements and the 64-slice
 // batch unchanged within 0.6%).
@@ -1048,7 +1056,7 @@ __global__ void adj_special_batch_kernel(const AdjJob* __restrict__ jobs, const 
 }
 
 template <int M, int TX, int TY>
-__global__ void __launch_bounds__(TX * TY, VCT_ADJ_BATCH_MINBLOCKS)
+__global__ void __launch_bounds__(TX * TY, adj_batch_min_blocks(M, TX * TY))
 adj_gather_batch_kernel(const AdjJob* __restrict__ jobs, const unsigned int* __restrict__ first, int n) {
   __shared__ AdjStage<M, TX * TY / 32 * kAdjW> S;
   const unsigned int total = first[n];

@@ -44,6 +44,28 @@ def test_fbp_transpose_matches_fp64(cuda_device, N, views, channels, filt):
     assert abs(lhs - rhs) <= DOT_REL * float(np.abs(img.astype(np.float64) * u).sum())
 
 
+def test_fbp_transpose_large_grid_more_parts(cuda_device):
+    """1024^2 at 0.05 cm: the scatter splits each base view's 512^2 orbit
+    pixels into 64 parts (at most 4096 pixels each, so a shared slot's 32-bit
+    fixed-point sums cannot overflow) instead of 16."""
+    views, channels, N = 40, 800, 1024
+    p, u = _case(N, views, channels, 7)
+    g = O.geom(views=views, channels=channels, recon_size=N, pixel_cm=0.05)
+    c, s = O.trig_tables(views)
+    ref = O.fbp_transpose(g, u.astype(np.float64), 1, c, s)
+    geo = vct.Geometry.with_channels(channels, views=views, recon_size=N, pixel_cm=0.05)
+    with vct.Context(geo) as ctx:
+        out = ctx.fbp_transpose(u, filter=1)
+        img = ctx.fbp(p, filter=1)
+    d = out.astype(np.float64) - ref
+    assert np.abs(d).max() <= T_MAX_REL * np.abs(ref).max()
+    assert np.linalg.norm(d) <= T_L2_REL * np.linalg.norm(ref)
+    lam = -np.log(p.astype(np.float64))
+    lhs = float((img.astype(np.float64) * u).sum())
+    rhs = float((lam * out.astype(np.float64)).sum())
+    assert abs(lhs - rhs) <= DOT_REL * float(np.abs(img.astype(np.float64) * u).sum())
+
+
 @pytest.mark.parametrize("filt", [1, 2])
 def test_fbp_transpose_dot_product_full_size(cuda_device, filt):
     import torch

@@ -1059,15 +1059,24 @@ template <int M, int TX, int TY>
 __global__ void __launch_bounds__(TX * TY, adj_batch_min_blocks(M, TX * TY))
 adj_gather_batch_kernel(const AdjJob* __restrict__ jobs, const unsigned int* __restrict__ first, int n) {
   __shared__ AdjStage<M, TX * TY / 32 * kAdjW> S;
+  // The job's geometry in shared memory, read where it is used (as the
+  // single-slice kernel reads its parameters) rather than held in registers:
+  // 96 -> 80 registers at 6 elements, the 64-slice batched gradient 59.9 ->
+  // 58.6 ms.
+  __shared__ AdjGeom sa;
   const unsigned int total = first[n];
   for (unsigned int b = blockIdx.x; b < total; b += gridDim.x) {
     // the same view ranges as the single-slice gather, so the sums (and the
     // gradient) are bit-identical to it
     const int jx = adj_job_of(first, n, b);
     const AdjJob& J = jobs[jx];
-    const int ntiles = ((J.a.N + TX) / TX) * ((J.a.N + TY) / TY);  // tiles of the (N+1)^2 cells
+    __syncthreads();  // every thread is done with the previous item's copy
+    if (threadIdx.x == 0) sa = J.a;
+    __syncthreads();
+    const AdjGeom& a = sa;
+    const int ntiles = ((a.N + TX) / TX) * ((a.N + TY) / TY);  // tiles of the (N+1)^2 cells
     const int item = (int)(b - first[jx]);
-    adj_gather_tile<M, TX, TY, adj_chunks(M)>(J.a, item % ntiles, item / ntiles, J.cos_t, J.sin_t, J.dir, J.rec, J.gr,
+    adj_gather_tile<M, TX, TY, adj_chunks(M)>(a, item % ntiles, item / ntiles, J.cos_t, J.sin_t, J.dir, J.rec, J.gr,
                                            reinterpret_cast<const AdjTileView*>(J.tv), J.ext, S);
   }
 }
